@@ -1,0 +1,74 @@
+"""Build libmaxlq_b200.so in-tree with nvcc for sm_100a.
+
+    python -m maxlq_b200.build [--force] [--verbose]
+
+The shared library is the product: the C ABI of include/maxlq.h.  It links
+the CUDA runtime statically so it loads on any box of this image without a
+library path.  Only sm_100a code is generated (B200).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libmaxlq_b200.so")
+SOURCES = ["engine.cu", "solver.cu", "capi.cu"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "engine.cuh", "solver.cuh"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def host_cxx() -> str:
+    # the system g++ (the environment's CXX wrapper may lack runtime specs)
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(ROOT, "include", "maxlq.h")]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> str:
+    if not force and not _stale():
+        return LIB
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc(), "-ccbin", host_cxx(), "-std=c++17", "-O3", "-lineinfo", *ARCH,
+              "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
+    if ptxas_v:
+        common += ["-Xptxas", "-v"]
+    objs = []
+    for src in SOURCES:
+        obj = os.path.join(objdir, src.replace(".cu", ".o"))
+        cmd = common + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    link = [nvcc(), "-ccbin", host_cxx(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
+    if verbose:
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="--verbose" in sys.argv, ptxas_v="--ptxas-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,204 @@
+// engine.cuh -- the B200 engine behind the C ABI.
+//
+// State: every CG vector (u, d, gradients, transported vectors) lives on the
+// device as pruned FP64 Fourier coefficients of the 2/3-dealiased band
+// (the only modes a band-limited field has).  Work: each operator of the
+// reference is a pipeline of pass kernels (kernels.cuh) in precision T with
+// the pointwise products fused into the x stage (functors.cuh) and the
+// spectral multiplies, masks and Parseval reductions in the z stage.
+#pragma once
+
+#include <cmath>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "functors.cuh"
+#include "kernels.cuh"
+
+namespace mlq {
+
+int band_cut_for_order(int n, double order);
+
+struct PhysField;  // fwd
+
+// Engine-independent part (device, stream, params, bands, twiddles).
+class EngineBase {
+   public:
+    explicit EngineBase(const mlq_params& p);
+    virtual ~EngineBase();
+
+    mlq_params P;
+    int n;
+    long n3;
+    Band b2;            // P2 band: the state band
+    Band bfull;         // no cut
+    cudaStream_t stream = nullptr;
+    long long launches = 0;
+    long long bytes = 0;
+    bool use_e_u = false;
+
+    // twiddles: pool of W_L tables
+    cpx<double>* d_tw = nullptr;
+    std::map<int, int> tw_off;  // L -> offset
+    FftPlan plan(int L) const;
+
+    // device reductions
+    double* d_partials = nullptr;
+    long partials_cap = 0;
+    double* d_results = nullptr;  // 256 slots
+    static constexpr int NRES = 256;
+    double h_results[NRES];
+    void fetch_results();  // sync + copy all slots
+
+    // FP64 state spectra (3 components each) of band b2
+    long spec_ncomp() const { return (long)b2.nb * b2.nb * b2.nx; }
+    double2* alloc_state();
+    void free_dev(void* p);
+    void* dev_alloc(size_t bytes);
+    SpecGeom geom(const Band& b) const {
+        SpecGeom g;
+        g.n = n;
+        g.nx = b.nx;
+        g.nb = b.nb;
+        g.band = b;
+        g.ncomp = (long)b.nb * b.nb * b.nx;
+        return g;
+    }
+    Band make_band(int cut) const;
+
+    // spectral state ops (FP64)
+    void lincomb(double2* out, double a, const double2* x, double b = 0, const double2* y = nullptr, double c = 0,
+                 const double2* z = nullptr);
+    void hilbert(double2* f, double order);
+    void leray(double2* f);
+    // up to 6 vector inner products; kinds 0 L2, 1 H_l, 2 div energy
+    void dots(const SpecDotPair* pairs, int np, double* out);
+    void zeroth(const double2* f, double out[3]);
+
+    void finalize(int nblocks, int nr, double scale, int dst, bool accumulate = false);
+    void ensure_partials(long n);
+    // count a launch and surface launch-configuration errors immediately
+    void launched(int k = 1) {
+        launches += k;
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);
+    }
+
+    std::vector<void*> allocs_;
+};
+
+// A physical-space power field |u|^k as computed by calc_uk.
+struct PowField {
+    enum Kind { ONE, RAW, BAND } kind = ONE;
+    double k = 0;
+    int phys = -1;       // phys pool index when materialised
+    int spec = -1;       // work-spectrum index (band b2) when available
+};
+
+template <typename T>
+class Engine : public EngineBase {
+   public:
+    explicit Engine(const mlq_params& p);
+    ~Engine() override;
+
+    // ---- buffers ----
+    T* phys(int i);                       // N^3 physical scratch, lazily allocated
+    cpx<T>* xsbuf(int i);                 // [n][n][nxcap]
+    cpx<T>* ysbuf(int i);                 // [n][nbcap][nxcap]
+    cpx<T>* wspec(int i);                 // work spectrum in band b2, nb*nb*nx
+    int nxcap, nbcap;
+    std::vector<T*> phys_;
+    std::vector<cpx<T>*> xs_, ys_, ws_;
+
+    // ---- pipelines ----
+    struct FwdOut {
+        void* spec = nullptr;
+        int spec_f64 = 0;
+        int phys_out = -1;   // round trip destination (phys index), -1 none
+        int sym = SYM_ONE, ab = 0;
+        const void* add = nullptr;
+        int add_f64 = 0, add_sym = SYM_ONE, add_ab = 0;
+        double add_coef = 0;
+        int red_self = -1;
+        const void* red_with = nullptr;
+        int red_with_f64 = 0, red_with_slot = -1;
+    };
+    // Forward pipeline of functor outputs through band b; reductions of the
+    // z stage land in results[red_dst + slot] (slot < MAX_RED); functor
+    // reductions in results[fred_dst + r].
+    template <class F>
+    void fwd(const Band& b, const F& f, const std::vector<const T*>& in, std::vector<FwdOut> outs, int red_dst = -1,
+             int fred_dst = -1, double norm = -1.0);
+    struct InvOut {
+        ZSrc src[3];
+        int nsrc = 0;
+        int phys_out = -1;
+    };
+    void inv(const Band& b, const std::vector<InvOut>& outs);
+    template <class F>
+    void pointwise(const F& f, const std::vector<const T*>& in, const std::vector<T*>& out, int fred_dst = -1);
+    void yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const std::vector<int>& phys_out);
+
+    // ---- programs ----
+    // R parts at phi = u + tau*d (d may be null) -> results; also ||phi||_q^q.
+    void R_eval(const double2* u, const double2* d, double tau, double out[3], double* lqq);
+    // L2 gradient of R at u (GradL2ForLq) into v (FP64 spectra); also the
+    // dealiased |u|^{q-2} u spectra (for calcConstraintDerivativeL2) into
+    // c (FP64, may be null) and ||u||_q^q.
+    void grad_l2(const double2* u, double2* v, double2* c, double* lqq);
+    // vectorTransport pieces at w = u + tau*d: ir[i] = <P2(|w|^{q-2} w), xi_i>,
+    // returns ||w||_q^q.
+    double transport_pieces(const double2* u, const double2* d, double tau, const double2* const* xi, int nxi,
+                            double* ir);
+    double lq_pow(const double2* u, const double2* d, double tau);  // ||u + tau d||_q^q
+    // |u|^k physical (calc_uk) of the state u, into phys index dst
+    void calc_uk(const double2* u, double k, int dst);
+
+    // ---- state <-> host ----
+    // Forward transform of a host FP64 vector field into state spectra.
+    // Returns the relative energy outside the band.
+    double load_vec(const double* host, double2* spec);
+    void store_vec(const double2* spec, double* host);
+    void load_scalar_phys(const double* host, int dst);
+    void store_scalar_phys(int src, double* host);
+
+    // ---- full-band FFT API (fftwfunction.f90) ----
+    void fft_c2c(const double* in, double* out, int sign);
+    void fft_r2c(const double* in, double* out);
+    void fft_c2r(const double* in, double* out);
+    void dealias_scalar(double* g, double order);
+    // function_ops.f90 operators on arbitrary (not band-limited) fields, in
+    // the full band: gradient (3147), divergence (3200), laplacian (3248),
+    // solve_poisson (1951)
+    void gradient_full(const double* f, double* grad);
+    void divergence_full(const double* u, double* div);
+    void laplacian_full(double* u);
+    void poisson_full(const double* f, double l, double* phi);
+    void widen_to(const Band& b);
+
+    double2* c_tmp_ = nullptr;  // FP64 spectra of P2(|w|^{q-2} w) for the transport
+
+   private:
+    // |u|^k chain (calc_uk); memoised per program
+    std::map<double, PowField> memo_;
+    int tmp_next_ = 0, spec_next_ = 0;
+    void chain_reset() {
+        memo_.clear();
+        tmp_next_ = 0;
+        spec_next_ = 0;
+    }
+    PowField chain(double k);
+    void ensure_p2_spec(PowField& f);
+    void ensure_phys(PowField& f);
+    cpx<T>* ones_spec();
+    void A_and_S(bool need_A_phys);
+    int lx_for(int nout, size_t extra = 0) const;
+    int tx_for() const;
+    double* h_stage_ = nullptr;  // pinned staging for host copies
+    size_t h_stage_bytes_ = 0;
+    void* stage(size_t bytes);
+};
+
+}  // namespace mlq

@@ -1,0 +1,649 @@
+// kernels.cuh -- the pass kernels of the pruned spectral pipeline.
+//
+// HBM layouts (T = float or double, cpx<T> interleaved):
+//   phys  : T        [z][y][x]             N^3, x fastest (Fortran (n1,n2,n3))
+//   xs    : cpx<T>   [z][y][kx]            after the x real FFT, kx < nx
+//   ys    : cpx<T>   [z][ky'][kx]          after the y FFT, ky' < nb (band order)
+//   spec  : cpx<T|double> [kz'][ky'][kx]   pruned Fourier coefficients (1/N^3)
+// Forward pipeline : phys --x-stage(functor, r2c)--> xs --y fwd--> ys --z stage--> spec
+// Inverse pipeline : spec --z stage--> ys --y inv--> xs --x inv (c2r)--> phys
+// The z stage is where the whole wavevector is known: masks, derivative and
+// Poisson symbols, Parseval reductions and spectral round trips live there.
+#pragma once
+
+#include "fft.cuh"
+
+namespace mlq {
+
+constexpr int MAX_ARR = 8;    // arrays per pass launch
+constexpr int MAX_RED = 8;    // reduction slots per launch
+constexpr int RED_THREADS = 256;
+
+// ----------------------------------------------------------------------------
+// Block reduction of NR doubles into partials[blockLinear*NR + r].
+// ----------------------------------------------------------------------------
+template <int NR>
+__device__ __forceinline__ void block_reduce_store(const double* acc, double* partials, int block_lin) {
+    __shared__ double red_smem[32][NR > 0 ? NR : 1];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        double v = acc[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red_smem[warp][r] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            double v = lane < nw ? red_smem[lane][r] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) partials[(long)block_lin * NR + r] = v;
+        }
+    }
+}
+
+// results[dst + r] = scale * sum_b partials[b*nr + r]   (fixed order: deterministic)
+static __global__ void finalize_partials_kernel(const double* __restrict__ partials, int nblocks, int nr, double scale,
+                                         double* __restrict__ results, int dst, int accumulate) {
+    __shared__ double sm[RED_THREADS];
+    for (int r = 0; r < nr; ++r) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += partials[(long)b * nr + r];
+        sm[threadIdx.x] = v;
+        __syncthreads();
+        for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+            if ((int)threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) results[dst + r] = (accumulate ? results[dst + r] : 0.0) + scale * sm[0];
+        __syncthreads();
+    }
+}
+
+// ----------------------------------------------------------------------------
+// x stage, forward: functor on physical inputs, then real FFT along x.
+// Each CTA owns `lx` consecutive (y,z) lines.
+// ----------------------------------------------------------------------------
+template <typename T>
+struct XFwdArgs {
+    int n, nx;          // grid, kept kx per output line
+    int lx;             // lines per CTA
+    const T* in[24];    // physical inputs
+    cpx<T>* out[MAX_ARR];
+    FftPlan plan_half;  // length n/2
+    int tw_n_off;       // offset of W_n (length n) in the twiddle pool
+    const cpx<double>* tw;
+    double* partials;
+};
+
+template <typename T, class F>
+__global__ void __launch_bounds__(256) xfwd_kernel(XFwdArgs<T> a, F f) {
+    constexpr int NIN = F::NIN, NOUT = F::NOUT, NR = F::NRED;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, h = n / 2, lx = a.lx;
+    const int nl = NOUT * lx;  // FFT lines in this CTA
+    cpx<T>* bufA = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* bufB = bufA + (long)h * nl;
+    T* rA = reinterpret_cast<T*>(bufA);
+    const long line0 = (long)blockIdx.x * lx;
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+
+    for (int p = threadIdx.x; p < lx * n; p += blockDim.x) {
+        const int l = p / n, x = p - l * n;
+        const long g = (line0 + l) * n + x;
+        T vin[NIN];
+#pragma unroll
+        for (int i = 0; i < NIN; ++i) vin[i] = a.in[i][g];
+        T vout[NOUT > 0 ? NOUT : 1];
+        f(vin, vout, acc);
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) rA[2 * ((long)(x >> 1) * nl + o * lx + l) + (x & 1)] = vout[o];
+    }
+    __syncthreads();
+    cpx<T>* Z = fft_lines<-1, T>(bufA, bufB, a.plan_half, nl, nl, a.tw, threadIdx.x, blockDim.x);
+    // split into the half spectrum of the real line: X[k] = E[k] + W_n^k O[k]
+    const double2* twn = reinterpret_cast<const double2*>(a.tw + a.tw_n_off);
+    for (int p = threadIdx.x; p < nl * a.nx; p += blockDim.x) {
+        const int lo = p / a.nx, k = p - lo * a.nx;
+        const int o = lo / lx, l = lo - o * lx;
+        const cpx<T> zk = Z[(long)(k % h) * nl + lo];
+        const cpx<T> zc = conj(Z[(long)((h - k) % h) * nl + lo]);
+        const cpx<T> E = (zk + zc) * T(0.5);
+        const cpx<T> D = (zk - zc) * T(0.5);
+        const cpx<T> O = mk<T>(D.y, -D.x);  // -i * D
+        const double2 w = __ldg(twn + k);   // exp(-2 pi i k / n)
+        const cpx<T> X = E + O * mk<T>((T)w.x, (T)w.y);
+        a.out[o][(line0 + l) * a.nx + k] = X;
+    }
+    if constexpr (NR > 0) block_reduce_store<NR>(acc, a.partials, blockIdx.x);
+}
+
+// ----------------------------------------------------------------------------
+// Pointwise physical-space kernels: reduce-only (NOUT = 0) or map.
+// ----------------------------------------------------------------------------
+template <typename T>
+struct PArgs {
+    long npts;
+    const T* in[24];
+    T* out[MAX_ARR];
+    double* partials;
+};
+
+template <typename T, class F>
+__global__ void __launch_bounds__(RED_THREADS) pointwise_kernel(PArgs<T> a, F f) {
+    constexpr int NIN = F::NIN, NOUT = F::NOUT, NR = F::NRED;
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+    for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < a.npts; g += (long)gridDim.x * blockDim.x) {
+        T vin[NIN > 0 ? NIN : 1];
+#pragma unroll
+        for (int i = 0; i < NIN; ++i) vin[i] = a.in[i][g];
+        T vout[NOUT > 0 ? NOUT : 1];
+        f(vin, vout, acc);
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) a.out[o][g] = vout[o];
+    }
+    if constexpr (NR > 0) block_reduce_store<NR>(acc, a.partials, blockIdx.x);
+}
+
+// ----------------------------------------------------------------------------
+// x stage, inverse: half spectrum (kx < nx_in, zero above) -> real line.
+// ----------------------------------------------------------------------------
+template <typename T>
+struct XInvArgs {
+    int n, nx_in, lx;
+    const cpx<T>* in[MAX_ARR];
+    T* out[MAX_ARR];
+    FftPlan plan_half;
+    int tw_n_off;
+    const cpx<double>* tw;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) xinv_kernel(XInvArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, h = n / 2, lx = a.lx;
+    const int arr = blockIdx.y;
+    cpx<T>* X = reinterpret_cast<cpx<T>*>(smem_raw);  // (h+1) x lx
+    cpx<T>* bufA = X + (long)(h + 1) * lx;             // h x lx
+    cpx<T>* bufB = bufA + (long)h * lx;
+    const long line0 = (long)blockIdx.x * lx;
+    const cpx<T>* src = a.in[arr];
+    for (int p = threadIdx.x; p < lx * (h + 1); p += blockDim.x) {
+        const int l = p / (h + 1), k = p - l * (h + 1);
+        X[(long)k * lx + l] = k < a.nx_in ? src[(line0 + l) * a.nx_in + k] : czero<T>();
+    }
+    __syncthreads();
+    const double2* twn = reinterpret_cast<const double2*>(a.tw + a.tw_n_off);
+    for (int p = threadIdx.x; p < lx * h; p += blockDim.x) {
+        const int k = p / lx, l = p - k * lx;
+        const cpx<T> xk = X[(long)k * lx + l];
+        const cpx<T> xc = conj(X[(long)(h - k) * lx + l]);
+        const cpx<T> Fk = xk + xc;
+        const double2 w = __ldg(twn + k);  // exp(-2 pi i k/n); need exp(+...)
+        const cpx<T> G = (xk - xc) * mk<T>((T)w.x, (T)(-w.y));
+        bufA[(long)k * lx + l] = Fk + mk<T>(-G.y, G.x);  // F + i G
+    }
+    __syncthreads();
+    cpx<T>* z = fft_lines<+1, T>(bufA, bufB, a.plan_half, lx, lx, a.tw, threadIdx.x, blockDim.x);
+    T* dst = a.out[arr];
+    for (int p = threadIdx.x; p < lx * h; p += blockDim.x) {
+        const int l = p / h, m = p - l * h;
+        const cpx<T> v = z[(long)m * lx + l];
+        reinterpret_cast<cpx<T>*>(dst + (line0 + l) * n)[m] = v;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Complex x pass (c2c along x, full length) for the fftfwd/fftbwd API.
+// ----------------------------------------------------------------------------
+template <typename T>
+struct XC2CArgs {
+    int n, lx;
+    const cpx<T>* in;
+    cpx<T>* out;
+    FftPlan plan;
+    const cpx<double>* tw;
+    double scale;
+};
+
+template <int SIGN, typename T>
+__global__ void __launch_bounds__(256) xc2c_kernel(XC2CArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, lx = a.lx;
+    cpx<T>* bufA = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* bufB = bufA + (long)n * lx;
+    const long line0 = (long)blockIdx.x * lx;
+    for (int p = threadIdx.x; p < lx * n; p += blockDim.x) {
+        const int l = p / n, x = p - l * n;
+        bufA[(long)x * lx + l] = a.in[(line0 + l) * n + x];
+    }
+    __syncthreads();
+    cpx<T>* r = fft_lines<SIGN, T>(bufA, bufB, a.plan, lx, lx, a.tw, threadIdx.x, blockDim.x);
+    for (int p = threadIdx.x; p < lx * n; p += blockDim.x) {
+        const int l = p / n, x = p - l * n;
+        a.out[(line0 + l) * n + x] = r[(long)x * lx + l] * (T)a.scale;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// y pass.  Forward: [z][y<n][kx] -> [z][ky'<nb][kx] (rows outside the band
+// dropped).  Inverse: [z][ky'][kx] (zero-padded) -> [z][y<n][kx].
+// grid = (ceil(nx/tx), n, narr)
+// ----------------------------------------------------------------------------
+template <typename T>
+struct YArgs {
+    int n, nx, tx;       // nx = columns processed (and the row stride of both sides)
+    Band band;           // ky band
+    const cpx<T>* in[MAX_ARR];
+    cpx<T>* out[MAX_ARR];
+    FftPlan plan;
+    const cpx<double>* tw;
+};
+
+template <int SIGN, typename T>
+__global__ void __launch_bounds__(256) ypass_kernel(YArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, tx = a.tx, nx = a.nx, nb = a.band.nb;
+    cpx<T>* bufA = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* bufB = bufA + (long)n * tx;
+    const int kx0 = blockIdx.x * tx;
+    const int z = blockIdx.y;
+    const int arr = blockIdx.z;
+    const int w = min(tx, nx - kx0);
+    const cpx<T>* src = a.in[arr];
+    cpx<T>* dst = a.out[arr];
+    if (SIGN < 0) {
+        for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+            const int y = p / tx, l = p - y * tx;
+            bufA[p] = l < w ? src[((long)z * n + y) * nx + kx0 + l] : czero<T>();
+        }
+    } else {
+        for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+            const int fi = p / tx, l = p - fi * tx;
+            const int ci = band_compact_index(a.band, fi);
+            bufA[p] = (l < w && ci >= 0) ? src[((long)z * nb + ci) * nx + kx0 + l] : czero<T>();
+        }
+    }
+    __syncthreads();
+    cpx<T>* r = fft_lines<SIGN, T>(bufA, bufB, a.plan, tx, tx, a.tw, threadIdx.x, blockDim.x);
+    if (SIGN < 0) {
+        for (int p = threadIdx.x; p < nb * tx; p += blockDim.x) {
+            const int ci = p / tx, l = p - ci * tx;
+            if (l < w) dst[((long)z * nb + ci) * nx + kx0 + l] = r[(long)band_fft_index(a.band, ci) * tx + l];
+        }
+    } else {
+        for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+            const int y = p / tx, l = p - y * tx;
+            if (l < w) dst[((long)z * n + y) * nx + kx0 + l] = r[p];
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Spectral symbols.  K_j = 2 pi j (initialize.f90:170-192).  On a full band the
+// Nyquist index of an axis contributes nothing to an odd (first-derivative)
+// factor: c2c followed by REAL() keeps only the Hermitian part
+// (function_ops.f90:3186 etc.), which cancels it.
+// ----------------------------------------------------------------------------
+enum Sym : int {
+    SYM_ZERO = 0,
+    SYM_ONE,
+    SYM_IKX,
+    SYM_IKY,
+    SYM_IKZ,
+    SYM_NEG_KSQ,      // laplacian: -|K|^2
+    SYM_INV_KSQ,      // +1/|K|^2, 0 at k=0
+    SYM_NEG_INV_KSQ,  // -1/|K|^2, 0 at k=0 (solve_poisson with l=1)
+    SYM_KK_KSQ,       // + K_a K_b / |K|^2 (a,b from sym_ab), 0 at k=0
+};
+
+struct Kvec {
+    double kx, ky, kz;        // true wavenumbers
+    double ox, oy, oz;        // odd-factor wavenumbers (0 at a Nyquist index)
+    double ksq;
+};
+
+__device__ __forceinline__ Kvec make_k(int n, int fx, int fy, int fz) {
+    const double twopi = 2.0 * 3.14159265358979311600;  // 2.0_pr*PI, PI = 4 atan2(1,1)
+    Kvec k;
+    const int jx = signed_j(n, fx), jy = signed_j(n, fy), jz = signed_j(n, fz);
+    k.kx = twopi * (double)jx;
+    k.ky = twopi * (double)jy;
+    k.kz = twopi * (double)jz;
+    const bool even = (n & 1) == 0;
+    k.ox = (even && fx == n / 2) ? 0.0 : k.kx;
+    k.oy = (even && fy == n / 2) ? 0.0 : k.ky;
+    k.oz = (even && fz == n / 2) ? 0.0 : k.kz;
+    k.ksq = k.kx * k.kx + k.ky * k.ky + k.kz * k.kz;
+    return k;
+}
+
+__device__ __forceinline__ cpx<double> apply_sym(int sym, int ab, const Kvec& k, cpx<double> v) {
+    switch (sym) {
+        case SYM_ZERO: return mk(0.0, 0.0);
+        case SYM_ONE: return v;
+        case SYM_IKX: return mk(-k.ox * v.y, k.ox * v.x);
+        case SYM_IKY: return mk(-k.oy * v.y, k.oy * v.x);
+        case SYM_IKZ: return mk(-k.oz * v.y, k.oz * v.x);
+        case SYM_NEG_KSQ: return v * (-k.ksq);
+        case SYM_INV_KSQ: return k.ksq == 0.0 ? mk(0.0, 0.0) : v * (1.0 / k.ksq);
+        case SYM_NEG_INV_KSQ: return k.ksq == 0.0 ? mk(0.0, 0.0) : v * (-1.0 / k.ksq);
+        case SYM_KK_KSQ: {
+            if (k.ksq == 0.0) return mk(0.0, 0.0);
+            const double o[3] = {k.ox, k.oy, k.oz};
+            return v * (o[ab / 3] * o[ab % 3] / k.ksq);
+        }
+    }
+    return v;
+}
+
+__device__ __forceinline__ cpx<double> ld_spec(const void* p, int f64, long idx) {
+    if (f64) {
+        const double2 v = reinterpret_cast<const double2*>(p)[idx];
+        return mk(v.x, v.y);
+    }
+    const float2 v = reinterpret_cast<const float2*>(p)[idx];
+    return mk((double)v.x, (double)v.y);
+}
+__device__ __forceinline__ void st_spec(void* p, int f64, long idx, cpx<double> v) {
+    if (f64)
+        reinterpret_cast<double2*>(p)[idx] = make_double2(v.x, v.y);
+    else
+        reinterpret_cast<float2*>(p)[idx] = make_float2((float)v.x, (float)v.y);
+}
+// Parseval weight of a half-spectrum column (real fields)
+__device__ __forceinline__ double kx_weight(int n, int fx) { return (fx == 0 || 2 * fx == n) ? 1.0 : 2.0; }
+
+// ----------------------------------------------------------------------------
+// z stage, forward (optionally round trip).  grid = (ceil(nx/tx), nb, narr).
+// For each array: z FFT, keep |kz| <= cut, scale 1/N^3, multiply by `sym`,
+// add coef*add_sym*add_spec, reductions, write the pruned spectrum and/or
+// transform back along z into ys_out.
+// ----------------------------------------------------------------------------
+struct ZFwdOp {
+    const void* in;       // ys array, work type
+    void* spec_out;       // optional pruned spectrum
+    int spec_f64;
+    void* ys_out;         // optional round-trip output (work type)
+    int sym, sym_ab;
+    const void* add;      // optional second term
+    int add_f64, add_sym, add_ab;
+    double add_coef;
+    int red_self;         // slot for sum w|Y|^2, -1 none
+    const void* red_with; // slot for sum w Re(Y conj(W)), -1 none
+    int red_with_f64, red_with_slot;
+};
+
+template <typename T>
+struct ZFwdArgs {
+    int n, nx, tx;
+    Band band;
+    ZFwdOp op[MAX_ARR];
+    FftPlan plan;
+    const cpx<double>* tw;
+    double* partials;  // [blocks][MAX_RED]
+    double norm;       // 1/N^3
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) zfwd_kernel(ZFwdArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, tx = a.tx, nx = a.nx, nb = a.band.nb;
+    cpx<T>* bufA = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* bufB = bufA + (long)n * tx;
+    const int kx0 = blockIdx.x * tx;
+    const int cy = blockIdx.y;
+    const ZFwdOp& op = a.op[blockIdx.z];
+    const int w = min(tx, nx - kx0);
+    const cpx<T>* src = reinterpret_cast<const cpx<T>*>(op.in);
+    const long plane = (long)nb * nx;
+    for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+        const int z = p / tx, l = p - z * tx;
+        bufA[p] = l < w ? src[(long)z * plane + (long)cy * nx + kx0 + l] : czero<T>();
+    }
+    __syncthreads();
+    cpx<T>* r = fft_lines<-1, T>(bufA, bufB, a.plan, tx, tx, a.tw, threadIdx.x, blockDim.x);
+    cpx<T>* o = (r == bufA) ? bufB : bufA;  // free buffer for the round trip
+    double acc[MAX_RED];
+#pragma unroll
+    for (int i = 0; i < MAX_RED; ++i) acc[i] = 0.0;
+    const int fy = band_fft_index(a.band, cy);
+    for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+        const int fz = p / tx, l = p - fz * tx;
+        const int cz = band_compact_index(a.band, fz);
+        cpx<double> Y = mk(0.0, 0.0);
+        if (cz >= 0 && l < w) {
+            const int fx = kx0 + l;
+            const Kvec k = make_k(n, fx, fy, fz);
+            const cpx<T> v = r[p];
+            Y = apply_sym(op.sym, op.sym_ab, k, mk((double)v.x, (double)v.y) * a.norm);
+            const long si = ((long)cz * nb + cy) * nx + fx;
+            if (op.add) Y = Y + apply_sym(op.add_sym, op.add_ab, k, ld_spec(op.add, op.add_f64, si)) * op.add_coef;
+            const double wgt = kx_weight(n, fx);
+            if (op.red_self >= 0) acc[op.red_self] += wgt * (Y.x * Y.x + Y.y * Y.y);
+            if (op.red_with) {
+                const cpx<double> W = ld_spec(op.red_with, op.red_with_f64, si);
+                acc[op.red_with_slot] += wgt * (Y.x * W.x + Y.y * W.y);
+            }
+            if (op.spec_out) st_spec(op.spec_out, op.spec_f64, si, Y);
+        }
+        if (op.ys_out) o[p] = mk((T)Y.x, (T)Y.y);
+    }
+    const int block_lin = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+    block_reduce_store<MAX_RED>(acc, a.partials, block_lin);
+    if (op.ys_out) {
+        __syncthreads();
+        cpx<T>* other = (o == bufA) ? bufB : bufA;
+        cpx<T>* q = fft_lines<+1, T>(o, other, a.plan, tx, tx, a.tw, threadIdx.x, blockDim.x);
+        cpx<T>* dst = reinterpret_cast<cpx<T>*>(op.ys_out);
+        for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+            const int z = p / tx, l = p - z * tx;
+            if (l < w) dst[(long)z * plane + (long)cy * nx + kx0 + l] = q[p];
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// z stage, inverse from spectra: out = IFFT_z( sum_s coef_s * sym_s(k) spec_s ).
+// grid = (ceil(nx/tx), nb, narr)
+// ----------------------------------------------------------------------------
+struct ZSrc {
+    const void* spec;
+    int f64, sym, ab;
+    double coef;
+};
+struct ZInvOp {
+    ZSrc src[3];
+    int nsrc;
+    void* ys_out;
+};
+
+template <typename T>
+struct ZInvArgs {
+    int n, nx, tx;
+    Band band;
+    ZInvOp op[MAX_ARR];
+    FftPlan plan;
+    const cpx<double>* tw;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) zinv_kernel(ZInvArgs<T> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = a.n, tx = a.tx, nx = a.nx, nb = a.band.nb;
+    cpx<T>* bufA = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* bufB = bufA + (long)n * tx;
+    const int kx0 = blockIdx.x * tx;
+    const int cy = blockIdx.y;
+    const ZInvOp& op = a.op[blockIdx.z];
+    const int w = min(tx, nx - kx0);
+    const int fy = band_fft_index(a.band, cy);
+    for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+        const int fz = p / tx, l = p - fz * tx;
+        const int cz = band_compact_index(a.band, fz);
+        cpx<double> Y = mk(0.0, 0.0);
+        if (cz >= 0 && l < w) {
+            const int fx = kx0 + l;
+            const Kvec k = make_k(n, fx, fy, fz);
+            const long si = ((long)cz * nb + cy) * nx + fx;
+            for (int s = 0; s < op.nsrc; ++s)
+                Y = Y + apply_sym(op.src[s].sym, op.src[s].ab, k, ld_spec(op.src[s].spec, op.src[s].f64, si)) *
+                            op.src[s].coef;
+        }
+        bufA[p] = mk((T)Y.x, (T)Y.y);
+    }
+    __syncthreads();
+    cpx<T>* q = fft_lines<+1, T>(bufA, bufB, a.plan, tx, tx, a.tw, threadIdx.x, blockDim.x);
+    cpx<T>* dst = reinterpret_cast<cpx<T>*>(op.ys_out);
+    const long plane = (long)nb * nx;
+    for (int p = threadIdx.x; p < n * tx; p += blockDim.x) {
+        const int z = p / tx, l = p - z * tx;
+        if (l < w) dst[(long)z * plane + (long)cy * nx + kx0 + l] = q[p];
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Spectral-state kernels on pruned FP64 vector spectra [3][nb][nb][nx].
+// ----------------------------------------------------------------------------
+struct SpecGeom {
+    int n, nx, nb;
+    Band band;
+    long ncomp;  // nb*nb*nx
+};
+
+__device__ __forceinline__ void spec_coords(const SpecGeom& g, long i, int& fx, int& fy, int& fz) {
+    const int cx = (int)(i % g.nx);
+    const long t = i / g.nx;
+    const int cy = (int)(t % g.nb);
+    const int cz = (int)(t / g.nb);
+    fx = cx;
+    fy = band_fft_index(g.band, cy);
+    fz = band_fft_index(g.band, cz);
+}
+
+// out = a*x + b*y + c*z  (any pointer may alias out; y/z may be null)
+static __global__ void spec_lincomb_kernel(SpecGeom g, double2* out, double a, const double2* x, double b,
+                                    const double2* y, double c, const double2* z) {
+    const long nt = 3 * g.ncomp;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += (long)gridDim.x * blockDim.x) {
+        double2 v = x[i];
+        double2 r = make_double2(a * v.x, a * v.y);
+        if (y) {
+            const double2 w = y[i];
+            r.x += b * w.x;
+            r.y += b * w.y;
+        }
+        if (z) {
+            const double2 w = z[i];
+            r.x += c * w.x;
+            r.y += c * w.y;
+        }
+        out[i] = r;
+    }
+}
+
+// Hilbert gradient symbol 1/(1+(lambda1|K|)^(2 order)) (function_ops.f90:3611)
+static __global__ void spec_hilbert_kernel(SpecGeom g, double2* f, double lambda1, double order2) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
+        int fx, fy, fz;
+        spec_coords(g, i, fx, fy, fz);
+        const Kvec k = make_k(g.n, fx, fy, fz);
+        const double s = 1.0 / (1.0 + pow(lambda1 * sqrt(k.ksq), order2));
+        for (int c = 0; c < 3; ++c) {
+            double2 v = f[c * g.ncomp + i];
+            f[c * g.ncomp + i] = make_double2(v.x * s, v.y * s);
+        }
+    }
+}
+
+// divAvg_free (function_ops.f90:2843-2918): u - K(K.u)/|K|^2 with the odd
+// (first-derivative) factors of the divergence/gradient round trip, k=0 -> 0.
+static __global__ void spec_leray_kernel(SpecGeom g, double2* f) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
+        int fx, fy, fz;
+        spec_coords(g, i, fx, fy, fz);
+        const Kvec k = make_k(g.n, fx, fy, fz);
+        double2 u0 = f[i], u1 = f[g.ncomp + i], u2 = f[2 * g.ncomp + i];
+        if (k.ksq > MACH_EPSILON) {
+            const double dr = k.ox * u0.x + k.oy * u1.x + k.oz * u2.x;
+            const double di = k.ox * u0.y + k.oy * u1.y + k.oz * u2.y;
+            const double s = 1.0 / k.ksq;
+            u0.x -= k.ox * dr * s; u0.y -= k.ox * di * s;
+            u1.x -= k.oy * dr * s; u1.y -= k.oy * di * s;
+            u2.x -= k.oz * dr * s; u2.y -= k.oz * di * s;
+        } else {
+            u0 = u1 = u2 = make_double2(0.0, 0.0);
+        }
+        f[i] = u0;
+        f[g.ncomp + i] = u1;
+        f[2 * g.ncomp + i] = u2;
+    }
+}
+
+// Up to 6 vector inner products in one pass.  kind: 0 L2, 1 H_l weight
+// (1+(lambda1|K|)^order)^2 (function_ops.f90:3472), 2 divergence energy
+// |K_odd . f|^2 of pair.a (pair.b ignored).
+struct SpecDotPair {
+    const double2* a;
+    const double2* b;
+    int kind;
+};
+struct SpecDotArgs {
+    SpecGeom g;
+    SpecDotPair pr[6];
+    int npairs;
+    double lambda1, order;
+    double* partials;
+};
+
+static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    const SpecGeom& g = a.g;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
+        int fx, fy, fz;
+        spec_coords(g, i, fx, fy, fz);
+        const Kvec k = make_k(g.n, fx, fy, fz);
+        const double wgt = kx_weight(g.n, fx);
+        double hw = 1.0;
+        bool need_h = false;
+        for (int p = 0; p < a.npairs; ++p) need_h |= a.pr[p].kind == 1;
+        if (need_h) {
+            const double f = 1.0 + pow(a.lambda1 * sqrt(k.ksq), a.order);
+            hw = f * f;
+        }
+        for (int p = 0; p < a.npairs; ++p) {
+            const SpecDotPair& q = a.pr[p];
+            if (q.kind == 2) {
+                double dr = 0.0, di = 0.0;
+                const double o[3] = {k.ox, k.oy, k.oz};
+                for (int c = 0; c < 3; ++c) {
+                    const double2 v = q.a[c * g.ncomp + i];
+                    dr += o[c] * v.x;
+                    di += o[c] * v.y;
+                }
+                acc[p] += wgt * (dr * dr + di * di);
+            } else {
+                double s = 0.0;
+                for (int c = 0; c < 3; ++c) {
+                    const double2 u = q.a[c * g.ncomp + i], v = q.b[c * g.ncomp + i];
+                    s += u.x * v.x + u.y * v.y;
+                }
+                acc[p] += wgt * (q.kind == 1 ? hw : 1.0) * s;
+            }
+        }
+    }
+    block_reduce_store<6>(acc, a.partials, blockIdx.x);
+}
+
+// Fourier coefficients of a physical scalar restricted to a band, full-band
+// energy outside the band: used to check that a loaded field is band-limited.
+// (Implemented with the forward pipeline plus a reduction; see engine.)
+
+}  // namespace mlq

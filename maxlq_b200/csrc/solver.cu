@@ -1,0 +1,537 @@
+// solver.cu -- the CG search (optimization.f90) on the engine.
+#include "solver.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+namespace mlq {
+
+void seed_spectrum_host(int n, unsigned long long seed, double slope, double k0, const Band& b, double* out);
+
+namespace {
+const double TAU_MAX = 1.0e2;  // global_variables.f90:29
+}
+
+template <typename T>
+class Solver : public SolverBase {
+   public:
+    Engine<T> e;
+    double2 *u, *d1, *gu0, *gu1, *vtg0, *vtd0, *c, *tmp, *tmp2;
+    // CG memory of the resident loop
+    bool started = false;
+    int iter = 0, start_iter = 0;
+    double J0 = 0, tau0 = 100.0;
+    std::vector<double> roll;
+    double avg_imp = 1.0;
+    int while_flag = 0;
+    std::map<double, Trial> trials;
+
+    explicit Solver(const mlq_params& p) : e(p) {
+        u = e.alloc_state();
+        d1 = e.alloc_state();
+        gu0 = e.alloc_state();
+        gu1 = e.alloc_state();
+        vtg0 = e.alloc_state();
+        vtd0 = e.alloc_state();
+        c = e.alloc_state();
+        tmp = e.alloc_state();
+        tmp2 = nullptr;
+    }
+    EngineBase& eng() override { return e; }
+    long nc() const { return e.spec_ncomp(); }
+    double q() const { return e.P.q; }
+    double B() const { return e.P.B; }
+
+    void zero(double2* f) { MLQ_CUDA(cudaMemsetAsync(f, 0, 3 * nc() * sizeof(double2), e.stream)); }
+
+    // load a host vector field, refusing fields with modes outside the band
+    void load(const double* host, double2* spec) {
+        const double rel = e.load_vec(host, spec);
+        const double tol = sizeof(T) == 8 ? 1e-20 : 1e-10;
+        if (rel > tol)
+            throw CudaError("input field is not band-limited to the 2/3 dealiasing cube (relative energy outside: " +
+                                std::to_string(rel) + ")",
+                            MLQ_ERR_NOT_BANDLIMITED);
+    }
+
+    // ---- line search -------------------------------------------------------
+    Trial trial(const double2* base, const double2* dir, double tau) {
+        auto it = trials.find(tau);
+        if (it != trials.end()) return it->second;
+        Trial t;
+        e.R_eval(base, dir, tau, t.R, &t.lqq);
+        trials[tau] = t;
+        return t;
+    }
+    // eval_J(phi + tau d, "LineMin") (optimization.f90:537-539)
+    double lm_eval(const double2* base, const double2* dir, double tau) {
+        ++eval_count;
+        ++evals_this_iter;
+        const Trial t = trial(base, dir, tau);
+        return -1.0 * scaled_R(t);
+    }
+    double scaled_R(const Trial& t) const {
+        const double nrm = std::pow(t.lqq, 1.0 / q());
+        const double cs = B() / nrm;
+        return std::pow(cs, q()) * t.R[1] + std::pow(cs, q() + 1.0) * t.R[2];
+    }
+    int evals_this_iter = 0;
+
+    // mnbrak (optimization.f90:613-778)
+    int mnbrak(const double2* phi, const double2* grad, double tA0, double tB0, double tau_brack[2], int* myflag) {
+        const double GOLD = (1.0 + std::sqrt(5.0)) / 2.0;
+        const double CGOLD = 1.0 / GOLD;
+        const double GLIMIT = 10.0;
+        const int ITMAX = 100;
+        double tA = tA0, tB = std::max(tB0, MACH_EPSILON), tC = 0.0, tP, FP, Pmax, R, Q;
+        double FA = lm_eval(phi, grad, tA);
+        double FB = lm_eval(phi, grad, tB);
+        double FC = 0.0;
+        int brakIter = 0;
+        while (FB > FA && tB > MACH_EPSILON) {
+            tB = CGOLD * tB;
+            FB = lm_eval(phi, grad, tB);
+        }
+        if (tB <= MACH_EPSILON) {
+            *myflag = 1;
+            return 1;
+        }
+        tC = GOLD * tB;
+        FC = lm_eval(phi, grad, tC);
+        while (FB >= FC && brakIter < ITMAX) {
+            brakIter++;
+            tC = GOLD * tC;
+            FC = lm_eval(phi, grad, tC);
+            R = (tB - tA) * (FB - FC);
+            Q = (tB - tC) * (FB - FA);
+            tP = tB - 0.5 * ((tB - tC) * Q - (tB - tA) * R) /
+                          std::copysign(std::max(std::fabs(Q - R), MACH_EPSILON), Q - R);
+            Pmax = tB + GLIMIT * (tC - tB);
+            if ((tB - tP) * (tP - tC) > 0) {
+                FP = lm_eval(phi, grad, tP);
+                if (FP < FC) {
+                    tA = tB; FA = FB; tB = tP; FB = FP;
+                    break;
+                } else if (FP > FB) {
+                    tC = tP; FC = FP;
+                    break;
+                }
+                tP = tC + GOLD * (tC - tB);
+                FP = lm_eval(phi, grad, tP);
+            } else if ((tC - tP) * (tP - Pmax) > 0) {
+                FP = lm_eval(phi, grad, tP);
+                if (FP < FC) {
+                    tB = tC; tC = tP; FB = FC; FC = FP;
+                    tP = tC + GOLD * (tC - tB);
+                    FP = lm_eval(phi, grad, tP);
+                }
+            } else if ((tP - Pmax) * (Pmax - tC) >= 0) {
+                tP = Pmax;
+                FP = lm_eval(phi, grad, tP);
+            } else {
+                tP = tC + GOLD * (tC - tB);
+                FP = lm_eval(phi, grad, tP);
+            }
+            tA = tB; tB = tC; tC = tP;
+            FA = FB; FB = FC; FC = FP;
+        }
+        tau_brack[0] = tA;
+        tau_brack[1] = tC;
+        *myflag = brakIter >= ITMAX ? 2 : 0;
+        return *myflag;
+    }
+
+    // brent (optimization.f90:784-951); the constants are the Fortran
+    // default-real literals TOL = 1E-6, ZEPS = 1E-8, CGOLD = .381966 widened
+    // to double (804-806)
+    double brent(const double2* phi, const double2* grad, const double tau_brack[2], double* fx_out) {
+        const int ITMAX = 300;
+        const double TOL = (double)1E-6f;
+        const double ZEPS = (double)1E-8f;
+        const double CGOLD = (double).381966f;
+        double D = 0.0, A = std::min(tau_brack[0], tau_brack[1]), Bb = std::max(tau_brack[0], tau_brack[1]);
+        double V = tau_brack[1] * CGOLD, W = V, X = V, E = 0.0, ETEMP, P = 0, Q = 0, R, U, XM, TOL1, TOL2;
+        double FX = lm_eval(phi, grad, D);  // value at tau = 0 written to brent-info (833-840)
+        FX = lm_eval(phi, grad, X);
+        double FV = FX, FW = FX, FU;
+        for (int j = 1; j <= ITMAX; ++j) {
+            XM = 0.5 * (A + Bb);
+            TOL1 = TOL * std::fabs(X) + ZEPS;
+            TOL2 = 2.0 * TOL1;
+            if (std::fabs(X - XM) <= (TOL2 - 0.5 * (Bb - A))) break;
+            int FLAG = 1;
+            if (std::fabs(E) > TOL1) {
+                R = (X - W) * (FX - FV);
+                Q = (X - V) * (FX - FW);
+                P = (X - V) * Q - (X - W) * R;
+                Q = 2.0 * (Q - R);
+                if (Q > 0.0) P = -P;
+                Q = std::fabs(Q);
+                ETEMP = E;
+                E = D;
+                if ((std::fabs(P) >= std::fabs(0.5 * Q * ETEMP)) || (P <= Q * (A - X)) || (P >= Q * (Bb - X)))
+                    FLAG = 1;
+                else
+                    FLAG = 2;
+            }
+            if (FLAG == 1) {
+                E = (X >= XM) ? A - X : Bb - X;
+                D = CGOLD * E;
+            } else {
+                D = P / Q;
+                U = X + D;
+                if ((U - A < TOL2) || (Bb - U < TOL2)) D = std::copysign(TOL1, XM - X);
+            }
+            U = (std::fabs(D) >= TOL1) ? X + D : X + std::copysign(TOL1, D);
+            FU = lm_eval(phi, grad, U);
+            if (FU <= FX) {
+                if (U >= X) A = X; else Bb = X;
+                V = W; FV = FW; W = X; FW = FX; X = U; FX = FU;
+            } else {
+                if (U < X) A = U; else Bb = U;
+                if ((FU <= FW) || (W == X)) {
+                    V = W; FV = FW; W = U; FW = FU;
+                } else if ((FU <= FV) || (V == X) || (V == W)) {
+                    V = U; FV = FU;
+                }
+            }
+        }
+        if (fx_out) *fx_out = FX;
+        return X;
+    }
+
+    // ---- CG loop -------------------------------------------------------------
+    double H(const double2* a, const double2* b) {
+        SpecDotPair p{a, b, 1};
+        double r;
+        e.dots(&p, 1, &r);
+        return r;
+    }
+
+    void pre_loop() {
+        // rescaleLqNorm + divAvg_free (optimization.f90:61-62)
+        const double nrm = std::pow(e.lq_pow(u, nullptr, 0.0), 1.0 / q());
+        e.lincomb(u, B() / nrm, u);
+        e.leray(u);
+        Trial t;
+        e.R_eval(u, nullptr, 0.0, t.R, &t.lqq);
+        J0 = t.R[0];  // 78
+        iter = start_iter;
+        tau0 = std::pow(10.0, 2.0);
+        zero(gu0);
+        zero(vtg0);
+        zero(vtd0);
+        roll.assign(std::max(1, e.P.rolling_size), 0.0);
+        avg_imp = 1.0;
+        while_flag = 0;
+        started = true;
+    }
+
+    // one iteration of optimization.f90:136-446; returns status
+    int one_iteration(mlq_iter_info& info) {
+        auto t0 = std::chrono::steady_clock::now();
+        std::memset(&info, 0, sizeof(info));
+        iter++;
+        info.iter = iter;
+        evals_this_iter = 0;
+        trials.clear();
+        const double qq = q(), Bc = B();
+        const double s = (3.0 / 2.0) - (1.0 / qq);  // 150
+        double2* g1 = gu1;
+        double lqq_u = 0;
+        e.grad_l2(u, g1, c, &lqq_u);  // 146
+        e.hilbert(g1, s);             // 151
+        e.leray(g1);                  // 153
+        // normal of the tangent space: ||u||_q^{1-q} P2(|u|^{q-2} u) (162)
+        const double unorm = std::pow(lqq_u, 1.0 / qq);
+        e.lincomb(c, std::pow(unorm, 1.0 - qq), c);
+        e.hilbert(c, s);  // 164
+        e.leray(c);       // 169
+        double dd[6];
+        {
+            SpecDotPair p[2] = {{c, g1, 1}, {c, c, 1}};
+            e.dots(p, 2, dd);
+        }
+        const double alpha = dd[0] / dd[1];  // 170-171
+        info.alpha = alpha;
+        e.lincomb(g1, 1.0, g1, -alpha, c);  // gradJproj (177), kept in gu1
+        {
+            // 180-193: orthogonality and divergence checks
+            e.lincomb(tmp, 1.0, g1, 1.0, c);
+            SpecDotPair p[4] = {{g1, c, 1}, {tmp, tmp, 1}, {g1, nullptr, 2}, {g1, g1, 1}};
+            e.dots(p, 4, dd);
+            info.ortho_check = std::fabs(dd[0] / dd[1]);
+            info.div_check = dd[2] / dd[3];
+        }
+        if (!e.P.use_tangential_gradient) throw CudaError("useTangentialGradient=.false. is not supported",
+                                                          MLQ_ERR_BADARG);
+        if (e.P.normalize_gradient) {
+            SpecDotPair p[2] = {{u, u, 1}, {g1, g1, 1}};
+            e.dots(p, 2, dd);
+            e.lincomb(g1, std::sqrt(dd[0] / dd[1]), g1);  // 213
+        }
+        double beta = 0.0;
+        if (e.P.use_conjugate_gradient) {
+            e.lincomb(tmp, 1.0, g1, -1.0, vtg0);
+            SpecDotPair p[2] = {{g1, tmp, 1}, {gu0, gu0, 1}};
+            e.dots(p, 2, dd);
+            beta = dd[0];  // 226
+            const double g0n = dd[1];  // 227
+            if (g0n < MACH_EPSILON || beta < MACH_EPSILON)
+                beta = 0.0;
+            else
+                beta = beta / g0n;
+            if (e.P.reset_momentum_every > 0 && iter % e.P.reset_momentum_every == 0) beta = 0.0;  // 235-238
+            e.lincomb(d1, 1.0, g1, beta, vtd0);                                                      // 240
+        } else {
+            e.lincomb(d1, 1.0, g1);
+        }
+        info.beta = beta;
+        {
+            SpecDotPair p[3] = {{g1, g1, 1}, {vtd0, vtd0, 1}, {d1, d1, 1}};
+            e.dots(p, 3, dd);
+            info.norm_grad = std::sqrt(dd[0]);
+            info.norm_td0 = std::sqrt(dd[1]);
+            info.norm_d1 = std::sqrt(dd[2]);
+        }
+        e.zeroth(d1, info.mean_d1);  // 251
+        e.zeroth(u, info.mean_u);    // 257
+        // line search (269-318)
+        double tb[2] = {0, 0};
+        int mflag = 0;
+        mnbrak(u, d1, 0.0, tau0, tb, &mflag);
+        info.J0 = J0;
+        info.mnbrak_flag = mflag;
+        if (mflag != 0) {
+            info.n_evals = evals_this_iter;
+            info.status = mflag == 1 ? MLQ_ERR_MNBRAK_UPHILL : MLQ_ERR_MNBRAK_ITMAX;
+            while_flag = 1;
+            info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            return info.status;
+        }
+        double fx = 0;
+        double tau1 = brent(u, d1, tb, &fx);  // 297
+        info.tau_a = tb[0];
+        info.tau_b = tb[1];
+        int status = MLQ_OK;
+        if (tau1 > TAU_MAX) {  // 310-314
+            while_flag = 1;
+            status = MLQ_ERR_TAU_MAX;
+            tau1 = 0.0;
+        }
+        info.tau = tau1;
+        // vector transport of gu1 and d1 to the new point (324-328)
+        double ir[2];
+        const double2* xi[2] = {g1, d1};
+        double lqw;
+        if (e.P.use_riemannian_geometry)
+            lqw = e.transport_pieces(u, d1, tau1, xi, 2, ir);
+        else
+            lqw = e.lq_pow(u, d1, tau1);
+        const double ln = std::pow(lqw, 1.0 / qq);
+        if (e.P.use_riemannian_geometry) {
+            const double f = std::pow(ln, -qq);
+            e.lincomb(vtg0, Bc / ln, g1, -Bc / ln * f * ir[0], u, -Bc / ln * f * ir[0] * tau1, d1);
+            e.lincomb(vtd0, Bc / ln, d1, -Bc / ln * f * ir[1], u, -Bc / ln * f * ir[1] * tau1, d1);
+        } else {
+            e.lincomb(vtg0, 1.0, g1);
+            e.lincomb(vtd0, 1.0, d1);
+        }
+        // R at the retracted point from the accepted trial (homogeneity), as
+        // eval_J(Uvec, "maxdLqdt") after rescaleLqNorm (344-349)
+        const Trial tr = trial(u, d1, tau1);
+        const double cs = Bc / std::pow(tr.lqq, 1.0 / qq);
+        const double R12n = std::pow(cs, qq) * tr.R[1], R3n = std::pow(cs, qq + 1.0) * tr.R[2];
+        e.lincomb(u, Bc / ln, u, Bc / ln * tau1, d1);
+        trials.clear();
+        const double J1 = R12n + R3n;
+        const double deltaJ = (J1 - J0) / std::fabs(J0);
+        info.J1 = J1;
+        info.deltaJ = deltaJ;
+        info.n_evals = evals_this_iter;
+        if (deltaJ < -MACH_EPSILON) {  // 351-366
+            while_flag = 1;
+            info.status = MLQ_ERR_J_DECREASED;
+            info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            return info.status;
+        }
+        info.u_norm_q = cs * std::pow(tr.lqq, 1.0 / qq);  // ||u||_q after the retraction (421)
+        info.R = J1;
+        info.R12 = R12n;
+        info.R3 = R3n;
+        // 432-445
+        J0 = J1;
+        std::swap(gu0, gu1);
+        tau0 = tau1;
+        for (int i = (int)roll.size() - 1; i >= 1; --i) roll[i] = roll[i - 1];
+        roll[0] = deltaJ;
+        double ssum = 0.0;
+        for (double r : roll) ssum += r;
+        avg_imp = ssum / (double)(iter - start_iter);
+        info.status = status;
+        info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return status;
+    }
+
+    int state_iterate(int n_iter, mlq_iter_cb cb, void* user, int* iters) override {
+        if (!started) pre_loop();
+        int done = 0, status = MLQ_OK;
+        while (done < n_iter && std::fabs(avg_imp) > e.P.optim_tol && iter < e.P.max_iter && while_flag < 1) {
+            mlq_iter_info info;
+            status = one_iteration(info);
+            ++done;
+            if (cb) cb(&info, user);
+            if (status != MLQ_OK) break;
+        }
+        if (iters) *iters = iter;
+        return status;
+    }
+
+    // ---- host-array entry points ----------------------------------------------
+    void R_parts(const double* uh, double out[3]) override {
+        load(uh, tmp);
+        double lqq;
+        e.R_eval(tmp, nullptr, 0.0, out, &lqq);
+    }
+    double eval_J(const double* uh, int mode) override {
+        load(uh, tmp);
+        Trial t;
+        switch (mode) {
+            case MLQ_J_MAXDLQDT:
+                e.R_eval(tmp, nullptr, 0.0, t.R, &t.lqq);
+                return t.R[0];
+            case MLQ_J_LINEMIN:
+                ++eval_count;
+                e.R_eval(tmp, nullptr, 0.0, t.R, &t.lqq);
+                return -1.0 * scaled_R(t);
+            case MLQ_J_LQNORM:
+                return std::pow(e.lq_pow(tmp, nullptr, 0.0), 1.0 / q());
+        }
+        throw CudaError("unknown eval_J mode", MLQ_ERR_BADARG);
+    }
+    void grad_l2(const double* uh, double* v) override {
+        load(uh, tmp);
+        e.grad_l2(tmp, d1, c, nullptr);
+        e.store_vec(d1, v);
+        started = false;
+    }
+    double lq_norm(const double* uh) override {
+        load(uh, tmp);
+        return std::pow(e.lq_pow(tmp, nullptr, 0.0), 1.0 / q());
+    }
+    void rescale(double* uh, double Bv) override {
+        const double nrm = lq_norm(uh);
+        const long m = 3 * e.n3;
+        for (long i = 0; i < m; ++i) uh[i] = Bv / nrm * uh[i];
+    }
+    void normal_l2(const double* uh, double* out) override {
+        load(uh, tmp);
+        // |u|^{q-2}u dealiased (984-1006): the same spectra grad_l2 builds
+        double lqq;
+        e.grad_l2(tmp, d1, c, &lqq);
+        const double nrm = std::pow(lqq, 1.0 / q());
+        e.lincomb(c, std::pow(nrm, 1.0 - q()), c);
+        e.store_vec(c, out);
+        started = false;
+    }
+    void vector_transport(const double* uh, double qv, double Bv, const double* eta, const double* xi,
+                          double* out) override {
+        if (qv != q()) throw CudaError("vectorTransport q must equal the context's q", MLQ_ERR_BADARG);
+        load(uh, tmp);
+        load(eta, d1);
+        load(xi, gu1);
+        double ir;
+        const double2* xs[1] = {gu1};
+        const double lqq = e.transport_pieces(tmp, d1, 1.0, xs, 1, &ir);
+        const double ln = std::pow(lqq, 1.0 / qv);
+        const double f = std::pow(ln, -qv) * ir;
+        e.lincomb(c, Bv / ln, gu1, -Bv / ln * f, tmp, -Bv / ln * f, d1);
+        e.store_vec(c, out);
+        started = false;
+    }
+    void hilbert_host(double* g, double order) override {
+        load(g, tmp);
+        e.hilbert(tmp, order);
+        e.store_vec(tmp, g);
+    }
+    void divavg_host(double* g) override {
+        load(g, tmp);
+        e.leray(tmp);
+        e.store_vec(tmp, g);
+    }
+    double inner_host(const double* f, const double* g, int type) override {
+        load(f, tmp);
+        load(g, c);
+        SpecDotPair p{tmp, c, type == MLQ_INNER_HL ? 1 : 0};
+        double r;
+        e.dots(&p, 1, &r);
+        started = false;
+        return r;
+    }
+    void zeroth_host(const double* uh, double out[3]) override {
+        load(uh, tmp);
+        e.zeroth(tmp, out);
+    }
+    void calc_uk_host(const double* uh, double k, double* out) override {
+        load(uh, tmp);
+        e.calc_uk(tmp, k, 40);
+        e.store_scalar_phys(40, out);
+    }
+    int mnbrak_host(const double* phi, const double* d, double tA0, double tB0, double br[2], int* flag) override {
+        load(phi, tmp);
+        load(d, c);
+        trials.clear();
+        *flag = 0;
+        mnbrak(tmp, c, tA0, tB0, br, flag);
+        trials.clear();
+        started = false;
+        return *flag;
+    }
+    double brent_host(const double* phi, const double* d, const double br[2]) override {
+        load(phi, tmp);
+        load(d, c);
+        trials.clear();
+        const double x = brent(tmp, c, br, nullptr);
+        trials.clear();
+        started = false;
+        return x;
+    }
+    void state_load(const double* uh) override {
+        load(uh, u);
+        started = false;
+    }
+    void state_store(double* uh) override { e.store_vec(u, uh); }
+    void state_R(double out[3], double* lqn) override {
+        double lqq;
+        e.R_eval(u, nullptr, 0.0, out, &lqq);
+        if (lqn) *lqn = std::pow(lqq, 1.0 / q());
+    }
+    void seed_field(unsigned long long seed, double slope, double k0, double* out) override {
+        std::vector<double> h(3 * nc() * 2);
+        seed_spectrum_host(e.n, seed, slope, k0, e.b2, h.data());
+        MLQ_CUDA(cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
+        MLQ_CUDA(cudaStreamSynchronize(e.stream));
+        e.store_vec(tmp, out);
+    }
+    void set_B(double Bv) override {
+        e.P.B = Bv;
+        started = false;
+    }
+    void set_start_iter(int s) override { start_iter = s; }
+};
+
+std::unique_ptr<SolverBase> make_solver(const mlq_params& p) {
+    if (p.precision == MLQ_PREC_MIXED) return std::unique_ptr<SolverBase>(new Solver<float>(p));
+    return std::unique_ptr<SolverBase>(new Solver<double>(p));
+}
+
+std::unique_ptr<EngineBase> make_fft_engine(const mlq_params& p) {
+    mlq_params q = p;
+    q.precision = MLQ_PREC_FP64;
+    return std::unique_ptr<EngineBase>(new Engine<double>(q));
+}
+
+}  // namespace mlq

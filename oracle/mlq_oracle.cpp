@@ -1,0 +1,988 @@
+// mlq_oracle.cpp -- CPU FP64 restatement of maxLq's CG hot path, reference order.
+//
+// TEST INFRASTRUCTURE ONLY: the checker for the CUDA product (see mlq_oracle.h).
+// Each function cites the Fortran routine it restates (paths are relative to
+// the reference project root).  Arithmetic follows the Fortran expression
+// order where it matters for masks and thresholds.
+#include "mlq_oracle.h"
+
+#include <cmath>
+#include <complex>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+typedef std::complex<double> cplx;
+
+const double MACH_EPSILON = 2.0e-16;  // global_variables.f90:28
+const double TAU_MAX = 1.0e2;         // global_variables.f90:29
+
+// ---------------------------------------------------------------------------
+// 1D mixed-radix Stockham FFT (radices 4, 2, 3, 5, generic).  The oracle's
+// own FFT; FFTW is not vendored by the reference (makefile:20-21), so parity
+// at this boundary is the mathematical DFT.
+// ---------------------------------------------------------------------------
+struct Fft1D {
+    int n = 0;
+    std::vector<int> radix;
+    std::vector<cplx> w;  // w[k] = exp(-2 pi i k / n)
+
+    void init(int nn) {
+        n = nn;
+        radix.clear();
+        int m = n;
+        while (m % 4 == 0) { radix.push_back(4); m /= 4; }
+        while (m % 2 == 0) { radix.push_back(2); m /= 2; }
+        for (int p = 3; m > 1; p += 2) {
+            while (m % p == 0) { radix.push_back(p); m /= p; }
+        }
+        w.resize(n);
+        for (int k = 0; k < n; ++k) {
+            // angle reduced to [0, 2pi) exactly in integers first
+            double a = 2.0 * M_PI * (double)k / (double)n;
+            w[k] = cplx(std::cos(a), -std::sin(a));
+        }
+    }
+    inline cplx tw(long e, int sign) const {
+        long k = ((e % n) + n) % n;
+        cplx v = w[k];
+        return sign < 0 ? v : std::conj(v);
+    }
+    // sign -1: forward exp(-i...), +1: backward exp(+i...).  Unnormalised.
+    void exec(cplx* x, cplx* work, int sign) const {
+        cplx* src = x;
+        cplx* dst = work;
+        int ns = 1;
+        for (int R : radix) {
+            int nr = n / R;
+            cplx v[16], o[16];
+            for (int j = 0; j < nr; ++j) {
+                int k = j % ns;
+                long step = (long)n / ((long)ns * R);
+                for (int r = 0; r < R; ++r) v[r] = src[j + r * nr] * tw((long)r * k * step, sign);
+                for (int m = 0; m < R; ++m) {
+                    cplx acc = 0.0;
+                    for (int r = 0; r < R; ++r) acc += v[r] * tw((long)r * m * (n / R), sign);
+                    o[m] = acc;
+                }
+                int idxD = (j / ns) * ns * R + k;
+                for (int r = 0; r < R; ++r) dst[idxD + r * ns] = o[r];
+            }
+            std::swap(src, dst);
+            ns *= R;
+        }
+        if (src != x) std::memcpy(x, src, sizeof(cplx) * n);
+    }
+};
+
+}  // namespace
+
+struct orc_ctx {
+    orc_params p;
+    int n;
+    long n3;
+    double dV, PI;
+    std::vector<double> K;  // K1 = K2 = K3 (initialize.f90:170-192)
+    Fft1D fft;
+    int n_evals = 0;
+};
+
+namespace {
+
+inline long IDX(const orc_ctx* c, int x, int y, int z) {
+    return ((long)z * c->n + y) * c->n + x;
+}
+
+// 3D c2c over [z][y][x], all three axes; sign as Fft1D.
+void fft3(orc_ctx* c, cplx* a, int sign) {
+    const int n = c->n;
+#pragma omp parallel
+    {
+        std::vector<cplx> line(n), work(n);
+        // x lines (contiguous)
+#pragma omp for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y) c->fft.exec(a + IDX(c, 0, y, z), work.data(), sign);
+        // y lines
+#pragma omp for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int x = 0; x < n; ++x) {
+                for (int y = 0; y < n; ++y) line[y] = a[IDX(c, x, y, z)];
+                c->fft.exec(line.data(), work.data(), sign);
+                for (int y = 0; y < n; ++y) a[IDX(c, x, y, z)] = line[y];
+            }
+        // z lines
+#pragma omp for collapse(2)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                for (int z = 0; z < n; ++z) line[z] = a[IDX(c, x, y, z)];
+                c->fft.exec(line.data(), work.data(), sign);
+                for (int z = 0; z < n; ++z) a[IDX(c, x, y, z)] = line[z];
+            }
+    }
+}
+
+// fftfwd (fftwfunction.f90:62-93): unnormalised forward.  The NaN scan with
+// `stop 1` (78-89) is mirrored by the caller-visible status of the product,
+// not here.
+void fftfwd(orc_ctx* c, cplx* a) { fft3(c, a, -1); }
+
+// fftbwd (fftwfunction.f90:98-113): backward then /product(n).
+void fftbwd(orc_ctx* c, cplx* a) {
+    fft3(c, a, +1);
+    const double s = (double)c->n * (double)c->n * (double)c->n;
+#pragma omp parallel for
+    for (long i = 0; i < c->n3; ++i) a[i] /= s;
+}
+
+typedef std::vector<double> RV;
+typedef std::vector<cplx> CV;
+
+CV to_complex(const orc_ctx* c, const double* f) {
+    CV a(c->n3);
+#pragma omp parallel for
+    for (long i = 0; i < c->n3; ++i) a[i] = cplx(f[i], 0.0);
+    return a;
+}
+void real_part(const orc_ctx* c, const CV& a, double* f) {
+#pragma omp parallel for
+    for (long i = 0; i < c->n3; ++i) f[i] = a[i].real();
+}
+
+inline double Kx(const orc_ctx* c, int i) { return c->K[i]; }
+
+// dealiasing_cutoff_scalar_complex (function_ops.f90:3358-3398): zero modes
+// with max(|K1|,|K2|,|K3|) > 2 pi n / (order+1).
+void dealias_cut(orc_ctx* c, CV& f, double order) {
+    const double kcut = 2.0 * c->PI * (double)c->n / (order + 1.0);
+    const int n = c->n;
+    std::vector<char> keep(n);
+    for (int i = 0; i < n; ++i) keep[i] = std::fabs(c->K[i]) > kcut ? 0 : 1;
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x)
+                if (!(keep[x] && keep[y] && keep[z])) f[IDX(c, x, y, z)] = 0.0;
+}
+
+// dealias_scalar (function_ops.f90:3332-3350)
+void dealias_scalar(orc_ctx* c, double* g, double order) {
+    CV a = to_complex(c, g);
+    fftfwd(c, a.data());
+    dealias_cut(c, a, order);
+    fftbwd(c, a.data());
+    real_part(c, a, g);
+}
+
+inline void maybe_dealias(orc_ctx* c, double* g, double order) {
+    if (c->p.to_dealias) dealias_scalar(c, g, order);
+}
+
+// gradient (function_ops.f90:3147-3195): grad is [3][n3]
+void gradient(orc_ctx* c, const double* u, double* grad) {
+    const int n = c->n;
+    CV fu = to_complex(c, u);
+    fftfwd(c, fu.data());
+    for (int d = 0; d < 3; ++d) {
+        CV g(c->n3);
+#pragma omp parallel for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) {
+                    double k = d == 0 ? Kx(c, x) : (d == 1 ? Kx(c, y) : Kx(c, z));
+                    g[IDX(c, x, y, z)] = cplx(0.0, k) * fu[IDX(c, x, y, z)];
+                }
+        fftbwd(c, g.data());
+        real_part(c, g, grad + d * c->n3);
+    }
+}
+
+// divergence (function_ops.f90:3200-3243)
+void divergence(orc_ctx* c, const double* u, double* div) {
+    const int n = c->n;
+    CV uh[3];
+    for (int d = 0; d < 3; ++d) {
+        uh[d] = to_complex(c, u + d * c->n3);
+        fftfwd(c, uh[d].data());
+    }
+    CV dh(c->n3);
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                long i = IDX(c, x, y, z);
+                dh[i] = cplx(0.0, Kx(c, x)) * uh[0][i] + cplx(0.0, Kx(c, y)) * uh[1][i] +
+                        cplx(0.0, Kx(c, z)) * uh[2][i];
+            }
+    fftbwd(c, dh.data());
+    real_part(c, dh, div);
+}
+
+inline double ksq_of(const orc_ctx* c, int x, int y, int z) {
+    return Kx(c, x) * Kx(c, x) + Kx(c, y) * Kx(c, y) + Kx(c, z) * Kx(c, z);
+}
+
+// laplacian (function_ops.f90:3248-3282), in place on a vector field
+void laplacian(orc_ctx* c, double* f) {
+    const int n = c->n;
+    for (int d = 0; d < 3; ++d) {
+        CV a = to_complex(c, f + d * c->n3);
+        fftfwd(c, a.data());
+#pragma omp parallel for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) a[IDX(c, x, y, z)] *= -ksq_of(c, x, y, z);
+        fftbwd(c, a.data());
+        real_part(c, a, f + d * c->n3);
+    }
+}
+
+// solve_poisson (function_ops.f90:1951-1996): l^2 Delta phi = f, k=0 -> 0
+void solve_poisson(orc_ctx* c, const double* f, double l, double* phi) {
+    const int n = c->n;
+    CV a = to_complex(c, f);
+    fftfwd(c, a.data());
+    const double l2 = std::pow(l, 2.0);
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                long i = IDX(c, x, y, z);
+                double ksq = ksq_of(c, x, y, z);
+                a[i] = ksq == 0.0 ? cplx(0.0, 0.0) : -a[i] / (l2 * ksq);
+            }
+    fftbwd(c, a.data());
+    real_part(c, a, phi);
+}
+
+// calc_gk_order2 (function_ops.f90:2281-2319), recursive
+void calc_gk_order2(orc_ctx* c, const double* g, double k, double* gk) {
+    const long n3 = c->n3;
+    if (k + MACH_EPSILON < 0.0) {
+#pragma omp parallel for
+        for (long i = 0; i < n3; ++i) gk[i] = std::fabs(g[i]) < MACH_EPSILON ? 0.0 : std::pow(g[i], k);
+    } else if (k + MACH_EPSILON < 2.0) {
+#pragma omp parallel for
+        for (long i = 0; i < n3; ++i) gk[i] = std::pow(g[i], k);
+        maybe_dealias(c, gk, k);
+    } else {
+        RV g2(n3), gkm2(n3);
+#pragma omp parallel for
+        for (long i = 0; i < n3; ++i) g2[i] = g[i] * g[i];
+        maybe_dealias(c, g2.data(), 2.0);
+        calc_gk_order2(c, g, k - 2.0, gkm2.data());
+#pragma omp parallel for
+        for (long i = 0; i < n3; ++i) gk[i] = g2[i] * gkm2[i];
+        maybe_dealias(c, gk, 2.0);
+    }
+}
+
+// calc_uk (function_ops.f90:2324-2343)
+void calc_uk(orc_ctx* c, const double* u, double k, double* uk) {
+    const long n3 = c->n3;
+    RV s(n3);
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) {
+        double a = u[i], b = u[n3 + i], d = u[2 * n3 + i];
+        s[i] = a * a + b * b + d * d;
+    }
+    maybe_dealias(c, s.data(), 2.0);
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) s[i] = s[i] <= 0.0 ? 0.0 : std::pow(s[i], 0.5);
+    calc_gk_order2(c, s.data(), k, uk);
+}
+
+// calc_pointwiseVectorNorm (1775-1791) + calc_unitVectorInUdirection (1822-1858)
+void unit_vector(orc_ctx* c, const double* u, double* e) {
+    const long n3 = c->n3;
+    RV nrm(n3);
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i)
+        nrm[i] = u[i] * u[i] + u[n3 + i] * u[n3 + i] + u[2 * n3 + i] * u[2 * n3 + i];
+    maybe_dealias(c, nrm.data(), 2.0);
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) nrm[i] = std::sqrt(std::fabs(nrm[i]));
+    for (int d = 0; d < 3; ++d)
+#pragma omp parallel for
+        for (long i = 0; i < n3; ++i) e[d * n3 + i] = nrm[i] < MACH_EPSILON ? 0.0 : u[d * n3 + i] / nrm[i];
+}
+
+// gradU[i][j] = partial_j u_i as 9 scalar fields
+RV grad_tensor(orc_ctx* c, const double* u) {
+    RV g(9 * c->n3);
+    for (int i = 0; i < 3; ++i) gradient(c, u + i * c->n3, g.data() + 3 * i * c->n3);
+    return g;
+}
+inline const double* GU(const RV& g, const orc_ctx* c, int i, int j) { return g.data() + (3 * i + j) * c->n3; }
+
+// calc_nablaUnablaUt (1912-1945): sum_ij d_j u_i d_i u_j
+void nabla_u_nabla_ut(orc_ctx* c, const double* u, double* out) {
+    RV g = grad_tensor(c, u);
+    const long n3 = c->n3;
+#pragma omp parallel for
+    for (long p = 0; p < n3; ++p) {
+        double s = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) s += GU(g, c, j, i)[p] * GU(g, c, i, j)[p];
+        out[p] = s;
+    }
+    maybe_dealias(c, out, 2.0);
+}
+
+bool dealias_for_e_u(const orc_ctx* c) {
+    if (!c->p.to_dealias) return false;
+    return !c->p.use_e_u || c->p.dealias_e_u;
+}
+
+// calc_vvgradu (2001-2064): v . (v . nabla) u
+void vvgradu(orc_ctx* c, const double* u, const double* v, double* res) {
+    RV g = grad_tensor(c, u);
+    const long n3 = c->n3;
+    RV aux(3 * n3);
+#pragma omp parallel for
+    for (long p = 0; p < n3; ++p)
+        for (int jj = 0; jj < 3; ++jj) {
+            double s = 0.0;
+            for (int ii = 0; ii < 3; ++ii) s += v[ii * n3 + p] * GU(g, c, ii, jj)[p];
+            aux[jj * n3 + p] = s;
+        }
+    if (dealias_for_e_u(c))
+        for (int d = 0; d < 3; ++d) dealias_scalar(c, aux.data() + d * n3, 2.0);
+#pragma omp parallel for
+    for (long p = 0; p < n3; ++p) {
+        double s = 0.0;
+        for (int jj = 0; jj < 3; ++jj) s += v[jj * n3 + p] * aux[jj * n3 + p];
+        res[p] = s;
+    }
+    if (dealias_for_e_u(c)) dealias_scalar(c, res, 2.0);
+}
+
+// calc_vgraduvgradu (2165-2218): v_i d_j u_i v_k d_j u_k
+void vgraduvgradu(orc_ctx* c, const double* u, const double* v, double* res) {
+    RV g = grad_tensor(c, u);
+    const long n3 = c->n3;
+    RV vg(3 * n3);
+#pragma omp parallel for
+    for (long p = 0; p < n3; ++p)
+        for (int jj = 0; jj < 3; ++jj) {
+            double s = 0.0;
+            for (int ii = 0; ii < 3; ++ii) s += v[ii * n3 + p] * GU(g, c, ii, jj)[p];
+            vg[jj * n3 + p] = s;
+        }
+    if (dealias_for_e_u(c))
+        for (int d = 0; d < 3; ++d) dealias_scalar(c, vg.data() + d * n3, 2.0);
+#pragma omp parallel for
+    for (long p = 0; p < n3; ++p) {
+        double s = 0.0;
+        for (int jj = 0; jj < 3; ++jj) s += vg[jj * n3 + p] * vg[jj * n3 + p];
+        res[p] = s;
+    }
+    maybe_dealias(c, res, 2.0);
+}
+
+// calc_nablaModSquared (2366-2389)
+void nabla_mod_squared(orc_ctx* c, const double* u, double* out) {
+    const long n3 = c->n3;
+    std::memset(out, 0, sizeof(double) * n3);
+    RV g(3 * n3);
+    for (int i = 0; i < 3; ++i) {
+        gradient(c, u + i * n3, g.data());
+#pragma omp parallel for
+        for (long p = 0; p < n3; ++p)
+            for (int j = 0; j < 3; ++j) out[p] += g[j * n3 + p] * g[j * n3 + p];
+    }
+    maybe_dealias(c, out, 2.0);
+}
+
+// inner_product "L2" (3427-3437)
+double inner_l2(const orc_ctx* c, const double* f, const double* g) {
+    double s = 0.0;
+    // fixed (serial) order: the reference sums i1 fastest, one rank
+    for (long i = 0; i < c->n3; ++i) s += f[i] * g[i];
+    return s * c->dV;
+}
+
+// inner_product "H_l^(3/2-1/q)" (3462-3483)
+double inner_hl(orc_ctx* c, const double* f, const double* g) {
+    const int n = c->n;
+    CV fh = to_complex(c, f), gh = to_complex(c, g);
+    fftfwd(c, fh.data());
+    fftfwd(c, gh.data());
+    const double order = (3.0 / 2.0) - (1.0 / c->p.q);
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                long i = IDX(c, x, y, z);
+                double ks = std::sqrt(ksq_of(c, x, y, z));
+                double factor = 1.0 + std::pow(c->p.lambda1 * ks, order);
+                fh[i] *= factor;
+                gh[i] *= factor;
+            }
+    fftbwd(c, fh.data());
+    fftbwd(c, gh.data());
+    RV fa(c->n3), ga(c->n3);
+    real_part(c, fh, fa.data());
+    real_part(c, gh, ga.data());
+    return inner_l2(c, fa.data(), ga.data());
+}
+
+double inner(orc_ctx* c, const double* f, const double* g, int htype) {
+    return htype ? inner_hl(c, f, g) : inner_l2(c, f, g);
+}
+
+// global_summed_field_inner_product (3557-3577)
+double field_inner(orc_ctx* c, const double* f, const double* g, int htype) {
+    double s = 0.0;
+    for (int d = 0; d < 3; ++d) s += inner(c, f + d * c->n3, g + d * c->n3, htype);
+    return s;
+}
+
+// calc_local_dLqdt_inclParts (1304-1358); one rank so local == global (1392-1405)
+void R_parts(orc_ctx* c, const double* u, double out[3]) {
+    const long n3 = c->n3;
+    const double q = c->p.q, nu = c->p.visc, vc = c->p.visc_coef, pc = c->p.press_coef;
+    RV a_q2(n3), aux(n3), e(3 * n3), a_q4(n3), p(n3), tmp(n3);
+    calc_uk(c, u, q - 2.0, a_q2.data());
+    nabla_mod_squared(c, u, aux.data());
+    double R1 = -vc * nu * inner_l2(c, a_q2.data(), aux.data());
+    unit_vector(c, u, e.data());  // computed unconditionally (1323)
+    double R2;
+    if (c->p.use_e_u) {
+        vgraduvgradu(c, u, e.data(), aux.data());
+        R2 = -vc * (q - 2.0) * nu * inner_l2(c, a_q2.data(), aux.data());
+    } else {
+        calc_uk(c, u, q - 4.0, a_q4.data());
+        vgraduvgradu(c, u, u, aux.data());
+        R2 = -vc * (q - 2.0) * nu * inner_l2(c, a_q4.data(), aux.data());
+    }
+    nabla_u_nabla_ut(c, u, aux.data());
+    for (long i = 0; i < n3; ++i) tmp[i] = -aux[i];
+    solve_poisson(c, tmp.data(), 1.0, p.data());
+    double R3;
+    const double* mult = c->p.use_e_u ? a_q2.data() : a_q4.data();
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) aux[i] = p[i] * mult[i];
+    maybe_dealias(c, aux.data(), 2.0);
+    vvgradu(c, u, c->p.use_e_u ? e.data() : u, tmp.data());
+    R3 = pc * (q - 2.0) * inner_l2(c, aux.data(), tmp.data());
+    out[0] = R1 + R2 + R3;
+    out[1] = R1 + R2;
+    out[2] = R3;
+}
+
+// calc_global_Lq_norm (1675-1692)
+double lq_norm(orc_ctx* c, const double* u) {
+    RV a(c->n3);
+    calc_uk(c, u, c->p.q / 2.0, a.data());
+    double ip = inner_l2(c, a.data(), a.data());
+    return std::pow(ip, 1.0 / c->p.q);
+}
+
+// rescaleLqNorm (1699-1709)
+void rescale(orc_ctx* c, double* u, double B) {
+    double nrm = lq_norm(c, u);
+    const long m = 3 * c->n3;
+    for (long i = 0; i < m; ++i) u[i] = B / nrm * u[i];
+}
+
+// divAvg_free (2843-2918)
+void divavg_free(orc_ctx* c, double* f) {
+    const int n = c->n;
+    const long n3 = c->n3;
+    RV div(n3);
+    divergence(c, f, div.data());
+    CV dh = to_complex(c, div.data());
+    fftfwd(c, dh.data());
+    CV uh[3], gp[3];
+    for (int d = 0; d < 3; ++d) {
+        uh[d] = to_complex(c, f + d * n3);
+        fftfwd(c, uh[d].data());
+        gp[d].assign(n3, 0.0);
+    }
+#pragma omp parallel for collapse(2)
+    for (int z = 0; z < n; ++z)
+        for (int y = 0; y < n; ++y)
+            for (int x = 0; x < n; ++x) {
+                long i = IDX(c, x, y, z);
+                double ksq = ksq_of(c, x, y, z);
+                if (ksq > MACH_EPSILON) {
+                    gp[0][i] = -cplx(0.0, Kx(c, x)) * dh[i] / ksq;
+                    gp[1][i] = -cplx(0.0, Kx(c, y)) * dh[i] / ksq;
+                    gp[2][i] = -cplx(0.0, Kx(c, z)) * dh[i] / ksq;
+                } else {
+                    for (int d = 0; d < 3; ++d) { gp[d][i] = 0.0; uh[d][i] = 0.0; }
+                }
+            }
+    RV g(n3);
+    for (int d = 0; d < 3; ++d) {
+        fftbwd(c, gp[d].data());
+        real_part(c, gp[d], g.data());
+        fftbwd(c, uh[d].data());
+        real_part(c, uh[d], f + d * n3);
+        for (long i = 0; i < n3; ++i) f[d * n3 + i] -= g[i];
+    }
+}
+
+// HilbertGradient (3583-3627)
+void hilbert(orc_ctx* c, double* g, double order) {
+    const int n = c->n;
+    for (int d = 0; d < 3; ++d) {
+        CV a = to_complex(c, g + d * c->n3);
+        fftfwd(c, a.data());
+#pragma omp parallel for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) {
+                    double ks = std::sqrt(ksq_of(c, x, y, z));
+                    a[IDX(c, x, y, z)] /= (1.0 + std::pow(c->p.lambda1 * ks, 2.0 * order));
+                }
+        fftbwd(c, a.data());
+        real_part(c, a, g + d * c->n3);
+    }
+}
+
+// calc0thFourierModes (3048-3094): unnormalised k=0 coefficient
+void zeroth_modes(orc_ctx* c, const double* u, double out[3]) {
+    for (int d = 0; d < 3; ++d) {
+        CV a = to_complex(c, u + d * c->n3);
+        fftfwd(c, a.data());
+        out[d] = a[0].real();
+    }
+}
+
+// calcConstraintDerivativeL2 (984-1006)
+void normal_l2(orc_ctx* c, const double* u, double* out) {
+    const long n3 = c->n3;
+    const double q = c->p.q;
+    double nrm = lq_norm(c, u);
+    RV a(n3);
+    calc_uk(c, u, q - 2.0, a.data());
+    for (int d = 0; d < 3; ++d) {
+        for (long i = 0; i < n3; ++i) out[d * n3 + i] = a[i] * u[d * n3 + i];
+        if (c->p.to_dealias && (q - 2.0 > MACH_EPSILON)) dealias_scalar(c, out + d * n3, 2.0);
+    }
+    const double f = std::pow(nrm, 1.0 - q);
+    for (long i = 0; i < 3 * n3; ++i) out[i] = f * out[i];
+}
+
+// vectorTransport (1716-1768)
+void vector_transport(orc_ctx* c, const double* u, double q, double B, const double* eta,
+                      const double* xi, double* out) {
+    const long n3 = c->n3, m = 3 * n3;
+    RV w(m), a(n3), aux(m);
+    for (long i = 0; i < m; ++i) w[i] = u[i] + eta[i];
+    calc_uk(c, w.data(), q - 2.0, a.data());
+    for (int d = 0; d < 3; ++d) {
+        for (long i = 0; i < n3; ++i) aux[d * n3 + i] = a[i] * w[d * n3 + i];
+        if (c->p.to_dealias && (q - 2.0 > MACH_EPSILON)) dealias_scalar(c, aux.data() + d * n3, 2.0);
+    }
+    double ir = field_inner(c, aux.data(), xi, 0);
+    double ln = lq_norm(c, w.data());
+    for (long i = 0; i < m; ++i) out[i] = xi[i] - std::pow(ln, -q) * ir * w[i];
+    for (long i = 0; i < m; ++i) out[i] = B / ln * out[i];
+}
+
+// GradL2ForLq (1066-1211)
+void grad_l2(orc_ctx* c, const double* u, double* v) {
+    const long n3 = c->n3, m = 3 * n3;
+    const double q = c->p.q, nu = c->p.visc, vc = c->p.visc_coef, pc = c->p.press_coef;
+    RV a_q2(n3), aux(n3), aux2(n3), aux3(n3), aux4(n3), p(n3), a_q4(n3), tmp(n3);
+    RV gradP(m), dU(m), uq2u(m), a3v(m), a4v(m), a5v(m), a6v(m), a7v(m), e(m);
+    calc_uk(c, u, q - 2.0, a_q2.data());
+    nabla_u_nabla_ut(c, u, aux.data());
+    for (long i = 0; i < n3; ++i) tmp[i] = -aux[i];
+    solve_poisson(c, tmp.data(), 1.0, p.data());
+    gradient(c, p.data(), gradP.data());
+    std::memcpy(dU.data(), u, sizeof(double) * m);
+    laplacian(c, dU.data());
+    std::fill(aux2.begin(), aux2.end(), 0.0);
+    if (c->p.use_e_u) {
+        unit_vector(c, u, e.data());
+        for (int d = 0; d < 3; ++d)
+            for (long i = 0; i < n3; ++i)
+                aux2[i] = aux2[i] + e[d * n3 + i] * (vc * nu * dU[d * n3 + i] - pc * gradP[d * n3 + i]);
+        if (c->p.to_dealias && c->p.dealias_e_u) dealias_scalar(c, aux2.data(), 2.0);
+        for (long i = 0; i < n3; ++i) aux2[i] = a_q2[i] * aux2[i];
+        maybe_dealias(c, aux2.data(), 2.0);
+        for (int d = 0; d < 3; ++d) {
+            for (long i = 0; i < n3; ++i) a3v[d * n3 + i] = aux2[i] * e[d * n3 + i];
+            if (c->p.to_dealias && c->p.dealias_e_u) dealias_scalar(c, a3v.data() + d * n3, 2.0);
+        }
+    } else {
+        for (int d = 0; d < 3; ++d)
+            for (long i = 0; i < n3; ++i)
+                aux2[i] = aux2[i] + u[d * n3 + i] * (vc * nu * dU[d * n3 + i] - pc * gradP[d * n3 + i]);
+        maybe_dealias(c, aux2.data(), 2.0);
+        calc_uk(c, u, q - 4.0, a_q4.data());
+        for (long i = 0; i < n3; ++i) aux2[i] = a_q4[i] * aux2[i];
+        maybe_dealias(c, aux2.data(), 2.0);
+        for (int d = 0; d < 3; ++d) {
+            for (long i = 0; i < n3; ++i) a3v[d * n3 + i] = aux2[i] * u[d * n3 + i];
+            maybe_dealias(c, a3v.data() + d * n3, 2.0);
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        for (long i = 0; i < n3; ++i) uq2u[d * n3 + i] = a_q2[i] * u[d * n3 + i];
+        maybe_dealias(c, uq2u.data() + d * n3, 2.0);
+    }
+    divergence(c, uq2u.data(), aux3.data());
+    solve_poisson(c, aux3.data(), 1.0, aux4.data());
+    gradient(c, aux4.data(), a4v.data());
+    RV gU = grad_tensor(c, u);  // gU[k][i] = d_i u_k  (gradUk(:,:,:,ii))
+    for (int ii = 0; ii < 3; ++ii) {
+        for (long i = 0; i < n3; ++i)
+            a5v[ii * n3 + i] = GU(gU, c, 0, ii)[i] * a4v[0 * n3 + i] + GU(gU, c, 1, ii)[i] * a4v[1 * n3 + i] +
+                               GU(gU, c, 2, ii)[i] * a4v[2 * n3 + i];
+        maybe_dealias(c, a5v.data() + ii * n3, 2.0);
+    }
+    std::memcpy(a7v.data(), uq2u.data(), sizeof(double) * m);
+    laplacian(c, a7v.data());
+    for (int d = 0; d < 3; ++d) {
+        for (long i = 0; i < n3; ++i) a4v[d * n3 + i] = a_q2[i] * gradP[d * n3 + i];
+        maybe_dealias(c, a4v.data() + d * n3, 2.0);
+        for (long i = 0; i < n3; ++i) a6v[d * n3 + i] = a_q2[i] * dU[d * n3 + i];
+        maybe_dealias(c, a6v.data() + d * n3, 2.0);
+        for (long i = 0; i < n3; ++i)
+            v[d * n3 + i] = (q - 2.0) * a3v[d * n3 + i] - pc * a4v[d * n3 + i] + pc * 2.0 * a5v[d * n3 + i] +
+                            vc * nu * a6v[d * n3 + i] + vc * nu * a7v[d * n3 + i];
+    }
+}
+
+// eval_J (optimization.f90:520-547)
+double eval_J(orc_ctx* c, const double* field, int mode) {
+    const long m = 3 * c->n3;
+    RV aux(field, field + m);
+    double out[3];
+    switch (mode) {
+        case 0:
+            R_parts(c, aux.data(), out);
+            return out[0];
+        case 1:
+            c->n_evals++;
+            rescale(c, aux.data(), c->p.B);
+            R_parts(c, aux.data(), out);
+            return -1.0 * out[0];
+        case 2:
+            return lq_norm(c, aux.data());
+    }
+    return 0.0;
+}
+
+double lm_eval(orc_ctx* c, const double* phi, const double* d, double t, RV& buf) {
+    const long m = 3 * c->n3;
+    for (long i = 0; i < m; ++i) buf[i] = phi[i] + t * d[i];
+    return eval_J(c, buf.data(), 1);
+}
+
+// mnbrak (optimization.f90:613-778) without the save_linemin_data I/O.
+// Returns 0 ok; flag as the reference (1 uphill, 2 ITMAX).
+int mnbrak(orc_ctx* c, const double* phi, const double* grad, double tA0, double tB0, double tau_brack[2],
+           int* myflag) {
+    const double GOLD = (1.0 + std::sqrt(5.0)) / 2.0;
+    const double CGOLD = 1.0 / GOLD;
+    const double GLIMIT = 10.0;
+    const int ITMAX = 100;
+    RV buf(3 * c->n3);
+    double tA = tA0, tB = std::max(tB0, MACH_EPSILON), tC = 0.0, tP, FP, Pmax, R, Q;
+    double FA = lm_eval(c, phi, grad, tA, buf);
+    double FB = lm_eval(c, phi, grad, tB, buf);
+    double FC = 0.0;
+    int brakIter = 0;
+    while (FB > FA && tB > MACH_EPSILON) {
+        tB = CGOLD * tB;
+        FB = lm_eval(c, phi, grad, tB, buf);
+    }
+    if (tB <= MACH_EPSILON) {
+        *myflag = 1;
+        return 1;
+    }
+    tC = GOLD * tB;
+    FC = lm_eval(c, phi, grad, tC, buf);
+    while (FB >= FC && brakIter < ITMAX) {
+        brakIter++;
+        tC = GOLD * tC;
+        FC = lm_eval(c, phi, grad, tC, buf);
+        R = (tB - tA) * (FB - FC);
+        Q = (tB - tC) * (FB - FA);
+        tP = tB - 0.5 * ((tB - tC) * Q - (tB - tA) * R) / std::copysign(std::max(std::fabs(Q - R), MACH_EPSILON), Q - R);
+        Pmax = tB + GLIMIT * (tC - tB);
+        if ((tB - tP) * (tP - tC) > 0) {
+            FP = lm_eval(c, phi, grad, tP, buf);
+            if (FP < FC) {
+                tA = tB; FA = FB; tB = tP; FB = FP;
+                break;
+            } else if (FP > FB) {
+                tC = tP; FC = FP;
+                break;
+            }
+            tP = tC + GOLD * (tC - tB);
+            FP = lm_eval(c, phi, grad, tP, buf);
+        } else if ((tC - tP) * (tP - Pmax) > 0) {
+            FP = lm_eval(c, phi, grad, tP, buf);
+            if (FP < FC) {
+                tB = tC; tC = tP; FB = FC; FC = FP;
+                tP = tC + GOLD * (tC - tB);
+                FP = lm_eval(c, phi, grad, tP, buf);
+            }
+        } else if ((tP - Pmax) * (Pmax - tC) >= 0) {
+            tP = Pmax;
+            FP = lm_eval(c, phi, grad, tP, buf);
+        } else {
+            tP = tC + GOLD * (tC - tB);
+            FP = lm_eval(c, phi, grad, tP, buf);
+        }
+        tA = tB; tB = tC; tC = tP;
+        FA = FB; FB = FC; FC = FP;
+    }
+    tau_brack[0] = tA;
+    tau_brack[1] = tC;
+    *myflag = brakIter >= ITMAX ? 2 : 0;
+    return *myflag;
+}
+
+// brent (optimization.f90:784-951) without the brent-info file I/O.  The
+// constants are Fortran default-real literals widened to double (804-806).
+double brent(orc_ctx* c, const double* phi, const double* grad, const double tau_brack[2]) {
+    const int ITMAX = 300;
+    const double TOL = (double)1E-6f;
+    const double ZEPS = (double)1E-8f;
+    const double CGOLD = (double).381966f;
+    RV buf(3 * c->n3);
+    double D = 0.0, A = std::min(tau_brack[0], tau_brack[1]), B = std::max(tau_brack[0], tau_brack[1]);
+    double V = tau_brack[1] * CGOLD, W = V, X = V, E = 0.0, ETEMP, P, Q, R, U, XM, TOL1, TOL2;
+    double FX = lm_eval(c, phi, grad, D, buf);  // logged value at tau = 0 (833-834)
+    FX = lm_eval(c, phi, grad, X, buf);
+    double FV = FX, FW = FX, FU;
+    for (int j = 1; j <= ITMAX; ++j) {
+        XM = 0.5 * (A + B);
+        TOL1 = TOL * std::fabs(X) + ZEPS;
+        TOL2 = 2.0 * TOL1;
+        if (std::fabs(X - XM) <= (TOL2 - 0.5 * (B - A))) break;
+        int FLAG = 1;
+        if (std::fabs(E) > TOL1) {
+            R = (X - W) * (FX - FV);
+            Q = (X - V) * (FX - FW);
+            P = (X - V) * Q - (X - W) * R;
+            Q = 2.0 * (Q - R);
+            if (Q > 0.0) P = -P;
+            Q = std::fabs(Q);
+            ETEMP = E;
+            E = D;
+            if ((std::fabs(P) >= std::fabs(0.5 * Q * ETEMP)) || (P <= Q * (A - X)) || (P >= Q * (B - X)))
+                FLAG = 1;
+            else
+                FLAG = 2;
+        }
+        if (FLAG == 1) {
+            E = (X >= XM) ? A - X : B - X;
+            D = CGOLD * E;
+        } else {
+            D = P / Q;
+            U = X + D;
+            if ((U - A < TOL2) || (B - U < TOL2)) D = std::copysign(TOL1, XM - X);
+        }
+        U = (std::fabs(D) >= TOL1) ? X + D : X + std::copysign(TOL1, D);
+        FU = lm_eval(c, phi, grad, U, buf);
+        if (FU <= FX) {
+            if (U >= X) A = X; else B = X;
+            V = W; FV = FW; W = X; FW = FX; X = U; FX = FU;
+        } else {
+            if (U < X) A = U; else B = U;
+            if ((FU <= FW) || (W == X)) {
+                V = W; FV = FW; W = U; FW = FU;
+            } else if ((FU <= FV) || (V == X) || (V == W)) {
+                V = U; FV = FU;
+            }
+        }
+    }
+    return X;
+}
+
+}  // namespace
+
+extern "C" {
+
+void orc_default_params(orc_params* p, int n, double q, double B) {
+    p->n = n;
+    p->q = q;
+    p->B = B;
+    p->visc = 1.0;
+    p->lambda1 = 0.1;
+    p->visc_coef = 1.0;
+    p->press_coef = 1.0;
+    p->to_dealias = 1;
+    // set_e_u_or_just_u with use_e_u_auto_for_q_less_4 (initialize.f90:75-86)
+    p->use_e_u = (q < 4.0 - MACH_EPSILON) ? 1 : 0;
+    p->dealias_e_u = 1;
+    p->threads = 0;
+}
+
+orc_ctx* orc_create(const orc_params* p) {
+    orc_ctx* c = new orc_ctx;
+    c->p = *p;
+    c->n = p->n;
+    c->n3 = (long)p->n * p->n * p->n;
+    c->dV = 1.0 / ((double)p->n * (double)p->n * (double)p->n);  // initialize.f90:162
+    c->PI = 4.0 * std::atan2(1.0, 1.0);                          // initialize.f90:164
+    c->K.resize(p->n);
+    for (int i = 0; i < p->n; ++i)
+        c->K[i] = (i <= p->n / 2) ? 2.0 * c->PI * (double)i : 2.0 * c->PI * (double)(i - p->n);
+    c->fft.init(p->n);
+#ifdef _OPENMP
+    if (p->threads > 0) omp_set_num_threads(p->threads);
+#endif
+    return c;
+}
+
+void orc_destroy(orc_ctx* c) { delete c; }
+int orc_eval_count(orc_ctx* c) { return c->n_evals; }
+
+void orc_fft_c2c(orc_ctx* c, double* data, int dir) {
+    cplx* a = reinterpret_cast<cplx*>(data);
+    if (dir < 0) fftfwd(c, a); else fftbwd(c, a);
+}
+
+void orc_dealias_scalar(orc_ctx* c, double* g, double order) { dealias_scalar(c, g, order); }
+void orc_gradient(orc_ctx* c, const double* u, double* grad) { gradient(c, u, grad); }
+void orc_divergence(orc_ctx* c, const double* u, double* div) { divergence(c, u, div); }
+void orc_laplacian(orc_ctx* c, double* f) { laplacian(c, f); }
+void orc_solve_poisson(orc_ctx* c, const double* f, double l, double* phi) { solve_poisson(c, f, l, phi); }
+void orc_calc_uk(orc_ctx* c, const double* u, double k, double* uk) { calc_uk(c, u, k, uk); }
+void orc_unit_vector(orc_ctx* c, const double* u, double* e) { unit_vector(c, u, e); }
+void orc_divavg_free(orc_ctx* c, double* u) { divavg_free(c, u); }
+void orc_hilbert_gradient(orc_ctx* c, double* g, double order) { hilbert(c, g, order); }
+double orc_inner_product(orc_ctx* c, const double* f, const double* g, int htype) { return inner(c, f, g, htype); }
+double orc_field_inner(orc_ctx* c, const double* f, const double* g, int htype) { return field_inner(c, f, g, htype); }
+void orc_zeroth_modes(orc_ctx* c, const double* u, double out[3]) { zeroth_modes(c, u, out); }
+double orc_lq_norm(orc_ctx* c, const double* u) { return lq_norm(c, u); }
+void orc_rescale(orc_ctx* c, double* u, double B) { rescale(c, u, B); }
+void orc_normal_l2(orc_ctx* c, const double* u, double* out) { normal_l2(c, u, out); }
+void orc_vector_transport(orc_ctx* c, const double* u, double q, double B, const double* eta, const double* xi,
+                          double* out) {
+    vector_transport(c, u, q, B, eta, xi, out);
+}
+void orc_R_parts(orc_ctx* c, const double* u, double out[3]) { R_parts(c, u, out); }
+void orc_grad_l2(orc_ctx* c, const double* u, double* v) { grad_l2(c, u, v); }
+double orc_eval_J(orc_ctx* c, const double* u, int mode) { return eval_J(c, u, mode); }
+int orc_mnbrak(orc_ctx* c, const double* phi, const double* d, double tA0, double tB0, double tau_brack[2],
+               int* flag) {
+    *flag = 0;
+    return mnbrak(c, phi, d, tA0, tB0, tau_brack, flag);
+}
+double orc_brent(orc_ctx* c, const double* phi, const double* d, const double tau_brack[2]) {
+    return brent(c, phi, d, tau_brack);
+}
+
+// maxdLqdt (optimization.f90:7-514), flags at their defaults
+// (useTangentialGradient, useConjugateGradient, useRiemannianGeometry,
+// normalizeGradient all true; kappaTest off; no file output).
+int orc_maxdlqdt(orc_ctx* c, double* uvec, int max_iter, double optim_tol, int start_iter, orc_iter_cb cb,
+                 void* user, int* flag) {
+    const long n3 = c->n3, m = 3 * n3;
+    const double q = c->p.q, Bc = c->p.B;
+    const int resetEvery = 25, rollSize = 10;
+    RV gradJ1(m), gradJproj(m), normalL2(m), normalHs(m), gu0(m, 0.0), gu1(m), d0(m, 0.0), d1(m), vtg0(m, 0.0),
+        vtd0(m, 0.0), tmp(m), tmp2(m);
+    *flag = 0;
+    rescale(c, uvec, Bc);          // 61
+    divavg_free(c, uvec);          // 62
+    double J0 = eval_J(c, uvec, 0);  // 78
+    double J1 = J0, deltaJ;
+    int iter = start_iter;
+    double tau0 = std::pow(10.0, 2.0), tau1 = tau0;
+    std::vector<double> roll(rollSize, 0.0);
+    double avgImp = 1.0;
+    int while_flag = 0;
+    double tau_brack[2] = {0.0, 0.0};
+    while (std::fabs(avgImp) > optim_tol && iter < max_iter && while_flag < 1) {
+        iter++;
+        int ev0 = c->n_evals;
+        grad_l2(c, uvec, gradJ1.data());                       // 146
+        const double s = (3.0 / 2.0) - (1.0 / q);              // 150
+        hilbert(c, gradJ1.data(), s);                          // 151
+        divavg_free(c, gradJ1.data());                         // 153
+        normal_l2(c, uvec, normalL2.data());                   // 162
+        normalHs = normalL2;
+        hilbert(c, normalHs.data(), s);                        // 164
+        divavg_free(c, normalHs.data());                       // 169
+        double alpha = field_inner(c, normalHs.data(), gradJ1.data(), 1);
+        alpha = alpha / field_inner(c, normalHs.data(), normalHs.data(), 1);  // 170-171
+        for (long i = 0; i < m; ++i) gradJproj[i] = gradJ1[i] - alpha * normalHs[i];  // 177
+        gu1 = gradJproj;                                                             // 202
+        {
+            double r = std::sqrt(field_inner(c, uvec, uvec, 1) / field_inner(c, gu1.data(), gu1.data(), 1));
+            for (long i = 0; i < m; ++i) gu1[i] = r * gu1[i];  // 213
+        }
+        for (long i = 0; i < m; ++i) tmp[i] = gu1[i] - vtg0[i];
+        double beta = field_inner(c, gu1.data(), tmp.data(), 1);       // 226
+        double g0n = field_inner(c, gu0.data(), gu0.data(), 1);        // 227
+        if (g0n < MACH_EPSILON || beta < MACH_EPSILON) beta = 0.0; else beta = beta / g0n;
+        if (iter % resetEvery == 0) beta = 0.0;                        // 235-238
+        for (long i = 0; i < m; ++i) d1[i] = gu1[i] + beta * vtd0[i];  // 240
+        double nG = std::sqrt(field_inner(c, gu1.data(), gu1.data(), 1));
+        double nT = std::sqrt(field_inner(c, vtd0.data(), vtd0.data(), 1));
+        double nD = std::sqrt(field_inner(c, d1.data(), d1.data(), 1));
+        int mflag = 0;
+        mnbrak(c, uvec, d1.data(), 0.0, tau0, tau_brack, &mflag);      // 269
+        if (mflag != 0) {
+            *flag = mflag;
+            if (cb) {
+                orc_iter_info info = {};
+                info.iter = iter; info.J0 = J0; info.mnbrak_flag = mflag; info.beta = beta;
+                info.n_evals = c->n_evals - ev0;
+                cb(&info, user);
+            }
+            while_flag = 1;
+            break;
+        }
+        tau1 = brent(c, uvec, d1.data(), tau_brack);  // 297
+        if (tau1 > TAU_MAX) {                          // 310-314
+            while_flag = 1;
+            *flag = 4;
+            tau1 = 0.0;
+        }
+        for (long i = 0; i < m; ++i) tmp2[i] = tau1 * d1[i];
+        vector_transport(c, uvec, q, Bc, tmp2.data(), gu1.data(), vtg0.data());  // 326
+        vector_transport(c, uvec, q, Bc, tmp2.data(), d1.data(), vtd0.data());   // 327
+        for (long i = 0; i < m; ++i) uvec[i] = uvec[i] + tau1 * d1[i];           // 345
+        rescale(c, uvec, Bc);                                                   // 346
+        J1 = eval_J(c, uvec, 0);                                                // 349
+        deltaJ = (J1 - J0) / std::fabs(J0);
+        orc_iter_info info = {};
+        info.iter = iter; info.tau_a = tau_brack[0]; info.tau = tau1; info.tau_b = tau_brack[1];
+        info.J0 = J0; info.deltaJ = deltaJ; info.J1 = J1; info.beta = beta; info.alpha = alpha;
+        info.norm_grad = nG; info.norm_td0 = nT; info.norm_d1 = nD;
+        info.n_evals = c->n_evals - ev0; info.mnbrak_flag = 0;
+        if (deltaJ < -MACH_EPSILON) {  // 351-366
+            *flag = 5;
+            if (cb) cb(&info, user);
+            while_flag = 1;
+            break;
+        }
+        info.u_norm_q = lq_norm(c, uvec);  // 421
+        {
+            double parts[3];
+            R_parts(c, uvec, parts);  // 423
+            info.R = parts[0]; info.R12 = parts[1]; info.R3 = parts[2];
+        }
+        if (cb) cb(&info, user);
+        J0 = J1;      // 432
+        gu0 = gu1;    // 434
+        tau0 = tau1;  // 435
+        d0 = d1;      // 436
+        for (int i = rollSize - 1; i >= 1; --i) roll[i] = roll[i - 1];  // 439
+        roll[0] = deltaJ;                                               // 443
+        double ssum = 0.0;
+        for (int i = 0; i < rollSize; ++i) ssum += roll[i];
+        avgImp = ssum / (double)(iter - start_iter);  // 445
+    }
+    return iter;
+}
+
+}  // extern "C"
