@@ -1,0 +1,377 @@
+"""Benchmark: maxLq Riemannian CG iterations per second on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n 512] [--q 4]
+    python bench.py --impl reference ...      # the reference algorithm on the host cores
+
+A step is one full CG iteration of maxdLqdt (optimization.f90:136-446):
+GradL2ForLq, Hilbert gradient, tangent projection, Polak-Ribiere beta, the
+mnbrak + Brent line search (each trial a full R evaluation), two vector
+transports and the retraction.  Workload: N = 512^3, q = 4, B = 1, seeded
+divergence-free field with spectrum |j|^-2 exp(-(|j|/(N/32))^2) (synthetic:
+the reference ships no input fields).  The headline value is the
+mixed-precision path (FP32 fields and FFTs, FP64 state, reductions and
+control); the all-FP64 path is timed the same way and reported beside it.
+
+With N > 1 (torchrun) every rank runs an independent replica (seed = rank):
+the path does not shard (one GPU holds the whole box), so value = all ranks'
+iterations / the slowest rank's time, and there is no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "CG iters/s at 512³ q=4: mixed vs FP64 GPU (rel ΔR≤1e-6); FFT HBM GB/s"
+# c2c transforms per CG iteration in the reference at q >= 4 (outside the line
+# search) and per eval_J("LineMin") trial: SURVEY-derived counts of the
+# reference's operator sequence ("Reference arm").
+REF_T_PER_ITER = 548
+REF_T_PER_TRIAL = 94
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=512)
+    ap.add_argument("--q", type=float, default=4.0)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison path")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+class Dist:
+    """Rank bookkeeping; torch.distributed only when WORLD_SIZE > 1."""
+
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+
+            backend = "nccl" if torch.cuda.is_available() else "gloo"
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v: float) -> float:
+        return self._reduce(v, "max")
+
+    def sum(self, v: float) -> float:
+        return self._reduce(v, "sum")
+
+    def _reduce(self, v, op):
+        if not self.pg:
+            return v
+        import torch
+
+        dev = f"cuda:{self.local}" if torch.cuda.is_available() else "cpu"
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX if op == "max" else self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def device_sync():
+    try:
+        import torch
+
+        if torch.cuda.is_available():
+            torch.cuda.synchronize()
+    except Exception:
+        pass
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, f[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of kernels from a committed ncu summary (or {})."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return {}
+    return {}
+
+
+def run_path(ctx, u0, K, W, dist, profile=False):
+    """W warm-up iterations then exactly K timed ones on the resident state."""
+    ctx.state_load(u0)
+    recs = []
+    for _ in range(W):
+        _, st, r = ctx.state_iterate(1)
+        recs += r
+    dist.barrier()
+    device_sync()
+    l0 = ctx.kernel_launches
+    if profile:
+        ctx.profile(True)
+        ctx.profile_report(reset=True)
+    t0 = time.perf_counter()
+    timed = []
+    for _ in range(K):
+        _, st, r = ctx.state_iterate(1)
+        timed += r
+        if st != 0:
+            break
+    device_sync()
+    wall = time.perf_counter() - t0
+    dist.barrier()
+    prof = ctx.profile_report(reset=True) if profile else {}
+    if profile:
+        ctx.profile(False)
+    launches = ctx.kernel_launches - l0
+    dev = sum(r["seconds"] for r in timed)
+    return {"records": timed, "device_s": dev, "wall_s": wall, "launches": launches, "prof": prof,
+            "iters": len(timed)}
+
+
+def cpu_reference_sample(n, q, n_evals, workers):
+    """One reference-order dealias round trip (2 c2c transforms) of an N^3 field
+    with the CPU transcription; returns (seconds per c2c transform, sample text)."""
+    from oracle.ref_numpy import RefNumpy
+
+    r = RefNumpy(n, q, workers=workers)
+    g = np.random.default_rng(0).standard_normal((n, n, n))
+    t0 = time.perf_counter()
+    r.dealias(g, 2.0)
+    dt = time.perf_counter() - t0
+    return dt / 2.0
+
+
+def bench_reference(args, dist):
+    """--impl reference: the reference algorithm (reference-order CPU
+    transcription, scipy pocketfft on all host threads) on the host cores."""
+    if dist.rank != 0:
+        dist.close()
+        return
+    n, q = args.n, args.q
+    workers = os.cpu_count() or 1
+    n_evals = REF_TRIALS_PER_ITER
+    per_iter = []
+    for i in range(args.warmup + args.steps):
+        t_T = cpu_reference_sample(n, q, n_evals, workers)
+        if i >= args.warmup:
+            per_iter.append(t_T * (REF_T_PER_ITER + REF_T_PER_TRIAL * n_evals))
+    tot = sum(per_iter)
+    value = len(per_iter) / tot
+    sample = (f"one reference-order dealias_scalar round trip (2 c2c {n}^3 FFTs, scipy pocketfft, "
+              f"{workers} threads) per step, scaled by the reference's {REF_T_PER_ITER} + {REF_T_PER_TRIAL} x "
+              f"{n_evals} transforms per CG iteration")
+    line = {"metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * tot / len(per_iter), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"maxdLqdt CG iteration, N={n}^3, q={q:g}, B=1", "n": n, "q": q},
+            "cpu_baseline": {"value": value, "unit": "iters/s", "cores": workers, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    dist.close()
+
+
+# trials per CG iteration used to scale the CPU sample: the mean count the GPU
+# run measures on this workload is reported beside it in our arm's line
+REF_TRIALS_PER_ITER = 12
+
+
+def main():
+    args = parse()
+    dist = Dist()
+    if args.impl == "reference":
+        return bench_reference(args, dist)
+
+    import maxlq_b200 as mlq
+
+    n, q, K, W = args.n, args.q, args.steps, args.warmup
+    k0 = n / 32.0
+    dev = dist.local
+    seed = dist.rank
+    peak, peak_kind = load_peaks()
+
+    mixed = mlq.MaxLq(n, q, 1.0, precision="mixed", device=dev, optim_tol=0.0)
+    u0 = mixed.seed_field(seed, 2.0, k0)
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    res_m = run_path(mixed, u0, K, W, dist, profile=True)
+    clk = clocks.stop()
+
+    # the all-FP64 path, and the accuracy of the mixed path against it on the
+    # same field: relative |R_mixed - R_fp64| / |R_fp64|
+    res_d, rel_dR = None, None
+    if not args.no_fp64:
+        fp64 = mlq.MaxLq(n, q, 1.0, precision="fp64", device=dev, optim_tol=0.0)
+        res_d = run_path(fp64, u0, K, W, dist)
+        fp64.state_load(u0)
+        R_d0, _ = fp64.state_R()
+        mixed.state_load(u0)
+        R_m0, _ = mixed.state_R()
+        rel_dR = abs(R_m0[0] - R_d0[0]) / abs(R_d0[0])
+        fp64.close()
+
+    # e2e: each step copies u host->device, iterates once, copies u back
+    e2e = None
+    if not args.no_e2e:
+        uh = np.ascontiguousarray(u0.copy())
+        mixed.state_load(uh)
+        for _ in range(min(W, 1)):
+            mixed.state_step(uh)
+        dist.barrier()
+        device_sync()
+        t0 = time.perf_counter()
+        ke = 0
+        for _ in range(K):
+            st, _ = mixed.state_step(uh)
+            ke += 1
+            if st != 0:
+                break
+        device_sync()
+        te = dist.max(time.perf_counter() - t0)
+        e2e = {"value": dist.world * ke / te, "unit": "iters/s", "h2d_bytes_per_step": int(uh.nbytes),
+               "d2h_bytes_per_step": int(uh.nbytes)}
+
+    # whole-job throughput: all ranks' iterations over the slowest rank's device time
+    t_m = dist.max(res_m["device_s"])
+    value = dist.world * res_m["iters"] / t_m
+    fp64_value = (dist.world * res_d["iters"] / dist.max(res_d["device_s"])) if res_d else None
+
+    # roofline of the dominant kernel (live CUDA-event timing of the timed region)
+    prof = res_m["prof"]
+    top = max(prof.items(), key=lambda kv: kv[1]["ms"]) if prof else (None, None)
+    traffic = load_traffic()
+    roof = None
+    if top[0]:
+        name, st = top
+        achieved = st["bytes"] / (st["ms"] * 1e-3) / 1e9
+        per_launch_bytes = st["bytes"] / max(st["launches"], 1)
+        tr = traffic.get(name)
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (tr["dram_bytes_per_alg_byte"] * per_launch_bytes) if tr else None,
+                "kernel": name, "peak_kind": peak_kind,
+                "share": st["ms"] / sum(v["ms"] for v in prof.values()),
+                "alg_bytes_per_launch": per_launch_bytes}
+
+    n_evals = [r["n_evals"] for r in res_m["records"]]
+    cpu = None
+    if dist.rank == 0 and not args.no_cpu:
+        workers = os.cpu_count() or 1
+        ne = float(np.mean(n_evals)) if n_evals else REF_TRIALS_PER_ITER
+        t_T = cpu_reference_sample(n, q, ne, workers)
+        it_s = t_T * (REF_T_PER_ITER + REF_T_PER_TRIAL * ne)
+        cpu = {"value": 1.0 / it_s, "unit": "iters/s", "cores": workers, "kind": "port",
+               "sample": (f"one reference-order dealias_scalar round trip (2 c2c {n}^3 FFTs, scipy pocketfft, "
+                          f"{workers} threads), scaled by the reference's {REF_T_PER_ITER} + {REF_T_PER_TRIAL} x "
+                          f"{ne:.1f} transforms per CG iteration")}
+
+    per_kernel = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
+                      "GB/s": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in prof.items()}
+    if dist.rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": dist.world, "steps": K, "warmup": W,
+            "ms_per_step": 1000.0 * t_m / max(res_m["iters"], 1), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
+            "config": {"workload": f"maxdLqdt CG iteration, N={n}^3, q={q:g}, B=1, seeded spectrum "
+                                   f"|j|^-2 exp(-(|j|/{k0:g})^2), one independent replica per GPU",
+                       "n": n, "q": q, "precision": "mixed: FP32 fields and FFTs, FP64 state/reductions/control",
+                       "fp64_iters_per_s": fp64_value,
+                       "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
+                       "rel_dR_mixed_vs_fp64": rel_dR,
+                       "line_search_trials_per_iter": float(np.mean(n_evals)) if n_evals else None,
+                       "l2": "working set (GBs) far above the 126 MB L2; no flush needed",
+                       "parallelism": f"replicas x{dist.world}"},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": res_m["launches"],
+            "clocks": clk, "wall_s_timed": res_m["wall_s"], "per_kernel": per_kernel,
+        }
+        print(json.dumps(line), flush=True)
+    mixed.close()
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -157,6 +157,18 @@ int mlq_state_store(mlq_ctx* ctx, double* u);
 int mlq_state_iterate(mlq_ctx* ctx, int n_iter, mlq_iter_cb cb, void* user, int* iterations);
 /* Resident-state R(u) parts and ||u||_q. */
 int mlq_state_R(mlq_ctx* ctx, double out[3], double* lq_norm);
+/* One CG iteration on u in host memory: u (reference layout) replaces the
+ * resident field, the CG memory of earlier steps is kept, one iteration runs
+ * and the updated u is copied back.  The first step performs the pre-loop
+ * steps like mlq_state_iterate. */
+int mlq_state_step(mlq_ctx* ctx, double* u, mlq_iter_cb cb, void* user);
+
+/* ---- measurement ----------------------------------------------------------- */
+/* Per-kernel CUDA-event timing on the context's stream (off by default). */
+int mlq_profile_enable(mlq_ctx* ctx, int on);
+/* JSON object {kernel: [launches, total_ms, algorithmic_bytes]} of the launches
+ * since the last reset; resets when reset != 0.  Returns the length needed. */
+int mlq_profile_report(mlq_ctx* ctx, char* buf, int len, int reset);
 
 /* ---- synthetic inputs ------------------------------------------------------ */
 /* Seeded divergence-free, 2/3-dealiased field with amplitude

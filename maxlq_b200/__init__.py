@@ -322,6 +322,29 @@ class MaxLq:
         self._check(self._lib.mlq_state_R(self._ctx, dptr(out), C.byref(nrm)), "state_R")
         return out, nrm.value
 
+    def state_step(self, u, callback=None):
+        """One CG iteration on a host field (H2D, iterate, D2H); u updated in place."""
+        if not (isinstance(u, np.ndarray) and u.dtype == np.float64 and u.flags.c_contiguous
+                and u.shape == (3, self.n, self.n, self.n)):
+            raise ValueError("state_step needs a C-contiguous float64 (3,N,N,N) array")
+        records, cb = self._runner(callback)
+        st = self._lib.mlq_state_step(self._ctx, dptr(u), cb, None)
+        if st not in (MLQ_OK,) + _LOOP_STOPS:
+            self._check(st, "state_step")
+        return st, records
+
+    def profile(self, on: bool = True):
+        self._check(self._lib.mlq_profile_enable(self._ctx, 1 if on else 0), "profile_enable")
+
+    def profile_report(self, reset: bool = True) -> dict:
+        import json
+        need = self._lib.mlq_profile_report(self._ctx, None, 0, 0)
+        if need < 0:
+            self._check(-need, "profile_report")
+        buf = C.create_string_buffer(need + 16)
+        self._lib.mlq_profile_report(self._ctx, buf, need + 16, 1 if reset else 0)
+        return {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in json.loads(buf.value.decode()).items()}
+
     def seed_field(self, seed: int = 0, slope: float = 2.0, k0: float = 4.0):
         u = np.empty((3, self.n, self.n, self.n))
         self._check(self._lib.mlq_seed_field(self._ctx, seed, slope, k0, dptr(u)), "seed_field")

@@ -286,6 +286,31 @@ int mlq_state_R(mlq_ctx* c, double out[3], double* lq_norm) {
     return guard(c, [&] { c->solver->state_R(out, lq_norm); });
 }
 
+int mlq_state_step(mlq_ctx* c, double* u, mlq_iter_cb cb, void* user) {
+    int status = MLQ_OK;
+    int st = guard(c, [&] { status = c->solver->state_step(u, cb, user); });
+    return st != MLQ_OK ? st : status;
+}
+
+int mlq_profile_enable(mlq_ctx* c, int on) {
+    return guard(c, [&] {
+        c->solver->eng().prof_flush();
+        c->solver->eng().prof_on = on != 0;
+    });
+}
+
+int mlq_profile_report(mlq_ctx* c, char* buf, int len, int reset) {
+    if (!c) return -MLQ_ERR_BADARG;
+    std::string r;
+    int st = guard(c, [&] { r = c->solver->eng().prof_report(reset != 0); });
+    if (st != MLQ_OK) return -st;
+    if (buf && len > 0) {
+        std::strncpy(buf, r.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)r.size() + 1;
+}
+
 int mlq_seed_field(mlq_ctx* c, unsigned long long seed, double slope, double k0, double* u) {
     return guard(c, [&] { c->solver->seed_field(seed, slope, k0, u); });
 }

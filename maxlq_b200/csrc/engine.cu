@@ -153,9 +153,10 @@ void EngineBase::ensure_partials(long cnt) {
 }
 
 void EngineBase::finalize(int nblocks, int nr, double scale, int dst, bool accumulate) {
+    cudaEvent_t ev = prof_mark();
     finalize_partials_kernel<<<1, RED_THREADS, 0, stream>>>(d_partials, nblocks, nr, scale, d_results, dst,
                                                            accumulate ? 1 : 0);
-    launched();
+    launched("finalize", 8.0 * nblocks * nr, ev);
 }
 
 void EngineBase::fetch_results() {
@@ -163,23 +164,88 @@ void EngineBase::fetch_results() {
     MLQ_CUDA(cudaStreamSynchronize(stream));
 }
 
+cudaEvent_t EngineBase::ev_take() {
+    if (!evpool_.empty()) {
+        cudaEvent_t e = evpool_.back();
+        evpool_.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    MLQ_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+cudaEvent_t EngineBase::prof_mark() {
+    if (!prof_on) return nullptr;
+    cudaEvent_t e = ev_take();
+    MLQ_CUDA(cudaEventRecord(e, stream));
+    return e;
+}
+
+void EngineBase::launched(const char* name, double alg_bytes, cudaEvent_t a) {
+    launches += 1;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);
+    if (a) {
+        cudaEvent_t b = ev_take();
+        MLQ_CUDA(cudaEventRecord(b, stream));
+        pend_.push_back(Pend{name ? name : "other", a, b, alg_bytes});
+        if (pend_.size() > 4096) prof_flush();
+    }
+}
+
+void EngineBase::prof_flush() {
+    if (pend_.empty()) return;
+    MLQ_CUDA(cudaStreamSynchronize(stream));
+    for (const Pend& p : pend_) {
+        float ms = 0.f;
+        MLQ_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+        KStat& k = prof[p.name];
+        k.n += 1;
+        k.ms += ms;
+        k.bytes += p.bytes;
+        evpool_.push_back(p.a);
+        evpool_.push_back(p.b);
+    }
+    pend_.clear();
+}
+
+std::string EngineBase::prof_report(bool reset) {
+    prof_flush();
+    std::string s = "{";
+    bool first = true;
+    for (const auto& kv : prof) {
+        char b[256];
+        snprintf(b, sizeof(b), "%s\"%s\": [%lld, %.6f, %.1f]", first ? "" : ", ", kv.first.c_str(), kv.second.n,
+                 kv.second.ms, kv.second.bytes);
+        s += b;
+        first = false;
+    }
+    s += "}";
+    if (reset) prof.clear();
+    return s;
+}
+
 void EngineBase::lincomb(double2* out, double a, const double2* x, double b, const double2* y, double c,
                          const double2* z) {
     SpecGeom g = geom(b2);
+    cudaEvent_t ev = prof_mark();
     spec_lincomb_kernel<<<grid_for(3 * g.ncomp, 256), 256, 0, stream>>>(g, out, a, x, b, y, c, z);
-    launched();
+    launched("spec_lincomb", 48.0 * g.ncomp * (2 + (y ? 1 : 0) + (z ? 1 : 0)), ev);
 }
 
 void EngineBase::hilbert(double2* f, double order) {
     SpecGeom g = geom(b2);
+    cudaEvent_t ev = prof_mark();
     spec_hilbert_kernel<<<grid_for(g.ncomp, 256), 256, 0, stream>>>(g, f, P.lambda1, 2.0 * order);
-    launched();
+    launched("spec_hilbert", 96.0 * g.ncomp, ev);
 }
 
 void EngineBase::leray(double2* f) {
     SpecGeom g = geom(b2);
+    cudaEvent_t ev = prof_mark();
     spec_leray_kernel<<<grid_for(g.ncomp, 256), 256, 0, stream>>>(g, f);
-    launched();
+    launched("spec_leray", 96.0 * g.ncomp, ev);
 }
 
 void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
@@ -191,8 +257,16 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
     a.order = 1.5 - 1.0 / P.q;  // (3/2)-(1/q), function_ops.f90:3467
     a.partials = d_partials;
     const int grid = grid_for(a.g.ncomp, RED_THREADS, 148 * 4);
+    cudaEvent_t ev = prof_mark();
     spec_dot_kernel<<<grid, RED_THREADS, 0, stream>>>(a);
-    launched();
+    {
+        std::set<const void*> uniq;
+        for (int i = 0; i < np; ++i) {
+            uniq.insert(pairs[i].a);
+            if (pairs[i].kind != 2) uniq.insert(pairs[i].b);
+        }
+        launched("spec_dot", 48.0 * a.g.ncomp * uniq.size(), ev);
+    }
     finalize(grid, 6, 1.0, 200);
     fetch_results();
     for (int i = 0; i < np; ++i) out[i] = h_results[200 + i];
@@ -312,8 +386,9 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
     xa.partials = d_partials;
     const size_t xsm = (size_t)2 * NOUT * xa.lx * h * sizeof(cpx<T>);
     allow_smem(xfwd_kernel<T, F>);
+    cudaEvent_t ev = prof_mark();
     xfwd_kernel<T, F><<<xgrid, 256, xsm, stream>>>(xa, f);
-    launched();
+    launched("x_fwd", (double)n3 * sizeof(T) * F::NIN + (double)n * n * b.nx * sizeof(cpx<T>) * NOUT, ev);
     if (F::NRED > 0 && fred_dst >= 0) finalize(xgrid, F::NRED, 1.0 / (double)n3, fred_dst);
     if (NOUT == 0) return;
     // y forward
@@ -332,8 +407,9 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
     const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
     allow_smem(ypass_kernel<-1, T>);
     dim3 yg((b.nx + tx - 1) / tx, n, NOUT);
+    ev = prof_mark();
     ypass_kernel<-1, T><<<yg, 256, ysm, stream>>>(ya);
-    launched();
+    launched("y_fwd", (double)NOUT * (n * (double)n * b.nx + n * (double)b.nb * b.nx) * sizeof(cpx<T>), ev);
     // z stage
     ZFwdArgs<T> za;
     za.n = n;
@@ -369,8 +445,22 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
     ensure_partials(zblocks * MAX_RED);
     za.partials = d_partials;
     allow_smem(zfwd_kernel<T>);
+    double zbytes = 0;
+    {
+        const double ys_b = (double)n * b.nb * b.nx * sizeof(cpx<T>);
+        const double sp_elems = (double)b.nb * b.nb * b.nx;
+        for (int o = 0; o < NOUT; ++o) {
+            const FwdOut& fo = outs[o];
+            zbytes += ys_b;
+            if (fo.spec) zbytes += sp_elems * (fo.spec_f64 ? 16 : 8);
+            if (fo.phys_out >= 0) zbytes += ys_b;
+            if (fo.add) zbytes += sp_elems * (fo.add_f64 ? 16 : 8);
+            if (fo.red_with) zbytes += sp_elems * (fo.red_with_f64 ? 16 : 8);
+        }
+    }
+    ev = prof_mark();
     zfwd_kernel<T><<<zg, 256, ysm, stream>>>(za);
-    launched();
+    launched(any_rt ? "z_roundtrip" : "z_fwd", zbytes, ev);
     if (red_dst >= 0) finalize((int)zblocks, MAX_RED, 1.0, red_dst);
     if (any_rt) {
         std::vector<cpx<T>*> ys;
@@ -408,8 +498,9 @@ void Engine<T>::yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const 
     const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
     allow_smem(ypass_kernel<+1, T>);
     dim3 yg((b.nx + tx - 1) / tx, n, k);
+    cudaEvent_t ev = prof_mark();
     ypass_kernel<+1, T><<<yg, 256, ysm, stream>>>(ya);
-    launched();
+    launched("y_inv", (double)k * (n * (double)b.nb * b.nx + n * (double)n * b.nx) * sizeof(cpx<T>), ev);
     // x inverse
     XInvArgs<T> xa;
     xa.n = n;
@@ -427,8 +518,9 @@ void Engine<T>::yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const 
     xa.tw = d_tw;
     allow_smem(xinv_kernel<T>);
     dim3 xg((unsigned)(((long)n * n) / lx), k);
+    ev = prof_mark();
     xinv_kernel<T><<<xg, 256, per * lx, stream>>>(xa);
-    launched();
+    launched("x_inv", (double)k * ((double)n * n * b.nx * sizeof(cpx<T>) + (double)n3 * sizeof(T)), ev);
 }
 
 template <typename T>
@@ -459,8 +551,15 @@ void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
         za.tw = d_tw;
         allow_smem(zinv_kernel<T>);
         dim3 zg((b.nx + tx - 1) / tx, b.nb, k);
+        double zb = 0;
+        for (int i = 0; i < k; ++i) {
+            const InvOut& io = outs[g0 + i];
+            zb += (double)n * b.nb * b.nx * sizeof(cpx<T>);
+            for (int s2 = 0; s2 < io.nsrc; ++s2) zb += (double)b.nb * b.nb * b.nx * (io.src[s2].f64 ? 16 : 8);
+        }
+        cudaEvent_t ev = prof_mark();
         zinv_kernel<T><<<zg, 256, zsm, stream>>>(za);
-        launched();
+        launched("z_inv", zb, ev);
         yx_inverse(b, ys, po);
     }
 }
@@ -475,8 +574,9 @@ void Engine<T>::pointwise(const F& f, const std::vector<const T*>& in, const std
     const int grid = grid_for(n3, RED_THREADS, 148 * 8);
     ensure_partials((long)grid * std::max(F::NRED, 1));
     a.partials = d_partials;
+    cudaEvent_t ev = prof_mark();
     pointwise_kernel<T, F><<<grid, RED_THREADS, 0, stream>>>(a, f);
-    launched();
+    launched("pointwise", (double)n3 * sizeof(T) * (F::NIN + F::NOUT), ev);
     if (F::NRED > 0 && fred_dst >= 0) finalize(grid, F::NRED, 1.0 / (double)n3, fred_dst);
 }
 
@@ -676,8 +776,9 @@ static void sdots(Engine<T>& e, const std::vector<std::pair<const cpx<T>*, const
     const int grid = grid_for(a.g.ncomp, RED_THREADS, 148 * 4);
     e.ensure_partials((long)grid * 6);
     a.partials = e.d_partials;
+    cudaEvent_t ev = e.prof_mark();
     spec_sdot_kernel<T><<<grid, RED_THREADS, 0, e.stream>>>(a);
-    e.launched();
+    e.launched("spec_sdot", 2.0 * a.np * a.g.ncomp * sizeof(cpx<T>), ev);
     e.finalize(grid, 6, 1.0, dst);
 }
 
@@ -1098,25 +1199,27 @@ void Engine<T>::store_scalar_phys(int src, double* host) {
         for (long i = 0; i < n3; ++i) host[i] = (double)st[i];
 }
 
+// Forward transform of a host vector field into band-b2 state spectra.  The
+// energy the band drops is measured directly, as ||u - F^-1 P2 F u||^2.
 template <typename T>
 double Engine<T>::load_vec(const double* host, double2* spec) {
     const long nc = spec_ncomp();
-    double tot = 0, inb = 0;
     for (int c = 0; c < 3; ++c) {
         load_scalar_phys(host + c * n3, PIO);
-        pointwise(FSqRed{}, {phys(PIO)}, {}, 30 + c);
         FwdOut o;
         o.spec = spec + c * nc;
         o.spec_f64 = 1;
-        o.red_self = 0;
-        fwd(b2, FCopy{}, {phys(PIO)}, {o}, 40 + 8 * c);
+        o.phys_out = PIO2;
+        fwd(b2, FCopy{}, {phys(PIO)}, {o});
+        pointwise(FDiffSq{}, {phys(PIO), phys(PIO2)}, {}, 30 + 2 * c);
     }
     fetch_results();
+    double out = 0, tot = 0;
     for (int c = 0; c < 3; ++c) {
-        tot += h_results[30 + c];
-        inb += h_results[40 + 8 * c];
+        out += h_results[30 + 2 * c];
+        tot += h_results[31 + 2 * c];
     }
-    return tot > 0 ? (tot - inb) / tot : 0.0;
+    return tot > 0 ? out / tot : 0.0;
 }
 
 template <typename T>

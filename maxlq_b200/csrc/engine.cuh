@@ -79,12 +79,32 @@ class EngineBase {
 
     void finalize(int nblocks, int nr, double scale, int dst, bool accumulate = false);
     void ensure_partials(long n);
-    // count a launch and surface launch-configuration errors immediately
-    void launched(int k = 1) {
-        launches += k;
-        const cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) throw CudaError(std::string("kernel launch: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);
-    }
+    // Count a launch and surface launch-configuration errors immediately.
+    // With profiling on, `a` is the event recorded before the launch; the
+    // launch's device time and its algorithmic bytes (compulsory reads +
+    // writes) are accumulated per kernel name.
+    void launched(const char* name = nullptr, double alg_bytes = 0.0, cudaEvent_t a = nullptr);
+    cudaEvent_t prof_mark();
+    bool prof_on = false;
+    struct KStat {
+        long long n = 0;
+        double ms = 0.0, bytes = 0.0;
+    };
+    std::map<std::string, KStat> prof;
+    void prof_flush();
+    std::string prof_report(bool reset);
+
+   private:
+    struct Pend {
+        const char* name;
+        cudaEvent_t a, b;
+        double bytes;
+    };
+    std::vector<Pend> pend_;
+    std::vector<cudaEvent_t> evpool_;
+    cudaEvent_t ev_take();
+
+   public:
 
     std::vector<void*> allocs_;
 };

@@ -277,6 +277,17 @@ struct FC3 {
     }
 };
 
+// sum (a-b)^2 and sum a^2: energy of a field outside its band projection
+struct FDiffSq {
+    static constexpr int NIN = 2, NOUT = 0, NRED = 2;
+    template <typename T>
+    __device__ void operator()(const T* in, T*, double* acc) const {
+        const double d = (double)in[0] - (double)in[1];
+        acc[0] += d * d;
+        acc[1] += (double)in[0] * (double)in[0];
+    }
+};
+
 // sum of squares of three stored fields (energy check of a loaded field)
 struct FEnergy3 {
     static constexpr int NIN = 3, NOUT = 3, NRED = 1;

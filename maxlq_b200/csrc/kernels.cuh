@@ -177,7 +177,11 @@ __global__ void __launch_bounds__(256) xinv_kernel(XInvArgs<T> a) {
     const cpx<T>* src = a.in[arr];
     for (int p = threadIdx.x; p < lx * (h + 1); p += blockDim.x) {
         const int l = p / (h + 1), k = p - l * (h + 1);
-        X[(long)k * lx + l] = k < a.nx_in ? src[(line0 + l) * a.nx_in + k] : czero<T>();
+        cpx<T> v = k < a.nx_in ? src[(line0 + l) * a.nx_in + k] : czero<T>();
+        // c2c + REAL() (function_ops.f90, e.g. 3186) keeps the Hermitian part of
+        // a spectrum: on the kx = 0 and kx = n/2 columns that is the real part
+        if (k == 0 || k == h) v.y = T(0);
+        X[(long)k * lx + l] = v;
     }
     __syncthreads();
     const double2* twn = reinterpret_cast<const double2*>(a.tw + a.tw_n_off);

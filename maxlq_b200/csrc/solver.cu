@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 namespace mlq {
@@ -13,7 +14,12 @@ void seed_spectrum_host(int n, unsigned long long seed, double slope, double k0,
 
 namespace {
 const double TAU_MAX = 1.0e2;  // global_variables.f90:29
+std::string fmt_e(double v) {
+    char b[32];
+    snprintf(b, sizeof(b), "%.3e", v);
+    return b;
 }
+}  // namespace
 
 template <typename T>
 class Solver : public SolverBase {
@@ -28,6 +34,18 @@ class Solver : public SolverBase {
     double avg_imp = 1.0;
     int while_flag = 0;
     std::map<double, Trial> trials;
+
+    // Host transfers of FP64 state always go through an FP64 pipeline, so a
+    // stored field is the exact field of the FP64 state spectra in both modes.
+    std::unique_ptr<Engine<double>> io64_;
+    Engine<double>& io() {
+        if constexpr (std::is_same<T, double>::value) {
+            return e;
+        } else {
+            if (!io64_) io64_.reset(new Engine<double>(e.P));
+            return *io64_;
+        }
+    }
 
     explicit Solver(const mlq_params& p) : e(p) {
         u = e.alloc_state();
@@ -49,11 +67,12 @@ class Solver : public SolverBase {
 
     // load a host vector field, refusing fields with modes outside the band
     void load(const double* host, double2* spec) {
-        const double rel = e.load_vec(host, spec);
-        const double tol = sizeof(T) == 8 ? 1e-20 : 1e-10;
+        MLQ_CUDA(cudaStreamSynchronize(e.stream));
+        const double rel = io().load_vec(host, spec);
+        const double tol = 1e-24;  // relative energy; FP64 FFT round-trip noise is ~1e-32
         if (rel > tol)
             throw CudaError("input field is not band-limited to the 2/3 dealiasing cube (relative energy outside: " +
-                                std::to_string(rel) + ")",
+                                fmt_e(rel) + ")",
                             MLQ_ERR_NOT_BANDLIMITED);
     }
 
@@ -231,8 +250,25 @@ class Solver : public SolverBase {
     }
 
     // one iteration of optimization.f90:136-446; returns status
+    cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+    // device time of one iteration: CUDA events on the engine's stream
+    void iter_clock_start() {
+        if (!ev0_) {
+            MLQ_CUDA(cudaEventCreate(&ev0_));
+            MLQ_CUDA(cudaEventCreate(&ev1_));
+        }
+        MLQ_CUDA(cudaEventRecord(ev0_, e.stream));
+    }
+    double iter_clock_stop() {
+        MLQ_CUDA(cudaEventRecord(ev1_, e.stream));
+        MLQ_CUDA(cudaEventSynchronize(ev1_));
+        float ms = 0.f;
+        MLQ_CUDA(cudaEventElapsedTime(&ms, ev0_, ev1_));
+        return ms * 1e-3;
+    }
+
     int one_iteration(mlq_iter_info& info) {
-        auto t0 = std::chrono::steady_clock::now();
+        iter_clock_start();
         std::memset(&info, 0, sizeof(info));
         iter++;
         info.iter = iter;
@@ -309,7 +345,7 @@ class Solver : public SolverBase {
             info.n_evals = evals_this_iter;
             info.status = mflag == 1 ? MLQ_ERR_MNBRAK_UPHILL : MLQ_ERR_MNBRAK_ITMAX;
             while_flag = 1;
-            info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            info.seconds = iter_clock_stop();
             return info.status;
         }
         double fx = 0;
@@ -355,7 +391,7 @@ class Solver : public SolverBase {
         if (deltaJ < -MACH_EPSILON) {  // 351-366
             while_flag = 1;
             info.status = MLQ_ERR_J_DECREASED;
-            info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            info.seconds = iter_clock_stop();
             return info.status;
         }
         info.u_norm_q = cs * std::pow(tr.lqq, 1.0 / qq);  // ||u||_q after the retraction (421)
@@ -372,7 +408,7 @@ class Solver : public SolverBase {
         for (double r : roll) ssum += r;
         avg_imp = ssum / (double)(iter - start_iter);
         info.status = status;
-        info.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        info.seconds = iter_clock_stop();
         return status;
     }
 
@@ -415,7 +451,7 @@ class Solver : public SolverBase {
     void grad_l2(const double* uh, double* v) override {
         load(uh, tmp);
         e.grad_l2(tmp, d1, c, nullptr);
-        e.store_vec(d1, v);
+        store(d1, v);
         started = false;
     }
     double lq_norm(const double* uh) override {
@@ -434,7 +470,7 @@ class Solver : public SolverBase {
         e.grad_l2(tmp, d1, c, &lqq);
         const double nrm = std::pow(lqq, 1.0 / q());
         e.lincomb(c, std::pow(nrm, 1.0 - q()), c);
-        e.store_vec(c, out);
+        store(c, out);
         started = false;
     }
     void vector_transport(const double* uh, double qv, double Bv, const double* eta, const double* xi,
@@ -449,18 +485,18 @@ class Solver : public SolverBase {
         const double ln = std::pow(lqq, 1.0 / qv);
         const double f = std::pow(ln, -qv) * ir;
         e.lincomb(c, Bv / ln, gu1, -Bv / ln * f, tmp, -Bv / ln * f, d1);
-        e.store_vec(c, out);
+        store(c, out);
         started = false;
     }
     void hilbert_host(double* g, double order) override {
         load(g, tmp);
         e.hilbert(tmp, order);
-        e.store_vec(tmp, g);
+        store(tmp, g);
     }
     void divavg_host(double* g) override {
         load(g, tmp);
         e.leray(tmp);
-        e.store_vec(tmp, g);
+        store(tmp, g);
     }
     double inner_host(const double* f, const double* g, int type) override {
         load(f, tmp);
@@ -503,7 +539,18 @@ class Solver : public SolverBase {
         load(uh, u);
         started = false;
     }
-    void state_store(double* uh) override { e.store_vec(u, uh); }
+    void store(const double2* spec, double* host) {
+        MLQ_CUDA(cudaStreamSynchronize(e.stream));
+        io().store_vec(spec, host);
+    }
+    void state_store(double* uh) override { store(u, uh); }
+    int state_step(double* uh, mlq_iter_cb cb, void* user) override {
+        load(uh, u);  // CG memory (gu0, vtg0, vtd0, tau0, J0, rolling average) kept
+        int it = 0;
+        const int st = state_iterate(1, cb, user, &it);
+        store(u, uh);
+        return st;
+    }
     void state_R(double out[3], double* lqn) override {
         double lqq;
         e.R_eval(u, nullptr, 0.0, out, &lqq);
@@ -513,8 +560,7 @@ class Solver : public SolverBase {
         std::vector<double> h(3 * nc() * 2);
         seed_spectrum_host(e.n, seed, slope, k0, e.b2, h.data());
         MLQ_CUDA(cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-        MLQ_CUDA(cudaStreamSynchronize(e.stream));
-        e.store_vec(tmp, out);
+        store(tmp, out);
     }
     void set_B(double Bv) override {
         e.P.B = Bv;

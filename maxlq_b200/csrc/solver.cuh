@@ -47,6 +47,7 @@ class SolverBase {
     virtual void state_store(double* u) = 0;
     virtual int state_iterate(int n_iter, mlq_iter_cb cb, void* user, int* iters) = 0;
     virtual void state_R(double out[3], double* lqn) = 0;
+    virtual int state_step(double* u, mlq_iter_cb cb, void* user) = 0;
     virtual void seed_field(unsigned long long seed, double slope, double k0, double* u) = 0;
     virtual void set_B(double B) = 0;
     virtual void set_start_iter(int s) = 0;

@@ -18,8 +18,10 @@ MACH_EPSILON = 2.0e-16
 
 
 class RefNumpy:
-    def __init__(self, n, q, B=1.0, visc=1.0, lambda1=0.1, use_e_u=None, dealias_e_u=True, to_dealias=True):
+    def __init__(self, n, q, B=1.0, visc=1.0, lambda1=0.1, use_e_u=None, dealias_e_u=True, to_dealias=True,
+                 workers=None):
         self.n, self.q, self.B = n, float(q), float(B)
+        self.workers = workers  # scipy.fft threads (None: numpy.fft, single thread)
         self.visc, self.lambda1 = visc, lambda1
         self.use_e_u = (q < 4.0 - MACH_EPSILON) if use_e_u is None else use_e_u
         self.dealias_e_u, self.to_dealias = dealias_e_u, to_dealias
@@ -36,9 +38,15 @@ class RefNumpy:
 
     # fftfwd / fftbwd (fftwfunction.f90:62-113)
     def fwd(self, f):
+        if self.workers:
+            import scipy.fft
+            return scipy.fft.fftn(f.astype(np.complex128), workers=self.workers, overwrite_x=True)
         return np.fft.fftn(f.astype(np.complex128))
 
     def bwd(self, fh):
+        if self.workers:
+            import scipy.fft
+            return scipy.fft.ifftn(fh, workers=self.workers)
         return np.fft.ifftn(fh)  # ifftn already divides by N^3
 
     def dealias(self, g, order):  # FO 3332-3398

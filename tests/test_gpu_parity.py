@@ -197,3 +197,20 @@ def test_resident_state_iterations_continue_cg_memory():
     assert [r["J1"] for r in r1 + r2] == pytest.approx([r["J1"] for r in r3], rel=1e-12)
     a.close()
     b.close()
+
+
+def test_mixed_store_roundtrips_into_fp64_context():
+    """Host transfers go through FP64 in both modes: a field stored by a
+    mixed-precision context loads into an FP64 one."""
+    n, q = 32, 4.0
+    m = mlq.MaxLq(n, q, 1.0, precision="mixed")
+    d = mlq.MaxLq(n, q, 1.0)
+    u = m.seed_field(4, 2.0, 2.0)
+    assert rel(u, seed_field(n, 4, 2.0, 2.0)) < 1e-13
+    m.state_load(u)
+    m.state_iterate(1)
+    v = m.state_store()
+    d.state_load(v)
+    assert rel(d.state_store(), v) < 1e-13
+    m.close()
+    d.close()
