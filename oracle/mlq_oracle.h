@@ -11,6 +11,11 @@
  * function_ops.f90 does, with FFTW's conventions (forward e^{-i}, unnormalised;
  * backward e^{+i} then /N^3, fftwfunction.f90:62-113).
  *
+ * Parity unpinned: the reference ships no golden vectors and cannot be built
+ * here (no Fortran compiler, MPI, FFTW or netCDF).  The restatement is checked
+ * against analytic answers, an independent numpy transcription
+ * (ref_numpy.py) and the reference's own kappa (Taylor) test instead.
+ *
  * Field layout is the reference's: Fortran (n1,n2,n3[,3]) column-major, x
  * fastest, i.e. C index [c][z][y][x].  One rank holds the whole box
  * (local_N = N, local_k_offset = 0).

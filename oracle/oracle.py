@@ -4,6 +4,9 @@ TEST INFRASTRUCTURE ONLY: tests/, __graft_entry__.smoke() and bench.py's
 CPU-baseline / reference arm import this module as the checker.  The product
 package (maxlq_b200) never imports it.
 
+Parity unpinned: no golden vectors exist in the reference and its Fortran
+build is unavailable here; see mlq_oracle.h for how the oracle is checked.
+
 Fields are numpy float64 arrays shaped (3, N, N, N) indexed [c, z, y, x]:
 byte-for-byte the reference's Fortran array Uvec(1:n1, 1:n2, 1:n3, 1:3)
 (column-major, x fastest).  Scalars are (N, N, N).

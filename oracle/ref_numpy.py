@@ -7,6 +7,9 @@ golden fixtures under tests/golden/.  Same conventions as oracle.py: fields
 are float64 arrays [c, z, y, x]; reference-order semantics (each operator is
 a c2c FFT round trip followed by REAL()).
 
+Parity unpinned (the reference's own outputs are unavailable); agreement with
+the C++ oracle is what the two transcriptions establish.
+
 Citations are to the reference project's function_ops.f90 (FO) and
 optimization.f90 (OPT).
 """
