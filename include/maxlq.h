@@ -182,6 +182,23 @@ int mlq_seed_field(mlq_ctx* ctx, unsigned long long seed, double slope, double k
 int mlq_seed_spectrum(int n, unsigned long long seed, double slope, double k0, double* spec, int* cut);
 int mlq_band_cut(int n, double order); /* largest |j| kept by a dealias of that order */
 
+/* ---- allocation-free variant ----------------------------------------------- */
+/* No counterpart in the reference.  dealias_scalar for callers that cannot
+ * allocate device memory -- a host program whose device memory is owned by
+ * another runtime, or code that must not trigger an allocation (which can
+ * synchronise the device) -- so it needs no context: g is the host scalar
+ * field (n,n,n), dealiased in place exactly as mlq_dealias_scalar does.  All
+ * device memory it uses is one static array of about 6.4 MiB that every GPU
+ * loading this library holds until exit, which limits n to
+ * MLQ_NOALLOC_MAX_N; larger n is rejected with MLQ_ERR_BADARG (message on
+ * stderr).  The first call on a device looks up the array's device address,
+ * so make that call before any stream capture.  Calls run on the legacy
+ * default stream and share the array: calls that overlap on the GPU (from
+ * several host threads) race.  Every call overwrites all of the array it
+ * reads, so nothing carries over from the previous call. */
+#define MLQ_NOALLOC_MAX_N 64
+int mlq_dealias_scalar_noalloc(double* g, int n, double order);
+
 #ifdef __cplusplus
 }
 #endif

@@ -116,6 +116,7 @@ SIGNATURES = {
     "mlq_seed_field": (C.c_int, [_VP, C.c_ulonglong, C.c_double, C.c_double, _DP]),
     "mlq_seed_spectrum": (C.c_int, [C.c_int, C.c_ulonglong, C.c_double, C.c_double, _DP, C.POINTER(C.c_int)]),
     "mlq_band_cut": (C.c_int, [C.c_int, C.c_double]),
+    "mlq_dealias_scalar_noalloc": (C.c_int, [_DP, C.c_int, C.c_double]),
 }
 
 _lib = None
