@@ -18,7 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmaxlq_b200.so")
 SOURCES = ["engine.cu", "solver.cu", "capi.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "engine.cuh", "solver.cuh"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "regfft.cuh", "engine.cuh", "solver.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

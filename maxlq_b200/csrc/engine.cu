@@ -301,6 +301,235 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
     widen(P.q - 2.0);
     widen(P.q / 2.0);
     if (!use_e_u) widen(P.q - 4.0);
+    reg_ok_ = n >= 64 && (n & (n - 1)) == 0;
+    ereg_ = (n > 512 && sizeof(T) == 4) ? 16 : 8;
+    long ntw = 0;
+    for (const auto& kv : tw_off) ntw = std::max<long>(ntw, kv.second + kv.first);
+    if (sizeof(T) == 8) {
+        d_twT_ = reinterpret_cast<cpx<T>*>(d_tw);
+    } else {
+        d_twT_ = (cpx<T>*)dev_alloc(ntw * sizeof(cpx<T>));
+        std::vector<cpx<double>> h(ntw);
+        MLQ_CUDA(cudaMemcpy(h.data(), d_tw, ntw * sizeof(cpx<double>), cudaMemcpyDeviceToHost));
+        std::vector<cpx<T>> hf(ntw);
+        for (long i = 0; i < ntw; ++i) hf[i] = mk<T>((T)h[i].x, (T)h[i].y);
+        MLQ_CUDA(cudaMemcpy(d_twT_, hf.data(), ntw * sizeof(cpx<T>), cudaMemcpyHostToDevice));
+    }
+}
+
+template <typename T>
+RPlan Engine<T>::rplan(int L) const {
+    RPlan p;
+    p.L = L;
+    p.nst = 0;
+    p.tw_off = tw_off.at(L);
+    int m = L;
+    for (int r : {16, 8, 4, 2}) {
+        if (r > ereg_) continue;
+        while (m % r == 0 && m > 1) {
+            p.radix[p.nst++] = r;
+            m /= r;
+        }
+    }
+    if (m != 1) throw CudaError("register FFT needs a power-of-two length", MLQ_ERR_BADARG);
+    return p;
+}
+
+// columns per y/z tile: up to 128-byte rows within a 256-thread block
+template <typename T>
+int Engine<T>::reg_tx() const {
+    const int nT = n / ereg_;
+    int tx = 128 / (int)sizeof(cpx<T>);
+    while (tx > 1 && (tx * nT > 256 || (size_t)n * tx * sizeof(cpx<T>) > 96 * 1024)) tx /= 2;
+    return tx;
+}
+
+// rows per x-stage block: nrows_per_line FFT rows of pitch `pitch` per line
+template <typename T>
+int Engine<T>::reg_lx(int nrows_per_line, size_t pitch) const {
+    const int nT = (n / 2) / ereg_;
+    int lx = 32;
+    while (lx > 1 && (nrows_per_line * lx * nT > 256 || nrows_per_line * lx * pitch * sizeof(cpx<T>) > 96 * 1024 ||
+                      ((long)n * n) % lx != 0))
+        lx /= 2;
+    return lx;
+}
+
+template <typename T>
+template <class F>
+void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b) {
+    const int h = n / 2;
+    const double bytes = (double)n3 * sizeof(T) * F::NIN + (double)n * n * b.nx * sizeof(cpx<T>) * nout;
+    if (reg_ok_) {
+        xa.lx = reg_lx(nout, row_pitch(h));
+        xa.tw_n_off = tw_off.at(n);
+        const int grid = (int)(((long)n * n) / xa.lx);
+        if (F::NRED > 0) ensure_partials((long)grid * F::NRED);
+        xa.partials = d_partials;
+        const size_t sm = (size_t)nout * xa.lx * row_pitch(h) * sizeof(cpx<T>);
+        const int thr = nout * xa.lx * (h / ereg_);
+        cudaEvent_t ev = prof_mark();
+        if (ereg_ == 8) {
+            allow_smem(xfwd_reg_kernel<8, T, F>);
+            xfwd_reg_kernel<8, T, F><<<grid, thr, sm, stream>>>(xa, f, rplan(h), d_twT_);
+        } else {
+            allow_smem(xfwd_reg_kernel<16, T, F>);
+            xfwd_reg_kernel<16, T, F><<<grid, thr, sm, stream>>>(xa, f, rplan(h), d_twT_);
+        }
+        launched("x_fwd", bytes, ev);
+        return;
+    }
+    xa.lx = lx_for(nout);
+    const int xgrid = (int)(((long)n * n) / xa.lx);
+    if (F::NRED > 0) ensure_partials((long)xgrid * F::NRED);
+    xa.partials = d_partials;
+    const size_t xsm = (size_t)2 * nout * xa.lx * h * sizeof(cpx<T>);
+    allow_smem(xfwd_kernel<T, F>);
+    cudaEvent_t ev = prof_mark();
+    xfwd_kernel<T, F><<<xgrid, 256, xsm, stream>>>(xa, f);
+    launched("x_fwd", bytes, ev);
+}
+
+template <typename T>
+void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
+    const double bytes = (double)narr * (n * (double)n * b.nx + n * (double)b.nb * b.nx) * sizeof(cpx<T>);
+    const char* nm = sign < 0 ? "y_fwd" : "y_inv";
+    if (reg_ok_) {
+        const int tx = reg_tx();
+        ya.tx = tx;
+        const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
+        dim3 g((b.nx + tx - 1) / tx, n, narr);
+        const int thr = tx * (n / ereg_);
+        cudaEvent_t ev = prof_mark();
+        if (ereg_ == 8) {
+            if (sign < 0) {
+                allow_smem(ypass_reg_kernel<8, -1, T>);
+                ypass_reg_kernel<8, -1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
+            } else {
+                allow_smem(ypass_reg_kernel<8, +1, T>);
+                ypass_reg_kernel<8, +1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
+            }
+        } else {
+            if (sign < 0) {
+                allow_smem(ypass_reg_kernel<16, -1, T>);
+                ypass_reg_kernel<16, -1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
+            } else {
+                allow_smem(ypass_reg_kernel<16, +1, T>);
+                ypass_reg_kernel<16, +1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
+            }
+        }
+        launched(nm, bytes, ev);
+        return;
+    }
+    const int tx = tx_for();
+    ya.tx = tx;
+    ya.plan = plan(n);
+    ya.tw = d_tw;
+    const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
+    dim3 yg((b.nx + tx - 1) / tx, n, narr);
+    cudaEvent_t ev = prof_mark();
+    if (sign < 0) {
+        allow_smem(ypass_kernel<-1, T>);
+        ypass_kernel<-1, T><<<yg, 256, ysm, stream>>>(ya);
+    } else {
+        allow_smem(ypass_kernel<+1, T>);
+        ypass_kernel<+1, T><<<yg, 256, ysm, stream>>>(ya);
+    }
+    launched(nm, bytes, ev);
+}
+
+template <typename T>
+void Engine<T>::launch_zfwd(ZFwdArgs<T>& za, int narr, const Band& b, bool any_rt, double zbytes) {
+    const int tx = reg_ok_ ? reg_tx() : tx_for();
+    za.tx = tx;
+    dim3 zg((b.nx + tx - 1) / tx, b.nb, narr);
+    const long zblocks = (long)zg.x * zg.y * zg.z;
+    ensure_partials(zblocks * MAX_RED);
+    za.partials = d_partials;
+    if (reg_ok_) {
+        const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
+        const int thr = tx * (n / ereg_);
+        cudaEvent_t ev = prof_mark();
+        if (ereg_ == 8) {
+            allow_smem(zfwd_reg_kernel<8, T>);
+            zfwd_reg_kernel<8, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
+        } else {
+            allow_smem(zfwd_reg_kernel<16, T>);
+            zfwd_reg_kernel<16, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
+        }
+        launched(any_rt ? "z_roundtrip" : "z_fwd", zbytes, ev);
+    } else {
+        za.plan = plan(n);
+        za.tw = d_tw;
+        const size_t sm = (size_t)2 * n * tx * sizeof(cpx<T>);
+        allow_smem(zfwd_kernel<T>);
+        cudaEvent_t ev = prof_mark();
+        zfwd_kernel<T><<<zg, 256, sm, stream>>>(za);
+        launched(any_rt ? "z_roundtrip" : "z_fwd", zbytes, ev);
+    }
+    last_zblocks_ = zblocks;
+}
+
+template <typename T>
+void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zbytes) {
+    const int tx = reg_ok_ ? reg_tx() : tx_for();
+    za.tx = tx;
+    dim3 zg((b.nx + tx - 1) / tx, b.nb, narr);
+    if (reg_ok_) {
+        const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
+        const int thr = tx * (n / ereg_);
+        cudaEvent_t ev = prof_mark();
+        if (ereg_ == 8) {
+            allow_smem(zinv_reg_kernel<8, T>);
+            zinv_reg_kernel<8, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
+        } else {
+            allow_smem(zinv_reg_kernel<16, T>);
+            zinv_reg_kernel<16, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
+        }
+        launched("z_inv", zbytes, ev);
+    } else {
+        za.plan = plan(n);
+        za.tw = d_tw;
+        const size_t sm = (size_t)2 * n * tx * sizeof(cpx<T>);
+        allow_smem(zinv_kernel<T>);
+        cudaEvent_t ev = prof_mark();
+        zinv_kernel<T><<<zg, 256, sm, stream>>>(za);
+        launched("z_inv", zbytes, ev);
+    }
+}
+
+template <typename T>
+void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
+    const int h = n / 2;
+    const double bytes = (double)narr * ((double)n * n * b.nx * sizeof(cpx<T>) + (double)n3 * sizeof(T));
+    xa.tw_n_off = tw_off.at(n);
+    if (reg_ok_) {
+        xa.lx = reg_lx(1, row_pitch(h + 1));
+        const size_t sm = (size_t)xa.lx * row_pitch(h + 1) * sizeof(cpx<T>);
+        dim3 xg((unsigned)(((long)n * n) / xa.lx), narr);
+        const int thr = xa.lx * (h / ereg_);
+        cudaEvent_t ev = prof_mark();
+        if (ereg_ == 8) {
+            allow_smem(xinv_reg_kernel<8, T>);
+            xinv_reg_kernel<8, T><<<xg, thr, sm, stream>>>(xa, rplan(h), d_twT_);
+        } else {
+            allow_smem(xinv_reg_kernel<16, T>);
+            xinv_reg_kernel<16, T><<<xg, thr, sm, stream>>>(xa, rplan(h), d_twT_);
+        }
+        launched("x_inv", bytes, ev);
+        return;
+    }
+    const size_t per = (size_t)(3 * h + 1) * sizeof(cpx<T>);
+    int lx = 8;
+    while (lx > 1 && (per * lx > 96 * 1024 || ((long)n * n) % lx != 0)) lx /= 2;
+    xa.lx = lx;
+    xa.plan_half = plan(h);
+    xa.tw = d_tw;
+    allow_smem(xinv_kernel<T>);
+    dim3 xg((unsigned)(((long)n * n) / lx), narr);
+    cudaEvent_t ev = prof_mark();
+    xinv_kernel<T><<<xg, 256, per * lx, stream>>>(xa);
+    launched("x_inv", bytes, ev);
 }
 
 template <typename T>
@@ -374,47 +603,29 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
     XFwdArgs<T> xa;
     xa.n = n;
     xa.nx = b.nx;
-    xa.lx = lx_for(NOUT);
     for (int i = 0; i < F::NIN; ++i) xa.in[i] = in[i];
     for (int o = 0; o < NOUT; ++o) xa.out[o] = xsbuf(o);
     xa.plan_half = plan(h);
     xa.tw_n_off = tw_off.at(n);
     xa.tw = d_tw;
-    xa.partials = d_partials;
+    launch_xfwd(xa, f, NOUT, b);
     const int xgrid = (int)(((long)n * n) / xa.lx);
-    if (F::NRED > 0) ensure_partials((long)xgrid * F::NRED);
-    xa.partials = d_partials;
-    const size_t xsm = (size_t)2 * NOUT * xa.lx * h * sizeof(cpx<T>);
-    allow_smem(xfwd_kernel<T, F>);
-    cudaEvent_t ev = prof_mark();
-    xfwd_kernel<T, F><<<xgrid, 256, xsm, stream>>>(xa, f);
-    launched("x_fwd", (double)n3 * sizeof(T) * F::NIN + (double)n * n * b.nx * sizeof(cpx<T>) * NOUT, ev);
     if (F::NRED > 0 && fred_dst >= 0) finalize(xgrid, F::NRED, 1.0 / (double)n3, fred_dst);
     if (NOUT == 0) return;
     // y forward
-    const int tx = tx_for();
     YArgs<T> ya;
     ya.n = n;
     ya.nx = b.nx;
-    ya.tx = tx;
     ya.band = b;
     for (int o = 0; o < NOUT; ++o) {
         ya.in[o] = xsbuf(o);
         ya.out[o] = ysbuf(o);
     }
-    ya.plan = plan(n);
-    ya.tw = d_tw;
-    const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
-    allow_smem(ypass_kernel<-1, T>);
-    dim3 yg((b.nx + tx - 1) / tx, n, NOUT);
-    ev = prof_mark();
-    ypass_kernel<-1, T><<<yg, 256, ysm, stream>>>(ya);
-    launched("y_fwd", (double)NOUT * (n * (double)n * b.nx + n * (double)b.nb * b.nx) * sizeof(cpx<T>), ev);
+    launch_y(ya, -1, NOUT, b);
     // z stage
     ZFwdArgs<T> za;
     za.n = n;
     za.nx = b.nx;
-    za.tx = tx;
     za.band = b;
     bool any_rt = false;
     for (int o = 0; o < NOUT; ++o) {
@@ -437,14 +648,7 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
         op.red_with_f64 = fo.red_with_f64;
         op.red_with_slot = fo.red_with_slot;
     }
-    za.plan = plan(n);
-    za.tw = d_tw;
     za.norm = norm > 0 ? norm : 1.0 / (double)n3;
-    dim3 zg((b.nx + tx - 1) / tx, b.nb, NOUT);
-    const long zblocks = (long)zg.x * zg.y * zg.z;
-    ensure_partials(zblocks * MAX_RED);
-    za.partials = d_partials;
-    allow_smem(zfwd_kernel<T>);
     double zbytes = 0;
     {
         const double ys_b = (double)n * b.nb * b.nx * sizeof(cpx<T>);
@@ -458,9 +662,8 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
             if (fo.red_with) zbytes += sp_elems * (fo.red_with_f64 ? 16 : 8);
         }
     }
-    ev = prof_mark();
-    zfwd_kernel<T><<<zg, 256, ysm, stream>>>(za);
-    launched(any_rt ? "z_roundtrip" : "z_fwd", zbytes, ev);
+    launch_zfwd(za, NOUT, b, any_rt, zbytes);
+    const long zblocks = last_zblocks_;
     if (red_dst >= 0) finalize((int)zblocks, MAX_RED, 1.0, red_dst);
     if (any_rt) {
         std::vector<cpx<T>*> ys;
@@ -478,14 +681,10 @@ template <typename T>
 void Engine<T>::yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const std::vector<int>& phys_out) {
     const int k = (int)ys.size();
     if (k == 0) return;
-    const int tx = tx_for();
-    const int h = n / 2;
-    // y inverse: ys[i] -> xs (index by position; xs buffers beyond the
-    // forward's outputs are free at this point)
+    // y inverse: ys[i] -> xs (xs buffers are free once the forward's y pass ran)
     YArgs<T> ya;
     ya.n = n;
     ya.nx = b.nx;
-    ya.tx = tx;
     ya.band = b;
     std::vector<cpx<T>*> xs(k);
     for (int i = 0; i < k; ++i) {
@@ -493,48 +692,29 @@ void Engine<T>::yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const 
         ya.in[i] = ys[i];
         ya.out[i] = xs[i];
     }
-    ya.plan = plan(n);
-    ya.tw = d_tw;
-    const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
-    allow_smem(ypass_kernel<+1, T>);
-    dim3 yg((b.nx + tx - 1) / tx, n, k);
-    cudaEvent_t ev = prof_mark();
-    ypass_kernel<+1, T><<<yg, 256, ysm, stream>>>(ya);
-    launched("y_inv", (double)k * (n * (double)b.nb * b.nx + n * (double)n * b.nx) * sizeof(cpx<T>), ev);
+    launch_y(ya, +1, k, b);
     // x inverse
     XInvArgs<T> xa;
     xa.n = n;
     xa.nx_in = b.nx;
-    const size_t per = (size_t)(3 * h + 1) * sizeof(cpx<T>);
-    int lx = 8;
-    while (lx > 1 && (per * lx > 96 * 1024 || ((long)n * n) % lx != 0)) lx /= 2;
-    xa.lx = lx;
     for (int i = 0; i < k; ++i) {
         xa.in[i] = xs[i];
         xa.out[i] = phys(phys_out[i]);
     }
-    xa.plan_half = plan(h);
-    xa.tw_n_off = tw_off.at(n);
+    xa.plan_half = plan(n / 2);
     xa.tw = d_tw;
-    allow_smem(xinv_kernel<T>);
-    dim3 xg((unsigned)(((long)n * n) / lx), k);
-    ev = prof_mark();
-    xinv_kernel<T><<<xg, 256, per * lx, stream>>>(xa);
-    launched("x_inv", (double)k * ((double)n * n * b.nx * sizeof(cpx<T>) + (double)n3 * sizeof(T)), ev);
+    launch_xinv(xa, k, b);
 }
 
 template <typename T>
 void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
     if (b.nx > nxcap || b.nb > nbcap) throw CudaError("inv: band exceeds buffers", MLQ_ERR_BADARG);
     const int G = 6;
-    const int tx = tx_for();
-    const size_t zsm = (size_t)2 * n * tx * sizeof(cpx<T>);
     for (size_t g0 = 0; g0 < outs.size(); g0 += G) {
         const int k = (int)std::min<size_t>(G, outs.size() - g0);
         ZInvArgs<T> za;
         za.n = n;
         za.nx = b.nx;
-        za.tx = tx;
         za.band = b;
         std::vector<cpx<T>*> ys(k);
         std::vector<int> po(k);
@@ -547,19 +727,13 @@ void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
             op.ys_out = ys[i];
             po[i] = io.phys_out;
         }
-        za.plan = plan(n);
-        za.tw = d_tw;
-        allow_smem(zinv_kernel<T>);
-        dim3 zg((b.nx + tx - 1) / tx, b.nb, k);
         double zb = 0;
         for (int i = 0; i < k; ++i) {
             const InvOut& io = outs[g0 + i];
             zb += (double)n * b.nb * b.nx * sizeof(cpx<T>);
             for (int s2 = 0; s2 < io.nsrc; ++s2) zb += (double)b.nb * b.nb * b.nx * (io.src[s2].f64 ? 16 : 8);
         }
-        cudaEvent_t ev = prof_mark();
-        zinv_kernel<T><<<zg, 256, zsm, stream>>>(za);
-        launched("z_inv", zb, ev);
+        launch_zinv(za, k, b, zb);
         yx_inverse(b, ys, po);
     }
 }

@@ -16,6 +16,7 @@
 
 #include "functors.cuh"
 #include "kernels.cuh"
+#include "regfft.cuh"
 
 namespace mlq {
 
@@ -199,6 +200,22 @@ class Engine : public EngineBase {
     void widen_to(const Band& b);
 
     double2* c_tmp_ = nullptr;  // FP64 spectra of P2(|w|^{q-2} w) for the transport
+
+    // register-resident FFT kernels (power-of-two n >= 64); E elements per thread
+    int ereg_ = 8;  // elements per thread: 8 up to n = 512, 16 above
+    bool reg_ok_ = false;
+    cpx<T>* d_twT_ = nullptr;  // twiddle pool in T
+    RPlan rplan(int L) const;
+    int reg_tx() const;
+    int reg_lx(int nrows_per_line, size_t pitch) const;
+    // pass launchers (register kernels when reg_ok_, shared-memory Stockham otherwise)
+    template <class F>
+    void launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b);
+    void launch_y(YArgs<T>& ya, int sign, int narr, const Band& b);
+    void launch_zfwd(ZFwdArgs<T>& za, int narr, const Band& b, bool any_rt, double zbytes);
+    void launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zbytes);
+    void launch_xinv(XInvArgs<T>& xa, int narr, const Band& b);
+    long last_zblocks_ = 0;
 
    private:
     // |u|^k chain (calc_uk); memoised per program

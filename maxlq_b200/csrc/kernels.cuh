@@ -341,8 +341,10 @@ __device__ __forceinline__ cpx<double> apply_sym(int sym, int ab, const Kvec& k,
         case SYM_NEG_INV_KSQ: return k.ksq == 0.0 ? mk(0.0, 0.0) : v * (-1.0 / k.ksq);
         case SYM_KK_KSQ: {
             if (k.ksq == 0.0) return mk(0.0, 0.0);
-            const double o[3] = {k.ox, k.oy, k.oz};
-            return v * (o[ab / 3] * o[ab % 3] / k.ksq);
+            const int ia = ab / 3, ib = ab % 3;
+            const double ka = ia == 0 ? k.ox : (ia == 1 ? k.oy : k.oz);
+            const double kb = ib == 0 ? k.ox : (ib == 1 ? k.oy : k.oz);
+            return v * (ka * kb / k.ksq);
         }
     }
     return v;
