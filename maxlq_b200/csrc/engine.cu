@@ -644,9 +644,11 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
         op.add_ab = fo.add_ab;
         op.add_coef = fo.add_coef;
         op.red_self = fo.red_self;
-        op.red_with = fo.red_with;
-        op.red_with_f64 = fo.red_with_f64;
-        op.red_with_slot = fo.red_with_slot;
+        for (int r = 0; r < 3; ++r) {
+            op.red_with[r] = fo.red_with[r];
+            op.red_with_f64[r] = fo.red_with_f64[r];
+            op.red_with_slot[r] = fo.red_with_slot[r];
+        }
     }
     za.norm = norm > 0 ? norm : 1.0 / (double)n3;
     double zbytes = 0;
@@ -659,7 +661,8 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
             if (fo.spec) zbytes += sp_elems * (fo.spec_f64 ? 16 : 8);
             if (fo.phys_out >= 0) zbytes += ys_b;
             if (fo.add) zbytes += sp_elems * (fo.add_f64 ? 16 : 8);
-            if (fo.red_with) zbytes += sp_elems * (fo.red_with_f64 ? 16 : 8);
+            for (int r = 0; r < 3; ++r)
+                if (fo.red_with[r]) zbytes += sp_elems * (fo.red_with_f64[r] ? 16 : 8);
         }
     }
     launch_zfwd(za, NOUT, b, any_rt, zbytes);
@@ -1349,6 +1352,121 @@ void Engine<T>::calc_uk(const double2* u, double k, int dst) {
 }
 
 // ----------------------------------------------------------------------------
+// line search along phi = u + tau d at q = 4
+// ----------------------------------------------------------------------------
+namespace {
+enum : int {
+    LU = 60,    // u (3)
+    LD = 63,    // d (3)
+    LDU = 66,   // d_j u_i at 66+3i+j
+    LDD = 75,   // d_j d_i at 75+3i+j
+    LS = 84,    // S_a = P2 coefficients of |phi|^2 (3)
+    LV = 87,    // V_aj = P2 coefficients of W_j at 87+3a+j
+    LP = 96,    // p_a (3)
+    WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
+};
+}  // namespace
+
+template <typename T>
+void Engine<T>::ls_setup(const double2* u, const double2* d) {
+    const long nc = spec_ncomp();
+    // phi's pieces: u, d and their gradients (function_ops.f90:3147-3195)
+    std::vector<InvOut> io;
+    for (int f = 0; f < 2; ++f)
+        for (int i = 0; i < 3; ++i)
+            for (int j = -1; j < 3; ++j) {
+                InvOut o;
+                o.nsrc = 1;
+                o.src[0] = ZSrc{(f == 0 ? u : d) + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+                o.phys_out = j < 0 ? (f == 0 ? LU : LD) + i : (f == 0 ? LDU : LDD) + 3 * i + j;
+                io.push_back(o);
+            }
+    inv(b2, io);
+    std::vector<const T*> ud = {phys(LU), phys(LU + 1), phys(LU + 2), phys(LD), phys(LD + 1), phys(LD + 2)};
+    std::vector<const T*> all;
+    for (int i = 0; i < 3; ++i) all.push_back(phys(LU + i));
+    for (int i = 0; i < 9; ++i) all.push_back(phys(LDU + i));
+    for (int i = 0; i < 3; ++i) all.push_back(phys(LD + i));
+    for (int i = 0; i < 9; ++i) all.push_back(phys(LDD + i));
+    std::vector<const T*> grads;
+    for (int i = 0; i < 9; ++i) grads.push_back(phys(LDU + i));
+    for (int i = 0; i < 9; ++i) grads.push_back(phys(LDD + i));
+    // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333)
+    {
+        FwdOut o[3];
+        for (int a = 0; a < 3; ++a) o[a].phys_out = LS + a;
+        fwd(b2, FLSS{}, ud, {o[0], o[1], o[2]});
+    }
+    // P2 of the coefficients of W_j (calc_vgraduvgradu / calc_vvgradu, v = phi)
+    {
+        FwdOut o[3];
+        for (int j = 0; j < 3; ++j) o[j].phys_out = LV + j;
+        fwd(b2, FLSW<0>{}, all, {o[0], o[1], o[2]});
+        for (int j = 0; j < 3; ++j) o[j].phys_out = LV + 3 + j;
+        fwd(b2, FLSW<1>{}, all, {o[0], o[1], o[2]});
+        for (int j = 0; j < 3; ++j) o[j].phys_out = LV + 6 + j;
+        fwd(b2, FLSW<2>{}, all, {o[0], o[1], o[2]});
+    }
+    // p_a = -Lap^-1 P2(Q_a) and the spectra of P2(|grad phi|^2)_a
+    {
+        FwdOut o[6];
+        for (int a = 0; a < 3; ++a) {
+            o[a].sym = SYM_INV_KSQ;
+            o[a].phys_out = LP + a;
+            o[3 + a].spec = wspec(WLG + a);
+            o[3 + a].spec_f64 = wf64<T>();
+        }
+        fwd(b2, FLSQG{}, grads, {o[0], o[1], o[2], o[3], o[4], o[5]});
+    }
+    // R2 and R3 integrands as polynomials in tau
+    std::vector<const T*> rin;
+    for (int i = 0; i < 9; ++i) rin.push_back(phys(LV + i));
+    for (int a = 0; a < 3; ++a) rin.push_back(phys(LP + a));
+    for (int i = 0; i < 6; ++i) rin.push_back(ud[i]);
+    pointwise(FLSRed{}, rin, {}, 100);
+    fetch_results();
+    const double* r = h_results + 100;
+    const double M[3][3] = {{r[0], r[1], r[2]}, {r[1], r[3], r[4]}, {r[2], r[4], r[5]}};
+    for (int k = 0; k < 5; ++k) ls_r2_[k] = 0.0;
+    for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b) ls_r2_[a + b] += M[a][b];
+    for (int k = 0; k < 6; ++k) ls_r3_[k] = 0.0;
+    for (int a = 0; a < 3; ++a)
+        for (int cc = 0; cc < 2; ++cc)
+            for (int b = 0; b < 3; ++b) ls_r3_[a + cc + b] += r[6 + 3 * (2 * a + cc) + b];
+}
+
+template <typename T>
+void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
+    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
+    // A(tau) = P2(g^2) with its Parseval products: ||A||^2 (= ||phi||_4^4) and
+    // <A, P2(|grad phi|^2)_a>, a = 0..2
+    FwdOut o;
+    o.red_self = 0;
+    for (int a = 0; a < 3; ++a) {
+        o.red_with[a] = wspec(WLG + a);
+        o.red_with_f64[a] = wf64<T>();
+        o.red_with_slot[a] = 1 + a;
+    }
+    FLSA f;
+    f.tau = tau;
+    fwd(b2, f, {phys(LS), phys(LS + 1), phys(LS + 2)}, {o}, 130);
+    fetch_results();
+    const double* r = h_results + 130;
+    const double I1 = r[1] + tau * (r[2] + tau * r[3]);
+    double I2 = 0.0, I3 = 0.0;
+    for (int k = 4; k >= 0; --k) I2 = I2 * tau + ls_r2_[k];
+    for (int k = 5; k >= 0; --k) I3 = I3 * tau + ls_r3_[k];
+    const double R1 = -cv * I1;                 // -nu <|u|^2, P2 |grad u|^2>  (1318)
+    const double R2 = -cv * (q - 2.0) * I2;     // -(q-2) nu <1, P2 sum_j V_j^2> (1333)
+    const double R3 = cp * (q - 2.0) * I3;      // (q-2) <p, u.V>  (1352)
+    out[0] = R1 + R2 + R3;
+    out[1] = R1 + R2;
+    out[2] = R3;
+    if (lqq) *lqq = r[0];
+}
+
+// ----------------------------------------------------------------------------
 // state <-> host
 // ----------------------------------------------------------------------------
 template <typename T>
@@ -1479,7 +1597,7 @@ void Engine<T>::fft_c2c(const double* in, double* out, int sign) {
             op.spec_f64 = 1;
             op.sym = SYM_ONE;
             op.red_self = -1;
-            op.red_with_slot = -1;
+            for (int r = 0; r < 3; ++r) op.red_with_slot[r] = -1;
             za.op[0] = op;
             za.plan = plan(n);
             za.tw = d_tw;

@@ -143,8 +143,8 @@ class Engine : public EngineBase {
         int add_f64 = 0, add_sym = SYM_ONE, add_ab = 0;
         double add_coef = 0;
         int red_self = -1;
-        const void* red_with = nullptr;
-        int red_with_f64 = 0, red_with_slot = -1;
+        const void* red_with[3] = {nullptr, nullptr, nullptr};
+        int red_with_f64[3] = {0, 0, 0}, red_with_slot[3] = {-1, -1, -1};
     };
     // Forward pipeline of functor outputs through band b; reductions of the
     // z stage land in results[red_dst + slot] (slot < MAX_RED); functor
@@ -176,6 +176,14 @@ class Engine : public EngineBase {
     double lq_pow(const double2* u, const double2* d, double tau);  // ||u + tau d||_q^q
     // |u|^k physical (calc_uk) of the state u, into phys index dst
     void calc_uk(const double2* u, double k, int dst);
+
+    // Line search along phi = u + tau d when q = 4 (|u|^{q-4} = 1): the
+    // setup forms the tau-coefficient fields once; a trial is then one
+    // forward transform of g(tau)^2 plus polynomial evaluations.
+    bool ls_ok() const { return !use_e_u && P.q == 4.0; }
+    void ls_setup(const double2* u, const double2* d);
+    void ls_trial(double tau, double out[3], double* lqq);
+    double ls_r2_[5] = {0}, ls_r3_[6] = {0};
 
     // ---- state <-> host ----
     // Forward transform of a host FP64 vector field into state spectra.

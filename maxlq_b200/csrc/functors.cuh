@@ -288,6 +288,124 @@ struct FDiffSq {
     }
 };
 
+// ---- line search along phi = u + tau d (q = 4) -------------------------------
+// Every product that R needs is quadratic in tau; these functors form the
+// coefficient fields, whose dealias/Poisson images then combine linearly.
+
+// S_a of |phi|^2 = |u|^2 + tau 2 u.d + tau^2 |d|^2.  inputs u(3), d(3)
+struct FLSS {
+    static constexpr int NIN = 6, NOUT = 3, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        out[0] = in[0] * in[0] + in[1] * in[1] + in[2] * in[2];
+        out[1] = T(2) * (in[0] * in[3] + in[1] * in[4] + in[2] * in[5]);
+        out[2] = in[3] * in[3] + in[4] * in[4] + in[5] * in[5];
+    }
+};
+
+// tau^A coefficient of W_j = sum_i phi_i d_j phi_i.  inputs u(3), Du(9), d(3), Dd(9)
+template <int A>
+struct FLSW {
+    static constexpr int NIN = 24, NOUT = 3, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        const T* u = in;
+        const T* du = in + 3;
+        const T* d = in + 12;
+        const T* dd = in + 15;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            T w = 0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) {
+                if (A == 0) w += u[i] * du[3 * i + j];
+                if (A == 1) w += u[i] * dd[3 * i + j] + d[i] * du[3 * i + j];
+                if (A == 2) w += d[i] * dd[3 * i + j];
+            }
+            out[j] = w;
+        }
+    }
+};
+
+// tau^a coefficients of Q = d_j phi_i d_i phi_j (out 0..2) and of
+// G2 = |grad phi|^2 (out 3..5).  inputs Du(9), Dd(9)
+struct FLSQG {
+    static constexpr int NIN = 18, NOUT = 6, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        const T* du = in;
+        const T* dd = in + 9;
+        T q0 = 0, q1 = 0, q2 = 0, g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) {
+                const T a = du[3 * i + j], b = dd[3 * i + j];  // d_j u_i, d_j d_i
+                const T at = du[3 * j + i], bt = dd[3 * j + i];
+                q0 += a * at;
+                q1 += a * bt + b * at;
+                q2 += b * bt;
+                g0 += a * a;
+                g1 += a * b;
+                g2 += b * b;
+            }
+        out[0] = q0;
+        out[1] = q1;
+        out[2] = q2;
+        out[3] = g0;
+        out[4] = T(2) * g1;
+        out[5] = g2;
+    }
+};
+
+// g^2 at tau: g = sqrt(max(S0 + tau S1 + tau^2 S2, 0)).  inputs S_a (dealiased)
+struct FLSA {
+    static constexpr int NIN = 3, NOUT = 1, NRED = 0;
+    double tau;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        const T t = (T)tau;
+        const T s = in[0] + t * (in[1] + t * in[2]);
+        const T g = s <= T(0) ? T(0) : sqrt(s);
+        out[0] = g * g;
+    }
+};
+
+// Polynomial coefficients of R2 and R3 along the line.  inputs V[a][j] at
+// 3a+j (9), p_a (3), u(3), d(3).  Slots: 0..5 sum_j V_aj V_bj for
+// (a,b) = 00,01,02,11,12,22; 6 + 3(2a+c) + b: p_a sum_j c_j V_bj, c = u, d.
+struct FLSRed {
+    static constexpr int NIN = 18, NOUT = 0, NRED = 24;
+    template <typename T>
+    __device__ void operator()(const T* in, T*, double* acc) const {
+        double V[3][3], p[3], c[2][3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) V[a][j] = (double)in[3 * a + j];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p[a] = (double)in[9 + a];
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            c[0][j] = (double)in[12 + j];
+            c[1][j] = (double)in[15 + j];
+        }
+        int s = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int b = a; b < 3; ++b) acc[s++] += V[a][0] * V[b][0] + V[a][1] * V[b][1] + V[a][2] * V[b][2];
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int cc = 0; cc < 2; ++cc)
+#pragma unroll
+                for (int b = 0; b < 3; ++b)
+                    acc[6 + 3 * (2 * a + cc) + b] +=
+                        p[a] * (c[cc][0] * V[b][0] + c[cc][1] * V[b][1] + c[cc][2] * V[b][2]);
+    }
+};
+
 // sum of squares of three stored fields (energy check of a loaded field)
 struct FEnergy3 {
     static constexpr int NIN = 3, NOUT = 3, NRED = 1;

@@ -382,9 +382,9 @@ struct ZFwdOp {
     const void* add;      // optional second term
     int add_f64, add_sym, add_ab;
     double add_coef;
-    int red_self;         // slot for sum w|Y|^2, -1 none
-    const void* red_with; // slot for sum w Re(Y conj(W)), -1 none
-    int red_with_f64, red_with_slot;
+    int red_self;               // slot for sum w|Y|^2, -1 none
+    const void* red_with[3];    // sum w Re(Y conj(W_i)) into red_with_slot[i] (null: none)
+    int red_with_f64[3], red_with_slot[3];
 };
 
 template <typename T>
@@ -434,10 +434,11 @@ __global__ void __launch_bounds__(256) zfwd_kernel(ZFwdArgs<T> a) {
             if (op.add) Y = Y + apply_sym(op.add_sym, op.add_ab, k, ld_spec(op.add, op.add_f64, si)) * op.add_coef;
             const double wgt = kx_weight(n, fx);
             if (op.red_self >= 0) acc[op.red_self] += wgt * (Y.x * Y.x + Y.y * Y.y);
-            if (op.red_with) {
-                const cpx<double> W = ld_spec(op.red_with, op.red_with_f64, si);
-                acc[op.red_with_slot] += wgt * (Y.x * W.x + Y.y * W.y);
-            }
+            for (int r = 0; r < 3; ++r)
+                if (op.red_with[r]) {
+                    const cpx<double> W = ld_spec(op.red_with[r], op.red_with_f64[r], si);
+                    acc[op.red_with_slot[r]] += wgt * (Y.x * W.x + Y.y * W.y);
+                }
             if (op.spec_out) st_spec(op.spec_out, op.spec_f64, si, Y);
         }
         if (op.ys_out) o[p] = mk((T)Y.x, (T)Y.y);

@@ -183,7 +183,7 @@ extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
     op.ys_out = ys;
     op.sym = SYM_ONE;
     op.red_self = -1;
-    op.red_with_slot = -1;
+    for (int r = 0; r < 3; ++r) op.red_with_slot[r] = -1;
     za.op[0] = op;
     za.plan = plan_n;
     za.tw = tw;

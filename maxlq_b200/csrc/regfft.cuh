@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(256, 3) zfwd_reg_kernel(ZFwdArgs<T> a, RPlan p
     }
     const ColIdx si{tx, l};
     reg_fft<E, -1>(v, t, nT, pl, sm, si, tw);
-    double acc_self = 0.0, acc_with = 0.0;
+    double acc_self = 0.0, acc_w0 = 0.0, acc_w1 = 0.0, acc_w2 = 0.0;
     const int fy = band_fft_index(a.band, cy);
     const double wgt = kx_weight(n, kx);
 #pragma unroll
@@ -174,24 +174,33 @@ __global__ void __launch_bounds__(256, 3) zfwd_reg_kernel(ZFwdArgs<T> a, RPlan p
             const long si2 = ((long)cz * nb + cy) * nx + kx;
             if (op.add) Y = Y + apply_sym(op.add_sym, op.add_ab, k, ld_spec(op.add, op.add_f64, si2)) * op.add_coef;
             if (op.red_self >= 0) acc_self += wgt * (Y.x * Y.x + Y.y * Y.y);
-            if (op.red_with) {
-                const cpx<double> W = ld_spec(op.red_with, op.red_with_f64, si2);
-                acc_with += wgt * (Y.x * W.x + Y.y * W.y);
+            if (op.red_with[0]) {
+                const cpx<double> W = ld_spec(op.red_with[0], op.red_with_f64[0], si2);
+                acc_w0 += wgt * (Y.x * W.x + Y.y * W.y);
+            }
+            if (op.red_with[1]) {
+                const cpx<double> W = ld_spec(op.red_with[1], op.red_with_f64[1], si2);
+                acc_w1 += wgt * (Y.x * W.x + Y.y * W.y);
+            }
+            if (op.red_with[2]) {
+                const cpx<double> W = ld_spec(op.red_with[2], op.red_with_f64[2], si2);
+                acc_w2 += wgt * (Y.x * W.x + Y.y * W.y);
             }
             if (op.spec_out) st_spec(op.spec_out, op.spec_f64, si2, Y);
         }
         v[m] = mk((T)Y.x, (T)Y.y);
     }
     const int block_lin = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-    if (op.red_self >= 0 || op.red_with) {
-        double acc2[2] = {acc_self, acc_with};
-        __shared__ double part2[2];
-        block_reduce_store<2>(acc2, part2, 0);
+    if (op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2]) {
+        double acc4[4] = {acc_self, acc_w0, acc_w1, acc_w2};
+        __shared__ double part4[4];
+        block_reduce_store<4>(acc4, part4, 0);
         __syncthreads();
         if (threadIdx.x < MAX_RED) {
             double v2 = 0.0;
-            if (threadIdx.x == op.red_self) v2 += part2[0];
-            if (op.red_with && threadIdx.x == op.red_with_slot) v2 += part2[1];
+            if ((int)threadIdx.x == op.red_self) v2 += part4[0];
+            for (int r = 0; r < 3; ++r)
+                if (op.red_with[r] && (int)threadIdx.x == op.red_with_slot[r]) v2 += part4[1 + r];
             a.partials[(long)block_lin * MAX_RED + threadIdx.x] = v2;
         }
     } else if (threadIdx.x < MAX_RED) {

@@ -77,11 +77,25 @@ class Solver : public SolverBase {
     }
 
     // ---- line search -------------------------------------------------------
+    // Line-search trials go through the polynomial path when q = 4: setup
+    // once per (base, dir), then one transform per trial.
+    bool ls_ready = false;
+    void ls_begin(const double2* base, const double2* dir) {
+        trials.clear();
+        ls_ready = false;
+        if (e.ls_ok() && dir) {
+            e.ls_setup(base, dir);
+            ls_ready = true;
+        }
+    }
     Trial trial(const double2* base, const double2* dir, double tau) {
         auto it = trials.find(tau);
         if (it != trials.end()) return it->second;
         Trial t;
-        e.R_eval(base, dir, tau, t.R, &t.lqq);
+        if (ls_ready)
+            e.ls_trial(tau, t.R, &t.lqq);
+        else
+            e.R_eval(base, dir, tau, t.R, &t.lqq);
         trials[tau] = t;
         return t;
     }
@@ -338,6 +352,7 @@ class Solver : public SolverBase {
         // line search (269-318)
         double tb[2] = {0, 0};
         int mflag = 0;
+        ls_begin(u, d1);
         mnbrak(u, d1, 0.0, tau0, tb, &mflag);
         info.J0 = J0;
         info.mnbrak_flag = mflag;
@@ -362,6 +377,7 @@ class Solver : public SolverBase {
         // vector transport of gu1 and d1 to the new point (324-328)
         double ir[2];
         const double2* xi[2] = {g1, d1};
+        ls_ready = false;
         double lqw;
         if (e.P.use_riemannian_geometry)
             lqw = e.transport_pieces(u, d1, tau1, xi, 2, ir);
@@ -519,7 +535,7 @@ class Solver : public SolverBase {
     int mnbrak_host(const double* phi, const double* d, double tA0, double tB0, double br[2], int* flag) override {
         load(phi, tmp);
         load(d, c);
-        trials.clear();
+        ls_begin(tmp, c);
         *flag = 0;
         mnbrak(tmp, c, tA0, tB0, br, flag);
         trials.clear();
@@ -529,7 +545,7 @@ class Solver : public SolverBase {
     double brent_host(const double* phi, const double* d, const double br[2]) override {
         load(phi, tmp);
         load(d, c);
-        trials.clear();
+        ls_begin(tmp, c);
         const double x = brent(tmp, c, br, nullptr);
         trials.clear();
         started = false;
