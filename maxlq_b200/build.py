@@ -12,13 +12,15 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmaxlq_b200.so")
-SOURCES = ["engine.cu", "solver.cu", "capi.cu", "noalloc.cu"]
-HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "regfft.cuh", "engine.cuh", "solver.cuh"]
+SOURCES = ["engine.cu", "engine_f32.cu", "engine_f64.cu", "solver.cu", "capi.cu", "noalloc.cu"]
+HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "regfft.cuh", "cfft.cuh", "engine.cuh",
+           "engine_common.cuh", "engine_impl.cuh", "solver.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -54,14 +56,21 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
               "-Xcompiler", "-fPIC", "-I", os.path.join(ROOT, "include")]
     if ptxas_v:
         common += ["-Xptxas", "-v"]
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = common + ["-c", os.path.join(CSRC, src), "-o", obj]
+        cmds.append(common + ["-c", os.path.join(CSRC, src), "-o", obj])
+        objs.append(obj)
+    # translation units compile in parallel; output of each kept together
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(lambda c: subprocess.run(c, capture_output=True, text=True), cmds))
+    for cmd, r in zip(cmds, results):
         if verbose:
             print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        if r.stdout or r.stderr:
+            print(r.stdout + r.stderr, end="", flush=True)
+        if r.returncode != 0:
+            raise subprocess.CalledProcessError(r.returncode, cmd)
     link = [nvcc(), "-ccbin", host_cxx(), *ARCH, "-shared", "-cudart", "static", "-o", LIB, *objs]
     if verbose:
         print(" ".join(link), flush=True)

@@ -1,0 +1,552 @@
+// cfft.cuh -- FFT pass kernels specialised at compile time for one grid size N.
+//
+// Every line length, radix sequence, register layout and shared-memory map is
+// a compile-time constant, so the only run-time index arithmetic left is the
+// work-item decomposition.  A line of length L is held by TPL = L/E threads,
+// thread t owning positions t + TPL*m (m < E) in registers before and after
+// every stage (Stockham autosort, see regfft.cuh for the generic form).
+//
+//  * x passes (rows of the physical field): TPL <= 32, so a line lives in one
+//    warp and the exchanges between stages need only __syncwarp.  The
+//    run-time twiddles of each stage depend only on t and are loaded once per
+//    thread into registers; the real-to-half-complex pre/post twiddle
+//    W_N^(t + TPL m) = W_N^t * W_N^(TPL m) uses a compile-time constant for
+//    the second factor.
+//  * y/z passes (columns): lanes walk the contiguous kx axis (TX columns per
+//    tile, 128-byte rows), the threads of a column span warps, and exchanges
+//    are block-wide.  Twiddles come from a per-block shared-memory table; the
+//    lanes of a row share t, so those reads are broadcasts.
+//
+// All kernels are persistent: a grid of a few blocks per SM walks the work
+// items with a fixed stride, so reduction partials are few and their order
+// is fixed (deterministic).
+#pragma once
+
+#include <type_traits>
+
+#include "functors.cuh"
+#include "kernels.cuh"
+
+namespace mlq {
+
+// ----------------------------------------------------------------------------
+// Compile-time helpers
+// ----------------------------------------------------------------------------
+__host__ __device__ constexpr int clog2(int v) {
+    int r = 0;
+    while ((1 << r) < v) ++r;
+    return r;
+}
+
+// sin x and cos x for |x| <= pi/4 by their Taylor series (compile time only;
+// the truncation error of 14 terms is below 1e-25).
+__host__ __device__ constexpr double ce_sin_small(double x) {
+    double term = x, sum = x;
+    for (int k = 1; k < 14; ++k) {
+        term *= -x * x / ((2.0 * k) * (2.0 * k + 1.0));
+        sum += term;
+    }
+    return sum;
+}
+__host__ __device__ constexpr double ce_cos_small(double x) {
+    double term = 1.0, sum = 1.0;
+    for (int k = 1; k < 14; ++k) {
+        term *= -x * x / ((2.0 * k - 1.0) * (2.0 * k));
+        sum += term;
+    }
+    return sum;
+}
+struct CeCS {
+    double c, s;
+};
+// cos and sin of 2 pi j / M: exact quadrant and octant reduction in integers,
+// then the series on an angle of at most pi/4.
+__host__ __device__ constexpr CeCS ce_cs2pi(long j, long M) {
+    j %= M;
+    if (j < 0) j += M;
+    const long q = (4 * j) / M;   // quadrant
+    const long r = 4 * j - q * M;  // angle within the quadrant = (pi/2) r / M
+    const double half_pi = 1.57079632679489661923;
+    double cq = 0.0, sq = 0.0;
+    if (2 * r <= M) {
+        const double x = half_pi * ((double)r / (double)M);
+        cq = ce_cos_small(x);
+        sq = ce_sin_small(x);
+    } else {
+        const double x = half_pi * ((double)(M - r) / (double)M);
+        cq = ce_sin_small(x);
+        sq = ce_cos_small(x);
+    }
+    if (q == 0) return {cq, sq};
+    if (q == 1) return {-sq, cq};
+    if (q == 2) return {-cq, -sq};
+    return {sq, -cq};
+}
+// W_M^J = exp(-2 pi i J / M) as a compile-time constant in precision T
+template <typename T, long M, long J>
+__device__ __forceinline__ cpx<T> cw() {
+    constexpr CeCS v = ce_cs2pi(J, M);
+    return mk<T>((T)v.c, (T)(-v.s));
+}
+
+// compile-time loop: f(std::integral_constant<int, I>) for I in [B, E)
+template <int B, int E>
+struct SFor {
+    template <class F>
+    __device__ __forceinline__ static void run(F&& f) {
+        if constexpr (B < E) {
+            f(std::integral_constant<int, B>{});
+            SFor<B + 1, E>::run(f);
+        }
+    }
+};
+
+// a * w (SIGN < 0) or a * conj(w) (SIGN > 0)
+template <int SIGN, typename T>
+__device__ __forceinline__ cpx<T> cmul_s(cpx<T> a, cpx<T> w) {
+    if constexpr (SIGN < 0)
+        return mk(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+    else
+        return mk(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+
+// ----------------------------------------------------------------------------
+// Plan of a length-L transform held as E elements per thread: radix-E stages,
+// then one smaller power-of-two radix for the remainder.
+// ----------------------------------------------------------------------------
+template <int L, int E>
+struct CPlan {
+    static_assert((L & (L - 1)) == 0 && (E & (E - 1)) == 0 && E >= 2 && E <= 16 && E <= L, "plan shape");
+    static constexpr int TPL = L / E;
+    static constexpr int LGL = clog2(L), LGE = clog2(E);
+    static constexpr int NFULL = LGL / LGE, REMLG = LGL % LGE;
+    static constexpr int NST = NFULL + (REMLG ? 1 : 0);
+    __host__ __device__ static constexpr int radix(int s) { return s < NFULL ? E : (1 << REMLG); }
+    __host__ __device__ static constexpr int ns(int s) {
+        int v = 1;
+        for (int i = 0; i < s; ++i) v *= radix(i);
+        return v;
+    }
+    // butterflies of stage s whose twiddles differ (1 when ns(s) divides TPL)
+    __host__ __device__ static constexpr int qd(int s) { return ns(s) <= TPL ? 1 : E / radix(s); }
+    __host__ __device__ static constexpr int twc(int s) { return s == 0 ? 0 : qd(s) * (radix(s) - 1); }
+    __host__ __device__ static constexpr int twoff(int s) {
+        int o = 0;
+        for (int i = 0; i < s; ++i) o += twc(i);
+        return o;
+    }
+    static constexpr int NTW = twoff(NST);
+};
+
+// Twiddles of one thread in registers; tab[j] = W_L^j in precision T.
+template <int L, int E, typename T>
+struct TwReg {
+    using P = CPlan<L, E>;
+    cpx<T> w[P::NTW > 0 ? P::NTW : 1];
+    __device__ __forceinline__ void load(const cpx<T>* __restrict__ tab, int t) {
+        SFor<1, P::NST>::run([&](auto sc) {
+            constexpr int S = decltype(sc)::value;
+            constexpr int R = P::radix(S), NS = P::ns(S), QD = P::qd(S), STEP = L / (NS * R);
+            SFor<0, QD>::run([&](auto ic) {
+                constexpr int I = decltype(ic)::value;
+                const int k = (t + P::TPL * I) & (NS - 1);
+#pragma unroll
+                for (int r = 1; r < R; ++r) w[P::twoff(S) + I * (R - 1) + r - 1] = tab[r * k * STEP];
+            });
+        });
+    }
+    template <int S, int I, int RI>
+    __device__ __forceinline__ cpx<T> get(int) const {
+        constexpr int QD = P::qd(S), R = P::radix(S);
+        return w[P::twoff(S) + (QD == 1 ? 0 : I) * (R - 1) + RI - 1];
+    }
+};
+
+// Twiddles read from a table W_L^j (shared memory) at run time.
+template <int L, int E, typename T>
+struct TwTab {
+    using P = CPlan<L, E>;
+    const cpx<T>* tab;
+    template <int S, int I, int RI>
+    __device__ __forceinline__ cpx<T> get(int k) const {
+        constexpr int R = P::radix(S), NS = P::ns(S), STEP = L / (NS * R);
+        return tab[RI * k * STEP];
+    }
+};
+
+struct SyncWarp {
+    __device__ __forceinline__ static void sync() { __syncwarp(); }
+};
+struct SyncBlock {
+    __device__ __forceinline__ static void sync() { __syncthreads(); }
+};
+
+// shared-memory maps of a line's positions
+template <int E>
+struct RowMap {  // one row per line, one pad element every E
+    int base;
+    __device__ __forceinline__ int operator()(int p) const { return base + p + p / E; }
+};
+template <int TX>
+struct ColMap {  // tile column l, position p at row p
+    int l;
+    __device__ __forceinline__ int operator()(int p) const { return p * TX + l; }
+};
+
+template <int L, int E, int S, int SIGN, class Sync, typename T, class Map, class Tw>
+__device__ __forceinline__ void cstage(cpx<T> (&v)[E], int t, cpx<T>* sm, const Map& map, const Tw& tw) {
+    using P = CPlan<L, E>;
+    constexpr int R = P::radix(S), NS = P::ns(S), Q = E / R, TPL = P::TPL;
+    constexpr bool LAST = S == P::NST - 1;
+    SFor<0, Q>::run([&](auto ic) {
+        constexpr int I = decltype(ic)::value;
+        const int b = t + TPL * I;
+        const int k = b & (NS - 1);
+        cpx<T> a[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) a[r] = v[I + Q * r];
+        if constexpr (S > 0) {
+            SFor<1, R>::run([&](auto rc) {
+                constexpr int RI = decltype(rc)::value;
+                a[RI] = cmul_s<SIGN>(a[RI], tw.template get<S, I, RI>(k));
+            });
+        }
+        dftR<R, SIGN>(a);
+        if constexpr (LAST) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) v[I + Q * r] = a[r];
+        } else {
+            const int base = (b - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm[map(base + r * NS)] = a[r];
+        }
+    });
+    if constexpr (!LAST) {
+        Sync::sync();
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = sm[map(t + TPL * m)];
+        Sync::sync();
+    }
+}
+
+// Length-L transform of the E register elements of every thread of a line.
+// Every thread of the sync scope must call it (it synchronises); the map's
+// shared memory must be free.
+template <int L, int E, int SIGN, class Sync, typename T, class Map, class Tw>
+__device__ __forceinline__ void cfft(cpx<T> (&v)[E], int t, cpx<T>* sm, const Map& map, const Tw& tw) {
+    SFor<0, CPlan<L, E>::NST>::run(
+        [&](auto sc) { cstage<L, E, decltype(sc)::value, SIGN, Sync>(v, t, sm, map, tw); });
+}
+
+// ----------------------------------------------------------------------------
+// Shapes per grid size and precision
+// ----------------------------------------------------------------------------
+template <int N, typename T>
+struct CShape {
+    static constexpr int L = N / 2;  // x lines: half-length complex transform
+    // x pass: elements per thread (a line stays within one warp)
+    static constexpr int EX = sizeof(T) == 4 ? (L >= 256 ? 16 : (L >= 64 ? 8 : 4)) : (L >= 512 ? 16 : (L >= 64 ? 8 : 4));
+    static constexpr int TPLX = L / EX;
+    // x pass twiddles: registers in FP32; a shared-memory table in FP64,
+    // where the registers are needed for the data
+    static constexpr bool XTW_REG = sizeof(T) == 4;
+    static constexpr int XLPB = 256 / TPLX;  // lines per x block
+    static constexpr int XPITCH = L + L / EX;
+    static constexpr size_t XSMEM = ((size_t)XLPB * XPITCH + (XTW_REG ? 0 : L)) * sizeof(cpx<T>);
+    // y/z passes: tile rows of TX columns (64 or 128 bytes)
+    static constexpr int TX = sizeof(T) == 4 ? (N >= 512 ? 8 : 16) : 8;
+    static constexpr int EY = sizeof(T) == 4 ? (N >= 256 ? 16 : (N >= 128 ? 8 : 4)) : (N >= 1024 ? 16 : (N >= 128 ? 8 : 4));
+    static constexpr int TPLY = N / EY;
+    static constexpr int YTHREADS = TX * TPLY;
+    static constexpr int YMINB = YTHREADS <= 256 ? 2 : 1;  // resident blocks the register budget aims at
+    static constexpr size_t YSMEM = ((size_t)N * TX + N) * sizeof(cpx<T>);
+    static_assert(TPLX <= 32 && 32 % TPLX == 0, "x line within a warp");
+    static_assert(YTHREADS % 32 == 0 && YTHREADS <= 512, "y/z block");
+};
+
+// block-wide deterministic reduction of NR accumulators into partials[slot]
+template <int NR>
+__device__ __forceinline__ void block_reduce_to(const double* acc, double* out) {
+    __shared__ double red_sm[32][NR];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        double v = acc[r];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if (lane == 0) red_sm[warp][r] = v;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int r = 0; r < NR; ++r) {
+            double v = lane < nw ? red_sm[lane][r] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0) out[r] = v;
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// x stage, inverse (c2r).  grid = (G, narr), block = 256.  Each block walks
+// groups of 256/TPL lines of array blockIdx.y.
+// ----------------------------------------------------------------------------
+template <int N, typename T>
+__global__ void __launch_bounds__(256, 2)
+    xinv_c_kernel(XInvArgs<T> a, const cpx<T>* __restrict__ twL, const cpx<T>* __restrict__ twN) {
+    using S = CShape<N, T>;
+    constexpr int L = S::L, E = S::EX, TPL = S::TPLX, LPB = S::XLPB, PITCH = S::XPITCH;
+    constexpr long NG = (long)N * N / LPB;  // line groups per array
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);  // LPB * PITCH, then the table
+    const int ls = threadIdx.x / TPL, t = threadIdx.x % TPL;
+    const RowMap<E> map{ls * PITCH};
+    std::conditional_t<S::XTW_REG, TwReg<L, E, T>, TwTab<L, E, T>> tw;
+    if constexpr (S::XTW_REG) {
+        tw.load(twL, t);
+    } else {
+        cpx<T>* stw = sm + LPB * PITCH;
+        for (int i = threadIdx.x; i < L; i += blockDim.x) stw[i] = twL[i];
+        __syncthreads();
+        tw.tab = stw;
+    }
+    const cpx<T> wt = twN[t];  // W_N^t
+    const int nx_in = a.nx_in;
+    const cpx<T>* __restrict__ src0 = a.in[blockIdx.y];
+    T* __restrict__ dst0 = a.out[blockIdx.y];
+    const int src_lane = (TPL - t) & (TPL - 1);
+    for (long g = blockIdx.x; g < NG; g += gridDim.x) {
+        const long line = g * LPB + ls;
+        const cpx<T>* __restrict__ src = src0 + line * nx_in;
+        cpx<T> v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int k = t + TPL * m;
+            v[m] = k < nx_in ? src[k] : czero<T>();
+        }
+        // c2c + REAL() keeps the Hermitian part: real part only on kx = 0, N/2
+        cpx<T> xh = czero<T>();
+        if (t == 0) {
+            v[0].y = T(0);
+            if (L < nx_in) xh = mk(src[L].x, T(0));
+        }
+        cpx<T> o[E];
+        SFor<0, E>::run([&](auto mc) {
+            constexpr int m = decltype(mc)::value;
+            cpx<T> xp;  // X[L - k], k = t + TPL m
+            xp.x = __shfl_sync(0xffffffffu, v[E - 1 - m].x, src_lane, TPL);
+            xp.y = __shfl_sync(0xffffffffu, v[E - 1 - m].y, src_lane, TPL);
+            if (t == 0) xp = (m == 0) ? xh : v[(E - m) % E];
+            const cpx<T> xk = v[m];
+            const cpx<T> xc = conj(xp);
+            const cpx<T> Fk = xk + xc;
+            // G = (xk - xc) * conj(W_N^k),  W_N^k = W_N^t * W_N^(TPL m)
+            const cpx<T> w = wt * cw<T, N, (long)TPL * m>();
+            const cpx<T> G = cmul_s<+1>(xk - xc, w);
+            o[m] = mk(Fk.x - G.y, Fk.y + G.x);  // F + i G
+        });
+        cfft<L, E, +1, SyncWarp>(o, t, sm, map, tw);
+        cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(dst0 + line * N);
+#pragma unroll
+        for (int m = 0; m < E; ++m) dst[t + TPL * m] = o[m];
+    }
+}
+
+// ----------------------------------------------------------------------------
+// y pass.  grid = (G, narr), block = TX * TPLY.  Items: (z, kx tile).
+// ----------------------------------------------------------------------------
+template <int N, int SIGN, typename T>
+__global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
+    ypass_c_kernel(YArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = CShape<N, T>;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* stw = sm + N * TX;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    __syncthreads();
+    const TwTab<N, E, T> tw{stw};
+    const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const ColMap<TX> map{l};
+    const int nx = a.nx, nb = a.band.nb;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)N * ntile;
+    const cpx<T>* __restrict__ src = a.in[blockIdx.y];
+    cpx<T>* __restrict__ dst = a.out[blockIdx.y];
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int z = (int)(it / ntile);
+        const int kx = (int)(it - (long)z * ntile) * TX + l;
+        const bool ok = kx < nx;
+        cpx<T> v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int p = t + TPL * m;
+            if constexpr (SIGN < 0) {
+                v[m] = ok ? src[((long)z * N + p) * nx + kx] : czero<T>();
+            } else {
+                const int ci = band_compact_index(a.band, p);
+                v[m] = (ok && ci >= 0) ? src[((long)z * nb + ci) * nx + kx] : czero<T>();
+            }
+        }
+        cfft<N, E, SIGN, SyncBlock>(v, t, sm, map, tw);
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int p = t + TPL * m;
+                if constexpr (SIGN < 0) {
+                    const int ci = band_compact_index(a.band, p);
+                    if (ci >= 0) dst[((long)z * nb + ci) * nx + kx] = v[m];
+                } else {
+                    dst[((long)z * N + p) * nx + kx] = v[m];
+                }
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// z stage, forward (+ optional round trip).  grid = (G, narr); items (cy, tile).
+// One reduction record of MAX_RED partials per block.
+// ----------------------------------------------------------------------------
+template <int N, typename T>
+__global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
+    zfwd_c_kernel(ZFwdArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = CShape<N, T>;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* stw = sm + N * TX;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    __syncthreads();
+    const TwTab<N, E, T> tw{stw};
+    const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const ColMap<TX> map{l};
+    const int nx = a.nx, nb = a.band.nb;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)nb * ntile;
+    const ZFwdOp& op = a.op[blockIdx.y];
+    const long plane = (long)nb * nx;
+    const cpx<T>* __restrict__ src = reinterpret_cast<const cpx<T>*>(op.in);
+    cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
+    const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
+    double acc_self = 0.0, acc_w0 = 0.0, acc_w1 = 0.0, acc_w2 = 0.0;
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + l;
+        const bool ok = kx < nx;
+        cpx<T> v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int p = t + TPL * m;
+            v[m] = ok ? src[(long)p * plane + (long)cy * nx + kx] : czero<T>();
+        }
+        cfft<N, E, -1, SyncBlock>(v, t, sm, map, tw);
+        const int fy = band_fft_index(a.band, cy);
+        const double wgt = kx_weight(N, kx);
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int fz = t + TPL * m;
+            const int cz = band_compact_index(a.band, fz);
+            cpx<double> Y = mk(0.0, 0.0);
+            if (cz >= 0 && ok) {
+                const Kvec k = make_k(N, kx, fy, fz);
+                Y = apply_sym(op.sym, op.sym_ab, k, mk((double)v[m].x, (double)v[m].y) * a.norm);
+                const long si2 = ((long)cz * nb + cy) * nx + kx;
+                if (op.add)
+                    Y = Y + apply_sym(op.add_sym, op.add_ab, k, ld_spec(op.add, op.add_f64, si2)) * op.add_coef;
+                if (op.red_self >= 0) acc_self += wgt * (Y.x * Y.x + Y.y * Y.y);
+                if (op.red_with[0]) {
+                    const cpx<double> W = ld_spec(op.red_with[0], op.red_with_f64[0], si2);
+                    acc_w0 += wgt * (Y.x * W.x + Y.y * W.y);
+                }
+                if (op.red_with[1]) {
+                    const cpx<double> W = ld_spec(op.red_with[1], op.red_with_f64[1], si2);
+                    acc_w1 += wgt * (Y.x * W.x + Y.y * W.y);
+                }
+                if (op.red_with[2]) {
+                    const cpx<double> W = ld_spec(op.red_with[2], op.red_with_f64[2], si2);
+                    acc_w2 += wgt * (Y.x * W.x + Y.y * W.y);
+                }
+                if (op.spec_out) st_spec(op.spec_out, op.spec_f64, si2, Y);
+            }
+            v[m] = mk((T)Y.x, (T)Y.y);
+        }
+        if (yout) {
+            cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
+            if (ok) {
+#pragma unroll
+                for (int m = 0; m < E; ++m) yout[(long)(t + TPL * m) * plane + (long)cy * nx + kx] = v[m];
+            }
+        }
+    }
+    const int block_lin = blockIdx.y * gridDim.x + blockIdx.x;
+    double* part = a.partials + (long)block_lin * MAX_RED;
+    if (any_red) {
+        double acc4[4] = {acc_self, acc_w0, acc_w1, acc_w2};
+        __shared__ double part4[4];
+        block_reduce_to<4>(acc4, part4);
+        __syncthreads();
+        if (threadIdx.x < MAX_RED) {
+            double s = 0.0;
+            if ((int)threadIdx.x == op.red_self) s += part4[0];
+            for (int r = 0; r < 3; ++r)
+                if (op.red_with[r] && (int)threadIdx.x == op.red_with_slot[r]) s += part4[1 + r];
+            part[threadIdx.x] = s;
+        }
+    } else if (threadIdx.x < MAX_RED) {
+        part[threadIdx.x] = 0.0;
+    }
+}
+
+// ----------------------------------------------------------------------------
+// z stage, inverse from spectra.  grid = (G, narr); items (cy, tile).
+// ----------------------------------------------------------------------------
+template <int N, typename T>
+__global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
+    zinv_c_kernel(ZInvArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = CShape<N, T>;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* stw = sm + N * TX;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    __syncthreads();
+    const TwTab<N, E, T> tw{stw};
+    const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const ColMap<TX> map{l};
+    const int nx = a.nx, nb = a.band.nb;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)nb * ntile;
+    const ZInvOp& op = a.op[blockIdx.y];
+    const long plane = (long)nb * nx;
+    cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out);
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + l;
+        const bool ok = kx < nx;
+        const int fy = band_fft_index(a.band, cy);
+        cpx<T> v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int fz = t + TPL * m;
+            const int cz = band_compact_index(a.band, fz);
+            cpx<double> Y = mk(0.0, 0.0);
+            if (cz >= 0 && ok) {
+                const Kvec k = make_k(N, kx, fy, fz);
+                const long si2 = ((long)cz * nb + cy) * nx + kx;
+                for (int s = 0; s < op.nsrc; ++s)
+                    Y = Y + apply_sym(op.src[s].sym, op.src[s].ab, k, ld_spec(op.src[s].spec, op.src[s].f64, si2)) *
+                                op.src[s].coef;
+            }
+            v[m] = mk((T)Y.x, (T)Y.y);
+        }
+        cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) dst[(long)(t + TPL * m) * plane + (long)cy * nx + kx] = v[m];
+        }
+    }
+}
+
+}  // namespace mlq

@@ -1,16 +1,8 @@
-// engine.cu -- pipelines and programs of the B200 engine (see engine.cuh).
-#include "engine.cuh"
-
-#include <algorithm>
-#include <cstring>
-#include <set>
+// engine.cu -- the precision-independent part of the engine (see engine.cuh):
+// bands, twiddles, device memory, reductions, profiling, spectral state ops.
+#include "engine_common.cuh"
 
 namespace mlq {
-
-// ----------------------------------------------------------------------------
-// helpers
-// ----------------------------------------------------------------------------
-static const double PI_REF = 4.0 * std::atan2(1.0, 1.0);  // initialize.f90:164
 
 // dealiasing_cutoff_scalar_complex (function_ops.f90:3374, 3391): a mode is
 // removed when max_i |K_i| > 2 pi n/(order+1); |K| = 2 pi |j|.  Returns the
@@ -23,35 +15,6 @@ int band_cut_for_order(int n, double order) {
         if (!(std::fabs(K) > kcut)) cut = j;
     }
     return cut;
-}
-
-static std::vector<int> factor_radices(int L) {
-    std::vector<int> r;
-    int m = L;
-    while (m % 16 == 0 && m > 1) { r.push_back(16); m /= 16; }
-    while (m % 8 == 0) { r.push_back(8); m /= 8; }
-    while (m % 4 == 0) { r.push_back(4); m /= 4; }
-    while (m % 2 == 0) { r.push_back(2); m /= 2; }
-    while (m % 3 == 0) { r.push_back(3); m /= 3; }
-    if (m != 1) throw CudaError("FFT length must be 2^a 3^b", MLQ_ERR_BADARG);
-    return r;
-}
-
-// raise the dynamic shared memory limit of each kernel once (per device
-// function address: kernels of equal type are distinct entries)
-template <typename K>
-static void allow_smem(K kernel) {
-    static std::set<const void*> done;
-    const void* key = reinterpret_cast<const void*>(kernel);
-    if (done.insert(key).second) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) throw CudaError(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);
-    }
-}
-
-static int grid_for(long work, int threads, int cap = 148 * 8) {
-    long g = (work + threads - 1) / threads;
-    return (int)std::max(1L, std::min<long>(g, cap));
 }
 
 // ----------------------------------------------------------------------------
@@ -281,1508 +244,5 @@ void EngineBase::zeroth(const double2* f, double out[3]) {
     const double s = (double)n3;  // unnormalised k=0 coefficient (function_ops.f90:3084-3086)
     for (int c = 0; c < 3; ++c) out[c] = h[c].x * s;
 }
-
-// ----------------------------------------------------------------------------
-// Engine<T>: buffers
-// ----------------------------------------------------------------------------
-template <typename T>
-Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
-    nxcap = b2.nx;
-    nbcap = b2.nb;
-    // bands of fractional dealias orders reached by the |u|^k chains
-    auto widen = [&](double k) {
-        while (k + MACH_EPSILON >= 2.0) k -= 2.0;
-        if (k > 1.0) {
-            const Band b = make_band(band_cut_for_order(n, k));
-            nxcap = std::max(nxcap, b.nx);
-            nbcap = std::max(nbcap, b.nb);
-        }
-    };
-    widen(P.q - 2.0);
-    widen(P.q / 2.0);
-    if (!use_e_u) widen(P.q - 4.0);
-    reg_ok_ = n >= 64 && (n & (n - 1)) == 0;
-    ereg_ = (n > 512 && sizeof(T) == 4) ? 16 : 8;
-    long ntw = 0;
-    for (const auto& kv : tw_off) ntw = std::max<long>(ntw, kv.second + kv.first);
-    if (sizeof(T) == 8) {
-        d_twT_ = reinterpret_cast<cpx<T>*>(d_tw);
-    } else {
-        d_twT_ = (cpx<T>*)dev_alloc(ntw * sizeof(cpx<T>));
-        std::vector<cpx<double>> h(ntw);
-        MLQ_CUDA(cudaMemcpy(h.data(), d_tw, ntw * sizeof(cpx<double>), cudaMemcpyDeviceToHost));
-        std::vector<cpx<T>> hf(ntw);
-        for (long i = 0; i < ntw; ++i) hf[i] = mk<T>((T)h[i].x, (T)h[i].y);
-        MLQ_CUDA(cudaMemcpy(d_twT_, hf.data(), ntw * sizeof(cpx<T>), cudaMemcpyHostToDevice));
-    }
-}
-
-template <typename T>
-RPlan Engine<T>::rplan(int L) const {
-    RPlan p;
-    p.L = L;
-    p.nst = 0;
-    p.tw_off = tw_off.at(L);
-    int m = L;
-    for (int r : {16, 8, 4, 2}) {
-        if (r > ereg_) continue;
-        while (m % r == 0 && m > 1) {
-            p.radix[p.nst++] = r;
-            m /= r;
-        }
-    }
-    if (m != 1) throw CudaError("register FFT needs a power-of-two length", MLQ_ERR_BADARG);
-    return p;
-}
-
-// columns per y/z tile: up to 128-byte rows within a 256-thread block
-template <typename T>
-int Engine<T>::reg_tx() const {
-    const int nT = n / ereg_;
-    int tx = 128 / (int)sizeof(cpx<T>);
-    while (tx > 1 && (tx * nT > 256 || (size_t)n * tx * sizeof(cpx<T>) > 96 * 1024)) tx /= 2;
-    return tx;
-}
-
-// rows per x-stage block: nrows_per_line FFT rows of pitch `pitch` per line
-template <typename T>
-int Engine<T>::reg_lx(int nrows_per_line, size_t pitch) const {
-    const int nT = (n / 2) / ereg_;
-    int lx = 32;
-    while (lx > 1 && (nrows_per_line * lx * nT > 256 || nrows_per_line * lx * pitch * sizeof(cpx<T>) > 96 * 1024 ||
-                      ((long)n * n) % lx != 0))
-        lx /= 2;
-    return lx;
-}
-
-template <typename T>
-template <class F>
-void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b) {
-    const int h = n / 2;
-    const double bytes = (double)n3 * sizeof(T) * F::NIN + (double)n * n * b.nx * sizeof(cpx<T>) * nout;
-    if (reg_ok_) {
-        xa.lx = reg_lx(nout, row_pitch(h));
-        xa.tw_n_off = tw_off.at(n);
-        const int grid = (int)(((long)n * n) / xa.lx);
-        if (F::NRED > 0) ensure_partials((long)grid * F::NRED);
-        xa.partials = d_partials;
-        const size_t sm = (size_t)nout * xa.lx * row_pitch(h) * sizeof(cpx<T>);
-        const int thr = nout * xa.lx * (h / ereg_);
-        cudaEvent_t ev = prof_mark();
-        if (ereg_ == 8) {
-            allow_smem(xfwd_reg_kernel<8, T, F>);
-            xfwd_reg_kernel<8, T, F><<<grid, thr, sm, stream>>>(xa, f, rplan(h), d_twT_);
-        } else {
-            allow_smem(xfwd_reg_kernel<16, T, F>);
-            xfwd_reg_kernel<16, T, F><<<grid, thr, sm, stream>>>(xa, f, rplan(h), d_twT_);
-        }
-        launched("x_fwd", bytes, ev);
-        return;
-    }
-    xa.lx = lx_for(nout);
-    const int xgrid = (int)(((long)n * n) / xa.lx);
-    if (F::NRED > 0) ensure_partials((long)xgrid * F::NRED);
-    xa.partials = d_partials;
-    const size_t xsm = (size_t)2 * nout * xa.lx * h * sizeof(cpx<T>);
-    allow_smem(xfwd_kernel<T, F>);
-    cudaEvent_t ev = prof_mark();
-    xfwd_kernel<T, F><<<xgrid, 256, xsm, stream>>>(xa, f);
-    launched("x_fwd", bytes, ev);
-}
-
-template <typename T>
-void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
-    const double bytes = (double)narr * (n * (double)n * b.nx + n * (double)b.nb * b.nx) * sizeof(cpx<T>);
-    const char* nm = sign < 0 ? "y_fwd" : "y_inv";
-    if (reg_ok_) {
-        const int tx = reg_tx();
-        ya.tx = tx;
-        const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
-        dim3 g((b.nx + tx - 1) / tx, n, narr);
-        const int thr = tx * (n / ereg_);
-        cudaEvent_t ev = prof_mark();
-        if (ereg_ == 8) {
-            if (sign < 0) {
-                allow_smem(ypass_reg_kernel<8, -1, T>);
-                ypass_reg_kernel<8, -1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
-            } else {
-                allow_smem(ypass_reg_kernel<8, +1, T>);
-                ypass_reg_kernel<8, +1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
-            }
-        } else {
-            if (sign < 0) {
-                allow_smem(ypass_reg_kernel<16, -1, T>);
-                ypass_reg_kernel<16, -1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
-            } else {
-                allow_smem(ypass_reg_kernel<16, +1, T>);
-                ypass_reg_kernel<16, +1, T><<<g, thr, sm, stream>>>(ya, rplan(n), d_twT_);
-            }
-        }
-        launched(nm, bytes, ev);
-        return;
-    }
-    const int tx = tx_for();
-    ya.tx = tx;
-    ya.plan = plan(n);
-    ya.tw = d_tw;
-    const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
-    dim3 yg((b.nx + tx - 1) / tx, n, narr);
-    cudaEvent_t ev = prof_mark();
-    if (sign < 0) {
-        allow_smem(ypass_kernel<-1, T>);
-        ypass_kernel<-1, T><<<yg, 256, ysm, stream>>>(ya);
-    } else {
-        allow_smem(ypass_kernel<+1, T>);
-        ypass_kernel<+1, T><<<yg, 256, ysm, stream>>>(ya);
-    }
-    launched(nm, bytes, ev);
-}
-
-template <typename T>
-void Engine<T>::launch_zfwd(ZFwdArgs<T>& za, int narr, const Band& b, bool any_rt, double zbytes) {
-    const int tx = reg_ok_ ? reg_tx() : tx_for();
-    za.tx = tx;
-    dim3 zg((b.nx + tx - 1) / tx, b.nb, narr);
-    const long zblocks = (long)zg.x * zg.y * zg.z;
-    ensure_partials(zblocks * MAX_RED);
-    za.partials = d_partials;
-    if (reg_ok_) {
-        const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
-        const int thr = tx * (n / ereg_);
-        cudaEvent_t ev = prof_mark();
-        if (ereg_ == 8) {
-            allow_smem(zfwd_reg_kernel<8, T>);
-            zfwd_reg_kernel<8, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
-        } else {
-            allow_smem(zfwd_reg_kernel<16, T>);
-            zfwd_reg_kernel<16, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
-        }
-        launched(any_rt ? "z_roundtrip" : "z_fwd", zbytes, ev);
-    } else {
-        za.plan = plan(n);
-        za.tw = d_tw;
-        const size_t sm = (size_t)2 * n * tx * sizeof(cpx<T>);
-        allow_smem(zfwd_kernel<T>);
-        cudaEvent_t ev = prof_mark();
-        zfwd_kernel<T><<<zg, 256, sm, stream>>>(za);
-        launched(any_rt ? "z_roundtrip" : "z_fwd", zbytes, ev);
-    }
-    last_zblocks_ = zblocks;
-}
-
-template <typename T>
-void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zbytes) {
-    const int tx = reg_ok_ ? reg_tx() : tx_for();
-    za.tx = tx;
-    dim3 zg((b.nx + tx - 1) / tx, b.nb, narr);
-    if (reg_ok_) {
-        const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
-        const int thr = tx * (n / ereg_);
-        cudaEvent_t ev = prof_mark();
-        if (ereg_ == 8) {
-            allow_smem(zinv_reg_kernel<8, T>);
-            zinv_reg_kernel<8, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
-        } else {
-            allow_smem(zinv_reg_kernel<16, T>);
-            zinv_reg_kernel<16, T><<<zg, thr, sm, stream>>>(za, rplan(n), d_twT_);
-        }
-        launched("z_inv", zbytes, ev);
-    } else {
-        za.plan = plan(n);
-        za.tw = d_tw;
-        const size_t sm = (size_t)2 * n * tx * sizeof(cpx<T>);
-        allow_smem(zinv_kernel<T>);
-        cudaEvent_t ev = prof_mark();
-        zinv_kernel<T><<<zg, 256, sm, stream>>>(za);
-        launched("z_inv", zbytes, ev);
-    }
-}
-
-template <typename T>
-void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
-    const int h = n / 2;
-    const double bytes = (double)narr * ((double)n * n * b.nx * sizeof(cpx<T>) + (double)n3 * sizeof(T));
-    xa.tw_n_off = tw_off.at(n);
-    if (reg_ok_) {
-        xa.lx = reg_lx(1, row_pitch(h + 1));
-        const size_t sm = (size_t)xa.lx * row_pitch(h + 1) * sizeof(cpx<T>);
-        dim3 xg((unsigned)(((long)n * n) / xa.lx), narr);
-        const int thr = xa.lx * (h / ereg_);
-        cudaEvent_t ev = prof_mark();
-        if (ereg_ == 8) {
-            allow_smem(xinv_reg_kernel<8, T>);
-            xinv_reg_kernel<8, T><<<xg, thr, sm, stream>>>(xa, rplan(h), d_twT_);
-        } else {
-            allow_smem(xinv_reg_kernel<16, T>);
-            xinv_reg_kernel<16, T><<<xg, thr, sm, stream>>>(xa, rplan(h), d_twT_);
-        }
-        launched("x_inv", bytes, ev);
-        return;
-    }
-    const size_t per = (size_t)(3 * h + 1) * sizeof(cpx<T>);
-    int lx = 8;
-    while (lx > 1 && (per * lx > 96 * 1024 || ((long)n * n) % lx != 0)) lx /= 2;
-    xa.lx = lx;
-    xa.plan_half = plan(h);
-    xa.tw = d_tw;
-    allow_smem(xinv_kernel<T>);
-    dim3 xg((unsigned)(((long)n * n) / lx), narr);
-    cudaEvent_t ev = prof_mark();
-    xinv_kernel<T><<<xg, 256, per * lx, stream>>>(xa);
-    launched("x_inv", bytes, ev);
-}
-
-template <typename T>
-Engine<T>::~Engine() {
-    if (h_stage_) cudaFreeHost(h_stage_);
-}
-
-template <typename T>
-T* Engine<T>::phys(int i) {
-    if ((int)phys_.size() <= i) phys_.resize(i + 1, nullptr);
-    if (!phys_[i]) phys_[i] = (T*)dev_alloc(n3 * sizeof(T));
-    return phys_[i];
-}
-template <typename T>
-cpx<T>* Engine<T>::xsbuf(int i) {
-    if ((int)xs_.size() <= i) xs_.resize(i + 1, nullptr);
-    if (!xs_[i]) xs_[i] = (cpx<T>*)dev_alloc((size_t)n * n * nxcap * sizeof(cpx<T>));
-    return xs_[i];
-}
-template <typename T>
-cpx<T>* Engine<T>::ysbuf(int i) {
-    if ((int)ys_.size() <= i) ys_.resize(i + 1, nullptr);
-    if (!ys_[i]) ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * nxcap * sizeof(cpx<T>));
-    return ys_[i];
-}
-template <typename T>
-cpx<T>* Engine<T>::wspec(int i) {
-    if ((int)ws_.size() <= i) ws_.resize(i + 1, nullptr);
-    if (!ws_[i]) ws_[i] = (cpx<T>*)dev_alloc((size_t)spec_ncomp() * sizeof(cpx<T>));
-    return ws_[i];
-}
-
-template <typename T>
-void* Engine<T>::stage(size_t b) {
-    if (b > h_stage_bytes_) {
-        if (h_stage_) cudaFreeHost(h_stage_);
-        MLQ_CUDA(cudaMallocHost((void**)&h_stage_, b));
-        h_stage_bytes_ = b;
-    }
-    return h_stage_;
-}
-
-template <typename T>
-int Engine<T>::lx_for(int nout, size_t extra) const {
-    const size_t per = (size_t)2 * std::max(nout, 1) * (n / 2) * sizeof(cpx<T>) + extra;
-    int lx = 8;
-    while (lx > 1 && (per * lx > 96 * 1024 || ((long)n * n) % lx != 0)) lx /= 2;
-    return lx;
-}
-
-template <typename T>
-int Engine<T>::tx_for() const {
-    int tx = 16;
-    while (tx > 1 && (size_t)2 * n * tx * sizeof(cpx<T>) > 96 * 1024) tx /= 2;
-    return tx;
-}
-
-// ----------------------------------------------------------------------------
-// pipelines
-// ----------------------------------------------------------------------------
-template <typename T>
-template <class F>
-void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, std::vector<FwdOut> outs,
-                    int red_dst, int fred_dst, double norm) {
-    constexpr int NOUT = F::NOUT;
-    static_assert(NOUT <= MAX_ARR, "too many outputs");
-    if ((int)in.size() != F::NIN || (int)outs.size() != NOUT) throw CudaError("fwd: arity", MLQ_ERR_BADARG);
-    if (b.nx > nxcap || b.nb > nbcap) throw CudaError("fwd: band exceeds buffers", MLQ_ERR_BADARG);
-    const int h = n / 2;
-    // x stage
-    XFwdArgs<T> xa;
-    xa.n = n;
-    xa.nx = b.nx;
-    for (int i = 0; i < F::NIN; ++i) xa.in[i] = in[i];
-    for (int o = 0; o < NOUT; ++o) xa.out[o] = xsbuf(o);
-    xa.plan_half = plan(h);
-    xa.tw_n_off = tw_off.at(n);
-    xa.tw = d_tw;
-    launch_xfwd(xa, f, NOUT, b);
-    const int xgrid = (int)(((long)n * n) / xa.lx);
-    if (F::NRED > 0 && fred_dst >= 0) finalize(xgrid, F::NRED, 1.0 / (double)n3, fred_dst);
-    if (NOUT == 0) return;
-    // y forward
-    YArgs<T> ya;
-    ya.n = n;
-    ya.nx = b.nx;
-    ya.band = b;
-    for (int o = 0; o < NOUT; ++o) {
-        ya.in[o] = xsbuf(o);
-        ya.out[o] = ysbuf(o);
-    }
-    launch_y(ya, -1, NOUT, b);
-    // z stage
-    ZFwdArgs<T> za;
-    za.n = n;
-    za.nx = b.nx;
-    za.band = b;
-    bool any_rt = false;
-    for (int o = 0; o < NOUT; ++o) {
-        const FwdOut& fo = outs[o];
-        ZFwdOp& op = za.op[o];
-        op.in = ysbuf(o);
-        op.spec_out = fo.spec;
-        op.spec_f64 = fo.spec_f64;
-        op.ys_out = fo.phys_out >= 0 ? (void*)ysbuf(o) : nullptr;
-        any_rt |= fo.phys_out >= 0;
-        op.sym = fo.sym;
-        op.sym_ab = fo.ab;
-        op.add = fo.add;
-        op.add_f64 = fo.add_f64;
-        op.add_sym = fo.add_sym;
-        op.add_ab = fo.add_ab;
-        op.add_coef = fo.add_coef;
-        op.red_self = fo.red_self;
-        for (int r = 0; r < 3; ++r) {
-            op.red_with[r] = fo.red_with[r];
-            op.red_with_f64[r] = fo.red_with_f64[r];
-            op.red_with_slot[r] = fo.red_with_slot[r];
-        }
-    }
-    za.norm = norm > 0 ? norm : 1.0 / (double)n3;
-    double zbytes = 0;
-    {
-        const double ys_b = (double)n * b.nb * b.nx * sizeof(cpx<T>);
-        const double sp_elems = (double)b.nb * b.nb * b.nx;
-        for (int o = 0; o < NOUT; ++o) {
-            const FwdOut& fo = outs[o];
-            zbytes += ys_b;
-            if (fo.spec) zbytes += sp_elems * (fo.spec_f64 ? 16 : 8);
-            if (fo.phys_out >= 0) zbytes += ys_b;
-            if (fo.add) zbytes += sp_elems * (fo.add_f64 ? 16 : 8);
-            for (int r = 0; r < 3; ++r)
-                if (fo.red_with[r]) zbytes += sp_elems * (fo.red_with_f64[r] ? 16 : 8);
-        }
-    }
-    launch_zfwd(za, NOUT, b, any_rt, zbytes);
-    const long zblocks = last_zblocks_;
-    if (red_dst >= 0) finalize((int)zblocks, MAX_RED, 1.0, red_dst);
-    if (any_rt) {
-        std::vector<cpx<T>*> ys;
-        std::vector<int> po;
-        for (int o = 0; o < NOUT; ++o)
-            if (outs[o].phys_out >= 0) {
-                ys.push_back(ysbuf(o));
-                po.push_back(outs[o].phys_out);
-            }
-        yx_inverse(b, ys, po);
-    }
-}
-
-template <typename T>
-void Engine<T>::yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const std::vector<int>& phys_out) {
-    const int k = (int)ys.size();
-    if (k == 0) return;
-    // y inverse: ys[i] -> xs (xs buffers are free once the forward's y pass ran)
-    YArgs<T> ya;
-    ya.n = n;
-    ya.nx = b.nx;
-    ya.band = b;
-    std::vector<cpx<T>*> xs(k);
-    for (int i = 0; i < k; ++i) {
-        xs[i] = xsbuf(i);
-        ya.in[i] = ys[i];
-        ya.out[i] = xs[i];
-    }
-    launch_y(ya, +1, k, b);
-    // x inverse
-    XInvArgs<T> xa;
-    xa.n = n;
-    xa.nx_in = b.nx;
-    for (int i = 0; i < k; ++i) {
-        xa.in[i] = xs[i];
-        xa.out[i] = phys(phys_out[i]);
-    }
-    xa.plan_half = plan(n / 2);
-    xa.tw = d_tw;
-    launch_xinv(xa, k, b);
-}
-
-template <typename T>
-void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
-    if (b.nx > nxcap || b.nb > nbcap) throw CudaError("inv: band exceeds buffers", MLQ_ERR_BADARG);
-    const int G = 6;
-    for (size_t g0 = 0; g0 < outs.size(); g0 += G) {
-        const int k = (int)std::min<size_t>(G, outs.size() - g0);
-        ZInvArgs<T> za;
-        za.n = n;
-        za.nx = b.nx;
-        za.band = b;
-        std::vector<cpx<T>*> ys(k);
-        std::vector<int> po(k);
-        for (int i = 0; i < k; ++i) {
-            const InvOut& io = outs[g0 + i];
-            ZInvOp& op = za.op[i];
-            for (int s = 0; s < 3; ++s) op.src[s] = io.src[s];
-            op.nsrc = io.nsrc;
-            ys[i] = ysbuf(i);
-            op.ys_out = ys[i];
-            po[i] = io.phys_out;
-        }
-        double zb = 0;
-        for (int i = 0; i < k; ++i) {
-            const InvOut& io = outs[g0 + i];
-            zb += (double)n * b.nb * b.nx * sizeof(cpx<T>);
-            for (int s2 = 0; s2 < io.nsrc; ++s2) zb += (double)b.nb * b.nb * b.nx * (io.src[s2].f64 ? 16 : 8);
-        }
-        launch_zinv(za, k, b, zb);
-        yx_inverse(b, ys, po);
-    }
-}
-
-template <typename T>
-template <class F>
-void Engine<T>::pointwise(const F& f, const std::vector<const T*>& in, const std::vector<T*>& out, int fred_dst) {
-    PArgs<T> a;
-    a.npts = n3;
-    for (int i = 0; i < F::NIN; ++i) a.in[i] = in[i];
-    for (int o = 0; o < F::NOUT; ++o) a.out[o] = out[o];
-    const int grid = grid_for(n3, RED_THREADS, 148 * 8);
-    ensure_partials((long)grid * std::max(F::NRED, 1));
-    a.partials = d_partials;
-    cudaEvent_t ev = prof_mark();
-    pointwise_kernel<T, F><<<grid, RED_THREADS, 0, stream>>>(a, f);
-    launched("pointwise", (double)n3 * sizeof(T) * (F::NIN + F::NOUT), ev);
-    if (F::NRED > 0 && fred_dst >= 0) finalize(grid, F::NRED, 1.0 / (double)n3, fred_dst);
-}
-
-// ----------------------------------------------------------------------------
-// programs
-// ----------------------------------------------------------------------------
-namespace {
-// physical scratch indices
-enum : int {
-    PU = 0,    // 0..2   u (or phi, w)
-    PD = 3,    // 3..11  d_j u_i at 3+3i+j
-    PL = 12,   // 12..14 Lap u
-    PGP = 15,  // 15..17 grad p
-    PS = 18,   // S = P2(|u|^2)
-    PA = 19,   // A = P2(g^2)
-    PV = 20,   // 20..22 V_j / E_j
-    PP = 23,   // p
-    PT = 24,   // aux2
-    PGA = 25,  // 25..27 grad aux4
-    PONES = 28,
-    PCH = 29,  // 29..39 chain fields
-    PIO = 40,  // host transfer scratch
-    PIO2 = 41,
-};
-// work spectra (band b2)
-enum : int { WG2 = 0, WA = 1, WP = 2, WT = 3 /*3..5*/, WONE = 6, WCH = 7 /*7..*/ };
-}  // namespace
-
-template <typename T>
-static constexpr int wf64() {
-    return sizeof(T) == 8 ? 1 : 0;
-}
-
-template <typename T>
-__global__ void fill_kernel(T* p, long cnt, T v) {
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (long)gridDim.x * blockDim.x) p[i] = v;
-}
-
-// Fourier coefficients of the constant 1 in band b2: a unit k=0 mode.
-template <typename T>
-cpx<T>* Engine<T>::ones_spec() {
-    static_assert(sizeof(cpx<T>) == 2 * sizeof(T), "layout");
-    const bool fresh = (int)ws_.size() <= WONE || ws_[WONE] == nullptr;
-    cpx<T>* w = wspec(WONE);
-    if (fresh) {
-        MLQ_CUDA(cudaMemsetAsync(w, 0, spec_ncomp() * sizeof(cpx<T>), stream));
-        const cpx<T> one = mk<T>(T(1), T(0));
-        MLQ_CUDA(cudaMemcpyAsync(w, &one, sizeof(cpx<T>), cudaMemcpyHostToDevice, stream));
-        MLQ_CUDA(cudaStreamSynchronize(stream));
-    }
-    return w;
-}
-
-template <typename T>
-void Engine<T>::ensure_phys(PowField& f) {
-    if (f.phys >= 0) return;
-    if (f.kind == PowField::ONE) {
-        if ((int)phys_.size() <= PONES || phys_[PONES] == nullptr) {
-            fill_kernel<T><<<grid_for(n3, 256), 256, 0, stream>>>(phys(PONES), n3, T(1));
-            launched();
-        }
-        f.phys = PONES;
-        return;
-    }
-    throw CudaError("power field without physical values", MLQ_ERR_CUDA);
-}
-
-// make sure a power field has a spectrum in band b2
-template <typename T>
-void Engine<T>::ensure_p2_spec(PowField& f) {
-    if (f.spec >= 0) return;
-    if (f.kind == PowField::ONE) {
-        ones_spec();
-        f.spec = WONE;
-        return;
-    }
-    f.spec = WCH + 16 + spec_next_++;
-    FwdOut o;
-    o.spec = wspec(f.spec);
-    o.spec_f64 = wf64<T>();
-    fwd(b2, FCopy{}, {phys(f.phys)}, {o});
-}
-
-// S = P2(|u|^2) (calc_uk 2332-2333) must already be in phys(PS) ; computes
-// A = P2(g^2), g = sqrt(max(S,0)) (2335-2339, 2309-2310): spectrum WA and,
-// when asked, phys(PA).
-template <typename T>
-void Engine<T>::A_and_S(bool need_A_phys) {
-    FwdOut oA;
-    oA.spec = wspec(WA);
-    oA.spec_f64 = wf64<T>();
-    if (need_A_phys) oA.phys_out = PA;
-    fwd(b2, FGSq{}, {phys(PS)}, {oA});
-}
-
-// calc_gk_order2 (function_ops.f90:2281-2319) on g = sqrt(max(S,0)), with
-// A = P2(g^2) already computed.  Every branch produces the same field as the
-// reference up to rounding: an order <= 1 dealias removes nothing, g**0 is 1,
-// and P2(A*1) = A.
-template <typename T>
-PowField Engine<T>::chain(double k) {
-    auto it = memo_.find(k);
-    if (it != memo_.end()) return it->second;
-    PowField f;
-    f.k = k;
-    if (k + MACH_EPSILON < 0.0) {
-        f.kind = PowField::RAW;
-        f.phys = PCH + tmp_next_++;
-        FGPow fp;
-        fp.k = k;
-        fp.thresh = 1;
-        pointwise(fp, {phys(PS)}, {phys(f.phys)});
-    } else if (k + MACH_EPSILON < 2.0) {
-        const int c = band_cut_for_order(n, k);
-        if (c >= n / 2) {
-            if (k == 0.0) {
-                f.kind = PowField::ONE;
-            } else {
-                f.kind = PowField::RAW;
-                f.phys = PCH + tmp_next_++;
-                FGPow fp;
-                fp.k = k;
-                fp.thresh = 0;
-                pointwise(fp, {phys(PS)}, {phys(f.phys)});
-            }
-        } else {
-            const Band bk = make_band(c);
-            f.kind = PowField::BAND;
-            f.phys = PCH + tmp_next_++;
-            FGPow fp;
-            fp.k = k;
-            fp.thresh = 0;
-            FwdOut o;
-            o.phys_out = f.phys;
-            if (c == b2.cut) {
-                f.spec = WCH + spec_next_++;
-                o.spec = wspec(f.spec);
-                o.spec_f64 = wf64<T>();
-            }
-            fwd(bk, fp, {phys(PS)}, {o});
-        }
-    } else {
-        PowField prev = chain(k - 2.0);
-        f.kind = PowField::BAND;
-        if (prev.kind == PowField::ONE) {
-            f.phys = PA;
-            f.spec = WA;
-        } else {
-            ensure_phys(prev);
-            f.phys = PCH + tmp_next_++;
-            f.spec = WCH + spec_next_++;
-            FwdOut o;
-            o.phys_out = f.phys;
-            o.spec = wspec(f.spec);
-            o.spec_f64 = wf64<T>();
-            fwd(b2, FMul{}, {phys(PA), phys(prev.phys)}, {o});
-        }
-    }
-    memo_[k] = f;
-    return f;
-}
-
-// scalar Parseval dots of band-b2 work spectra
-template <typename T>
-struct SDotArgs {
-    SpecGeom g;
-    const cpx<T>* a[6];
-    const cpx<T>* b[6];
-    int np;
-    double* partials;
-};
-
-template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) spec_sdot_kernel(SDotArgs<T> a) {
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < a.g.ncomp; i += (long)gridDim.x * blockDim.x) {
-        const int fx = (int)(i % a.g.nx);
-        const double w = kx_weight(a.g.n, fx);
-        for (int p = 0; p < a.np; ++p) {
-            const cpx<T> u = a.a[p][i], v = a.b[p][i];
-            acc[p] += w * ((double)u.x * (double)v.x + (double)u.y * (double)v.y);
-        }
-    }
-    block_reduce_store<6>(acc, a.partials, blockIdx.x);
-}
-
-template <typename T>
-static void sdots(Engine<T>& e, const std::vector<std::pair<const cpx<T>*, const cpx<T>*>>& pr, int dst) {
-    if (pr.size() > 6) throw CudaError("sdots: too many pairs", MLQ_ERR_BADARG);
-    SDotArgs<T> a;
-    a.g = e.geom(e.b2);
-    a.np = (int)pr.size();
-    for (int i = 0; i < a.np; ++i) {
-        a.a[i] = pr[i].first;
-        a.b[i] = pr[i].second;
-    }
-    const int grid = grid_for(a.g.ncomp, RED_THREADS, 148 * 4);
-    e.ensure_partials((long)grid * 6);
-    a.partials = e.d_partials;
-    cudaEvent_t ev = e.prof_mark();
-    spec_sdot_kernel<T><<<grid, RED_THREADS, 0, e.stream>>>(a);
-    e.launched("spec_sdot", 2.0 * a.np * a.g.ncomp * sizeof(cpx<T>), ev);
-    e.finalize(grid, 6, 1.0, dst);
-}
-
-// calc_local_dLqdt_inclParts (function_ops.f90:1304-1358) at phi = u + tau d,
-// together with ||phi||_q^q (calc_global_Lq_norm 1675-1692).  Products are
-// dealiased as the reference does; a dealias that is immediately followed by
-// an L2 inner product with a band-limited field is applied through Parseval
-// on the band instead of by a round trip (the projection is self-adjoint).
-template <typename T>
-void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double out[3], double* lqq) {
-    const Band& b = b2;
-    const long nc = spec_ncomp();
-    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
-    chain_reset();
-    // 1. phi and grad phi
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i)
-        for (int j = -1; j < 3; ++j) {
-            InvOut o;
-            o.nsrc = d ? 2 : 1;
-            const int sym = j < 0 ? SYM_ONE : SYM_IKX + j;
-            o.src[0] = ZSrc{u + i * nc, 1, sym, 0, 1.0};
-            if (d) o.src[1] = ZSrc{d + i * nc, 1, sym, 0, tau};
-            o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
-            io.push_back(o);
-        }
-    inv(b, io);
-    std::vector<const T*> uin;
-    for (int i = 0; i < 3; ++i) uin.push_back(phys(PU + i));
-    for (int i = 0; i < 9; ++i) uin.push_back(phys(PD + i));
-    // 2. first products: |u|^2 -> P2, W_j -> P2 (q>=4), grad u:grad u^T -> p,
-    //    |grad u|^2 -> spectrum
-    FwdOut oS, oQ, oG2;
-    oS.phys_out = PS;
-    oQ.sym = SYM_INV_KSQ;  // p = -Lap^-1 P2(grad u : grad u^T) (1339-1340)
-    oQ.phys_out = PP;
-    oG2.spec = wspec(WG2);
-    oG2.spec_f64 = wf64<T>();
-    if (!use_e_u) {
-        FwdOut oW[3];
-        for (int j = 0; j < 3; ++j) oW[j].phys_out = PV + j;
-        fwd(b, FRProd{}, uin, {oS, oW[0], oW[1], oW[2], oQ, oG2});
-    } else {
-        fwd(b, FRProdE{}, uin, {oS, oQ, oG2});
-    }
-    // 3. |u|^k fields
-    const bool needA = !(q == 4.0 && !use_e_u);  // for q = 4 only the spectrum of A is read
-    A_and_S(needA);
-    PowField a2 = chain(q - 2.0);
-    PowField a4;
-    if (!use_e_u) a4 = chain(q - 4.0);
-    PowField ah = chain(q / 2.0);
-    std::vector<std::pair<const cpx<T>*, const cpx<T>*>> pr;
-    // R1 = -vc nu <a2, P2|grad u|^2>  (1318)
-    ensure_p2_spec(a2);
-    pr.push_back({wspec(a2.spec), wspec(WG2)});
-    // ||phi||_q^q = int (|u|^{q/2})^2
-    bool norm_raw = false;
-    if (ah.kind == PowField::RAW) {
-        norm_raw = true;
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
-    } else if (ah.spec < 0) {
-        // a band-limited power in a wider band than P2: its full spectrum is
-        // needed; integrate its square in physical space instead
-        norm_raw = true;
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
-    } else {
-        if (ah.kind == PowField::ONE) ensure_p2_spec(ah);
-        pr.push_back({wspec(ah.spec), wspec(ah.spec)});
-    }
-    const bool direct = !use_e_u && a4.kind == PowField::ONE;
-    if (direct) {
-        // |u|^{q-4} = 1: R2 = -(q-2) vc nu int sum V^2, R3 = (q-2) pc int p u.V
-        pointwise(FRRed1{}, {phys(PV), phys(PV + 1), phys(PV + 2), phys(PP), phys(PU), phys(PU + 1), phys(PU + 2)},
-                  {}, 16);
-    } else if (!use_e_u) {
-        ensure_phys(a4);
-        ensure_p2_spec(a4);
-        FwdOut o[3];
-        for (int i = 0; i < 3; ++i) {
-            o[i].spec = wspec(WT + i);
-            o[i].spec_f64 = wf64<T>();
-        }
-        fwd(b, FRProd2{},
-            {phys(PV), phys(PV + 1), phys(PV + 2), phys(PP), phys(PU), phys(PU + 1), phys(PU + 2), phys(a4.phys)},
-            {o[0], o[1], o[2]});
-        pr.push_back({wspec(a4.spec), wspec(WT)});
-        pr.push_back({wspec(WT + 1), wspec(WT + 2)});
-    } else {
-        // E_j = P2(sum_i e_i d_j u_i) (calc_vgraduvgradu / calc_vvgradu, v = e_u)
-        std::vector<const T*> ein = uin;
-        ein.push_back(phys(PS));
-        FwdOut oE[3];
-        for (int j = 0; j < 3; ++j) oE[j].phys_out = PV + j;
-        fwd(b, FRE{}, ein, {oE[0], oE[1], oE[2]});
-        ensure_phys(a2);
-        FwdOut o[3];
-        for (int i = 0; i < 3; ++i) {
-            o[i].spec = wspec(WT + i);
-            o[i].spec_f64 = wf64<T>();
-        }
-        fwd(b, FRProd2E{},
-            {phys(PV), phys(PV + 1), phys(PV + 2), phys(PP), phys(PU), phys(PU + 1), phys(PU + 2), phys(PS),
-             phys(a2.phys)},
-            {o[0], o[1], o[2]});
-        pr.push_back({wspec(a2.spec), wspec(WT)});
-        pr.push_back({wspec(WT + 1), wspec(WT + 2)});
-    }
-    sdots(*this, pr, 0);
-    fetch_results();
-    int idx = 0;
-    const double I1 = h_results[idx++];
-    const double nrm = norm_raw ? h_results[20] : h_results[idx++];
-    double I2, I3;
-    if (direct) {
-        I2 = h_results[16];
-        I3 = h_results[17];
-    } else {
-        I2 = h_results[idx++];
-        I3 = h_results[idx++];
-    }
-    const double R1 = -cv * I1;
-    const double R2 = -cv * (q - 2.0) * I2;
-    const double R3 = cp * (q - 2.0) * I3;
-    out[0] = R1 + R2 + R3;
-    out[1] = R1 + R2;
-    out[2] = R3;
-    if (lqq) *lqq = nrm;
-}
-
-// GradL2ForLq (function_ops.f90:1066-1211).  Each of the reference's five
-// terms is a dealiased product; their sum is dealiased once (the projection
-// is linear), the fifth term nu Lap P2(|u|^{q-2}u) is added in the spectrum.
-template <typename T>
-void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
-    const Band& b = b2;
-    const long nc = spec_ncomp();
-    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
-    if (!c) throw CudaError("grad_l2 needs a spectrum buffer for |u|^{q-2}u", MLQ_ERR_BADARG);
-    chain_reset();
-    // 1. u, grad u, Lap u
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i) {
-        for (int j = -1; j < 3; ++j) {
-            InvOut o;
-            o.nsrc = 1;
-            o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
-            o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
-            io.push_back(o);
-        }
-        InvOut o;
-        o.nsrc = 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_NEG_KSQ, 0, 1.0};  // laplacian (3248-3282)
-        o.phys_out = PL + i;
-        io.push_back(o);
-    }
-    inv(b, io);
-    std::vector<const T*> uin;
-    for (int i = 0; i < 3; ++i) uin.push_back(phys(PU + i));
-    for (int i = 0; i < 9; ++i) uin.push_back(phys(PD + i));
-    // 2. S -> P2, Q -> p spectrum (1102-1107)
-    {
-        FwdOut oS, oQ;
-        oS.phys_out = PS;
-        oQ.sym = SYM_INV_KSQ;
-        oQ.spec = wspec(WP);
-        oQ.spec_f64 = wf64<T>();
-        fwd(b, FG1{}, uin, {oS, oQ});
-    }
-    // 3. grad p (1109)
-    {
-        std::vector<InvOut> g;
-        for (int j = 0; j < 3; ++j) {
-            InvOut o;
-            o.nsrc = 1;
-            o.src[0] = ZSrc{wspec(WP), wf64<T>(), SYM_IKX + j, 0, 1.0};
-            o.phys_out = PGP + j;
-            g.push_back(o);
-        }
-        inv(b, g);
-    }
-    // 4. |u|^k fields
-    A_and_S(true);
-    PowField a2 = chain(q - 2.0);
-    PowField a4;
-    if (!use_e_u) a4 = chain(q - 4.0);
-    PowField ah = chain(q / 2.0);
-    ensure_phys(a2);
-    // 5. aux2 and c = P2(a2 u) (1115-1153)
-    {
-        FwdOut oT, oc[3];
-        oT.phys_out = PT;
-        for (int i = 0; i < 3; ++i) {
-            oc[i].spec = c + i * nc;
-            oc[i].spec_f64 = 1;
-        }
-        std::vector<const T*> in2;
-        for (int i = 0; i < 3; ++i) in2.push_back(phys(PU + i));
-        for (int i = 0; i < 3; ++i) in2.push_back(phys(PL + i));
-        for (int i = 0; i < 3; ++i) in2.push_back(phys(PGP + i));
-        in2.push_back(phys(a2.phys));
-        if (!use_e_u) {
-            FG2 f;
-            f.cvisc = cv;
-            f.cpress = cp;
-            fwd(b, f, in2, {oT, oc[0], oc[1], oc[2]});
-            if (a4.kind != PowField::ONE) {
-                ensure_phys(a4);
-                FwdOut o;
-                o.phys_out = PT;
-                fwd(b, FMul{}, {phys(a4.phys), phys(PT)}, {o});
-            }
-        } else {
-            FG2E f;
-            f.cvisc = cv;
-            f.cpress = cp;
-            in2.push_back(phys(PS));
-            fwd(b, f, in2, {oT, oc[0], oc[1], oc[2]});
-            FwdOut o;
-            o.phys_out = PT;
-            fwd(b, FMul{}, {phys(a2.phys), phys(PT)}, {o});
-        }
-    }
-    // 6. grad aux4 = grad Lap^-1 div c (1155-1158)
-    {
-        std::vector<InvOut> g;
-        for (int k = 0; k < 3; ++k) {
-            InvOut o;
-            o.nsrc = 3;
-            for (int j = 0; j < 3; ++j) o.src[j] = ZSrc{c + j * nc, 1, SYM_KK_KSQ, 3 * k + j, 1.0};
-            o.phys_out = PGA + k;
-            g.push_back(o);
-        }
-        inv(b, g);
-    }
-    // 7. final sum, one dealias, plus vc nu Lap c (1172-1190)
-    {
-        std::vector<const T*> in3;
-        in3.push_back(phys(PT));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PU + i));
-        in3.push_back(phys(a2.phys));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PGP + i));
-        for (int i = 0; i < 9; ++i) in3.push_back(phys(PD + i));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PGA + i));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PL + i));
-        FwdOut o[3];
-        for (int i = 0; i < 3; ++i) {
-            o[i].spec = v + i * nc;
-            o[i].spec_f64 = 1;
-            o[i].add = c + i * nc;
-            o[i].add_f64 = 1;
-            o[i].add_sym = SYM_NEG_KSQ;
-            o[i].add_coef = cv;
-        }
-        if (!use_e_u) {
-            FG3<false> f;
-            f.qm2 = q - 2.0;
-            f.cvisc = cv;
-            f.cpress = cp;
-            fwd(b, f, in3, {o[0], o[1], o[2]});
-        } else {
-            FG3<true> f;
-            f.qm2 = q - 2.0;
-            f.cvisc = cv;
-            f.cpress = cp;
-            in3.push_back(phys(PS));
-            fwd(b, f, in3, {o[0], o[1], o[2]});
-        }
-    }
-    if (lqq) {
-        if (ah.kind == PowField::RAW || ah.spec < 0) {
-            pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
-            fetch_results();
-            *lqq = h_results[20];
-        } else {
-            ensure_p2_spec(ah);
-            sdots(*this, {{wspec(ah.spec), wspec(ah.spec)}}, 0);
-            fetch_results();
-            *lqq = h_results[0];
-        }
-    }
-}
-
-// ||u + tau d||_q^q (calc_global_Lq_norm)
-template <typename T>
-double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
-    const long nc = spec_ncomp();
-    chain_reset();
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i) {
-        InvOut o;
-        o.nsrc = d ? 2 : 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-        if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
-        o.phys_out = PU + i;
-        io.push_back(o);
-    }
-    inv(b2, io);
-    FwdOut oS;
-    oS.phys_out = PS;
-    fwd(b2, FSq3{}, {phys(PU), phys(PU + 1), phys(PU + 2)}, {oS});
-    A_and_S(true);
-    PowField ah = chain(P.q / 2.0);
-    if (ah.kind == PowField::RAW || ah.spec < 0) {
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
-        fetch_results();
-        return h_results[20];
-    }
-    ensure_p2_spec(ah);
-    sdots(*this, {{wspec(ah.spec), wspec(ah.spec)}}, 0);
-    fetch_results();
-    return h_results[0];
-}
-
-// vectorTransport (function_ops.f90:1716-1768) pieces at w = u + tau d.
-template <typename T>
-double Engine<T>::transport_pieces(const double2* u, const double2* d, double tau, const double2* const* xi,
-                                   int nxi, double* ir) {
-    const long nc = spec_ncomp();
-    const double q = P.q;
-    chain_reset();
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i) {
-        InvOut o;
-        o.nsrc = d ? 2 : 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-        if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
-        o.phys_out = PU + i;
-        io.push_back(o);
-    }
-    inv(b2, io);
-    FwdOut oS;
-    oS.phys_out = PS;
-    fwd(b2, FSq3{}, {phys(PU), phys(PU + 1), phys(PU + 2)}, {oS});
-    A_and_S(true);
-    PowField a2 = chain(q - 2.0);
-    PowField ah = chain(q / 2.0);
-    if (!c_tmp_) c_tmp_ = alloc_state();
-    double2* cbuf = c_tmp_;
-    if (q - 2.0 > MACH_EPSILON) {
-        // aux = P2(|w|^{q-2} w) (1737-1740)
-        ensure_phys(a2);
-        FwdOut o[3];
-        for (int i = 0; i < 3; ++i) {
-            o[i].spec = cbuf + i * nc;
-            o[i].spec_f64 = 1;
-        }
-        fwd(b2, FC3{}, {phys(a2.phys), phys(PU), phys(PU + 1), phys(PU + 2)}, {o[0], o[1], o[2]});
-    } else {
-        if (a2.kind != PowField::ONE) throw CudaError("vectorTransport with 2 < q < 2+eps", MLQ_ERR_BADARG);
-        lincomb(cbuf, 1.0, u, d ? tau : 0.0, d, 0.0, nullptr);
-    }
-    double lqq;
-    if (ah.kind == PowField::RAW || ah.spec < 0) {
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
-        fetch_results();
-        lqq = h_results[20];
-    } else {
-        ensure_p2_spec(ah);
-        sdots(*this, {{wspec(ah.spec), wspec(ah.spec)}}, 0);
-        fetch_results();
-        lqq = h_results[0];
-    }
-    for (int k = 0; k < nxi; k += 6) {
-        SpecDotPair pr[6];
-        const int m = std::min(6, nxi - k);
-        for (int i = 0; i < m; ++i) pr[i] = SpecDotPair{cbuf, xi[k + i], 0};
-        dots(pr, m, ir + k);
-    }
-    return lqq;
-}
-
-// calc_uk (function_ops.f90:2324-2343) of the state u into phys(dst)
-template <typename T>
-void Engine<T>::calc_uk(const double2* u, double k, int dst) {
-    const long nc = spec_ncomp();
-    chain_reset();
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i) {
-        InvOut o;
-        o.nsrc = 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-        o.phys_out = PU + i;
-        io.push_back(o);
-    }
-    inv(b2, io);
-    FwdOut oS;
-    oS.phys_out = PS;
-    fwd(b2, FSq3{}, {phys(PU), phys(PU + 1), phys(PU + 2)}, {oS});
-    A_and_S(true);
-    PowField f = chain(k);
-    ensure_phys(f);
-    MLQ_CUDA(cudaMemcpyAsync(phys(dst), phys(f.phys), n3 * sizeof(T), cudaMemcpyDeviceToDevice, stream));
-}
-
-// ----------------------------------------------------------------------------
-// line search along phi = u + tau d at q = 4
-// ----------------------------------------------------------------------------
-namespace {
-enum : int {
-    LU = 60,    // u (3)
-    LD = 63,    // d (3)
-    LDU = 66,   // d_j u_i at 66+3i+j
-    LDD = 75,   // d_j d_i at 75+3i+j
-    LS = 84,    // S_a = P2 coefficients of |phi|^2 (3)
-    LV = 87,    // V_aj = P2 coefficients of W_j at 87+3a+j
-    LP = 96,    // p_a (3)
-    WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
-};
-}  // namespace
-
-template <typename T>
-void Engine<T>::ls_setup(const double2* u, const double2* d) {
-    const long nc = spec_ncomp();
-    // phi's pieces: u, d and their gradients (function_ops.f90:3147-3195)
-    std::vector<InvOut> io;
-    for (int f = 0; f < 2; ++f)
-        for (int i = 0; i < 3; ++i)
-            for (int j = -1; j < 3; ++j) {
-                InvOut o;
-                o.nsrc = 1;
-                o.src[0] = ZSrc{(f == 0 ? u : d) + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
-                o.phys_out = j < 0 ? (f == 0 ? LU : LD) + i : (f == 0 ? LDU : LDD) + 3 * i + j;
-                io.push_back(o);
-            }
-    inv(b2, io);
-    std::vector<const T*> ud = {phys(LU), phys(LU + 1), phys(LU + 2), phys(LD), phys(LD + 1), phys(LD + 2)};
-    std::vector<const T*> all;
-    for (int i = 0; i < 3; ++i) all.push_back(phys(LU + i));
-    for (int i = 0; i < 9; ++i) all.push_back(phys(LDU + i));
-    for (int i = 0; i < 3; ++i) all.push_back(phys(LD + i));
-    for (int i = 0; i < 9; ++i) all.push_back(phys(LDD + i));
-    std::vector<const T*> grads;
-    for (int i = 0; i < 9; ++i) grads.push_back(phys(LDU + i));
-    for (int i = 0; i < 9; ++i) grads.push_back(phys(LDD + i));
-    // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333)
-    {
-        FwdOut o[3];
-        for (int a = 0; a < 3; ++a) o[a].phys_out = LS + a;
-        fwd(b2, FLSS{}, ud, {o[0], o[1], o[2]});
-    }
-    // P2 of the coefficients of W_j (calc_vgraduvgradu / calc_vvgradu, v = phi)
-    {
-        FwdOut o[3];
-        for (int j = 0; j < 3; ++j) o[j].phys_out = LV + j;
-        fwd(b2, FLSW<0>{}, all, {o[0], o[1], o[2]});
-        for (int j = 0; j < 3; ++j) o[j].phys_out = LV + 3 + j;
-        fwd(b2, FLSW<1>{}, all, {o[0], o[1], o[2]});
-        for (int j = 0; j < 3; ++j) o[j].phys_out = LV + 6 + j;
-        fwd(b2, FLSW<2>{}, all, {o[0], o[1], o[2]});
-    }
-    // p_a = -Lap^-1 P2(Q_a) and the spectra of P2(|grad phi|^2)_a
-    {
-        FwdOut o[6];
-        for (int a = 0; a < 3; ++a) {
-            o[a].sym = SYM_INV_KSQ;
-            o[a].phys_out = LP + a;
-            o[3 + a].spec = wspec(WLG + a);
-            o[3 + a].spec_f64 = wf64<T>();
-        }
-        fwd(b2, FLSQG{}, grads, {o[0], o[1], o[2], o[3], o[4], o[5]});
-    }
-    // R2 and R3 integrands as polynomials in tau
-    std::vector<const T*> rin;
-    for (int i = 0; i < 9; ++i) rin.push_back(phys(LV + i));
-    for (int a = 0; a < 3; ++a) rin.push_back(phys(LP + a));
-    for (int i = 0; i < 6; ++i) rin.push_back(ud[i]);
-    pointwise(FLSRed{}, rin, {}, 100);
-    fetch_results();
-    const double* r = h_results + 100;
-    const double M[3][3] = {{r[0], r[1], r[2]}, {r[1], r[3], r[4]}, {r[2], r[4], r[5]}};
-    for (int k = 0; k < 5; ++k) ls_r2_[k] = 0.0;
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) ls_r2_[a + b] += M[a][b];
-    for (int k = 0; k < 6; ++k) ls_r3_[k] = 0.0;
-    for (int a = 0; a < 3; ++a)
-        for (int cc = 0; cc < 2; ++cc)
-            for (int b = 0; b < 3; ++b) ls_r3_[a + cc + b] += r[6 + 3 * (2 * a + cc) + b];
-}
-
-template <typename T>
-void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
-    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
-    // A(tau) = P2(g^2) with its Parseval products: ||A||^2 (= ||phi||_4^4) and
-    // <A, P2(|grad phi|^2)_a>, a = 0..2
-    FwdOut o;
-    o.red_self = 0;
-    for (int a = 0; a < 3; ++a) {
-        o.red_with[a] = wspec(WLG + a);
-        o.red_with_f64[a] = wf64<T>();
-        o.red_with_slot[a] = 1 + a;
-    }
-    FLSA f;
-    f.tau = tau;
-    fwd(b2, f, {phys(LS), phys(LS + 1), phys(LS + 2)}, {o}, 130);
-    fetch_results();
-    const double* r = h_results + 130;
-    const double I1 = r[1] + tau * (r[2] + tau * r[3]);
-    double I2 = 0.0, I3 = 0.0;
-    for (int k = 4; k >= 0; --k) I2 = I2 * tau + ls_r2_[k];
-    for (int k = 5; k >= 0; --k) I3 = I3 * tau + ls_r3_[k];
-    const double R1 = -cv * I1;                 // -nu <|u|^2, P2 |grad u|^2>  (1318)
-    const double R2 = -cv * (q - 2.0) * I2;     // -(q-2) nu <1, P2 sum_j V_j^2> (1333)
-    const double R3 = cp * (q - 2.0) * I3;      // (q-2) <p, u.V>  (1352)
-    out[0] = R1 + R2 + R3;
-    out[1] = R1 + R2;
-    out[2] = R3;
-    if (lqq) *lqq = r[0];
-}
-
-// ----------------------------------------------------------------------------
-// state <-> host
-// ----------------------------------------------------------------------------
-template <typename T>
-void Engine<T>::load_scalar_phys(const double* host, int dst) {
-    T* st = (T*)stage(n3 * sizeof(T));
-    if (sizeof(T) == 8)
-        std::memcpy(st, host, n3 * sizeof(double));
-    else
-        for (long i = 0; i < n3; ++i) st[i] = (T)host[i];
-    MLQ_CUDA(cudaMemcpyAsync(phys(dst), st, n3 * sizeof(T), cudaMemcpyHostToDevice, stream));
-    MLQ_CUDA(cudaStreamSynchronize(stream));
-}
-
-template <typename T>
-void Engine<T>::store_scalar_phys(int src, double* host) {
-    T* st = (T*)stage(n3 * sizeof(T));
-    MLQ_CUDA(cudaMemcpyAsync(st, phys(src), n3 * sizeof(T), cudaMemcpyDeviceToHost, stream));
-    MLQ_CUDA(cudaStreamSynchronize(stream));
-    if (sizeof(T) == 8)
-        std::memcpy(host, st, n3 * sizeof(double));
-    else
-        for (long i = 0; i < n3; ++i) host[i] = (double)st[i];
-}
-
-// Forward transform of a host vector field into band-b2 state spectra.  The
-// energy the band drops is measured directly, as ||u - F^-1 P2 F u||^2.
-template <typename T>
-double Engine<T>::load_vec(const double* host, double2* spec) {
-    const long nc = spec_ncomp();
-    for (int c = 0; c < 3; ++c) {
-        load_scalar_phys(host + c * n3, PIO);
-        FwdOut o;
-        o.spec = spec + c * nc;
-        o.spec_f64 = 1;
-        o.phys_out = PIO2;
-        fwd(b2, FCopy{}, {phys(PIO)}, {o});
-        pointwise(FDiffSq{}, {phys(PIO), phys(PIO2)}, {}, 30 + 2 * c);
-    }
-    fetch_results();
-    double out = 0, tot = 0;
-    for (int c = 0; c < 3; ++c) {
-        out += h_results[30 + 2 * c];
-        tot += h_results[31 + 2 * c];
-    }
-    return tot > 0 ? out / tot : 0.0;
-}
-
-template <typename T>
-void Engine<T>::store_vec(const double2* spec, double* host) {
-    const long nc = spec_ncomp();
-    for (int c = 0; c < 3; ++c) {
-        InvOut o;
-        o.nsrc = 1;
-        o.src[0] = ZSrc{spec + c * nc, 1, SYM_ONE, 0, 1.0};
-        o.phys_out = PIO;
-        inv(b2, {o});
-        store_scalar_phys(PIO, host + c * n3);
-    }
-}
-
-// ----------------------------------------------------------------------------
-// fftwfunction.f90 API on the full band (FP64 engines only)
-// ----------------------------------------------------------------------------
-template <typename T>
-void Engine<T>::fft_c2c(const double* in, double* out, int sign) {
-    if (sizeof(T) != 8) throw CudaError("fft API runs in FP64", MLQ_ERR_BADARG);
-    const size_t bytes_c = (size_t)n3 * sizeof(cpx<double>);
-    cpx<double>* a = (cpx<double>*)dev_alloc(bytes_c);
-    cpx<double>* bbuf = (cpx<double>*)dev_alloc(bytes_c);
-    try {
-        double* st = (double*)stage(bytes_c);
-        std::memcpy(st, in, bytes_c);
-        MLQ_CUDA(cudaMemcpyAsync(a, st, bytes_c, cudaMemcpyHostToDevice, stream));
-        const double scale = sign < 0 ? 1.0 : 1.0 / (double)n3;
-        const Band full = make_band(n / 2);
-        Band bx = full;  // full complex columns along x
-        // x pass: a -> bbuf
-        XC2CArgs<double> xa;
-        xa.n = n;
-        int lx = 8;
-        while (lx > 1 && ((size_t)2 * n * lx * sizeof(cpx<double>) > 96 * 1024 || ((long)n * n) % lx != 0)) lx /= 2;
-        xa.lx = lx;
-        xa.in = a;
-        xa.out = bbuf;
-        xa.plan = plan(n);
-        xa.tw = d_tw;
-        xa.scale = 1.0;
-        const size_t xsm = (size_t)2 * n * lx * sizeof(cpx<double>);
-        if (sign < 0) {
-            allow_smem(xc2c_kernel<-1, double>);
-            xc2c_kernel<-1, double><<<(unsigned)(((long)n * n) / lx), 256, xsm, stream>>>(xa);
-        } else {
-            allow_smem(xc2c_kernel<+1, double>);
-            xc2c_kernel<+1, double><<<(unsigned)(((long)n * n) / lx), 256, xsm, stream>>>(xa);
-        }
-        launched();
-        // y pass over all n columns: bbuf -> a (full band = natural order)
-        const int tx = tx_for();
-        YArgs<double> ya;
-        ya.n = n;
-        ya.nx = n;
-        ya.tx = tx;
-        ya.band = full;
-        ya.in[0] = reinterpret_cast<cpx<double>*>(bbuf);
-        ya.out[0] = reinterpret_cast<cpx<double>*>(a);
-        ya.plan = plan(n);
-        ya.tw = d_tw;
-        const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<double>);
-        dim3 yg((n + tx - 1) / tx, n, 1);
-        if (sign < 0) {
-            allow_smem(ypass_kernel<-1, double>);
-            ypass_kernel<-1, double><<<yg, 256, ysm, stream>>>(ya);
-        } else {
-            allow_smem(ypass_kernel<+1, double>);
-            ypass_kernel<+1, double><<<yg, 256, ysm, stream>>>(ya);
-        }
-        launched();
-        // z pass: a -> bbuf
-        if (sign < 0) {
-            ZFwdArgs<double> za;
-            za.n = n;
-            za.nx = n;
-            za.tx = tx;
-            za.band = full;
-            ZFwdOp op = {};
-            op.in = a;
-            op.spec_out = bbuf;
-            op.spec_f64 = 1;
-            op.sym = SYM_ONE;
-            op.red_self = -1;
-            for (int r = 0; r < 3; ++r) op.red_with_slot[r] = -1;
-            za.op[0] = op;
-            za.plan = plan(n);
-            za.tw = d_tw;
-            za.norm = 1.0;
-            dim3 zg((n + tx - 1) / tx, n, 1);
-            ensure_partials((long)zg.x * zg.y * MAX_RED);
-            za.partials = d_partials;
-            allow_smem(zfwd_kernel<double>);
-            zfwd_kernel<double><<<zg, 256, ysm, stream>>>(za);
-        } else {
-            ZInvArgs<double> za;
-            za.n = n;
-            za.nx = n;
-            za.tx = tx;
-            za.band = full;
-            ZInvOp op = {};
-            op.src[0] = ZSrc{a, 1, SYM_ONE, 0, scale};
-            op.nsrc = 1;
-            op.ys_out = bbuf;
-            za.op[0] = op;
-            za.plan = plan(n);
-            za.tw = d_tw;
-            dim3 zg((n + tx - 1) / tx, n, 1);
-            allow_smem(zinv_kernel<double>);
-            zinv_kernel<double><<<zg, 256, ysm, stream>>>(za);
-        }
-        launched();
-        (void)bx;
-        MLQ_CUDA(cudaMemcpyAsync(st, bbuf, bytes_c, cudaMemcpyDeviceToHost, stream));
-        MLQ_CUDA(cudaStreamSynchronize(stream));
-        std::memcpy(out, st, bytes_c);
-    } catch (...) {
-        free_dev(a);
-        free_dev(bbuf);
-        throw;
-    }
-    free_dev(a);
-    free_dev(bbuf);
-}
-
-template <typename T>
-void Engine<T>::fft_r2c(const double* in, double* out) {
-    if (sizeof(T) != 8) throw CudaError("fft API runs in FP64", MLQ_ERR_BADARG);
-    const Band full = make_band(n / 2);
-    widen_to(full);
-    load_scalar_phys(in, PIO);
-    const size_t nspec = (size_t)full.nb * full.nb * full.nx;
-    cpx<double>* sp = (cpx<double>*)dev_alloc(nspec * sizeof(cpx<double>));
-    FwdOut o;
-    o.spec = sp;
-    o.spec_f64 = 1;
-    fwd(full, FCopy{}, {phys(PIO)}, {o}, -1, -1, 1.0);  // unnormalised like fftfwdr
-    double* st = (double*)stage(nspec * sizeof(cpx<double>));
-    MLQ_CUDA(cudaMemcpyAsync(st, sp, nspec * sizeof(cpx<double>), cudaMemcpyDeviceToHost, stream));
-    MLQ_CUDA(cudaStreamSynchronize(stream));
-    std::memcpy(out, st, nspec * sizeof(cpx<double>));
-    free_dev(sp);
-}
-
-template <typename T>
-void Engine<T>::fft_c2r(const double* in, double* out) {
-    if (sizeof(T) != 8) throw CudaError("fft API runs in FP64", MLQ_ERR_BADARG);
-    const Band full = make_band(n / 2);
-    widen_to(full);
-    const size_t nspec = (size_t)full.nb * full.nb * full.nx;
-    cpx<double>* sp = (cpx<double>*)dev_alloc(nspec * sizeof(cpx<double>));
-    double* st = (double*)stage(nspec * sizeof(cpx<double>));
-    std::memcpy(st, in, nspec * sizeof(cpx<double>));
-    MLQ_CUDA(cudaMemcpyAsync(sp, st, nspec * sizeof(cpx<double>), cudaMemcpyHostToDevice, stream));
-    InvOut o;
-    o.nsrc = 1;
-    o.src[0] = ZSrc{sp, 1, SYM_ONE, 0, 1.0 / (double)n3};  // fftbwdr scales by 1/N^3 (160)
-    o.phys_out = PIO;
-    inv(full, {o});
-    store_scalar_phys(PIO, out);
-    free_dev(sp);
-}
-
-template <typename T>
-void Engine<T>::dealias_scalar(double* g, double order) {
-    const int c = band_cut_for_order(n, order);
-    if (c >= n / 2) return;  // the mask removes nothing (order <= 1)
-    const Band bk = make_band(c);
-    widen_to(bk);
-    load_scalar_phys(g, PIO);
-    FwdOut o;
-    o.phys_out = PIO2;
-    fwd(bk, FCopy{}, {phys(PIO)}, {o});
-    store_scalar_phys(PIO2, g);
-}
-
-template <typename T>
-void Engine<T>::widen_to(const Band& b) {
-    if (nxcap >= b.nx && nbcap >= b.nb) return;
-    for (auto& p : xs_)
-        if (p) {
-            free_dev(p);
-            p = nullptr;
-        }
-    for (auto& p : ys_)
-        if (p) {
-            free_dev(p);
-            p = nullptr;
-        }
-    nxcap = std::max(nxcap, b.nx);
-    nbcap = std::max(nbcap, b.nb);
-}
-
-// Fourier coefficients of a host scalar on the full band (FP64 work spectrum)
-template <typename T>
-static cpx<double>* full_spectrum(Engine<T>& e, const double* host, int phys_idx) {
-    const Band full = e.make_band(e.n / 2);
-    e.widen_to(full);
-    e.load_scalar_phys(host, phys_idx);
-    const size_t nspec = (size_t)full.nb * full.nb * full.nx;
-    cpx<double>* sp = (cpx<double>*)e.dev_alloc(nspec * sizeof(cpx<double>));
-    typename Engine<T>::FwdOut o;
-    o.spec = sp;
-    o.spec_f64 = 1;
-    e.fwd(full, FCopy{}, {e.phys(phys_idx)}, {o});
-    return sp;
-}
-
-template <typename T>
-void Engine<T>::gradient_full(const double* f, double* grad) {
-    if (sizeof(T) != 8) throw CudaError("full-band operators run in FP64", MLQ_ERR_BADARG);
-    const Band full = make_band(n / 2);
-    cpx<double>* sp = full_spectrum(*this, f, PIO);
-    for (int j = 0; j < 3; ++j) {
-        InvOut o;
-        o.nsrc = 1;
-        o.src[0] = ZSrc{sp, 1, SYM_IKX + j, 0, 1.0};
-        o.phys_out = PIO2;
-        inv(full, {o});
-        store_scalar_phys(PIO2, grad + j * n3);
-    }
-    free_dev(sp);
-}
-
-template <typename T>
-void Engine<T>::divergence_full(const double* u, double* div) {
-    if (sizeof(T) != 8) throw CudaError("full-band operators run in FP64", MLQ_ERR_BADARG);
-    const Band full = make_band(n / 2);
-    cpx<double>* sp[3];
-    for (int c = 0; c < 3; ++c) sp[c] = full_spectrum(*this, u + c * n3, PIO);
-    InvOut o;
-    o.nsrc = 3;
-    for (int c = 0; c < 3; ++c) o.src[c] = ZSrc{sp[c], 1, SYM_IKX + c, 0, 1.0};
-    o.phys_out = PIO2;
-    inv(full, {o});
-    store_scalar_phys(PIO2, div);
-    for (int c = 0; c < 3; ++c) free_dev(sp[c]);
-}
-
-template <typename T>
-void Engine<T>::laplacian_full(double* u) {
-    if (sizeof(T) != 8) throw CudaError("full-band operators run in FP64", MLQ_ERR_BADARG);
-    const Band full = make_band(n / 2);
-    for (int c = 0; c < 3; ++c) {
-        cpx<double>* sp = full_spectrum(*this, u + c * n3, PIO);
-        InvOut o;
-        o.nsrc = 1;
-        o.src[0] = ZSrc{sp, 1, SYM_NEG_KSQ, 0, 1.0};
-        o.phys_out = PIO2;
-        inv(full, {o});
-        store_scalar_phys(PIO2, u + c * n3);
-        free_dev(sp);
-    }
-}
-
-template <typename T>
-void Engine<T>::poisson_full(const double* f, double l, double* phi) {
-    if (sizeof(T) != 8) throw CudaError("full-band operators run in FP64", MLQ_ERR_BADARG);
-    const Band full = make_band(n / 2);
-    cpx<double>* sp = full_spectrum(*this, f, PIO);
-    InvOut o;
-    o.nsrc = 1;
-    o.src[0] = ZSrc{sp, 1, SYM_NEG_INV_KSQ, 0, 1.0 / std::pow(l, 2.0)};  // -f_hat/(l^2 ksq), k=0 -> 0
-    o.phys_out = PIO2;
-    inv(full, {o});
-    store_scalar_phys(PIO2, phi);
-    free_dev(sp);
-}
-
-template class Engine<float>;
-template class Engine<double>;
 
 }  // namespace mlq

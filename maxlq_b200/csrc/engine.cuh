@@ -17,6 +17,7 @@
 #include "functors.cuh"
 #include "kernels.cuh"
 #include "regfft.cuh"
+#include "cfft.cuh"
 
 namespace mlq {
 
@@ -214,6 +215,19 @@ class Engine : public EngineBase {
     bool reg_ok_ = false;
     cpx<T>* d_twT_ = nullptr;  // twiddle pool in T
     RPlan rplan(int L) const;
+    // kernels specialised at compile time for n in {64, ..., 1024} (cfft.cuh)
+    bool cfft_ok_ = false;
+    int persistent_blocks(const void* kernel, int threads, size_t smem);
+    std::map<const void*, int> occ_;
+    int num_sms_ = 148;
+    template <int NN>
+    void xinv_c(XInvArgs<T>& xa, int narr);
+    template <int NN>
+    void y_c(YArgs<T>& ya, int sign, int narr);
+    template <int NN>
+    void zfwd_c(ZFwdArgs<T>& za, int narr);
+    template <int NN>
+    void zinv_c(ZInvArgs<T>& za, int narr);
     int reg_tx() const;
     int reg_lx(int nrows_per_line, size_t pitch) const;
     // pass launchers (register kernels when reg_ok_, shared-memory Stockham otherwise)

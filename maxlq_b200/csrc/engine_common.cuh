@@ -1,0 +1,59 @@
+// engine_common.cuh -- host helpers shared by the engine's translation units.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <set>
+
+#include "engine.cuh"
+
+namespace mlq {
+
+static const double PI_REF = 4.0 * std::atan2(1.0, 1.0);  // initialize.f90:164
+
+
+static std::vector<int> factor_radices(int L) {
+    std::vector<int> r;
+    int m = L;
+    while (m % 16 == 0 && m > 1) { r.push_back(16); m /= 16; }
+    while (m % 8 == 0) { r.push_back(8); m /= 8; }
+    while (m % 4 == 0) { r.push_back(4); m /= 4; }
+    while (m % 2 == 0) { r.push_back(2); m /= 2; }
+    while (m % 3 == 0) { r.push_back(3); m /= 3; }
+    if (m != 1) throw CudaError("FFT length must be 2^a 3^b", MLQ_ERR_BADARG);
+    return r;
+}
+
+// raise the dynamic shared memory limit of each kernel once (per device
+// function address: kernels of equal type are distinct entries)
+template <typename K>
+static void allow_smem(K kernel) {
+    static std::set<const void*> done;
+    const void* key = reinterpret_cast<const void*>(kernel);
+    if (done.insert(key).second) {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        if (e != cudaSuccess) throw CudaError(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);
+    }
+}
+
+// f(std::integral_constant<int, n>) for the sizes with compile-time kernels
+template <class Fn>
+static bool dispatch_n(int n, Fn&& f) {
+    switch (n) {
+        case 64: f(std::integral_constant<int, 64>{}); return true;
+        case 128: f(std::integral_constant<int, 128>{}); return true;
+        case 256: f(std::integral_constant<int, 256>{}); return true;
+        case 512: f(std::integral_constant<int, 512>{}); return true;
+        case 1024: f(std::integral_constant<int, 1024>{}); return true;
+        default: return false;
+    }
+}
+
+static int grid_for(long work, int threads, int cap = 148 * 8) {
+    long g = (work + threads - 1) / threads;
+    return (int)std::max(1L, std::min<long>(g, cap));
+}
+
+}  // namespace mlq

@@ -1,0 +1,79 @@
+"""Pass kernels specialised at compile time for power-of-two N (64 ... 1024):
+against the oracle at N = 64 and 128, and at N = 256 and 512 against the
+register kernels with run-time plans (MLQ_PASS_KERNELS=reg selects those for
+contexts created while it is set)."""
+import numpy as np
+import pytest
+
+import maxlq_b200 as mlq
+from oracle.oracle import Oracle
+from oracle.seedfield import seed_field
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+@pytest.mark.parametrize("n,q", [(64, 4.0), (64, 3.0), (128, 6.0)])
+def test_R_and_gradient_against_oracle(n, q):
+    o = Oracle(n, q, 1.0)
+    u = o.rescale(seed_field(n, 0, 2.0, n / 16))
+    with mlq.MaxLq(n, q, 1.0) as c:
+        R = c.calc_global_dLqdt_inclParts(u)
+        g = c.GradL2ForLq(u)
+    assert rel(R, o.R_parts(u)) < 1e-10
+    assert rel(g, o.grad_l2(u)) < 1e-10
+    with mlq.MaxLq(n, q, 1.0, precision="mixed") as m:
+        assert rel(m.calc_global_dLqdt_inclParts(u), o.R_parts(u)) < 2e-5
+        assert rel(m.GradL2ForLq(u), o.grad_l2(u)) < 1e-3
+
+
+@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("order", [2.0, 1.5])
+def test_dealias_against_oracle(n, order):
+    rng = np.random.default_rng(5)
+    g = rng.standard_normal((n, n, n))
+    with mlq.MaxLq(n, 4.0, 1.0) as c:
+        assert rel(c.dealias_scalar(g, order), Oracle(n, 4.0).dealias_scalar(g, order)) < 1e-12
+
+
+def test_full_band_operators_n64():
+    """Full band: the x inverse reads the Nyquist column (nx = N/2 + 1)."""
+    n = 64
+    rng = np.random.default_rng(12)
+    f = rng.standard_normal((n, n, n))
+    u = rng.standard_normal((3, n, n, n))
+    o = Oracle(n, 4.0)
+    with mlq.MaxLq(n, 4.0, 1.0) as c:
+        assert rel(c.gradient(f), o.gradient(f)) < 1e-12
+        assert rel(c.divergence(u), o.divergence(u)) < 1e-12
+        assert rel(c.laplacian(u), o.laplacian(u)) < 1e-12
+        assert rel(c.solve_poisson(f, 0.7), o.solve_poisson(f, 0.7)) < 1e-12
+
+
+def _state_run(n, precision, kernels, monkeypatch):
+    monkeypatch.setenv("MLQ_PASS_KERNELS", kernels)
+    with mlq.MaxLq(n, 4.0, 1.0, precision=precision, optim_tol=1e-14) as c:
+        u = c.seed_field(0, 2.0, n / 16)
+        c.state_load(u)
+        R, lq = c.state_R()
+        g = c.GradL2ForLq(u) if n <= 256 else None
+        it, st, rec = c.state_iterate(1)
+    return R, lq, g, rec[0]
+
+
+@pytest.mark.parametrize("n,precision,tol", [(256, "fp64", 1e-12), (256, "mixed", 2e-6), (512, "mixed", 2e-6)])
+def test_compile_time_kernels_match_runtime_plan_kernels(n, precision, tol, monkeypatch):
+    R0, lq0, g0, r0 = _state_run(n, precision, "reg", monkeypatch)
+    R1, lq1, g1, r1 = _state_run(n, precision, "compile-time", monkeypatch)
+    assert rel(R1, R0) < tol
+    assert lq1 == pytest.approx(lq0, rel=tol)
+    if g0 is not None:
+        assert rel(g1, g0) < (tol if precision == "fp64" else 1e-4)
+    if precision == "fp64":
+        assert r1["n_evals"] == r0["n_evals"]  # FP32 roundoff may move Brent by an evaluation
+    assert r1["J1"] == pytest.approx(r0["J1"], rel=tol)
+    assert r1["tau"] == pytest.approx(r0["tau"], rel=1e-3 if precision == "mixed" else 1e-9)
