@@ -260,6 +260,7 @@ struct CShape {
     static constexpr int YTHREADS = TX * TPLY;
     static constexpr int YMINB = YTHREADS <= 256 ? 2 : 1;  // resident blocks the register budget aims at
     static constexpr size_t YSMEM = ((size_t)N * TX + N) * sizeof(cpx<T>);
+    static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);  // + the K table
     static_assert(TPLX <= 32 && 32 % TPLX == 0, "x line within a warp");
     static_assert(YTHREADS % 32 == 0 && YTHREADS <= 512, "y/z block");
 };
@@ -406,6 +407,107 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
 }
 
 // ----------------------------------------------------------------------------
+// Spectral symbols in the pipeline precision C.  The wavenumbers come from a
+// per-block table K[f] = 2 pi j(f) (and its odd-factor copy, 0 at the Nyquist
+// index), built exactly as make_k does; with C = double every symbol is the
+// same arithmetic as apply_sym.  With C = float (mixed mode) the multiply by
+// the symbol rounds like the FP32 transforms around it; reductions stay FP64.
+// ----------------------------------------------------------------------------
+template <typename C>
+struct KvC {
+    C kx, ky, kz, ox, oy, oz, ksq;
+};
+
+template <typename C>
+__device__ __forceinline__ cpx<C> sym_c(int sym, int ab, const KvC<C>& k, cpx<C> v) {
+    switch (sym) {
+        case SYM_ZERO: return mk(C(0), C(0));
+        case SYM_ONE: return v;
+        case SYM_IKX: return mk(-k.ox * v.y, k.ox * v.x);
+        case SYM_IKY: return mk(-k.oy * v.y, k.oy * v.x);
+        case SYM_IKZ: return mk(-k.oz * v.y, k.oz * v.x);
+        case SYM_NEG_KSQ: return v * (-k.ksq);
+        case SYM_INV_KSQ: return k.ksq == C(0) ? mk(C(0), C(0)) : v * (C(1) / k.ksq);
+        case SYM_NEG_INV_KSQ: return k.ksq == C(0) ? mk(C(0), C(0)) : v * (C(-1) / k.ksq);
+        case SYM_KK_KSQ: {
+            if (k.ksq == C(0)) return mk(C(0), C(0));
+            const int ia = ab / 3, ib = ab % 3;
+            const C ka = ia == 0 ? k.ox : (ia == 1 ? k.oy : k.oz);
+            const C kb = ib == 0 ? k.ox : (ib == 1 ? k.oy : k.oz);
+            return v * (ka * kb / k.ksq);
+        }
+    }
+    return v;
+}
+
+template <typename C>
+__device__ __forceinline__ cpx<C> ld_spec_c(const void* p, int f64, long idx) {
+    if (f64) {
+        const double2 v = reinterpret_cast<const double2*>(p)[idx];
+        return mk((C)v.x, (C)v.y);
+    }
+    const float2 v = reinterpret_cast<const float2*>(p)[idx];
+    return mk((C)v.x, (C)v.y);
+}
+template <typename C>
+__device__ __forceinline__ void st_spec_c(void* p, int f64, long idx, cpx<C> v) {
+    if (f64)
+        reinterpret_cast<double2*>(p)[idx] = make_double2((double)v.x, (double)v.y);
+    else
+        reinterpret_cast<float2*>(p)[idx] = make_float2((float)v.x, (float)v.y);
+}
+
+// K table (2 pi j, then the odd-factor copy) of length 2N in shared memory
+template <int N, typename C>
+__device__ __forceinline__ void fill_k_table(C* kt) {
+    const double twopi = 2.0 * 3.14159265358979311600;  // 2.0_pr*PI, PI = 4 atan2(1,1)
+    for (int f = threadIdx.x; f < N; f += blockDim.x) {
+        const double K = twopi * (double)signed_j(N, f);
+        kt[f] = (C)K;
+        kt[N + f] = (f == N / 2) ? C(0) : (C)K;
+    }
+}
+
+// Batched spectrum loads: CH elements m0..m0+CH-1 of a column, every load
+// issued before any is used (indices are clamped in bounds, so no load sits
+// behind a per-element branch and CH loads per thread are in flight).
+template <int CH, typename C, class Idx>
+__device__ __forceinline__ void ld_chunk(const void* p, int f64, const Idx& idx, int m0, cpx<C> (&out)[CH]) {
+    if (f64) {
+        const double2* q = reinterpret_cast<const double2*>(p);
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+            const double2 v = q[idx(m0 + j)];
+            out[j] = mk((C)v.x, (C)v.y);
+        }
+    } else {
+        const float2* q = reinterpret_cast<const float2*>(p);
+#pragma unroll
+        for (int j = 0; j < CH; ++j) {
+            const float2 v = q[idx(m0 + j)];
+            out[j] = mk((C)v.x, (C)v.y);
+        }
+    }
+}
+
+// Column geometry of a z-stage item: compact z index of FFT position
+// t + TPL m, validity and the (clamped, in-bounds) spectrum index.
+template <int N, int TPL>
+struct ZCol {
+    int t, cut, nb, plane, col;
+    bool ok;
+    __device__ __forceinline__ int cz(int m) const {
+        const int fz = t + TPL * m;
+        return fz <= cut ? fz : (fz >= N - cut ? fz - (N - nb) : -1);
+    }
+    __device__ __forceinline__ bool valid(int m) const { return ok && cz(m) >= 0; }
+    __device__ __forceinline__ int operator()(int m) const {
+        const int c = cz(m);
+        return (c >= 0 ? c : 0) * plane + col;
+    }
+};
+
+// ----------------------------------------------------------------------------
 // z stage, forward (+ optional round trip).  grid = (G, narr); items (cy, tile).
 // One reduction record of MAX_RED partials per block.
 // ----------------------------------------------------------------------------
@@ -413,70 +515,108 @@ template <int N, typename T>
 __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
     zfwd_c_kernel(ZFwdArgs<T> a, const cpx<T>* __restrict__ twN) {
     using S = CShape<N, T>;
-    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
+    using C = T;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
     cpx<T>* stw = sm + N * TX;
+    C* kt = reinterpret_cast<C*>(stw + N);
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    fill_k_table<N>(kt);
     __syncthreads();
     const TwTab<N, E, T> tw{stw};
     const int l = threadIdx.x % TX, t = threadIdx.x / TX;
     const ColMap<TX> map{l};
-    const int nx = a.nx, nb = a.band.nb;
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)nb * ntile;
     const ZFwdOp& op = a.op[blockIdx.y];
-    const long plane = (long)nb * nx;
+    const int plane = nb * nx;
     const cpx<T>* __restrict__ src = reinterpret_cast<const cpx<T>*>(op.in);
     cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
+    const int sym = op.sym, sym_ab = op.sym_ab, add_sym = op.add_sym, add_ab = op.add_ab;
+    const C norm = (C)a.norm, add_coef = (C)op.add_coef;
     const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
     double acc_self = 0.0, acc_w0 = 0.0, acc_w1 = 0.0, acc_w2 = 0.0;
     for (long it = blockIdx.x; it < items; it += gridDim.x) {
         const int cy = (int)(it / ntile);
         const int kx = (int)(it - (long)cy * ntile) * TX + l;
         const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
         cpx<T> v[E];
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int p = t + TPL * m;
-            v[m] = ok ? src[(long)p * plane + (long)cy * nx + kx] : czero<T>();
-        }
+        for (int m = 0; m < E; ++m) v[m] = ok ? src[(t + TPL * m) * plane + col] : czero<T>();
         cfft<N, E, -1, SyncBlock>(v, t, sm, map, tw);
         const int fy = band_fft_index(a.band, cy);
+        KvC<C> k;
+        k.kx = kt[col - cy * nx];
+        k.ox = kt[N + col - cy * nx];
+        k.ky = kt[fy];
+        k.oy = kt[N + fy];
+        const C kxy2 = k.kx * k.kx + k.ky * k.ky;
         const double wgt = kx_weight(N, kx);
+        const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
+        cpx<C> Y[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int fz = t + TPL * m;
-            const int cz = band_compact_index(a.band, fz);
-            cpx<double> Y = mk(0.0, 0.0);
-            if (cz >= 0 && ok) {
-                const Kvec k = make_k(N, kx, fy, fz);
-                Y = apply_sym(op.sym, op.sym_ab, k, mk((double)v[m].x, (double)v[m].y) * a.norm);
-                const long si2 = ((long)cz * nb + cy) * nx + kx;
-                if (op.add)
-                    Y = Y + apply_sym(op.add_sym, op.add_ab, k, ld_spec(op.add, op.add_f64, si2)) * op.add_coef;
-                if (op.red_self >= 0) acc_self += wgt * (Y.x * Y.x + Y.y * Y.y);
-                if (op.red_with[0]) {
-                    const cpx<double> W = ld_spec(op.red_with[0], op.red_with_f64[0], si2);
-                    acc_w0 += wgt * (Y.x * W.x + Y.y * W.y);
+            k.kz = kt[fz];
+            k.oz = kt[N + fz];
+            k.ksq = kxy2 + k.kz * k.kz;
+            Y[m] = idx.valid(m) ? sym_c(sym, sym_ab, k, mk((C)v[m].x, (C)v[m].y) * norm) : mk(C(0), C(0));
+        }
+        if (op.add) {
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += CH) {
+                cpx<C> A[CH];
+                ld_chunk<CH>(op.add, op.add_f64, idx, m0, A);
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int fz = t + TPL * (m0 + j);
+                    k.kz = kt[fz];
+                    k.oz = kt[N + fz];
+                    k.ksq = kxy2 + k.kz * k.kz;
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_c(add_sym, add_ab, k, A[j]) * add_coef;
                 }
-                if (op.red_with[1]) {
-                    const cpx<double> W = ld_spec(op.red_with[1], op.red_with_f64[1], si2);
-                    acc_w1 += wgt * (Y.x * W.x + Y.y * W.y);
-                }
-                if (op.red_with[2]) {
-                    const cpx<double> W = ld_spec(op.red_with[2], op.red_with_f64[2], si2);
-                    acc_w2 += wgt * (Y.x * W.x + Y.y * W.y);
-                }
-                if (op.spec_out) st_spec(op.spec_out, op.spec_f64, si2, Y);
             }
-            v[m] = mk((T)Y.x, (T)Y.y);
+        }
+        if (op.red_self >= 0) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const double yx = (double)Y[m].x, yy = (double)Y[m].y;
+                acc_self += wgt * (yx * yx + yy * yy);  // zero outside the band
+            }
+        }
+#pragma unroll 1
+        for (int r = 0; r < 3; ++r) {
+            if (!op.red_with[r]) continue;
+            double s = 0.0;
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += CH) {
+                cpx<double> W[CH];
+                ld_chunk<CH>(op.red_with[r], op.red_with_f64[r], idx, m0, W);
+#pragma unroll
+                for (int j = 0; j < CH; ++j) s += (double)Y[m0 + j].x * W[j].x + (double)Y[m0 + j].y * W[j].y;
+            }
+            if (r == 0)
+                acc_w0 += wgt * s;
+            else if (r == 1)
+                acc_w1 += wgt * s;
+            else
+                acc_w2 += wgt * s;
+        }
+        if (op.spec_out) {
+#pragma unroll
+            for (int m = 0; m < E; ++m)
+                if (idx.valid(m)) st_spec_c(op.spec_out, op.spec_f64, idx(m), Y[m]);
         }
         if (yout) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) v[m] = mk((T)Y[m].x, (T)Y[m].y);
             cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
             if (ok) {
 #pragma unroll
-                for (int m = 0; m < E; ++m) yout[(long)(t + TPL * m) * plane + (long)cy * nx + kx] = v[m];
+                for (int m = 0; m < E; ++m) yout[(t + TPL * m) * plane + col] = v[m];
             }
         }
     }
@@ -506,45 +646,66 @@ template <int N, typename T>
 __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
     zinv_c_kernel(ZInvArgs<T> a, const cpx<T>* __restrict__ twN) {
     using S = CShape<N, T>;
-    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
+    using C = T;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
     cpx<T>* stw = sm + N * TX;
+    C* kt = reinterpret_cast<C*>(stw + N);
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    fill_k_table<N>(kt);
     __syncthreads();
     const TwTab<N, E, T> tw{stw};
     const int l = threadIdx.x % TX, t = threadIdx.x / TX;
     const ColMap<TX> map{l};
-    const int nx = a.nx, nb = a.band.nb;
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)nb * ntile;
     const ZInvOp& op = a.op[blockIdx.y];
-    const long plane = (long)nb * nx;
+    const int plane = nb * nx;
+    const int nsrc = op.nsrc;
     cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out);
     for (long it = blockIdx.x; it < items; it += gridDim.x) {
         const int cy = (int)(it / ntile);
         const int kx = (int)(it - (long)cy * ntile) * TX + l;
         const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
         const int fy = band_fft_index(a.band, cy);
+        KvC<C> k;
+        k.kx = kt[col - cy * nx];
+        k.ox = kt[N + col - cy * nx];
+        k.ky = kt[fy];
+        k.oy = kt[N + fy];
+        const C kxy2 = k.kx * k.kx + k.ky * k.ky;
+        const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
+        cpx<C> Y[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) Y[m] = mk(C(0), C(0));
+#pragma unroll 1
+        for (int s = 0; s < nsrc; ++s) {
+            const ZSrc zs = op.src[s];
+            const C coef = (C)zs.coef;
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += CH) {
+                cpx<C> V[CH];
+                ld_chunk<CH>(zs.spec, zs.f64, idx, m0, V);
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int fz = t + TPL * (m0 + j);
+                    k.kz = kt[fz];
+                    k.oz = kt[N + fz];
+                    k.ksq = kxy2 + k.kz * k.kz;
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_c(zs.sym, zs.ab, k, V[j]) * coef;
+                }
+            }
+        }
         cpx<T> v[E];
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int fz = t + TPL * m;
-            const int cz = band_compact_index(a.band, fz);
-            cpx<double> Y = mk(0.0, 0.0);
-            if (cz >= 0 && ok) {
-                const Kvec k = make_k(N, kx, fy, fz);
-                const long si2 = ((long)cz * nb + cy) * nx + kx;
-                for (int s = 0; s < op.nsrc; ++s)
-                    Y = Y + apply_sym(op.src[s].sym, op.src[s].ab, k, ld_spec(op.src[s].spec, op.src[s].f64, si2)) *
-                                op.src[s].coef;
-            }
-            v[m] = mk((T)Y.x, (T)Y.y);
-        }
+        for (int m = 0; m < E; ++m) v[m] = mk((T)Y[m].x, (T)Y[m].y);
         cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
         if (ok) {
 #pragma unroll
-            for (int m = 0; m < E; ++m) dst[(long)(t + TPL * m) * plane + (long)cy * nx + kx] = v[m];
+            for (int m = 0; m < E; ++m) dst[(t + TPL * m) * plane + col] = v[m];
         }
     }
 }

@@ -133,7 +133,7 @@ template <typename T>
 template <int NN>
 void Engine<T>::zfwd_c(ZFwdArgs<T>& za, int narr) {
     using S = CShape<NN, T>;
-    const size_t smem = S::YSMEM;
+    const size_t smem = S::ZSMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
     auto kern = zfwd_c_kernel<NN, T>;
     allow_smem(kern);
@@ -149,7 +149,7 @@ template <typename T>
 template <int NN>
 void Engine<T>::zinv_c(ZInvArgs<T>& za, int narr) {
     using S = CShape<NN, T>;
-    const size_t smem = S::YSMEM;
+    const size_t smem = S::ZSMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
     auto kern = zinv_c_kernel<NN, T>;
     allow_smem(kern);
