@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison path")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-detail", action="store_true", help="key x-stage kernel times by fused functor")
     return ap.parse_args()
 
 
@@ -191,7 +192,7 @@ def run_path(ctx, u0, K, W, dist, profile=False):
     device_sync()
     l0 = ctx.kernel_launches
     if profile:
-        ctx.profile(True)
+        ctx.profile(profile)
         ctx.profile_report(reset=True)
     t0 = time.perf_counter()
     timed = []
@@ -279,7 +280,7 @@ def main():
 
     clocks = ClockSampler(dev)
     clocks.start()
-    res_m = run_path(mixed, u0, K, W, dist, profile=True)
+    res_m = run_path(mixed, u0, K, W, dist, profile=2 if args.profile_detail else True)
     clk = clocks.stop()
 
     # the all-FP64 path, and the accuracy of the mixed path against it on the

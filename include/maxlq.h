@@ -164,7 +164,8 @@ int mlq_state_R(mlq_ctx* ctx, double out[3], double* lq_norm);
 int mlq_state_step(mlq_ctx* ctx, double* u, mlq_iter_cb cb, void* user);
 
 /* ---- measurement ----------------------------------------------------------- */
-/* Per-kernel CUDA-event timing on the context's stream (off by default). */
+/* Per-kernel CUDA-event timing on the context's stream (off by default).
+ * on = 2 also keys each x-stage launch by its fused pointwise functor. */
 int mlq_profile_enable(mlq_ctx* ctx, int on);
 /* JSON object {kernel: [launches, total_ms, algorithmic_bytes]} of the launches
  * since the last reset; resets when reset != 0.  Returns the length needed. */

@@ -333,8 +333,10 @@ class MaxLq:
             self._check(st, "state_step")
         return st, records
 
-    def profile(self, on: bool = True):
-        self._check(self._lib.mlq_profile_enable(self._ctx, 1 if on else 0), "profile_enable")
+    def profile(self, on: bool | int = True):
+        """Per-kernel device timing; on=2 also keys x-stage launches by functor."""
+        level = int(on) if not isinstance(on, bool) else (1 if on else 0)
+        self._check(self._lib.mlq_profile_enable(self._ctx, level), "profile_enable")
 
     def profile_report(self, reset: bool = True) -> dict:
         import json

@@ -296,6 +296,7 @@ int mlq_profile_enable(mlq_ctx* c, int on) {
     return guard(c, [&] {
         c->solver->eng().prof_flush();
         c->solver->eng().prof_on = on != 0;
+        c->solver->eng().prof_detail = on >= 2;
     });
 }
 

@@ -355,6 +355,107 @@ __global__ void __launch_bounds__(256, 2)
 }
 
 // ----------------------------------------------------------------------------
+// x stage, forward: functor on the physical inputs, then the real FFT of each
+// functor output along x (a complex transform of length N/2 of the packed
+// pairs, then the half-spectrum split).  grid = G, block = 256: each block
+// walks groups of 256/TPL lines; output 0 stays in registers, outputs 1.. are
+// parked in thread-private shared-memory slots until their turn.
+// ----------------------------------------------------------------------------
+template <int N, typename T, int NOUT>
+struct XFwdSmem {
+    using S = CShape<N, T>;
+    static constexpr size_t STAGE = (size_t)(NOUT > 1 ? NOUT - 1 : 0) * S::XLPB * S::L;
+    static constexpr size_t BYTES = (STAGE + (size_t)S::XLPB * S::XPITCH + (S::XTW_REG ? 0 : S::L)) * sizeof(cpx<T>);
+};
+
+// resident blocks the register budget aims at: light functors 2, heavy ones 1
+template <class F>
+constexpr int xfwd_minb() {
+    return F::NIN + F::NOUT <= 8 ? 2 : 1;
+}
+
+template <int N, typename T, class F>
+__global__ void __launch_bounds__(256, xfwd_minb<F>())
+    xfwd_c_kernel(XFwdArgs<T> a, F f, const cpx<T>* __restrict__ twL, const cpx<T>* __restrict__ twN) {
+    using S = CShape<N, T>;
+    constexpr int NIN = F::NIN, NOUT = F::NOUT, NR = F::NRED;
+    constexpr int L = S::L, E = S::EX, TPL = S::TPLX, LPB = S::XLPB, PITCH = S::XPITCH;
+    constexpr long NG = (long)N * N / LPB;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* stg = reinterpret_cast<cpx<T>*>(smem_raw);              // [NOUT-1][LPB][L]
+    cpx<T>* sm = stg + XFwdSmem<N, T, NOUT>::STAGE;                  // [LPB][PITCH]
+    const int ls = threadIdx.x / TPL, t = threadIdx.x % TPL;
+    const RowMap<E> map{ls * PITCH};
+    std::conditional_t<S::XTW_REG, TwReg<L, E, T>, TwTab<L, E, T>> tw;
+    if constexpr (S::XTW_REG) {
+        tw.load(twL, t);
+    } else {
+        cpx<T>* stw = sm + LPB * PITCH;
+        for (int i = threadIdx.x; i < L; i += blockDim.x) stw[i] = twL[i];
+        __syncthreads();
+        tw.tab = stw;
+    }
+    const cpx<T> wt = twN[t];  // W_N^t
+    const int nx = a.nx;
+    const int src_lane = (TPL - t) & (TPL - 1);
+    double acc[NR > 0 ? NR : 1];
+#pragma unroll
+    for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
+    for (long g = blockIdx.x; g < NG; g += gridDim.x) {
+        const long line = g * LPB + ls;
+        // 1. functor on the pairs (2p, 2p+1), p = t + TPL m
+        cpx<T> v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int p = t + TPL * m;
+            const long gi = line * N + 2 * p;
+            T in0[NIN], in1[NIN];
+#pragma unroll
+            for (int i = 0; i < NIN; ++i) {
+                const cpx<T> two = *reinterpret_cast<const cpx<T>*>(a.in[i] + gi);
+                in0[i] = two.x;
+                in1[i] = two.y;
+            }
+            T o0[NOUT > 0 ? NOUT : 1], o1[NOUT > 0 ? NOUT : 1];
+            f(in0, o0, acc);
+            f(in1, o1, acc);
+            v[m] = mk(o0[0], o1[0]);
+#pragma unroll
+            for (int o = 1; o < NOUT; ++o) stg[((o - 1) * LPB + ls) * L + p] = mk(o0[o], o1[o]);
+        }
+        // 2. per output: complex FFT of the packed row, half-spectrum split
+#pragma unroll 1
+        for (int o = 0; o < NOUT; ++o) {
+            if (o > 0) {
+#pragma unroll
+                for (int m = 0; m < E; ++m) v[m] = stg[((o - 1) * LPB + ls) * L + t + TPL * m];
+            }
+            cfft<L, E, -1, SyncWarp>(v, t, sm, map, tw);
+            cpx<T>* __restrict__ dst = a.out[o] + line * nx;
+            // X[k] = E[k] + W_N^k O[k], E = (Z_k + conj Z_{L-k})/2, O = -i (Z_k - conj Z_{L-k})/2
+            SFor<0, E>::run([&](auto mc) {
+                constexpr int m = decltype(mc)::value;
+                cpx<T> zp;  // Z[(L - k) mod L], k = t + TPL m
+                zp.x = __shfl_sync(0xffffffffu, v[E - 1 - m].x, src_lane, TPL);
+                zp.y = __shfl_sync(0xffffffffu, v[E - 1 - m].y, src_lane, TPL);
+                if (t == 0) zp = v[(E - m) % E];
+                const int k = t + TPL * m;
+                const cpx<T> zc = conj(zp);
+                const cpx<T> Ev = (v[m] + zc) * T(0.5);
+                const cpx<T> D = (v[m] - zc) * T(0.5);
+                const cpx<T> O = mk(D.y, -D.x);
+                const cpx<T> w = wt * cw<T, N, (long)TPL * m>();
+                if (k < nx) dst[k] = Ev + O * w;
+            });
+            // Nyquist column (full band only): X[N/2] = Re Z0 - Im Z0
+            if (t == 0 && L < nx) dst[L] = mk(v[0].x - v[0].y, T(0));
+            __syncwarp();
+        }
+    }
+    if constexpr (NR > 0) block_reduce_store<NR>(acc, a.partials, blockIdx.x);
+}
+
+// ----------------------------------------------------------------------------
 // y pass.  grid = (G, narr), block = TX * TPLY.  Items: (z, kx tile).
 // ----------------------------------------------------------------------------
 template <int N, int SIGN, typename T>

@@ -88,6 +88,7 @@ class EngineBase {
     void launched(const char* name = nullptr, double alg_bytes = 0.0, cudaEvent_t a = nullptr);
     cudaEvent_t prof_mark();
     bool prof_on = false;
+    bool prof_detail = false;  // x-stage launches keyed by functor as well
     struct KStat {
         long long n = 0;
         double ms = 0.0, bytes = 0.0;
@@ -222,6 +223,9 @@ class Engine : public EngineBase {
     int num_sms_ = 148;
     template <int NN>
     void xinv_c(XInvArgs<T>& xa, int narr);
+    template <int NN, class F>
+    void xfwd_c(XFwdArgs<T>& xa, const F& f);
+    long last_xblocks_ = 0;  // reduction records of the last x-stage launch
     template <int NN>
     void y_c(YArgs<T>& ya, int sign, int narr);
     template <int NN>

@@ -6,6 +6,10 @@
 #include <cstdlib>
 #include <cstring>
 #include <set>
+#include <string>
+#include <typeinfo>
+
+#include <cxxabi.h>
 
 #include "engine.cuh"
 
@@ -49,6 +53,21 @@ static bool dispatch_n(int n, Fn&& f) {
         case 1024: f(std::integral_constant<int, 1024>{}); return true;
         default: return false;
     }
+}
+
+// profile key of an x-stage launch: "x_fwd", or "x_fwd:<functor>" in detail mode
+template <class F>
+static const char* xfwd_name(bool detail) {
+    static const std::string name = [] {
+        int st = 0;
+        char* d = abi::__cxa_demangle(typeid(F).name(), nullptr, nullptr, &st);
+        std::string s = std::string("x_fwd:") + (st == 0 && d ? d : typeid(F).name());
+        std::free(d);
+        const std::string ns = "mlq::";
+        for (size_t p; (p = s.find(ns)) != std::string::npos;) s.erase(p, ns.size());
+        return s;
+    }();
+    return detail ? name.c_str() : "x_fwd";
 }
 
 static int grid_for(long work, int threads, int cap = 148 * 8) {

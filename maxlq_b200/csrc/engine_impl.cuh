@@ -159,14 +159,37 @@ void Engine<T>::zinv_c(ZInvArgs<T>& za, int narr) {
 }
 
 template <typename T>
+template <int NN, class F>
+void Engine<T>::xfwd_c(XFwdArgs<T>& xa, const F& f) {
+    using S = CShape<NN, T>;
+    const size_t smem = XFwdSmem<NN, T, F::NOUT>::BYTES;
+    auto kern = xfwd_c_kernel<NN, T, F>;
+    allow_smem(kern);
+    const int G = persistent_blocks((const void*)kern, 256, smem);
+    const long ng = (long)NN * NN / S::XLPB;
+    const int grid = (int)std::min<long>(ng, G);
+    last_xblocks_ = grid;
+    if (F::NRED > 0) ensure_partials((long)grid * F::NRED);
+    xa.partials = d_partials;
+    kern<<<grid, 256, smem, stream>>>(xa, f, d_twT_ + tw_off.at(NN / 2), d_twT_ + tw_off.at(NN));
+}
+
+template <typename T>
 template <class F>
 void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b) {
     const int h = n / 2;
     const double bytes = (double)n3 * sizeof(T) * F::NIN + (double)n * n * b.nx * sizeof(cpx<T>) * nout;
+    if (cfft_ok_) {
+        cudaEvent_t ev = prof_mark();
+        dispatch_n(n, [&](auto nc) { this->template xfwd_c<decltype(nc)::value>(xa, f); });
+        launched(xfwd_name<F>(prof_detail), bytes, ev);
+        return;
+    }
     if (reg_ok_) {
         xa.lx = reg_lx(nout, row_pitch(h));
         xa.tw_n_off = tw_off.at(n);
         const int grid = (int)(((long)n * n) / xa.lx);
+        last_xblocks_ = grid;
         if (F::NRED > 0) ensure_partials((long)grid * F::NRED);
         xa.partials = d_partials;
         const size_t sm = (size_t)nout * xa.lx * row_pitch(h) * sizeof(cpx<T>);
@@ -179,18 +202,19 @@ void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b
             allow_smem(xfwd_reg_kernel<16, T, F>);
             xfwd_reg_kernel<16, T, F><<<grid, thr, sm, stream>>>(xa, f, rplan(h), d_twT_);
         }
-        launched("x_fwd", bytes, ev);
+        launched(xfwd_name<F>(prof_detail), bytes, ev);
         return;
     }
     xa.lx = lx_for(nout);
     const int xgrid = (int)(((long)n * n) / xa.lx);
+    last_xblocks_ = xgrid;
     if (F::NRED > 0) ensure_partials((long)xgrid * F::NRED);
     xa.partials = d_partials;
     const size_t xsm = (size_t)2 * nout * xa.lx * h * sizeof(cpx<T>);
     allow_smem(xfwd_kernel<T, F>);
     cudaEvent_t ev = prof_mark();
     xfwd_kernel<T, F><<<xgrid, 256, xsm, stream>>>(xa, f);
-    launched("x_fwd", bytes, ev);
+    launched(xfwd_name<F>(prof_detail), bytes, ev);
 }
 
 template <typename T>
@@ -436,8 +460,7 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
     xa.tw_n_off = tw_off.at(n);
     xa.tw = d_tw;
     launch_xfwd(xa, f, NOUT, b);
-    const int xgrid = (int)(((long)n * n) / xa.lx);
-    if (F::NRED > 0 && fred_dst >= 0) finalize(xgrid, F::NRED, 1.0 / (double)n3, fred_dst);
+    if (F::NRED > 0 && fred_dst >= 0) finalize((int)last_xblocks_, F::NRED, 1.0 / (double)n3, fred_dst);
     if (NOUT == 0) return;
     // y forward
     YArgs<T> ya;
