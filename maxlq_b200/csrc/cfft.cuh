@@ -251,7 +251,9 @@ struct CShape {
     // where the registers are needed for the data
     static constexpr bool XTW_REG = sizeof(T) == 4;
     static constexpr int XLPB = 256 / TPLX;  // lines per x block
-    static constexpr int XPITCH = L + L / EX;
+    // row pitch: one pad element every EX; with two FP32 lines per warp the
+    // second line's row starts half the banks away
+    static constexpr int XPITCH = L + L / EX + (sizeof(T) == 4 && TPLX == 16 ? 8 : 0);
     static constexpr size_t XSMEM = ((size_t)XLPB * XPITCH + (XTW_REG ? 0 : L)) * sizeof(cpx<T>);
     // y/z passes: tile rows of TX columns (64 or 128 bytes)
     static constexpr int TX = sizeof(T) == 4 ? (N >= 512 ? 8 : 16) : 8;
@@ -368,6 +370,13 @@ struct XFwdSmem {
     static constexpr size_t BYTES = (STAGE + (size_t)S::XLPB * S::XPITCH + (S::XTW_REG ? 0 : S::L)) * sizeof(cpx<T>);
 };
 
+// positions whose inputs are loaded together: about 32 loads per thread
+__host__ __device__ constexpr int xfwd_chunk(int nin, int e) {
+    int c = 1;
+    while (2 * c <= e && 2 * c * nin <= 32) c *= 2;
+    return c;
+}
+
 // resident blocks the register budget aims at: light functors 2, heavy ones 1
 template <class F>
 constexpr int xfwd_minb() {
@@ -380,6 +389,7 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
     using S = CShape<N, T>;
     constexpr int NIN = F::NIN, NOUT = F::NOUT, NR = F::NRED;
     constexpr int L = S::L, E = S::EX, TPL = S::TPLX, LPB = S::XLPB, PITCH = S::XPITCH;
+    constexpr int CHX = xfwd_chunk(NIN, E);
     constexpr long NG = (long)N * N / LPB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* stg = reinterpret_cast<cpx<T>*>(smem_raw);              // [NOUT-1][LPB][L]
@@ -403,25 +413,34 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
     for (long g = blockIdx.x; g < NG; g += gridDim.x) {
         const long line = g * LPB + ls;
-        // 1. functor on the pairs (2p, 2p+1), p = t + TPL m
+        // 1. functor on the pairs (2p, 2p+1), p = t + TPL m.  The inputs of CHX
+        // positions are loaded before the functor runs on any of them, so
+        // CHX * NIN loads per thread are in flight.
         cpx<T> v[E];
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int p = t + TPL * m;
-            const long gi = line * N + 2 * p;
-            T in0[NIN], in1[NIN];
+        for (int m0 = 0; m0 < E; m0 += CHX) {
+            cpx<T> ld[CHX][NIN];
 #pragma unroll
-            for (int i = 0; i < NIN; ++i) {
-                const cpx<T> two = *reinterpret_cast<const cpx<T>*>(a.in[i] + gi);
-                in0[i] = two.x;
-                in1[i] = two.y;
+            for (int j = 0; j < CHX; ++j)
+#pragma unroll
+                for (int i = 0; i < NIN; ++i)
+                    ld[j][i] = *reinterpret_cast<const cpx<T>*>(a.in[i] + line * N + 2 * (t + TPL * (m0 + j)));
+#pragma unroll
+            for (int j = 0; j < CHX; ++j) {
+                const int p = t + TPL * (m0 + j);
+                T in0[NIN], in1[NIN];
+#pragma unroll
+                for (int i = 0; i < NIN; ++i) {
+                    in0[i] = ld[j][i].x;
+                    in1[i] = ld[j][i].y;
+                }
+                T o0[NOUT > 0 ? NOUT : 1], o1[NOUT > 0 ? NOUT : 1];
+                f(in0, o0, acc);
+                f(in1, o1, acc);
+                v[m0 + j] = mk(o0[0], o1[0]);
+#pragma unroll
+                for (int o = 1; o < NOUT; ++o) stg[((o - 1) * LPB + ls) * L + p] = mk(o0[o], o1[o]);
             }
-            T o0[NOUT > 0 ? NOUT : 1], o1[NOUT > 0 ? NOUT : 1];
-            f(in0, o0, acc);
-            f(in1, o1, acc);
-            v[m] = mk(o0[0], o1[0]);
-#pragma unroll
-            for (int o = 1; o < NOUT; ++o) stg[((o - 1) * LPB + ls) * L + p] = mk(o0[o], o1[o]);
         }
         // 2. per output: complex FFT of the packed row, half-spectrum split
 #pragma unroll 1
@@ -515,33 +534,6 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
 // the symbol rounds like the FP32 transforms around it; reductions stay FP64.
 // ----------------------------------------------------------------------------
 template <typename C>
-struct KvC {
-    C kx, ky, kz, ox, oy, oz, ksq;
-};
-
-template <typename C>
-__device__ __forceinline__ cpx<C> sym_c(int sym, int ab, const KvC<C>& k, cpx<C> v) {
-    switch (sym) {
-        case SYM_ZERO: return mk(C(0), C(0));
-        case SYM_ONE: return v;
-        case SYM_IKX: return mk(-k.ox * v.y, k.ox * v.x);
-        case SYM_IKY: return mk(-k.oy * v.y, k.oy * v.x);
-        case SYM_IKZ: return mk(-k.oz * v.y, k.oz * v.x);
-        case SYM_NEG_KSQ: return v * (-k.ksq);
-        case SYM_INV_KSQ: return k.ksq == C(0) ? mk(C(0), C(0)) : v * (C(1) / k.ksq);
-        case SYM_NEG_INV_KSQ: return k.ksq == C(0) ? mk(C(0), C(0)) : v * (C(-1) / k.ksq);
-        case SYM_KK_KSQ: {
-            if (k.ksq == C(0)) return mk(C(0), C(0));
-            const int ia = ab / 3, ib = ab % 3;
-            const C ka = ia == 0 ? k.ox : (ia == 1 ? k.oy : k.oz);
-            const C kb = ib == 0 ? k.ox : (ib == 1 ? k.oy : k.oz);
-            return v * (ka * kb / k.ksq);
-        }
-    }
-    return v;
-}
-
-template <typename C>
 __device__ __forceinline__ cpx<C> ld_spec_c(const void* p, int f64, long idx) {
     if (f64) {
         const double2 v = reinterpret_cast<const double2*>(p)[idx];
@@ -556,6 +548,50 @@ __device__ __forceinline__ void st_spec_c(void* p, int f64, long idx, cpx<C> v) 
         reinterpret_cast<double2*>(p)[idx] = make_double2((double)v.x, (double)v.y);
     else
         reinterpret_cast<float2*>(p)[idx] = make_float2((float)v.x, (float)v.y);
+}
+
+// A spectral symbol times a coefficient in branch-free form:
+//   f(k) = c1 + ck o_a + cq |K|^2 + (ci + ckk o_a o_b) / |K|^2   (last term 0 at K = 0)
+// applied as f v, or i f v for the odd (first-derivative) symbols.  Every Sym
+// is a special case; the per-element work is a few selects and FMAs instead
+// of a switch.
+template <typename C>
+struct SymD {
+    C c1, ck, cq, ci, ckk;
+    int a, b;
+    bool odd, inv;
+};
+template <typename C>
+__device__ __forceinline__ SymD<C> make_symd(int sym, int ab, double coef) {
+    SymD<C> d{C(0), C(0), C(0), C(0), C(0), 0, 0, false, false};
+    const C c = (C)coef;
+    switch (sym) {
+        case SYM_ONE: d.c1 = c; break;
+        case SYM_IKX: d.ck = c; d.a = 0; d.odd = true; break;
+        case SYM_IKY: d.ck = c; d.a = 1; d.odd = true; break;
+        case SYM_IKZ: d.ck = c; d.a = 2; d.odd = true; break;
+        case SYM_NEG_KSQ: d.cq = -c; break;
+        case SYM_INV_KSQ: d.ci = c; d.inv = true; break;
+        case SYM_NEG_INV_KSQ: d.ci = -c; d.inv = true; break;
+        case SYM_KK_KSQ: d.ckk = c; d.a = ab / 3; d.b = ab % 3; d.inv = true; break;
+        default: break;  // SYM_ZERO: f = 0
+    }
+    return d;
+}
+// rinv = 1/|K|^2 (0 at K = 0), needed only when d.inv
+template <typename C>
+__device__ __forceinline__ cpx<C> sym_apply(const SymD<C>& d, C ox, C oy, C oz, C ksq, C rinv, cpx<C> v) {
+    const C oa = d.a == 0 ? ox : (d.a == 1 ? oy : oz);
+    C f = d.c1 + d.ck * oa + d.cq * ksq;
+    if (d.inv) {
+        const C ob = d.b == 0 ? ox : (d.b == 1 ? oy : oz);
+        f += rinv * (d.ci + d.ckk * oa * ob);
+    }
+    return d.odd ? mk(-f * v.y, f * v.x) : mk(f * v.x, f * v.y);
+}
+template <typename C>
+__device__ __forceinline__ C rinv_of(C ksq) {
+    return ksq == C(0) ? C(0) : C(1) / ksq;
 }
 
 // K table (2 pi j, then the odd-factor copy) of length 2N in shared memory
@@ -635,8 +671,8 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
     const int plane = nb * nx;
     const cpx<T>* __restrict__ src = reinterpret_cast<const cpx<T>*>(op.in);
     cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
-    const int sym = op.sym, sym_ab = op.sym_ab, add_sym = op.add_sym, add_ab = op.add_ab;
-    const C norm = (C)a.norm, add_coef = (C)op.add_coef;
+    const SymD<C> dmain = make_symd<C>(op.sym, op.sym_ab, a.norm);  // the 1/N^3 folded in
+    const SymD<C> dadd = make_symd<C>(op.add_sym, op.add_ab, op.add_coef);
     const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
     double acc_self = 0.0, acc_w0 = 0.0, acc_w1 = 0.0, acc_w2 = 0.0;
     for (long it = blockIdx.x; it < items; it += gridDim.x) {
@@ -649,22 +685,19 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
         for (int m = 0; m < E; ++m) v[m] = ok ? src[(t + TPL * m) * plane + col] : czero<T>();
         cfft<N, E, -1, SyncBlock>(v, t, sm, map, tw);
         const int fy = band_fft_index(a.band, cy);
-        KvC<C> k;
-        k.kx = kt[col - cy * nx];
-        k.ox = kt[N + col - cy * nx];
-        k.ky = kt[fy];
-        k.oy = kt[N + fy];
-        const C kxy2 = k.kx * k.kx + k.ky * k.ky;
+        const int kxc = col - cy * nx;
+        const C kxv = kt[kxc], ox = kt[N + kxc], kyv = kt[fy], oy = kt[N + fy];
+        const C kxy2 = kxv * kxv + kyv * kyv;
         const double wgt = kx_weight(N, kx);
         const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
         cpx<C> Y[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int fz = t + TPL * m;
-            k.kz = kt[fz];
-            k.oz = kt[N + fz];
-            k.ksq = kxy2 + k.kz * k.kz;
-            Y[m] = idx.valid(m) ? sym_c(sym, sym_ab, k, mk((C)v[m].x, (C)v[m].y) * norm) : mk(C(0), C(0));
+            const C kz = kt[fz], oz = kt[N + fz];
+            const C ksq = kxy2 + kz * kz;
+            const C ri = dmain.inv ? rinv_of(ksq) : C(0);
+            Y[m] = idx.valid(m) ? sym_apply(dmain, ox, oy, oz, ksq, ri, mk((C)v[m].x, (C)v[m].y)) : mk(C(0), C(0));
         }
         if (op.add) {
 #pragma unroll
@@ -674,10 +707,10 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
 #pragma unroll
                 for (int j = 0; j < CH; ++j) {
                     const int fz = t + TPL * (m0 + j);
-                    k.kz = kt[fz];
-                    k.oz = kt[N + fz];
-                    k.ksq = kxy2 + k.kz * k.kz;
-                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_c(add_sym, add_ab, k, A[j]) * add_coef;
+                    const C kz = kt[fz], oz = kt[N + fz];
+                    const C ksq = kxy2 + kz * kz;
+                    const C ri = dadd.inv ? rinv_of(ksq) : C(0);
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(dadd, ox, oy, oz, ksq, ri, A[j]);
                 }
             }
         }
@@ -772,31 +805,29 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
         const bool ok = kx < nx;
         const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
         const int fy = band_fft_index(a.band, cy);
-        KvC<C> k;
-        k.kx = kt[col - cy * nx];
-        k.ox = kt[N + col - cy * nx];
-        k.ky = kt[fy];
-        k.oy = kt[N + fy];
-        const C kxy2 = k.kx * k.kx + k.ky * k.ky;
+        const int kxc = col - cy * nx;
+        const C kxv = kt[kxc], ox = kt[N + kxc], kyv = kt[fy], oy = kt[N + fy];
+        const C kxy2 = kxv * kxv + kyv * kyv;
         const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
         cpx<C> Y[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) Y[m] = mk(C(0), C(0));
 #pragma unroll 1
         for (int s = 0; s < nsrc; ++s) {
-            const ZSrc zs = op.src[s];
-            const C coef = (C)zs.coef;
+            const void* spec = op.src[s].spec;
+            const int f64 = op.src[s].f64;
+            const SymD<C> d = make_symd<C>(op.src[s].sym, op.src[s].ab, op.src[s].coef);
 #pragma unroll
             for (int m0 = 0; m0 < E; m0 += CH) {
                 cpx<C> V[CH];
-                ld_chunk<CH>(zs.spec, zs.f64, idx, m0, V);
+                ld_chunk<CH>(spec, f64, idx, m0, V);
 #pragma unroll
                 for (int j = 0; j < CH; ++j) {
                     const int fz = t + TPL * (m0 + j);
-                    k.kz = kt[fz];
-                    k.oz = kt[N + fz];
-                    k.ksq = kxy2 + k.kz * k.kz;
-                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_c(zs.sym, zs.ab, k, V[j]) * coef;
+                    const C kz = kt[fz], oz = kt[N + fz];
+                    const C ksq = kxy2 + kz * kz;
+                    const C ri = d.inv ? rinv_of(ksq) : C(0);
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(d, ox, oy, oz, ksq, ri, V[j]);
                 }
             }
         }

@@ -178,7 +178,14 @@ template <typename T>
 template <class F>
 void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b) {
     const int h = n / 2;
-    const double bytes = (double)n3 * sizeof(T) * F::NIN + (double)n * n * b.nx * sizeof(cpx<T>) * nout;
+    // compulsory bytes: each distinct input field read once, each output written once
+    int nin_distinct = 0;
+    for (int i = 0; i < F::NIN; ++i) {
+        bool seen = false;
+        for (int j = 0; j < i; ++j) seen = seen || xa.in[j] == xa.in[i];
+        nin_distinct += seen ? 0 : 1;
+    }
+    const double bytes = (double)n3 * sizeof(T) * nin_distinct + (double)n * n * b.nx * sizeof(cpx<T>) * nout;
     if (cfft_ok_) {
         cudaEvent_t ev = prof_mark();
         dispatch_n(n, [&](auto nc) { this->template xfwd_c<decltype(nc)::value>(xa, f); });
