@@ -350,6 +350,7 @@ def main():
                           f"{workers} threads), scaled by the reference's {REF_T_PER_ITER} + {REF_T_PER_TRIAL} x "
                           f"{ne:.1f} transforms per CG iteration")}
 
+    kcfg = mixed.kernel_config()
     per_kernel = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
                       "GB/s": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in prof.items()}
     if dist.rank == 0:
@@ -365,7 +366,8 @@ def main():
                        "rel_dR_mixed_vs_fp64": rel_dR,
                        "line_search_trials_per_iter": float(np.mean(n_evals)) if n_evals else None,
                        "l2": "working set (GBs) far above the 126 MB L2; no flush needed",
-                       "parallelism": f"replicas x{dist.world}"},
+                       "parallelism": f"replicas x{dist.world}",
+                       "kernels": kcfg},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": res_m["launches"],
             "clocks": clk, "wall_s_timed": res_m["wall_s"], "per_kernel": per_kernel,
         }

@@ -170,6 +170,11 @@ int mlq_profile_enable(mlq_ctx* ctx, int on);
 /* JSON object {kernel: [launches, total_ms, algorithmic_bytes]} of the launches
  * since the last reset; resets when reset != 0.  Returns the length needed. */
 int mlq_profile_report(mlq_ctx* ctx, char* buf, int len, int reset);
+/* JSON object describing the pass kernels the context runs: precision,
+ * kernel family (compile-time / register / shared-memory Stockham) and the
+ * y/z tile shapes the autotuner chose with their timings.  No counterpart in
+ * the reference (it has a single FFTW path).  Returns the length needed. */
+int mlq_kernel_config(mlq_ctx* ctx, char* buf, int len);
 
 /* ---- synthetic inputs ------------------------------------------------------ */
 /* Seeded divergence-free, 2/3-dealiased field with amplitude

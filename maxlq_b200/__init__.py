@@ -347,6 +347,16 @@ class MaxLq:
         self._lib.mlq_profile_report(self._ctx, buf, need + 16, 1 if reset else 0)
         return {k: {"launches": v[0], "ms": v[1], "bytes": v[2]} for k, v in json.loads(buf.value.decode()).items()}
 
+    def kernel_config(self) -> dict:
+        """Pass-kernel family, precision and the autotuned y/z tile shapes."""
+        import json
+        need = self._lib.mlq_kernel_config(self._ctx, None, 0)
+        if need < 0:
+            self._check(-need, "kernel_config")
+        buf = C.create_string_buffer(need + 16)
+        self._lib.mlq_kernel_config(self._ctx, buf, need + 16)
+        return json.loads(buf.value.decode())
+
     def seed_field(self, seed: int = 0, slope: float = 2.0, k0: float = 4.0):
         u = np.empty((3, self.n, self.n, self.n))
         self._check(self._lib.mlq_seed_field(self._ctx, seed, slope, k0, dptr(u)), "seed_field")

@@ -113,6 +113,7 @@ SIGNATURES = {
     "mlq_state_step": (C.c_int, [_VP, _DP, ITER_CB, _VP]),
     "mlq_profile_enable": (C.c_int, [_VP, C.c_int]),
     "mlq_profile_report": (C.c_int, [_VP, C.c_char_p, C.c_int, C.c_int]),
+    "mlq_kernel_config": (C.c_int, [_VP, C.c_char_p, C.c_int]),
     "mlq_seed_field": (C.c_int, [_VP, C.c_ulonglong, C.c_double, C.c_double, _DP]),
     "mlq_seed_spectrum": (C.c_int, [C.c_int, C.c_ulonglong, C.c_double, C.c_double, _DP, C.POINTER(C.c_int)]),
     "mlq_band_cut": (C.c_int, [C.c_int, C.c_double]),

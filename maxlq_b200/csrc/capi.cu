@@ -312,6 +312,18 @@ int mlq_profile_report(mlq_ctx* c, char* buf, int len, int reset) {
     return (int)r.size() + 1;
 }
 
+int mlq_kernel_config(mlq_ctx* c, char* buf, int len) {
+    if (!c) return -MLQ_ERR_BADARG;
+    std::string r;
+    int st = guard(c, [&] { r = c->solver->eng().kernel_config(); });
+    if (st != MLQ_OK) return -st;
+    if (buf && len > 0) {
+        std::strncpy(buf, r.c_str(), (size_t)len - 1);
+        buf[len - 1] = 0;
+    }
+    return (int)r.size() + 1;
+}
+
 int mlq_seed_field(mlq_ctx* c, unsigned long long seed, double slope, double k0, double* u) {
     return guard(c, [&] { c->solver->seed_field(seed, slope, k0, u); });
 }

@@ -260,11 +260,30 @@ struct CShape {
     static constexpr int EY = sizeof(T) == 4 ? (N >= 256 ? 16 : (N >= 128 ? 8 : 4)) : (N >= 1024 ? 16 : (N >= 128 ? 8 : 4));
     static constexpr int TPLY = N / EY;
     static constexpr int YTHREADS = TX * TPLY;
-    static constexpr int YMINB = YTHREADS <= 256 ? 2 : 1;  // resident blocks the register budget aims at
-    static constexpr size_t YSMEM = ((size_t)N * TX + N) * sizeof(cpx<T>);
-    static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);  // + the K table
     static_assert(TPLX <= 32 && 32 % TPLX == 0, "x line within a warp");
     static_assert(YTHREADS % 32 == 0 && YTHREADS <= 512, "y/z block");
+};
+
+// y/z tile shape, variant V of (N, T).  V = 0 is the default of CShape; V = 1
+// and V = 2 are the alternatives the engine's autotuner times at start-up
+// (FP32: 8 elements per thread, or 16-column tiles; FP64: 16 elements per
+// thread, or 4-column tiles).  `valid` is false for a variant that does not
+// fit a block or repeats V = 0; such variants are never instantiated.
+template <int N, typename T, int V>
+struct YShape {
+    static constexpr bool F32 = sizeof(T) == 4;
+    static constexpr int EY = V == 0 ? CShape<N, T>::EY : (V == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8));
+    static constexpr int TX = V == 0 ? CShape<N, T>::TX : (V == 1 ? 8 : (F32 ? 16 : 4));
+    static constexpr int TPLY = N / EY;
+    static constexpr int YTHREADS = TX * TPLY;
+    // resident blocks the register budget aims at (8 elements per thread in
+    // FP32 leave room for two 512-thread blocks: 64 registers)
+    static constexpr int YMINB = YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1);
+    static constexpr size_t YSMEM = ((size_t)N * TX + N) * sizeof(cpx<T>);
+    static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);  // + the K table
+    static constexpr bool valid =
+        V == 0 || (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 &&
+                   (EY != CShape<N, T>::EY || TX != CShape<N, T>::TX));
 };
 
 // block-wide deterministic reduction of NR accumulators into partials[slot]
@@ -477,10 +496,10 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
 // ----------------------------------------------------------------------------
 // y pass.  grid = (G, narr), block = TX * TPLY.  Items: (z, kx tile).
 // ----------------------------------------------------------------------------
-template <int N, int SIGN, typename T>
-__global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
+template <int N, int V, int SIGN, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
     ypass_c_kernel(YArgs<T> a, const cpx<T>* __restrict__ twN) {
-    using S = CShape<N, T>;
+    using S = YShape<N, T, V>;
     constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
@@ -648,10 +667,10 @@ struct ZCol {
 // z stage, forward (+ optional round trip).  grid = (G, narr); items (cy, tile).
 // One reduction record of MAX_RED partials per block.
 // ----------------------------------------------------------------------------
-template <int N, typename T>
-__global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
+template <int N, int V, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
     zfwd_c_kernel(ZFwdArgs<T> a, const cpx<T>* __restrict__ twN) {
-    using S = CShape<N, T>;
+    using S = YShape<N, T, V>;
     using C = T;
     constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -776,10 +795,10 @@ __global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
 // ----------------------------------------------------------------------------
 // z stage, inverse from spectra.  grid = (G, narr); items (cy, tile).
 // ----------------------------------------------------------------------------
-template <int N, typename T>
-__global__ void __launch_bounds__(CShape<N, T>::YTHREADS, CShape<N, T>::YMINB)
+template <int N, int V, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
     zinv_c_kernel(ZInvArgs<T> a, const cpx<T>* __restrict__ twN) {
-    using S = CShape<N, T>;
+    using S = YShape<N, T, V>;
     using C = T;
     constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];

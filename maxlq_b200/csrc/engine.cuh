@@ -96,6 +96,7 @@ class EngineBase {
     std::map<std::string, KStat> prof;
     void prof_flush();
     std::string prof_report(bool reset);
+    virtual std::string kernel_config() const { return "{}"; }
 
    private:
     struct Pend {
@@ -228,6 +229,20 @@ class Engine : public EngineBase {
     long last_xblocks_ = 0;  // reduction records of the last x-stage launch
     template <int NN>
     void y_c(YArgs<T>& ya, int sign, int narr);
+    template <int NN, int V>
+    void y_cv(YArgs<T>& ya, int sign, int narr);
+    template <int NN, int V>
+    void zfwd_cv(ZFwdArgs<T>& za, int narr);
+    template <int NN, int V>
+    void zinv_cv(ZInvArgs<T>& za, int narr);
+    template <int NN, class Fn>
+    void with_variant(int kind, Fn&& f);
+    // y/z tile-shape variant per pass kind, chosen by tune_yz()
+    enum { YV_YFWD = 0, YV_YINV = 1, YV_ZFWD = 2, YV_ZINV = 3, YV_KINDS = 4 };
+    int yvar_[YV_KINDS] = {0, 0, 0, 0};
+    void tune_yz();
+    std::string tune_report_;
+    std::string kernel_config() const override;
     template <int NN>
     void zfwd_c(ZFwdArgs<T>& za, int narr);
     template <int NN>

@@ -45,6 +45,7 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
         for (long i = 0; i < ntw; ++i) hf[i] = mk<T>((T)h[i].x, (T)h[i].y);
         MLQ_CUDA(cudaMemcpy(d_twT_, hf.data(), ntw * sizeof(cpx<T>), cudaMemcpyHostToDevice));
     }
+    tune_yz();
 }
 
 template <typename T>
@@ -111,10 +112,11 @@ void Engine<T>::xinv_c(XInvArgs<T>& xa, int narr) {
     kern<<<grid, 256, smem, stream>>>(xa, d_twT_ + tw_off.at(NN / 2), d_twT_ + tw_off.at(NN));
 }
 
+// y/z launches of tile-shape variant V (cfft.cuh YShape)
 template <typename T>
-template <int NN>
-void Engine<T>::y_c(YArgs<T>& ya, int sign, int narr) {
-    using S = CShape<NN, T>;
+template <int NN, int V>
+void Engine<T>::y_cv(YArgs<T>& ya, int sign, int narr) {
+    using S = YShape<NN, T, V>;
     const size_t smem = S::YSMEM;
     const long items = (long)NN * ((ya.nx + S::TX - 1) / S::TX);
     auto run = [&](auto kern) {
@@ -124,18 +126,18 @@ void Engine<T>::y_c(YArgs<T>& ya, int sign, int narr) {
         kern<<<grid, S::YTHREADS, smem, stream>>>(ya, d_twT_ + tw_off.at(NN));
     };
     if (sign < 0)
-        run(ypass_c_kernel<NN, -1, T>);
+        run(ypass_c_kernel<NN, V, -1, T>);
     else
-        run(ypass_c_kernel<NN, +1, T>);
+        run(ypass_c_kernel<NN, V, +1, T>);
 }
 
 template <typename T>
-template <int NN>
-void Engine<T>::zfwd_c(ZFwdArgs<T>& za, int narr) {
-    using S = CShape<NN, T>;
+template <int NN, int V>
+void Engine<T>::zfwd_cv(ZFwdArgs<T>& za, int narr) {
+    using S = YShape<NN, T, V>;
     const size_t smem = S::ZSMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
-    auto kern = zfwd_c_kernel<NN, T>;
+    auto kern = zfwd_c_kernel<NN, V, T>;
     allow_smem(kern);
     const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
     dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
@@ -146,16 +148,189 @@ void Engine<T>::zfwd_c(ZFwdArgs<T>& za, int narr) {
 }
 
 template <typename T>
-template <int NN>
-void Engine<T>::zinv_c(ZInvArgs<T>& za, int narr) {
-    using S = CShape<NN, T>;
+template <int NN, int V>
+void Engine<T>::zinv_cv(ZInvArgs<T>& za, int narr) {
+    using S = YShape<NN, T, V>;
     const size_t smem = S::ZSMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
-    auto kern = zinv_c_kernel<NN, T>;
+    auto kern = zinv_c_kernel<NN, V, T>;
     allow_smem(kern);
     const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
     dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
     kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+}
+
+// f(std::integral_constant<int, V>) for the variant chosen for pass `kind`
+template <typename T>
+template <int NN, class Fn>
+void Engine<T>::with_variant(int kind, Fn&& f) {
+    const int v = yvar_[kind];
+    if constexpr (YShape<NN, T, 1>::valid) {
+        if (v == 1) return f(std::integral_constant<int, 1>{});
+    }
+    if constexpr (YShape<NN, T, 2>::valid) {
+        if (v == 2) return f(std::integral_constant<int, 2>{});
+    }
+    f(std::integral_constant<int, 0>{});
+}
+
+template <typename T>
+template <int NN>
+void Engine<T>::y_c(YArgs<T>& ya, int sign, int narr) {
+    with_variant<NN>(sign < 0 ? YV_YFWD : YV_YINV,
+                     [&](auto vc) { this->template y_cv<NN, decltype(vc)::value>(ya, sign, narr); });
+}
+
+template <typename T>
+template <int NN>
+void Engine<T>::zfwd_c(ZFwdArgs<T>& za, int narr) {
+    with_variant<NN>(YV_ZFWD, [&](auto vc) { this->template zfwd_cv<NN, decltype(vc)::value>(za, narr); });
+}
+
+template <typename T>
+template <int NN>
+void Engine<T>::zinv_c(ZInvArgs<T>& za, int narr) {
+    with_variant<NN>(YV_ZINV, [&](auto vc) { this->template zinv_cv<NN, decltype(vc)::value>(za, narr); });
+}
+
+template <typename T>
+std::string Engine<T>::kernel_config() const {
+    const char* fam = cfft_ok_ ? "compile-time" : (reg_ok_ ? "register" : "shared-memory");
+    std::string r = std::string("{\"precision\": \"") + (sizeof(T) == 4 ? "fp32" : "fp64") +
+                    "\", \"pass_kernels\": \"" + fam + "\", \"yz_variants\": \"" +
+                    (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
+    return r;
+}
+
+// Autotuner: time every valid y/z tile-shape variant of each pass kind on
+// scratch buffers of the state band (three arrays, as the programs launch
+// them) and keep the fastest.  Runs once per engine, before the programs
+// allocate their buffers.  MLQ_AUTOTUNE=0 keeps variant 0 everywhere.
+template <typename T>
+void Engine<T>::tune_yz() {
+    tune_report_.clear();
+    if (!cfft_ok_) return;
+    if (const char* e = std::getenv("MLQ_AUTOTUNE"))
+        if (std::string(e) == "0") return;
+    bool any = false;
+    dispatch_n(n, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid;
+    });
+    if (!any) return;
+    if (const char* e = std::getenv("MLQ_YZ_VARIANT")) {  // fixed variant (measurement runs)
+        const int v = std::atoi(e);
+        bool ok = v == 0;
+        dispatch_n(n, [&](auto nc) {
+            constexpr int NN = decltype(nc)::value;
+            ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid);
+        });
+        if (ok)
+            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
+        tune_report_ = std::string("fixed by MLQ_YZ_VARIANT=") + e;
+        return;
+    }
+    const Band b = b2;
+    constexpr int NA = 3;
+    const long xs_n = (long)n * n * b.nx, ys_n = (long)n * b.nb * b.nx, sp_n = (long)b.nb * b.nb * b.nx;
+    cpx<T>* A = (cpx<T>*)dev_alloc(NA * xs_n * sizeof(cpx<T>));
+    cpx<T>* B = (cpx<T>*)dev_alloc(NA * ys_n * sizeof(cpx<T>));
+    double2* C = (double2*)dev_alloc(NA * sp_n * sizeof(double2));
+    MLQ_CUDA(cudaMemsetAsync(A, 0, NA * xs_n * sizeof(cpx<T>), stream));
+    MLQ_CUDA(cudaMemsetAsync(B, 0, NA * ys_n * sizeof(cpx<T>), stream));
+    MLQ_CUDA(cudaMemsetAsync(C, 0, NA * sp_n * sizeof(double2), stream));
+    YArgs<T> yf{}, yi{};
+    yf.n = yi.n = n;
+    yf.nx = yi.nx = b.nx;
+    yf.band = yi.band = b;
+    ZFwdArgs<T> zf{};
+    zf.n = n;
+    zf.nx = b.nx;
+    zf.band = b;
+    zf.norm = 1.0 / (double)n3;
+    ZInvArgs<T> zi{};
+    zi.n = n;
+    zi.nx = b.nx;
+    zi.band = b;
+    for (int a = 0; a < NA; ++a) {
+        yf.in[a] = A + a * xs_n;
+        yf.out[a] = B + a * ys_n;
+        yi.in[a] = B + a * ys_n;
+        yi.out[a] = A + a * xs_n;
+        ZFwdOp op = {};
+        op.in = B + a * ys_n;
+        op.spec_out = C + a * sp_n;
+        op.spec_f64 = 1;
+        op.sym = SYM_ONE;
+        op.red_self = 0;
+        for (int r = 0; r < 3; ++r) op.red_with_slot[r] = -1;
+        zf.op[a] = op;
+        ZInvOp oi = {};
+        oi.src[0] = ZSrc{C + a * sp_n, 1, SYM_IKX, 0, 1.0};
+        oi.nsrc = 1;
+        oi.ys_out = B + a * ys_n;
+        zi.op[a] = oi;
+    }
+    cudaEvent_t e0, e1;
+    MLQ_CUDA(cudaEventCreate(&e0));
+    MLQ_CUDA(cudaEventCreate(&e1));
+    const char* names[YV_KINDS] = {"y_fwd", "y_inv", "z_fwd", "z_inv"};
+    auto launch = [&](int kind) {
+        dispatch_n(n, [&](auto nc) {
+            constexpr int NN = decltype(nc)::value;
+            if (kind == YV_YFWD) y_c<NN>(yf, -1, NA);
+            if (kind == YV_YINV) y_c<NN>(yi, +1, NA);
+            if (kind == YV_ZFWD) zfwd_c<NN>(zf, NA);
+            if (kind == YV_ZINV) zinv_c<NN>(zi, NA);
+        });
+        MLQ_CUDA(cudaGetLastError());
+    };
+    bool valid[3] = {true, false, false};
+    dispatch_n(n, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        valid[1] = YShape<NN, T, 1>::valid;
+        valid[2] = YShape<NN, T, 2>::valid;
+    });
+    // every variant of every kind once first (clocks, attributes, page-in)
+    for (int kind = 0; kind < YV_KINDS; ++kind)
+        for (int v = 0; v < 3; ++v)
+            if (valid[v]) {
+                yvar_[kind] = v;
+                launch(kind);
+            }
+    // then round-robin single launches, best of 5 per variant; a variant
+    // replaces variant 0 only when it is at least 3 % faster
+    std::string rep;
+    for (int kind = 0; kind < YV_KINDS; ++kind) {
+        float best_ms[3] = {1e30f, 1e30f, 1e30f};
+        for (int r = 0; r < 5; ++r)
+            for (int v = 0; v < 3; ++v) {
+                if (!valid[v]) continue;
+                yvar_[kind] = v;
+                MLQ_CUDA(cudaEventRecord(e0, stream));
+                launch(kind);
+                MLQ_CUDA(cudaEventRecord(e1, stream));
+                MLQ_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                MLQ_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                best_ms[v] = std::min(best_ms[v], ms);
+            }
+        int bestv = 0;
+        std::string times;
+        for (int v = 0; v < 3; ++v) {
+            if (!valid[v]) continue;
+            times += (times.empty() ? "" : " ") + std::to_string(v) + ":" + std::to_string(best_ms[v]);
+            if (best_ms[v] < 0.97f * best_ms[bestv]) bestv = v;
+        }
+        yvar_[kind] = bestv;
+        rep += std::string(rep.empty() ? "" : "; ") + names[kind] + " v" + std::to_string(bestv) + " (" + times + " ms)";
+    }
+    MLQ_CUDA(cudaEventDestroy(e0));
+    MLQ_CUDA(cudaEventDestroy(e1));
+    free_dev(A);
+    free_dev(B);
+    free_dev(C);
+    tune_report_ = rep;
 }
 
 template <typename T>
