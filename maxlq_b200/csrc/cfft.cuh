@@ -181,6 +181,25 @@ struct SyncBlock {
     __device__ __forceinline__ static void sync() { __syncthreads(); }
 };
 
+// Asynchronous global -> shared copy of one complex element (cp.async, sm_80+):
+// the element is zero-filled when `valid` is false (src-size 0; the source
+// address must still be a mapped one).  Completion is awaited per thread with
+// cp_async_wait_all(), so a thread may read what it copied itself without a
+// barrier.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(cpx<T>* sdst, const cpx<T>* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (sizeof(cpx<T>) == 8) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0)
+                     : "memory");
+    } else {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 16 : 0)
+                     : "memory");
+    }
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
 // shared-memory maps of a line's positions
 template <int E>
 struct RowMap {  // one row per line, one pad element every E
@@ -256,7 +275,7 @@ struct CShape {
     static constexpr int XPITCH = L + L / EX + (sizeof(T) == 4 && TPLX == 16 ? 8 : 0);
     static constexpr size_t XSMEM = ((size_t)XLPB * XPITCH + (XTW_REG ? 0 : L)) * sizeof(cpx<T>);
     // y/z passes: tile rows of TX columns (64 or 128 bytes)
-    static constexpr int TX = sizeof(T) == 4 ? (N >= 512 ? 8 : 16) : 8;
+    static constexpr int TX = sizeof(T) == 4 ? (N >= 512 ? 8 : 16) : (N >= 1024 ? 4 : 8);
     static constexpr int EY = sizeof(T) == 4 ? (N >= 256 ? 16 : (N >= 128 ? 8 : 4)) : (N >= 1024 ? 16 : (N >= 128 ? 8 : 4));
     static constexpr int TPLY = N / EY;
     static constexpr int YTHREADS = TX * TPLY;
@@ -279,11 +298,15 @@ struct YShape {
     // resident blocks the register budget aims at (8 elements per thread in
     // FP32 leave room for two 512-thread blocks: 64 registers)
     static constexpr int YMINB = YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1);
-    static constexpr size_t YSMEM = ((size_t)N * TX + N) * sizeof(cpx<T>);
-    static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);  // + the K table
+    // two tiles (the staged next item, and the current item's exchange
+    // buffer) + the twiddle table; the z stage adds the K table
+    static constexpr size_t YSMEM = ((size_t)2 * N * TX + N) * sizeof(cpx<T>);
+    static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);
+    static constexpr size_t ZISMEM = ((size_t)N * TX + N) * sizeof(cpx<T>) + 2 * N * sizeof(T);  // z inverse: one tile
     static constexpr bool valid =
-        V == 0 || (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 &&
+        V == 0 || (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
                    (EY != CShape<N, T>::EY || TX != CShape<N, T>::TX));
+    static_assert(V != 0 || ZSMEM <= 200 * 1024, "default y/z tile fits the shared-memory limit");
 };
 
 // block-wide deterministic reduction of NR accumulators into partials[slot]
@@ -502,8 +525,9 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     using S = YShape<N, T, V>;
     constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* stw = sm + N * TX;
+    cpx<T>* buf0 = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* buf1 = buf0 + N * TX;
+    cpx<T>* stw = buf1 + N * TX;
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
     __syncthreads();
     const TwTab<N, E, T> tw{stw};
@@ -514,23 +538,41 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const long items = (long)N * ntile;
     const cpx<T>* __restrict__ src = a.in[blockIdx.y];
     cpx<T>* __restrict__ dst = a.out[blockIdx.y];
-    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+    // stage item `it` (column tile of plane z) into buffer b, asynchronously
+    auto stage = [&](long it, cpx<T>* b) {
         const int z = (int)(it / ntile);
         const int kx = (int)(it - (long)z * ntile) * TX + l;
         const bool ok = kx < nx;
-        cpx<T> v[E];
+        const int kxc = ok ? kx : nx - 1;
 #pragma unroll
         for (int m = 0; m < E; ++m) {
             const int p = t + TPL * m;
             if constexpr (SIGN < 0) {
-                v[m] = ok ? src[((long)z * N + p) * nx + kx] : czero<T>();
+                cp_async_elem(b + p * TX + l, src + ((long)z * N + p) * nx + kxc, ok);
             } else {
                 const int ci = band_compact_index(a.band, p);
-                v[m] = (ok && ci >= 0) ? src[((long)z * nb + ci) * nx + kx] : czero<T>();
+                cp_async_elem(b + p * TX + l, src + ((long)z * nb + (ci >= 0 ? ci : 0)) * nx + kxc, ok && ci >= 0);
             }
         }
-        cfft<N, E, SIGN, SyncBlock>(v, t, sm, map, tw);
-        if (ok) {
+        cp_async_commit();
+    };
+    long it = blockIdx.x;
+    if (it < items) stage(it, buf0);
+    for (int k = 0; it < items; it += gridDim.x, k ^= 1) {
+        cpx<T>* cur = k ? buf1 : buf0;
+        cpx<T>* nxt = k ? buf0 : buf1;
+        cp_async_wait_all();
+        cpx<T> v[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = cur[map(t + TPL * m)];
+        // every thread has its tile in registers and the previous transform is
+        // done: cur becomes this transform's exchange buffer, nxt the next stage
+        __syncthreads();
+        if (it + gridDim.x < items) stage(it + gridDim.x, nxt);
+        cfft<N, E, SIGN, SyncBlock>(v, t, cur, map, tw);
+        const int z = (int)(it / ntile);
+        const int kx = (int)(it - (long)z * ntile) * TX + l;
+        if (kx < nx) {
 #pragma unroll
             for (int m = 0; m < E; ++m) {
                 const int p = t + TPL * m;
@@ -674,8 +716,9 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     using C = T;
     constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
-    cpx<T>* stw = sm + N * TX;
+    cpx<T>* buf0 = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* buf1 = buf0 + N * TX;
+    cpx<T>* stw = buf1 + N * TX;
     C* kt = reinterpret_cast<C*>(stw + N);
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
     fill_k_table<N>(kt);
@@ -694,14 +737,32 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const SymD<C> dadd = make_symd<C>(op.add_sym, op.add_ab, op.add_coef);
     const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
     double acc_self = 0.0, acc_w0 = 0.0, acc_w1 = 0.0, acc_w2 = 0.0;
-    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+    // stage the ys column tile of item `it` into buffer b, asynchronously
+    auto stage = [&](long it, cpx<T>* b) {
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + l;
+        const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);
+#pragma unroll
+        for (int m = 0; m < E; ++m) cp_async_elem(b + (t + TPL * m) * TX + l, src + (t + TPL * m) * plane + col, ok);
+        cp_async_commit();
+    };
+    long it0 = blockIdx.x;
+    if (it0 < items) stage(it0, buf0);
+    int kbuf = 0;
+    for (long it = it0; it < items; it += gridDim.x, kbuf ^= 1) {
+        cpx<T>* sm = kbuf ? buf1 : buf0;  // this item's tile, then its exchange buffer
+        cpx<T>* nxt = kbuf ? buf0 : buf1;
         const int cy = (int)(it / ntile);
         const int kx = (int)(it - (long)cy * ntile) * TX + l;
         const bool ok = kx < nx;
         const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
+        cp_async_wait_all();
         cpx<T> v[E];
 #pragma unroll
-        for (int m = 0; m < E; ++m) v[m] = ok ? src[(t + TPL * m) * plane + col] : czero<T>();
+        for (int m = 0; m < E; ++m) v[m] = sm[map(t + TPL * m)];
+        __syncthreads();
+        if (it + gridDim.x < items) stage(it + gridDim.x, nxt);
         cfft<N, E, -1, SyncBlock>(v, t, sm, map, tw);
         const int fy = band_fft_index(a.band, cy);
         const int kxc = col - cy * nx;

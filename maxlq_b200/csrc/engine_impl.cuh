@@ -151,7 +151,7 @@ template <typename T>
 template <int NN, int V>
 void Engine<T>::zinv_cv(ZInvArgs<T>& za, int narr) {
     using S = YShape<NN, T, V>;
-    const size_t smem = S::ZSMEM;
+    const size_t smem = S::ZISMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
     auto kern = zinv_c_kernel<NN, V, T>;
     allow_smem(kern);
