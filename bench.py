@@ -170,15 +170,15 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# DRAM bytes per algorithmic byte of the pass kernels, from the full ncu
+# captures summarised in profiles/pass_kernels_256cubed_mixed_ncu.md (one
+# launch each at 256^3; traffic scales with the work of a launch).
+TRAFFIC_PER_ALG_BYTE = {"x_fwd": 0.94, "x_inv": 0.91, "y_inv": 0.77, "z_inv": 0.83}
+
+
 def load_traffic():
-    """Per-launch DRAM bytes of kernels from a committed ncu summary (or {})."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(p):
-        try:
-            return json.load(open(p))
-        except Exception:
-            return {}
-    return {}
+    """Per-kernel DRAM-traffic scale factors measured with ncu."""
+    return {k: {"dram_bytes_per_alg_byte": v} for k, v in TRAFFIC_PER_ALG_BYTE.items()}
 
 
 def run_path(ctx, u0, K, W, dist, profile=False):
