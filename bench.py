@@ -33,9 +33,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "CG iters/s at 512³ q=4: mixed vs FP64 GPU (rel ΔR≤1e-6); FFT HBM GB/s"
-# c2c transforms per CG iteration in the reference at q >= 4 (outside the line
-# search) and per eval_J("LineMin") trial: SURVEY-derived counts of the
-# reference's operator sequence ("Reference arm").
+# c2c N^3 transforms per CG iteration in the reference at q >= 4 (outside the
+# line search) and per eval_J("LineMin") trial, counted from its operator
+# sequence (optimization.f90:136-446 and the routines they call).
 REF_T_PER_ITER = 548
 REF_T_PER_TRIAL = 94
 
@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-detail", action="store_true", help="key x-stage kernel times by fused functor")
+    ap.add_argument("--config", default=None, choices=["c1", "c2", "c3"],
+                    help="run one of the other workload configurations instead of the headline one")
+    ap.add_argument("--max-iter", type=int, default=3000, help="iteration cap per B for --config c2")
     return ap.parse_args()
 
 
@@ -261,11 +264,123 @@ def bench_reference(args, dist):
 REF_TRIALS_PER_ITER = 12
 
 
+# ---------------------------------------------------------------------------
+# Other workload configurations (one JSON line each; rank 0 only)
+# ---------------------------------------------------------------------------
+def _rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-300))
+
+
+def _rel2(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
+
+
+def config_c1(args):
+    """All-FP64 CG at N = 64, q = 4, spectrum |j|^-2 exp(-(|j|/4)^2), seed 0,
+    B = 1: 50 iterations or relative improvement 1e-8."""
+    import maxlq_b200 as mlq
+
+    n, q = 64, 4.0
+    with mlq.MaxLq(n, q, 1.0, max_iter=50, optim_tol=1e-8) as c:
+        u0 = c.seed_field(0, 2.0, 4.0)
+        t0 = time.perf_counter()
+        u, iters, st, rec = c.maxdLqdt(u0.copy())
+        wall = time.perf_counter() - t0
+        R = c.calc_global_dLqdt_inclParts(u)
+        lq = c.calc_global_Lq_norm(u)
+        div = float(np.abs(c.divergence(u)).max())
+    dev = sum(r["seconds"] for r in rec)
+    return {"config": "c1", "workload": "maxdLqdt, N=64^3, q=4, B=1, FP64, seed 0, k0=4, 50 iterations or eps=1e-8",
+            "iterations": iters, "status": st, "iters_per_s": len(rec) / max(dev, 1e-12), "wall_s": wall,
+            "R_final": R.tolist(), "lq_norm_final": lq, "max_abs_div_final": div,
+            "J1_trajectory": [r["J1"] for r in rec], "n_evals": [r["n_evals"] for r in rec]}
+
+
+def config_c2(args):
+    """All-FP64 B-continuation at N = 256, q = 4, k0 = 8: B = 1 then five steps
+    B <- 1.1 B, each solved to relative improvement 1e-8 from the previous
+    optimum (the reference's continuation loop, maxdLpdt.f90:478-512)."""
+    import maxlq_b200 as mlq
+
+    n, q = 256, 4.0
+    Bs = [1.1 ** k for k in range(6)]
+    steps = []
+    with mlq.MaxLq(n, q, Bs[0], max_iter=args.max_iter, optim_tol=1e-8) as c:
+        u = c.seed_field(0, 2.0, 8.0)
+        for B in Bs:
+            c.set_B(B)
+            t0 = time.perf_counter()
+            u, iters, st, rec = c.maxdLqdt(u)
+            wall = time.perf_counter() - t0
+            R = c.calc_global_dLqdt_inclParts(u)
+            steps.append({"B": B, "iterations": iters, "status": st, "R": R.tolist(),
+                          "lq_norm": c.calc_global_Lq_norm(u), "wall_s": wall,
+                          "device_s": sum(r["seconds"] for r in rec),
+                          "last_rel_improvement": (rec[-1]["deltaJ"] / abs(rec[-1]["J1"])) if rec else None})
+    return {"config": "c2", "workload": "B-continuation, N=256^3, q=4, FP64, B=1.1^k k=0..5, eps=1e-8",
+            "steps": steps}
+
+
+def config_c3(args):
+    """N = 512, q = 6, B = 4, spectrum |j|^-5/3 exp(-(|j|/16)^2): errors of the
+    mixed path (FP32 fields and FFTs, FP64 reductions and retraction) against
+    the all-FP64 path for R, the L2 gradient and the first betas, and the
+    Taylor test of both gradients along a seeded divergence-free direction."""
+    import maxlq_b200 as mlq
+
+    n, q, B = 512, 6.0, 4.0
+    d = mlq.MaxLq(n, q, B, optim_tol=0.0)
+    m = mlq.MaxLq(n, q, B, precision="mixed", optim_tol=0.0)
+    u = d.rescaleLqNorm(d.seed_field(0, 5.0 / 3.0, 16.0), B)
+    phi = d.divAvg_free(d.seed_field(1, 5.0 / 3.0, 16.0))
+    phi *= np.sqrt(d.global_summed_field_inner_product(u, u) / d.global_summed_field_inner_product(phi, phi))
+    out = {"config": "c3", "workload": "N=512^3, q=6, B=4, seed 0, |j|^-5/3 exp(-(|j|/16)^2); direction seed 1"}
+    R_d, R_m = d.calc_global_dLqdt_inclParts(u), m.calc_global_dLqdt_inclParts(u)
+    g_d = d.GradL2ForLq(u)
+    g_m = m.GradL2ForLq(u)
+    # R_parts = (R, R1 + R2, R3)
+    out["rel_err_mixed_vs_fp64"] = {"R": abs(R_m[0] - R_d[0]) / abs(R_d[0]),
+                                    "R12_R3": [abs(a - b) / abs(b) for a, b in zip(R_m[1:], R_d[1:])],
+                                    "grad_max": _rel(g_m, g_d), "grad_l2": _rel2(g_m, g_d)}
+    taylor = []
+    ip_d = d.global_summed_field_inner_product(g_d, phi)
+    ip_m = m.global_summed_field_inner_product(g_m, phi)
+    J_d0, J_m0 = R_d[0], R_m[0]
+    del g_d, g_m
+    for e in range(1, 8):
+        h = 10.0 ** (-e)
+        w = u + h * phi
+        kd = (d.calc_global_dLqdt_inclParts(w)[0] - J_d0) / (h * ip_d)
+        km = (m.calc_global_dLqdt_inclParts(w)[0] - J_m0) / (h * ip_m)
+        taylor.append({"h": h, "kappa_fp64": kd, "kappa_mixed": km})
+    out["taylor"] = taylor
+    # first CG iterations from the same field: beta, tau, J1
+    recs = {}
+    for name, ctx in (("fp64", d), ("mixed", m)):
+        ctx.state_load(u)
+        _, st, rec = ctx.state_iterate(3)
+        recs[name] = rec
+    out["iterations"] = [{"iter": a["iter"], "beta_fp64": a["beta"], "beta_mixed": b["beta"],
+                          "tau_fp64": a["tau"], "tau_mixed": b["tau"], "J1_fp64": a["J1"], "J1_mixed": b["J1"]}
+                         for a, b in zip(recs["fp64"], recs["mixed"])]
+    d.close()
+    m.close()
+    return out
+
+
 def main():
     args = parse()
     dist = Dist()
     if args.impl == "reference":
         return bench_reference(args, dist)
+    if args.config:
+        if dist.rank == 0:
+            fn = {"c1": config_c1, "c2": config_c2, "c3": config_c3}[args.config]
+            print(json.dumps(fn(args)), flush=True)
+        dist.close()
+        return
 
     import maxlq_b200 as mlq
 
