@@ -52,9 +52,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-detail", action="store_true", help="key x-stage kernel times by fused functor")
-    ap.add_argument("--config", default=None, choices=["c1", "c2", "c3"],
+    ap.add_argument("--config", default=None, choices=["c1", "c2", "c3", "c4"],
                     help="run one of the other workload configurations instead of the headline one")
     ap.add_argument("--max-iter", type=int, default=3000, help="iteration cap per B for --config c2")
+    ap.add_argument("--c4-iters", type=int, default=5, help="CG iterations per instance for --config c4")
     return ap.parse_args()
 
 
@@ -370,6 +371,71 @@ def config_c3(args):
     return out
 
 
+def c4_instances(count=32, seed=2026):
+    """The batched-instance workload: N cycles through {48, 64, 96, 128}, q
+    through {3, 4, 6, 8} (every (N, q) pair twice in 32), B log-uniform in
+    [0.5, 8], field seed = instance index, spectrum |j|^-2 exp(-(|j|/(N/16))^2)."""
+    rng = np.random.default_rng(seed)
+    Ns, qs = (48, 64, 96, 128), (3.0, 4.0, 6.0, 8.0)
+    out = []
+    for i in range(count):
+        B = float(np.exp(rng.uniform(np.log(0.5), np.log(8.0))))
+        out.append({"seed": i, "n": Ns[i % 4], "q": qs[(i // 4) % 4], "B": B})
+    return out
+
+
+def run_instances(ctxs, fields, iters, concurrent):
+    """CG iterations of every context from its field: one at a time, or all at
+    once from one host thread per context (each context has its own stream;
+    the library releases the interpreter while it runs)."""
+    import threading
+
+    res = [None] * len(ctxs)
+
+    def work(j):
+        ctxs[j].state_load(fields[j])
+        res[j] = ctxs[j].state_iterate(iters)
+
+    t0 = time.perf_counter()
+    if concurrent:
+        th = [threading.Thread(target=work, args=(j,)) for j in range(len(ctxs))]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+    else:
+        for j in range(len(ctxs)):
+            work(j)
+    return time.perf_counter() - t0, res
+
+
+def config_c4(args):
+    """32 independent instances, mixed precision: aggregate CG iterations/s
+    with all instances in flight together (one stream and host thread each)
+    against running them one at a time; the per-instance trajectories of the
+    two runs must be identical (every reduction is deterministic)."""
+    import maxlq_b200 as mlq
+
+    spec = c4_instances()
+    K = args.c4_iters
+    ctxs = [mlq.MaxLq(s["n"], s["q"], s["B"], precision="mixed", optim_tol=0.0) for s in spec]
+    fields = [c.seed_field(s["seed"], 2.0, s["n"] / 16.0) for c, s in zip(ctxs, spec)]
+    run_instances(ctxs, fields, 1, concurrent=True)  # buffers, tuning, first-touch
+    t_seq, r_seq = run_instances(ctxs, fields, K, concurrent=False)
+    t_con, r_con = run_instances(ctxs, fields, K, concurrent=True)
+    its_seq = sum(len(r[2]) for r in r_seq)
+    its_con = sum(len(r[2]) for r in r_con)
+    same = all([x["J1"] for x in a[2]] == [x["J1"] for x in b[2]] for a, b in zip(r_seq, r_con))
+    for c in ctxs:
+        c.close()
+    return {"config": "c4", "workload": "32 instances, N in {48,64,96,128} x q in {3,4,6,8}, B log-uniform [0.5, 8], "
+                                        f"mixed precision, {K} CG iterations each",
+            "instances": spec, "iters_per_s_one_at_a_time": its_seq / t_seq,
+            "iters_per_s_concurrent": its_con / t_con, "speedup": (its_con / t_con) / (its_seq / t_seq),
+            "iterations": its_con, "identical_trajectories": same,
+            "timing": "host wall clock around all instances' iterations (each iteration ends in a stream sync)"}
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -377,7 +443,7 @@ def main():
         return bench_reference(args, dist)
     if args.config:
         if dist.rank == 0:
-            fn = {"c1": config_c1, "c2": config_c2, "c3": config_c3}[args.config]
+            fn = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c4": config_c4}[args.config]
             print(json.dumps(fn(args)), flush=True)
         dist.close()
         return

@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <set>
 #include <string>
 #include <typeinfo>
@@ -32,10 +33,16 @@ static std::vector<int> factor_radices(int L) {
 
 // raise the dynamic shared memory limit of each kernel once (per device
 // function address: kernels of equal type are distinct entries)
+// (contexts may be driven from several host threads at once)
+inline std::mutex& smem_attr_mutex() {
+    static std::mutex m;
+    return m;
+}
 template <typename K>
 static void allow_smem(K kernel) {
     static std::set<const void*> done;
     const void* key = reinterpret_cast<const void*>(kernel);
+    std::lock_guard<std::mutex> lock(smem_attr_mutex());
     if (done.insert(key).second) {
         cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         if (e != cudaSuccess) throw CudaError(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);

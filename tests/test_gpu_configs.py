@@ -74,3 +74,20 @@ def test_c3_mixed_precision_errors_and_taylor_128():
         # kappa(h) -> 1 linearly in h (first-order Taylor remainder)
         assert all(b < 0.2 * a for a, b in zip(err, err[1:]))
         assert err[-1] < 1e-3
+
+
+def test_c4_concurrent_instances_match_one_at_a_time():
+    """Independent contexts driven from several host threads at once give the
+    same trajectories as the same contexts run one after another."""
+    import bench
+
+    spec = [s for s in bench.c4_instances()[:8] if s["n"] <= 64]
+    ctxs = [mlq.MaxLq(s["n"], s["q"], s["B"], precision="mixed", optim_tol=0.0) for s in spec]
+    fields = [c.seed_field(s["seed"], 2.0, s["n"] / 16.0) for c, s in zip(ctxs, spec)]
+    _, r_seq = bench.run_instances(ctxs, fields, 2, concurrent=False)
+    _, r_con = bench.run_instances(ctxs, fields, 2, concurrent=True)
+    for a, b in zip(r_seq, r_con):
+        assert a[1] == b[1] and len(a[2]) == len(b[2]) == 2
+        assert [x["J1"] for x in a[2]] == [x["J1"] for x in b[2]]
+    for c in ctxs:
+        c.close()
