@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-detail", action="store_true", help="key x-stage kernel times by fused functor")
-    ap.add_argument("--config", default=None, choices=["c1", "c2", "c3", "c4"],
+    ap.add_argument("--config", default=None, choices=["c1", "c2", "c3", "c4", "c5"],
                     help="run one of the other workload configurations instead of the headline one")
     ap.add_argument("--max-iter", type=int, default=3000, help="iteration cap per B for --config c2")
     ap.add_argument("--c4-iters", type=int, default=5, help="CG iterations per instance for --config c4")
@@ -436,6 +436,49 @@ def config_c4(args):
             "timing": "host wall clock around all instances' iterations (each iteration ends in a stream sync)"}
 
 
+def config_c5(args):
+    """The largest single-GPU size: N = 1024, q = 4, B = 16, spectrum
+    |j|^-5/3 exp(-(|j|/32)^2), FP32 fields with FP64 reductions and state; 10
+    full CG iterations timed with per-kernel device time.  At this size the
+    engine runs in z-slab streaming mode (no N^3 field kept resident)."""
+    import maxlq_b200 as mlq
+
+    n, q, B = 1024, 4.0, 16.0
+    K, W = args.steps, min(args.warmup, 1)
+    # host side: the seeded field (26 GB) and pinned transfer staging (9 GB)
+    avail = 0
+    with open("/proc/meminfo") as fh:
+        for line in fh:
+            if line.startswith("MemAvailable:"):
+                avail = int(line.split()[1]) * 1024
+    if avail < 96 * 2**30:
+        return {"config": "c5", "skipped": f"needs about 96 GiB of free host memory, {avail / 2**30:.0f} GiB available"}
+    peak, peak_kind = load_peaks()
+    c = mlq.MaxLq(n, q, B, precision="mixed", optim_tol=0.0)
+    u0 = c.seed_field(0, 5.0 / 3.0, 32.0)
+    c.state_load(u0)
+    del u0
+    for _ in range(W):
+        c.state_iterate(1)
+    c.profile(True)
+    c.profile_report(reset=True)
+    t0 = time.perf_counter()
+    _, st, rec = c.state_iterate(K)
+    wall = time.perf_counter() - t0
+    prof = c.profile_report(reset=True)
+    c.profile(False)
+    dev = sum(r["seconds"] for r in rec)
+    per_kernel = {k: {"launches": v["launches"], "ms": round(v["ms"], 2),
+                      "GB/s": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1),
+                      "frac_of_peak": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6 / peak, 3)} for k, v in prof.items()}
+    out = {"config": "c5", "workload": "N=1024^3, q=4, B=16, seed 0, |j|^-5/3 exp(-(|j|/32)^2), mixed precision",
+           "iterations": len(rec), "status": st, "iters_per_s": len(rec) / max(dev, 1e-12), "wall_s": wall,
+           "device_bytes": c.device_bytes, "kernels": c.kernel_config(), "peak_gbs": peak, "peak_kind": peak_kind,
+           "J1": [r["J1"] for r in rec], "n_evals": [r["n_evals"] for r in rec], "per_kernel": per_kernel}
+    c.close()
+    return out
+
+
 def main():
     args = parse()
     dist = Dist()
@@ -443,7 +486,7 @@ def main():
         return bench_reference(args, dist)
     if args.config:
         if dist.rank == 0:
-            fn = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c4": config_c4}[args.config]
+            fn = {"c1": config_c1, "c2": config_c2, "c3": config_c3, "c4": config_c4, "c5": config_c5}[args.config]
             print(json.dumps(fn(args)), flush=True)
         dist.close()
         return

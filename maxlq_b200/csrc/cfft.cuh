@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(256, 2)
     xinv_c_kernel(XInvArgs<T> a, const cpx<T>* __restrict__ twL, const cpx<T>* __restrict__ twN) {
     using S = CShape<N, T>;
     constexpr int L = S::L, E = S::EX, TPL = S::TPLX, LPB = S::XLPB, PITCH = S::XPITCH;
-    constexpr long NG = (long)N * N / LPB;  // line groups per array
+    const long NG = a.nlines / LPB;  // line groups per array
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);  // LPB * PITCH, then the table
     const int ls = threadIdx.x / TPL, t = threadIdx.x % TPL;
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
     constexpr int NIN = F::NIN, NOUT = F::NOUT, NR = F::NRED;
     constexpr int L = S::L, E = S::EX, TPL = S::TPLX, LPB = S::XLPB, PITCH = S::XPITCH;
     constexpr int CHX = xfwd_chunk(NIN, E);
-    constexpr long NG = (long)N * N / LPB;
+    const long NG = a.nlines / LPB;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* stg = reinterpret_cast<cpx<T>*>(smem_raw);              // [NOUT-1][LPB][L]
     cpx<T>* sm = stg + XFwdSmem<N, T, NOUT>::STAGE;                  // [LPB][PITCH]
@@ -535,7 +535,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const ColMap<TX> map{l};
     const int nx = a.nx, nb = a.band.nb;
     const int ntile = (nx + TX - 1) / TX;
-    const long items = (long)N * ntile;
+    const long items = (long)a.nz * ntile;
     const cpx<T>* __restrict__ src = a.in[blockIdx.y];
     cpx<T>* __restrict__ dst = a.out[blockIdx.y];
     // stage item `it` (column tile of plane z) into buffer b, asynchronously

@@ -128,7 +128,36 @@ class Engine : public EngineBase {
     ~Engine() override;
 
     // ---- buffers ----
-    T* phys(int i);                       // N^3 physical scratch, lazily allocated
+    T* phys(int i);                       // N^3 physical scratch, lazily allocated (full mode)
+
+    // ---- z-slab streaming (large N) ----
+    // In slab mode no N^3 field is kept: a physical field index ("slot") is
+    // backed by its pruned y-stage array (the output of the z stage, exact for
+    // a band-limited field), by a pointwise recipe (a power of another slot),
+    // by the constant 1, or, for host transfers, by a full buffer.  A forward
+    // pipeline expands its inputs a slab of zs_ planes at a time through the
+    // y/x inverse passes, runs the fused x stage and the y pass per slab, and
+    // the z stages on whole arrays.
+    bool slab_ = false;
+    int zs_ = 0;  // planes per slab
+    struct PSlot {
+        enum Kind { NONE = 0, FULL, YS, RAW, ONE } kind = NONE;
+        Band band{};      // YS: band of the stored y-stage array
+        int src = -1;     // RAW: source slot
+        double pk = 0.0;  // RAW: FGPow exponent and threshold flag
+        int pthresh = 0;
+    };
+    std::vector<PSlot> slot_;
+    std::vector<cpx<T>*> slot_ys_;  // YS storage, n * nbcap * nxcap
+    PSlot& slot(int i);
+    cpx<T>* slot_ys(int i);         // storage of slot i, allocated on first use
+    std::vector<T*> slab_bufs_;     // zs_ * n^2 each
+    std::vector<cpx<T>*> xslab_;    // zs_ * n * nxcap each
+    T* slab_buf(int k);
+    cpx<T>* xslab(int k);
+    // physical values of slot i on planes [z0, z0 + zs_) into slab buffer k
+    const T* expand(int i, int z0, int k);
+    void release_io_buffers();      // drop lazily allocated work buffers (state and twiddles stay)
     cpx<T>* xsbuf(int i);                 // [n][n][nxcap]
     cpx<T>* ysbuf(int i);                 // [n][nbcap][nxcap]
     cpx<T>* wspec(int i);                 // work spectrum in band b2, nb*nb*nx
@@ -153,7 +182,7 @@ class Engine : public EngineBase {
     // z stage land in results[red_dst + slot] (slot < MAX_RED); functor
     // reductions in results[fred_dst + r].
     template <class F>
-    void fwd(const Band& b, const F& f, const std::vector<const T*>& in, std::vector<FwdOut> outs, int red_dst = -1,
+    void fwd(const Band& b, const F& f, const std::vector<int>& in, std::vector<FwdOut> outs, int red_dst = -1,
              int fred_dst = -1, double norm = -1.0);
     struct InvOut {
         ZSrc src[3];
@@ -161,8 +190,13 @@ class Engine : public EngineBase {
         int phys_out = -1;
     };
     void inv(const Band& b, const std::vector<InvOut>& outs);
+    template <int NOUT>
+    void fwd_z(const Band& b, const std::vector<FwdOut>& outs, int red_dst, double norm);
     template <class F>
-    void pointwise(const F& f, const std::vector<const T*>& in, const std::vector<T*>& out, int fred_dst = -1);
+    void fwd_slab(const Band& b, const F& f, const std::vector<int>& in, std::vector<FwdOut>& outs, int red_dst,
+                  int fred_dst, double norm);
+    template <class F>
+    void pointwise(const F& f, const std::vector<int>& in, const std::vector<int>& out, int fred_dst = -1);
     void yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const std::vector<int>& phys_out);
 
     // ---- programs ----
@@ -183,7 +217,7 @@ class Engine : public EngineBase {
     // Line search along phi = u + tau d when q = 4 (|u|^{q-4} = 1): the
     // setup forms the tau-coefficient fields once; a trial is then one
     // forward transform of g(tau)^2 plus polynomial evaluations.
-    bool ls_ok() const { return !use_e_u && P.q == 4.0; }
+    bool ls_ok() const { return !use_e_u && P.q == 4.0 && !slab_; }
     void ls_setup(const double2* u, const double2* d);
     void ls_trial(double tau, double out[3], double* lqq);
     double ls_r2_[5] = {0}, ls_r3_[6] = {0};

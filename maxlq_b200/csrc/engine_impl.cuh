@@ -46,6 +46,30 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
         MLQ_CUDA(cudaMemcpy(d_twT_, hf.data(), ntw * sizeof(cpx<T>), cudaMemcpyHostToDevice));
     }
     tune_yz();
+    // z-slab streaming when the physical fields the programs keep resident
+    // (up to ~72 with the line-search setup) would not fit in free memory;
+    // MLQ_SLAB_PLANES=k forces k planes per slab (0: never)
+    if (cfft_ok_) {
+        int want = -1;
+        if (const char* e = std::getenv("MLQ_SLAB_PLANES")) {
+            want = std::atoi(e) > 0 ? std::atoi(e) : -1;
+        } else {
+            size_t fr = 0, tot = 0;
+            MLQ_CUDA(cudaMemGetInfo(&fr, &tot));
+            if (72.0 * (double)n3 * sizeof(T) > 0.6 * (double)fr) want = 0;
+        }
+        if (want >= 0) {
+            int zs = 1;
+            if (want > 0) {
+                while (zs * 2 <= want && zs * 2 <= n) zs *= 2;
+            } else {
+                // about 4 GB of slab buffers for up to 24 distinct inputs
+                while (zs * 2 <= n && 24.0 * (zs * 2) * (double)n * n * sizeof(T) <= 4.0e9) zs *= 2;
+            }
+            slab_ = true;
+            zs_ = zs;
+        }
+    }
 }
 
 template <typename T>
@@ -107,7 +131,7 @@ void Engine<T>::xinv_c(XInvArgs<T>& xa, int narr) {
     auto kern = xinv_c_kernel<NN, T>;
     allow_smem(kern);
     const int G = persistent_blocks((const void*)kern, 256, smem);
-    const long ng = (long)NN * NN / LPB;
+    const long ng = xa.nlines / LPB;
     dim3 grid((unsigned)std::min<long>(ng, std::max(1, G / narr)), narr);
     kern<<<grid, 256, smem, stream>>>(xa, d_twT_ + tw_off.at(NN / 2), d_twT_ + tw_off.at(NN));
 }
@@ -118,7 +142,7 @@ template <int NN, int V>
 void Engine<T>::y_cv(YArgs<T>& ya, int sign, int narr) {
     using S = YShape<NN, T, V>;
     const size_t smem = S::YSMEM;
-    const long items = (long)NN * ((ya.nx + S::TX - 1) / S::TX);
+    const long items = (long)ya.nz * ((ya.nx + S::TX - 1) / S::TX);
     auto run = [&](auto kern) {
         allow_smem(kern);
         const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
@@ -197,8 +221,8 @@ template <typename T>
 std::string Engine<T>::kernel_config() const {
     const char* fam = cfft_ok_ ? "compile-time" : (reg_ok_ ? "register" : "shared-memory");
     std::string r = std::string("{\"precision\": \"") + (sizeof(T) == 4 ? "fp32" : "fp64") +
-                    "\", \"pass_kernels\": \"" + fam + "\", \"yz_variants\": \"" +
-                    (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
+                    "\", \"pass_kernels\": \"" + fam + "\", \"slab_planes\": " + std::to_string(slab_ ? zs_ : 0) +
+                    ", \"yz_variants\": \"" + (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
     return r;
 }
 
@@ -241,6 +265,7 @@ void Engine<T>::tune_yz() {
     MLQ_CUDA(cudaMemsetAsync(C, 0, NA * sp_n * sizeof(double2), stream));
     YArgs<T> yf{}, yi{};
     yf.n = yi.n = n;
+    yf.nz = yi.nz = n;
     yf.nx = yi.nx = b.nx;
     yf.band = yi.band = b;
     ZFwdArgs<T> zf{};
@@ -341,7 +366,7 @@ void Engine<T>::xfwd_c(XFwdArgs<T>& xa, const F& f) {
     auto kern = xfwd_c_kernel<NN, T, F>;
     allow_smem(kern);
     const int G = persistent_blocks((const void*)kern, 256, smem);
-    const long ng = (long)NN * NN / S::XLPB;
+    const long ng = xa.nlines / S::XLPB;
     const int grid = (int)std::min<long>(ng, G);
     last_xblocks_ = grid;
     if (F::NRED > 0) ensure_partials((long)grid * F::NRED);
@@ -360,7 +385,9 @@ void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b
         for (int j = 0; j < i; ++j) seen = seen || xa.in[j] == xa.in[i];
         nin_distinct += seen ? 0 : 1;
     }
-    const double bytes = (double)n3 * sizeof(T) * nin_distinct + (double)n * n * b.nx * sizeof(cpx<T>) * nout;
+    if (xa.nlines <= 0) xa.nlines = (long)n * n;
+    const double lines = (double)xa.nlines;
+    const double bytes = lines * n * sizeof(T) * nin_distinct + lines * b.nx * sizeof(cpx<T>) * nout;
     if (cfft_ok_) {
         cudaEvent_t ev = prof_mark();
         dispatch_n(n, [&](auto nc) { this->template xfwd_c<decltype(nc)::value>(xa, f); });
@@ -370,7 +397,7 @@ void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b
     if (reg_ok_) {
         xa.lx = reg_lx(nout, row_pitch(h));
         xa.tw_n_off = tw_off.at(n);
-        const int grid = (int)(((long)n * n) / xa.lx);
+        const int grid = (int)(xa.nlines / xa.lx);
         last_xblocks_ = grid;
         if (F::NRED > 0) ensure_partials((long)grid * F::NRED);
         xa.partials = d_partials;
@@ -388,7 +415,7 @@ void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b
         return;
     }
     xa.lx = lx_for(nout);
-    const int xgrid = (int)(((long)n * n) / xa.lx);
+    const int xgrid = (int)(xa.nlines / xa.lx);
     last_xblocks_ = xgrid;
     if (F::NRED > 0) ensure_partials((long)xgrid * F::NRED);
     xa.partials = d_partials;
@@ -401,7 +428,8 @@ void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b
 
 template <typename T>
 void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
-    const double bytes = (double)narr * (n * (double)n * b.nx + n * (double)b.nb * b.nx) * sizeof(cpx<T>);
+    if (ya.nz <= 0) ya.nz = n;
+    const double bytes = (double)narr * ya.nz * ((double)n * b.nx + (double)b.nb * b.nx) * sizeof(cpx<T>);
     const char* nm = sign < 0 ? "y_fwd" : "y_inv";
     if (cfft_ok_) {
         cudaEvent_t ev = prof_mark();
@@ -413,7 +441,7 @@ void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
         const int tx = reg_tx();
         ya.tx = tx;
         const size_t sm = (size_t)n * tx * sizeof(cpx<T>);
-        dim3 g((b.nx + tx - 1) / tx, n, narr);
+        dim3 g((b.nx + tx - 1) / tx, ya.nz, narr);
         const int thr = tx * (n / ereg_);
         cudaEvent_t ev = prof_mark();
         if (ereg_ == 8) {
@@ -441,7 +469,7 @@ void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
     ya.plan = plan(n);
     ya.tw = d_tw;
     const size_t ysm = (size_t)2 * n * tx * sizeof(cpx<T>);
-    dim3 yg((b.nx + tx - 1) / tx, n, narr);
+    dim3 yg((b.nx + tx - 1) / tx, ya.nz, narr);
     cudaEvent_t ev = prof_mark();
     if (sign < 0) {
         allow_smem(ypass_kernel<-1, T>);
@@ -528,7 +556,8 @@ void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zby
 template <typename T>
 void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
     const int h = n / 2;
-    const double bytes = (double)narr * ((double)n * n * b.nx * sizeof(cpx<T>) + (double)n3 * sizeof(T));
+    if (xa.nlines <= 0) xa.nlines = (long)n * n;
+    const double bytes = (double)narr * xa.nlines * ((double)b.nx * sizeof(cpx<T>) + (double)n * sizeof(T));
     xa.tw_n_off = tw_off.at(n);
     if (cfft_ok_) {
         cudaEvent_t ev = prof_mark();
@@ -539,7 +568,7 @@ void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
     if (reg_ok_) {
         xa.lx = reg_lx(1, row_pitch(h + 1));
         const size_t sm = (size_t)xa.lx * row_pitch(h + 1) * sizeof(cpx<T>);
-        dim3 xg((unsigned)(((long)n * n) / xa.lx), narr);
+        dim3 xg((unsigned)(xa.nlines / xa.lx), narr);
         const int thr = xa.lx * (h / ereg_);
         cudaEvent_t ev = prof_mark();
         if (ereg_ == 8) {
@@ -554,12 +583,12 @@ void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
     }
     const size_t per = (size_t)(3 * h + 1) * sizeof(cpx<T>);
     int lx = 8;
-    while (lx > 1 && (per * lx > 96 * 1024 || ((long)n * n) % lx != 0)) lx /= 2;
+    while (lx > 1 && (per * lx > 96 * 1024 || xa.nlines % lx != 0)) lx /= 2;
     xa.lx = lx;
     xa.plan_half = plan(h);
     xa.tw = d_tw;
     allow_smem(xinv_kernel<T>);
-    dim3 xg((unsigned)(((long)n * n) / lx), narr);
+    dim3 xg((unsigned)(xa.nlines / lx), narr);
     cudaEvent_t ev = prof_mark();
     xinv_kernel<T><<<xg, 256, per * lx, stream>>>(xa);
     launched("x_inv", bytes, ev);
@@ -625,18 +654,22 @@ int Engine<T>::tx_for() const {
 // ----------------------------------------------------------------------------
 template <typename T>
 template <class F>
-void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, std::vector<FwdOut> outs,
+void Engine<T>::fwd(const Band& b, const F& f, const std::vector<int>& in, std::vector<FwdOut> outs,
                     int red_dst, int fred_dst, double norm) {
     constexpr int NOUT = F::NOUT;
     static_assert(NOUT <= MAX_ARR, "too many outputs");
     if ((int)in.size() != F::NIN || (int)outs.size() != NOUT) throw CudaError("fwd: arity", MLQ_ERR_BADARG);
     if (b.nx > nxcap || b.nb > nbcap) throw CudaError("fwd: band exceeds buffers", MLQ_ERR_BADARG);
+    if (slab_) {
+        fwd_slab(b, f, in, outs, red_dst, fred_dst, norm);
+        return;
+    }
     const int h = n / 2;
     // x stage
     XFwdArgs<T> xa;
     xa.n = n;
     xa.nx = b.nx;
-    for (int i = 0; i < F::NIN; ++i) xa.in[i] = in[i];
+    for (int i = 0; i < F::NIN; ++i) xa.in[i] = phys(in[i]);
     for (int o = 0; o < NOUT; ++o) xa.out[o] = xsbuf(o);
     xa.plan_half = plan(h);
     xa.tw_n_off = tw_off.at(n);
@@ -654,7 +687,13 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
         ya.out[o] = ysbuf(o);
     }
     launch_y(ya, -1, NOUT, b);
-    // z stage
+    fwd_z<NOUT>(b, outs, red_dst, norm);
+}
+
+// z stage of a forward pipeline: ysbuf(o) -> spectra / reductions / round trips
+template <typename T>
+template <int NOUT>
+void Engine<T>::fwd_z(const Band& b, const std::vector<FwdOut>& outs, int red_dst, double norm) {
     ZFwdArgs<T> za;
     za.n = n;
     za.nx = b.nx;
@@ -666,7 +705,9 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
         op.in = ysbuf(o);
         op.spec_out = fo.spec;
         op.spec_f64 = fo.spec_f64;
-        op.ys_out = fo.phys_out >= 0 ? (void*)ysbuf(o) : nullptr;
+        // round trip: in place (then y/x inverse), or, in slab mode, into the
+        // output slot's y-stage storage
+        op.ys_out = fo.phys_out < 0 ? nullptr : (slab_ ? (void*)slot_ys(fo.phys_out) : (void*)ysbuf(o));
         any_rt |= fo.phys_out >= 0;
         op.sym = fo.sym;
         op.sym_ab = fo.ab;
@@ -700,6 +741,15 @@ void Engine<T>::fwd(const Band& b, const F& f, const std::vector<const T*>& in, 
     launch_zfwd(za, NOUT, b, any_rt, zbytes);
     const long zblocks = last_zblocks_;
     if (red_dst >= 0) finalize((int)zblocks, MAX_RED, 1.0, red_dst);
+    if (slab_) {
+        for (int o = 0; o < NOUT; ++o)
+            if (outs[o].phys_out >= 0) {
+                PSlot& sl = slot(outs[o].phys_out);
+                sl.kind = PSlot::YS;
+                sl.band = b;
+            }
+        return;
+    }
     if (any_rt) {
         std::vector<cpx<T>*> ys;
         std::vector<int> po;
@@ -758,7 +808,7 @@ void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
             ZInvOp& op = za.op[i];
             for (int s = 0; s < 3; ++s) op.src[s] = io.src[s];
             op.nsrc = io.nsrc;
-            ys[i] = ysbuf(i);
+            ys[i] = slab_ ? slot_ys(io.phys_out) : ysbuf(i);
             op.ys_out = ys[i];
             po[i] = io.phys_out;
         }
@@ -769,17 +819,67 @@ void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
             for (int s2 = 0; s2 < io.nsrc; ++s2) zb += (double)b.nb * b.nb * b.nx * (io.src[s2].f64 ? 16 : 8);
         }
         launch_zinv(za, k, b, zb);
+        if (slab_) {
+            for (int i = 0; i < k; ++i) {
+                PSlot& sl = slot(po[i]);
+                sl.kind = PSlot::YS;
+                sl.band = b;
+            }
+            continue;
+        }
         yx_inverse(b, ys, po);
     }
 }
 
 template <typename T>
+__global__ void fill_kernel(T* p, long cnt, T v) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (long)gridDim.x * blockDim.x) p[i] = v;
+}
+
+template <typename T>
 template <class F>
-void Engine<T>::pointwise(const F& f, const std::vector<const T*>& in, const std::vector<T*>& out, int fred_dst) {
+void Engine<T>::pointwise(const F& f, const std::vector<int>& in, const std::vector<int>& out, int fred_dst) {
+    if (slab_) {
+        if constexpr (F::NOUT > 0) {
+            // the only pointwise outputs are the |u|^k powers of the calc_uk
+            // chain: kept as a recipe, evaluated per slab where they are read
+            if constexpr (std::is_same<F, FGPow>::value) {
+                PSlot& o = slot(out[0]);
+                o.kind = PSlot::RAW;
+                o.src = in[0];
+                o.pk = f.k;
+                o.pthresh = f.thresh;
+                return;
+            } else {
+                throw CudaError("pointwise outputs are not kept in slab mode", MLQ_ERR_BADARG);
+            }
+        }
+        std::vector<int> uniq, which(F::NIN);
+        for (int i = 0; i < F::NIN; ++i) {
+            const auto it = std::find(uniq.begin(), uniq.end(), in[i]);
+            which[i] = (int)(it - uniq.begin());
+            if (it == uniq.end()) uniq.push_back(in[i]);
+        }
+        PArgs<T> a;
+        a.npts = (long)zs_ * n * n;
+        const int grid = grid_for(a.npts, RED_THREADS, 148 * 8);
+        for (int z0 = 0; z0 < n; z0 += zs_) {
+            std::vector<const T*> ptr(uniq.size());
+            for (size_t k = 0; k < uniq.size(); ++k) ptr[k] = expand(uniq[k], z0, (int)k);
+            for (int i = 0; i < F::NIN; ++i) a.in[i] = ptr[which[i]];
+            ensure_partials((long)grid * std::max(F::NRED, 1));
+            a.partials = d_partials;
+            cudaEvent_t ev = prof_mark();
+            pointwise_kernel<T, F><<<grid, RED_THREADS, 0, stream>>>(a, f);
+            launched("pointwise", (double)a.npts * sizeof(T) * (F::NIN + F::NOUT), ev);
+            if (F::NRED > 0 && fred_dst >= 0) finalize(grid, F::NRED, 1.0 / (double)n3, fred_dst, z0 > 0);
+        }
+        return;
+    }
     PArgs<T> a;
     a.npts = n3;
-    for (int i = 0; i < F::NIN; ++i) a.in[i] = in[i];
-    for (int o = 0; o < F::NOUT; ++o) a.out[o] = out[o];
+    for (int i = 0; i < F::NIN; ++i) a.in[i] = phys(in[i]);
+    for (int o = 0; o < F::NOUT; ++o) a.out[o] = phys(out[o]);
     const int grid = grid_for(n3, RED_THREADS, 148 * 8);
     ensure_partials((long)grid * std::max(F::NRED, 1));
     a.partials = d_partials;
@@ -787,6 +887,150 @@ void Engine<T>::pointwise(const F& f, const std::vector<const T*>& in, const std
     pointwise_kernel<T, F><<<grid, RED_THREADS, 0, stream>>>(a, f);
     launched("pointwise", (double)n3 * sizeof(T) * (F::NIN + F::NOUT), ev);
     if (F::NRED > 0 && fred_dst >= 0) finalize(grid, F::NRED, 1.0 / (double)n3, fred_dst);
+}
+
+// ---- slab mode -------------------------------------------------------------
+template <typename T>
+typename Engine<T>::PSlot& Engine<T>::slot(int i) {
+    if ((int)slot_.size() <= i) slot_.resize(i + 1);
+    return slot_[i];
+}
+
+template <typename T>
+cpx<T>* Engine<T>::slot_ys(int i) {
+    if ((int)slot_ys_.size() <= i) slot_ys_.resize(i + 1, nullptr);
+    if (!slot_ys_[i]) slot_ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * nxcap * sizeof(cpx<T>));
+    return slot_ys_[i];
+}
+
+template <typename T>
+T* Engine<T>::slab_buf(int k) {
+    if ((int)slab_bufs_.size() <= k) slab_bufs_.resize(k + 1, nullptr);
+    if (!slab_bufs_[k]) slab_bufs_[k] = (T*)dev_alloc((size_t)zs_ * n * n * sizeof(T));
+    return slab_bufs_[k];
+}
+
+template <typename T>
+cpx<T>* Engine<T>::xslab(int k) {
+    if ((int)xslab_.size() <= k) xslab_.resize(k + 1, nullptr);
+    if (!xslab_[k]) xslab_[k] = (cpx<T>*)dev_alloc((size_t)zs_ * n * nxcap * sizeof(cpx<T>));
+    return xslab_[k];
+}
+
+template <typename T>
+const T* Engine<T>::expand(int i, int z0, int k) {
+    const PSlot s = slot(i);
+    const long npts = (long)zs_ * n * n;
+    switch (s.kind) {
+        case PSlot::FULL: return phys_[i] + (long)z0 * n * n;
+        case PSlot::ONE: {
+            T* d = slab_buf(k);
+            fill_kernel<T><<<grid_for(npts, 256), 256, 0, stream>>>(d, npts, T(1));
+            launched();
+            return d;
+        }
+        case PSlot::YS: {
+            // y inverse of the slab's planes, then the x inverse (c2r)
+            YArgs<T> ya{};
+            ya.n = n;
+            ya.nx = s.band.nx;
+            ya.band = s.band;
+            ya.nz = zs_;
+            ya.in[0] = slot_ys_[i] + (long)z0 * s.band.nb * s.band.nx;
+            ya.out[0] = xslab(MAX_ARR);
+            launch_y(ya, +1, 1, s.band);
+            XInvArgs<T> xa{};
+            xa.n = n;
+            xa.nx_in = s.band.nx;
+            xa.nlines = (long)zs_ * n;
+            xa.in[0] = xslab(MAX_ARR);
+            xa.out[0] = slab_buf(k);
+            xa.plan_half = plan(n / 2);
+            xa.tw = d_tw;
+            launch_xinv(xa, 1, s.band);
+            return slab_buf(k);
+        }
+        case PSlot::RAW: {
+            const T* src = expand(s.src, z0, k);
+            FGPow fp;
+            fp.k = s.pk;
+            fp.thresh = s.pthresh;
+            PArgs<T> a;
+            a.npts = npts;
+            a.in[0] = src;
+            a.out[0] = slab_buf(k);
+            const int grid = grid_for(npts, RED_THREADS, 148 * 8);
+            a.partials = d_partials;
+            cudaEvent_t ev = prof_mark();
+            pointwise_kernel<T, FGPow><<<grid, RED_THREADS, 0, stream>>>(a, fp);
+            launched("pointwise", (double)npts * sizeof(T) * 2, ev);
+            return slab_buf(k);
+        }
+        default: break;
+    }
+    throw CudaError("physical field " + std::to_string(i) + " has no values", MLQ_ERR_CUDA);
+}
+
+template <typename T>
+template <class F>
+void Engine<T>::fwd_slab(const Band& b, const F& f, const std::vector<int>& in, std::vector<FwdOut>& outs,
+                         int red_dst, int fred_dst, double norm) {
+    constexpr int NOUT = F::NOUT;
+    std::vector<int> uniq, which(F::NIN);
+    for (int i = 0; i < F::NIN; ++i) {
+        const auto it = std::find(uniq.begin(), uniq.end(), in[i]);
+        which[i] = (int)(it - uniq.begin());
+        if (it == uniq.end()) uniq.push_back(in[i]);
+    }
+    XFwdArgs<T> xa{};
+    xa.n = n;
+    xa.nx = b.nx;
+    xa.nlines = (long)zs_ * n;
+    xa.plan_half = plan(n / 2);
+    xa.tw_n_off = tw_off.at(n);
+    xa.tw = d_tw;
+    for (int o = 0; o < NOUT; ++o) xa.out[o] = xslab(o);
+    YArgs<T> ya{};
+    ya.n = n;
+    ya.nx = b.nx;
+    ya.band = b;
+    ya.nz = zs_;
+    for (int z0 = 0; z0 < n; z0 += zs_) {
+        std::vector<const T*> ptr(uniq.size());
+        for (size_t k = 0; k < uniq.size(); ++k) ptr[k] = expand(uniq[k], z0, (int)k);
+        for (int i = 0; i < F::NIN; ++i) xa.in[i] = ptr[which[i]];
+        launch_xfwd(xa, f, NOUT, b);
+        if (F::NRED > 0 && fred_dst >= 0) finalize((int)last_xblocks_, F::NRED, 1.0 / (double)n3, fred_dst, z0 > 0);
+        if constexpr (NOUT > 0) {
+            for (int o = 0; o < NOUT; ++o) {
+                ya.in[o] = xslab(o);
+                ya.out[o] = ysbuf(o) + (long)z0 * b.nb * b.nx;
+            }
+            launch_y(ya, -1, NOUT, b);
+        }
+    }
+    if constexpr (NOUT > 0) fwd_z<NOUT>(b, outs, red_dst, norm);
+}
+
+template <typename T>
+void Engine<T>::release_io_buffers() {
+    for (auto* v : {&phys_}) {
+        for (auto*& p : *v) {
+            if (p) free_dev(p);
+            p = nullptr;
+        }
+    }
+    for (auto* v : {&xs_, &ys_, &ws_, &slot_ys_, &xslab_}) {
+        for (auto*& p : *v) {
+            if (p) free_dev(p);
+            p = nullptr;
+        }
+    }
+    for (auto*& p : slab_bufs_) {
+        if (p) free_dev(p);
+        p = nullptr;
+    }
+    slot_.clear();
 }
 
 // ----------------------------------------------------------------------------
@@ -819,11 +1063,6 @@ static constexpr int wf64() {
     return sizeof(T) == 8 ? 1 : 0;
 }
 
-template <typename T>
-__global__ void fill_kernel(T* p, long cnt, T v) {
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (long)gridDim.x * blockDim.x) p[i] = v;
-}
-
 // Fourier coefficients of the constant 1 in band b2: a unit k=0 mode.
 template <typename T>
 cpx<T>* Engine<T>::ones_spec() {
@@ -843,6 +1082,11 @@ template <typename T>
 void Engine<T>::ensure_phys(PowField& f) {
     if (f.phys >= 0) return;
     if (f.kind == PowField::ONE) {
+        if (slab_) {
+            slot(PONES).kind = PSlot::ONE;
+            f.phys = PONES;
+            return;
+        }
         if ((int)phys_.size() <= PONES || phys_[PONES] == nullptr) {
             fill_kernel<T><<<grid_for(n3, 256), 256, 0, stream>>>(phys(PONES), n3, T(1));
             launched();
@@ -866,7 +1110,7 @@ void Engine<T>::ensure_p2_spec(PowField& f) {
     FwdOut o;
     o.spec = wspec(f.spec);
     o.spec_f64 = wf64<T>();
-    fwd(b2, FCopy{}, {phys(f.phys)}, {o});
+    fwd(b2, FCopy{}, {f.phys}, {o});
 }
 
 // S = P2(|u|^2) (calc_uk 2332-2333) must already be in phys(PS) ; computes
@@ -878,7 +1122,7 @@ void Engine<T>::A_and_S(bool need_A_phys) {
     oA.spec = wspec(WA);
     oA.spec_f64 = wf64<T>();
     if (need_A_phys) oA.phys_out = PA;
-    fwd(b2, FGSq{}, {phys(PS)}, {oA});
+    fwd(b2, FGSq{}, {PS}, {oA});
 }
 
 // calc_gk_order2 (function_ops.f90:2281-2319) on g = sqrt(max(S,0)), with
@@ -897,7 +1141,7 @@ PowField Engine<T>::chain(double k) {
         FGPow fp;
         fp.k = k;
         fp.thresh = 1;
-        pointwise(fp, {phys(PS)}, {phys(f.phys)});
+        pointwise(fp, {PS}, {f.phys});
     } else if (k + MACH_EPSILON < 2.0) {
         const int c = band_cut_for_order(n, k);
         if (c >= n / 2) {
@@ -909,7 +1153,7 @@ PowField Engine<T>::chain(double k) {
                 FGPow fp;
                 fp.k = k;
                 fp.thresh = 0;
-                pointwise(fp, {phys(PS)}, {phys(f.phys)});
+                pointwise(fp, {PS}, {f.phys});
             }
         } else {
             const Band bk = make_band(c);
@@ -925,7 +1169,7 @@ PowField Engine<T>::chain(double k) {
                 o.spec = wspec(f.spec);
                 o.spec_f64 = wf64<T>();
             }
-            fwd(bk, fp, {phys(PS)}, {o});
+            fwd(bk, fp, {PS}, {o});
         }
     } else {
         PowField prev = chain(k - 2.0);
@@ -941,7 +1185,7 @@ PowField Engine<T>::chain(double k) {
             o.phys_out = f.phys;
             o.spec = wspec(f.spec);
             o.spec_f64 = wf64<T>();
-            fwd(b2, FMul{}, {phys(PA), phys(prev.phys)}, {o});
+            fwd(b2, FMul{}, {PA, prev.phys}, {o});
         }
     }
     memo_[k] = f;
@@ -1015,9 +1259,9 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
             io.push_back(o);
         }
     inv(b, io);
-    std::vector<const T*> uin;
-    for (int i = 0; i < 3; ++i) uin.push_back(phys(PU + i));
-    for (int i = 0; i < 9; ++i) uin.push_back(phys(PD + i));
+    std::vector<int> uin;
+    for (int i = 0; i < 3; ++i) uin.push_back(PU + i);
+    for (int i = 0; i < 9; ++i) uin.push_back(PD + i);
     // 2. first products: |u|^2 -> P2, W_j -> P2 (q>=4), grad u:grad u^T -> p,
     //    |grad u|^2 -> spectrum
     FwdOut oS, oQ, oG2;
@@ -1048,12 +1292,12 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
     bool norm_raw = false;
     if (ah.kind == PowField::RAW) {
         norm_raw = true;
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
+        pointwise(FSqRed{}, {ah.phys}, {}, 20);
     } else if (ah.spec < 0) {
         // a band-limited power in a wider band than P2: its full spectrum is
         // needed; integrate its square in physical space instead
         norm_raw = true;
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
+        pointwise(FSqRed{}, {ah.phys}, {}, 20);
     } else {
         if (ah.kind == PowField::ONE) ensure_p2_spec(ah);
         pr.push_back({wspec(ah.spec), wspec(ah.spec)});
@@ -1061,7 +1305,7 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
     const bool direct = !use_e_u && a4.kind == PowField::ONE;
     if (direct) {
         // |u|^{q-4} = 1: R2 = -(q-2) vc nu int sum V^2, R3 = (q-2) pc int p u.V
-        pointwise(FRRed1{}, {phys(PV), phys(PV + 1), phys(PV + 2), phys(PP), phys(PU), phys(PU + 1), phys(PU + 2)},
+        pointwise(FRRed1{}, {PV, PV + 1, PV + 2, PP, PU, PU + 1, PU + 2},
                   {}, 16);
     } else if (!use_e_u) {
         ensure_phys(a4);
@@ -1072,14 +1316,14 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
             o[i].spec_f64 = wf64<T>();
         }
         fwd(b, FRProd2{},
-            {phys(PV), phys(PV + 1), phys(PV + 2), phys(PP), phys(PU), phys(PU + 1), phys(PU + 2), phys(a4.phys)},
+            {PV, PV + 1, PV + 2, PP, PU, PU + 1, PU + 2, a4.phys},
             {o[0], o[1], o[2]});
         pr.push_back({wspec(a4.spec), wspec(WT)});
         pr.push_back({wspec(WT + 1), wspec(WT + 2)});
     } else {
         // E_j = P2(sum_i e_i d_j u_i) (calc_vgraduvgradu / calc_vvgradu, v = e_u)
-        std::vector<const T*> ein = uin;
-        ein.push_back(phys(PS));
+        std::vector<int> ein = uin;
+        ein.push_back(PS);
         FwdOut oE[3];
         for (int j = 0; j < 3; ++j) oE[j].phys_out = PV + j;
         fwd(b, FRE{}, ein, {oE[0], oE[1], oE[2]});
@@ -1090,8 +1334,8 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
             o[i].spec_f64 = wf64<T>();
         }
         fwd(b, FRProd2E{},
-            {phys(PV), phys(PV + 1), phys(PV + 2), phys(PP), phys(PU), phys(PU + 1), phys(PU + 2), phys(PS),
-             phys(a2.phys)},
+            {PV, PV + 1, PV + 2, PP, PU, PU + 1, PU + 2, PS,
+             a2.phys},
             {o[0], o[1], o[2]});
         pr.push_back({wspec(a2.spec), wspec(WT)});
         pr.push_back({wspec(WT + 1), wspec(WT + 2)});
@@ -1145,9 +1389,9 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
         io.push_back(o);
     }
     inv(b, io);
-    std::vector<const T*> uin;
-    for (int i = 0; i < 3; ++i) uin.push_back(phys(PU + i));
-    for (int i = 0; i < 9; ++i) uin.push_back(phys(PD + i));
+    std::vector<int> uin;
+    for (int i = 0; i < 3; ++i) uin.push_back(PU + i);
+    for (int i = 0; i < 9; ++i) uin.push_back(PD + i);
     // 2. S -> P2, Q -> p spectrum (1102-1107)
     {
         FwdOut oS, oQ;
@@ -1184,11 +1428,11 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
             oc[i].spec = c + i * nc;
             oc[i].spec_f64 = 1;
         }
-        std::vector<const T*> in2;
-        for (int i = 0; i < 3; ++i) in2.push_back(phys(PU + i));
-        for (int i = 0; i < 3; ++i) in2.push_back(phys(PL + i));
-        for (int i = 0; i < 3; ++i) in2.push_back(phys(PGP + i));
-        in2.push_back(phys(a2.phys));
+        std::vector<int> in2;
+        for (int i = 0; i < 3; ++i) in2.push_back(PU + i);
+        for (int i = 0; i < 3; ++i) in2.push_back(PL + i);
+        for (int i = 0; i < 3; ++i) in2.push_back(PGP + i);
+        in2.push_back(a2.phys);
         if (!use_e_u) {
             FG2 f;
             f.cvisc = cv;
@@ -1198,17 +1442,17 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
                 ensure_phys(a4);
                 FwdOut o;
                 o.phys_out = PT;
-                fwd(b, FMul{}, {phys(a4.phys), phys(PT)}, {o});
+                fwd(b, FMul{}, {a4.phys, PT}, {o});
             }
         } else {
             FG2E f;
             f.cvisc = cv;
             f.cpress = cp;
-            in2.push_back(phys(PS));
+            in2.push_back(PS);
             fwd(b, f, in2, {oT, oc[0], oc[1], oc[2]});
             FwdOut o;
             o.phys_out = PT;
-            fwd(b, FMul{}, {phys(a2.phys), phys(PT)}, {o});
+            fwd(b, FMul{}, {a2.phys, PT}, {o});
         }
     }
     // 6. grad aux4 = grad Lap^-1 div c (1155-1158)
@@ -1225,14 +1469,14 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
     }
     // 7. final sum, one dealias, plus vc nu Lap c (1172-1190)
     {
-        std::vector<const T*> in3;
-        in3.push_back(phys(PT));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PU + i));
-        in3.push_back(phys(a2.phys));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PGP + i));
-        for (int i = 0; i < 9; ++i) in3.push_back(phys(PD + i));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PGA + i));
-        for (int i = 0; i < 3; ++i) in3.push_back(phys(PL + i));
+        std::vector<int> in3;
+        in3.push_back(PT);
+        for (int i = 0; i < 3; ++i) in3.push_back(PU + i);
+        in3.push_back(a2.phys);
+        for (int i = 0; i < 3; ++i) in3.push_back(PGP + i);
+        for (int i = 0; i < 9; ++i) in3.push_back(PD + i);
+        for (int i = 0; i < 3; ++i) in3.push_back(PGA + i);
+        for (int i = 0; i < 3; ++i) in3.push_back(PL + i);
         FwdOut o[3];
         for (int i = 0; i < 3; ++i) {
             o[i].spec = v + i * nc;
@@ -1253,13 +1497,13 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
             f.qm2 = q - 2.0;
             f.cvisc = cv;
             f.cpress = cp;
-            in3.push_back(phys(PS));
+            in3.push_back(PS);
             fwd(b, f, in3, {o[0], o[1], o[2]});
         }
     }
     if (lqq) {
         if (ah.kind == PowField::RAW || ah.spec < 0) {
-            pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
+            pointwise(FSqRed{}, {ah.phys}, {}, 20);
             fetch_results();
             *lqq = h_results[20];
         } else {
@@ -1288,11 +1532,11 @@ double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
     inv(b2, io);
     FwdOut oS;
     oS.phys_out = PS;
-    fwd(b2, FSq3{}, {phys(PU), phys(PU + 1), phys(PU + 2)}, {oS});
+    fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
     A_and_S(true);
     PowField ah = chain(P.q / 2.0);
     if (ah.kind == PowField::RAW || ah.spec < 0) {
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
+        pointwise(FSqRed{}, {ah.phys}, {}, 20);
         fetch_results();
         return h_results[20];
     }
@@ -1321,7 +1565,7 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
     inv(b2, io);
     FwdOut oS;
     oS.phys_out = PS;
-    fwd(b2, FSq3{}, {phys(PU), phys(PU + 1), phys(PU + 2)}, {oS});
+    fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
     A_and_S(true);
     PowField a2 = chain(q - 2.0);
     PowField ah = chain(q / 2.0);
@@ -1335,14 +1579,14 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
             o[i].spec = cbuf + i * nc;
             o[i].spec_f64 = 1;
         }
-        fwd(b2, FC3{}, {phys(a2.phys), phys(PU), phys(PU + 1), phys(PU + 2)}, {o[0], o[1], o[2]});
+        fwd(b2, FC3{}, {a2.phys, PU, PU + 1, PU + 2}, {o[0], o[1], o[2]});
     } else {
         if (a2.kind != PowField::ONE) throw CudaError("vectorTransport with 2 < q < 2+eps", MLQ_ERR_BADARG);
         lincomb(cbuf, 1.0, u, d ? tau : 0.0, d, 0.0, nullptr);
     }
     double lqq;
     if (ah.kind == PowField::RAW || ah.spec < 0) {
-        pointwise(FSqRed{}, {phys(ah.phys)}, {}, 20);
+        pointwise(FSqRed{}, {ah.phys}, {}, 20);
         fetch_results();
         lqq = h_results[20];
     } else {
@@ -1376,10 +1620,18 @@ void Engine<T>::calc_uk(const double2* u, double k, int dst) {
     inv(b2, io);
     FwdOut oS;
     oS.phys_out = PS;
-    fwd(b2, FSq3{}, {phys(PU), phys(PU + 1), phys(PU + 2)}, {oS});
+    fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
     A_and_S(true);
     PowField f = chain(k);
     ensure_phys(f);
+    if (slab_) {
+        const PSlot src = slot(f.phys);
+        slot(dst) = src;
+        if (src.kind == PSlot::YS)
+            MLQ_CUDA(cudaMemcpyAsync(slot_ys(dst), slot_ys_[f.phys], (size_t)n * src.band.nb * src.band.nx * sizeof(cpx<T>),
+                                     cudaMemcpyDeviceToDevice, stream));
+        return;
+    }
     MLQ_CUDA(cudaMemcpyAsync(phys(dst), phys(f.phys), n3 * sizeof(T), cudaMemcpyDeviceToDevice, stream));
 }
 
@@ -1414,15 +1666,15 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
                 io.push_back(o);
             }
     inv(b2, io);
-    std::vector<const T*> ud = {phys(LU), phys(LU + 1), phys(LU + 2), phys(LD), phys(LD + 1), phys(LD + 2)};
-    std::vector<const T*> all;
-    for (int i = 0; i < 3; ++i) all.push_back(phys(LU + i));
-    for (int i = 0; i < 9; ++i) all.push_back(phys(LDU + i));
-    for (int i = 0; i < 3; ++i) all.push_back(phys(LD + i));
-    for (int i = 0; i < 9; ++i) all.push_back(phys(LDD + i));
-    std::vector<const T*> grads;
-    for (int i = 0; i < 9; ++i) grads.push_back(phys(LDU + i));
-    for (int i = 0; i < 9; ++i) grads.push_back(phys(LDD + i));
+    std::vector<int> ud = {LU, LU + 1, LU + 2, LD, LD + 1, LD + 2};
+    std::vector<int> all;
+    for (int i = 0; i < 3; ++i) all.push_back(LU + i);
+    for (int i = 0; i < 9; ++i) all.push_back(LDU + i);
+    for (int i = 0; i < 3; ++i) all.push_back(LD + i);
+    for (int i = 0; i < 9; ++i) all.push_back(LDD + i);
+    std::vector<int> grads;
+    for (int i = 0; i < 9; ++i) grads.push_back(LDU + i);
+    for (int i = 0; i < 9; ++i) grads.push_back(LDD + i);
     // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333)
     {
         FwdOut o[3];
@@ -1451,9 +1703,9 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
         fwd(b2, FLSQG{}, grads, {o[0], o[1], o[2], o[3], o[4], o[5]});
     }
     // R2 and R3 integrands as polynomials in tau
-    std::vector<const T*> rin;
-    for (int i = 0; i < 9; ++i) rin.push_back(phys(LV + i));
-    for (int a = 0; a < 3; ++a) rin.push_back(phys(LP + a));
+    std::vector<int> rin;
+    for (int i = 0; i < 9; ++i) rin.push_back(LV + i);
+    for (int a = 0; a < 3; ++a) rin.push_back(LP + a);
     for (int i = 0; i < 6; ++i) rin.push_back(ud[i]);
     pointwise(FLSRed{}, rin, {}, 100);
     fetch_results();
@@ -1482,7 +1734,7 @@ void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
     }
     FLSA f;
     f.tau = tau;
-    fwd(b2, f, {phys(LS), phys(LS + 1), phys(LS + 2)}, {o}, 130);
+    fwd(b2, f, {LS, LS + 1, LS + 2}, {o}, 130);
     fetch_results();
     const double* r = h_results + 130;
     const double I1 = r[1] + tau * (r[2] + tau * r[3]);
@@ -1510,12 +1762,20 @@ void Engine<T>::load_scalar_phys(const double* host, int dst) {
         for (long i = 0; i < n3; ++i) st[i] = (T)host[i];
     MLQ_CUDA(cudaMemcpyAsync(phys(dst), st, n3 * sizeof(T), cudaMemcpyHostToDevice, stream));
     MLQ_CUDA(cudaStreamSynchronize(stream));
+    if (slab_) slot(dst).kind = PSlot::FULL;
 }
 
 template <typename T>
 void Engine<T>::store_scalar_phys(int src, double* host) {
     T* st = (T*)stage(n3 * sizeof(T));
-    MLQ_CUDA(cudaMemcpyAsync(st, phys(src), n3 * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    if (slab_) {
+        const long per = (long)zs_ * n * n;
+        for (int z0 = 0; z0 < n; z0 += zs_)
+            MLQ_CUDA(cudaMemcpyAsync(st + (long)z0 * n * n, expand(src, z0, 0), per * sizeof(T), cudaMemcpyDeviceToHost,
+                                     stream));
+    } else {
+        MLQ_CUDA(cudaMemcpyAsync(st, phys(src), n3 * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    }
     MLQ_CUDA(cudaStreamSynchronize(stream));
     if (sizeof(T) == 8)
         std::memcpy(host, st, n3 * sizeof(double));
@@ -1534,8 +1794,8 @@ double Engine<T>::load_vec(const double* host, double2* spec) {
         o.spec = spec + c * nc;
         o.spec_f64 = 1;
         o.phys_out = PIO2;
-        fwd(b2, FCopy{}, {phys(PIO)}, {o});
-        pointwise(FDiffSq{}, {phys(PIO), phys(PIO2)}, {}, 30 + 2 * c);
+        fwd(b2, FCopy{}, {PIO}, {o});
+        pointwise(FDiffSq{}, {PIO, PIO2}, {}, 30 + 2 * c);
     }
     fetch_results();
     double out = 0, tot = 0;
@@ -1681,7 +1941,7 @@ void Engine<T>::fft_r2c(const double* in, double* out) {
     FwdOut o;
     o.spec = sp;
     o.spec_f64 = 1;
-    fwd(full, FCopy{}, {phys(PIO)}, {o}, -1, -1, 1.0);  // unnormalised like fftfwdr
+    fwd(full, FCopy{}, {PIO}, {o}, -1, -1, 1.0);  // unnormalised like fftfwdr
     double* st = (double*)stage(nspec * sizeof(cpx<double>));
     MLQ_CUDA(cudaMemcpyAsync(st, sp, nspec * sizeof(cpx<double>), cudaMemcpyDeviceToHost, stream));
     MLQ_CUDA(cudaStreamSynchronize(stream));
@@ -1717,7 +1977,7 @@ void Engine<T>::dealias_scalar(double* g, double order) {
     load_scalar_phys(g, PIO);
     FwdOut o;
     o.phys_out = PIO2;
-    fwd(bk, FCopy{}, {phys(PIO)}, {o});
+    fwd(bk, FCopy{}, {PIO}, {o});
     store_scalar_phys(PIO2, g);
 }
 
@@ -1734,6 +1994,16 @@ void Engine<T>::widen_to(const Band& b) {
             free_dev(p);
             p = nullptr;
         }
+    // slab-mode storage is sized by the caps too (slot contents are dropped:
+    // callers widen before a pipeline, never between its steps)
+    for (auto* v : {&slot_ys_, &xslab_})
+        for (auto& p : *v)
+            if (p) {
+                free_dev(p);
+                p = nullptr;
+            }
+    for (auto& sl : slot_)
+        if (sl.kind == PSlot::YS) sl.kind = PSlot::NONE;
     nxcap = std::max(nxcap, b.nx);
     nbcap = std::max(nbcap, b.nb);
 }
@@ -1749,7 +2019,7 @@ static cpx<double>* full_spectrum(Engine<T>& e, const double* host, int phys_idx
     typename Engine<T>::FwdOut o;
     o.spec = sp;
     o.spec_f64 = 1;
-    e.fwd(full, FCopy{}, {e.phys(phys_idx)}, {o});
+    e.fwd(full, FCopy{}, {phys_idx}, {o});
     return sp;
 }
 

@@ -77,6 +77,7 @@ struct XFwdArgs {
     int tw_n_off;       // offset of W_n (length n) in the twiddle pool
     const cpx<double>* tw;
     double* partials;
+    long nlines = 0;    // lines (rows along x) processed; a slab of planes is nlines = planes * n
 };
 
 template <typename T, class F>
@@ -163,6 +164,7 @@ struct XInvArgs {
     FftPlan plan_half;
     int tw_n_off;
     const cpx<double>* tw;
+    long nlines = 0;  // lines processed (planes * n for a slab)
 };
 
 template <typename T>
@@ -249,6 +251,7 @@ struct YArgs {
     cpx<T>* out[MAX_ARR];
     FftPlan plan;
     const cpx<double>* tw;
+    int nz = 0;          // z planes processed (a slab), n for a whole array
 };
 
 template <int SIGN, typename T>

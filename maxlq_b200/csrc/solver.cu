@@ -47,6 +47,12 @@ class Solver : public SolverBase {
         }
     }
 
+    // In slab mode memory is tight: the FP64 transfer pipeline of a mixed
+    // context gives its work buffers back after each host transfer.
+    void trim_io() {
+        if (e.slab_ && io64_) io64_->release_io_buffers();
+    }
+
     explicit Solver(const mlq_params& p) : e(p) {
         u = e.alloc_state();
         d1 = e.alloc_state();
@@ -69,6 +75,7 @@ class Solver : public SolverBase {
     void load(const double* host, double2* spec) {
         MLQ_CUDA(cudaStreamSynchronize(e.stream));
         const double rel = io().load_vec(host, spec);
+        trim_io();
         const double tol = 1e-24;  // relative energy; FP64 FFT round-trip noise is ~1e-32
         if (rel > tol)
             throw CudaError("input field is not band-limited to the 2/3 dealiasing cube (relative energy outside: " +
@@ -558,6 +565,7 @@ class Solver : public SolverBase {
     void store(const double2* spec, double* host) {
         MLQ_CUDA(cudaStreamSynchronize(e.stream));
         io().store_vec(spec, host);
+        trim_io();
     }
     void state_store(double* uh) override { store(u, uh); }
     int state_step(double* uh, mlq_iter_cb cb, void* user) override {
