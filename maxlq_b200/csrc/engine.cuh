@@ -149,6 +149,8 @@ class Engine : public EngineBase {
     };
     std::vector<PSlot> slot_;
     std::vector<cpx<T>*> slot_ys_;  // YS storage, n * nbcap * nxcap
+    std::vector<cpx<T>*> slot_pool_;  // released YS storage blocks, reused before allocating
+    void release_slots(int lo, int hi);  // slots [lo, hi) no longer hold values
     PSlot& slot(int i);
     cpx<T>* slot_ys(int i);         // storage of slot i, allocated on first use
     std::vector<T*> slab_bufs_;     // zs_ * n^2 each
@@ -157,6 +159,10 @@ class Engine : public EngineBase {
     cpx<T>* xslab(int k);
     // physical values of slot i on planes [z0, z0 + zs_) into slab buffer k
     const T* expand(int i, int z0, int k);
+    // physical values of several slots on planes [z0, z0 + zs_): slot in[k]
+    // lands in slab buffer k; y-stage slots of one band share launches
+    std::vector<const T*> expand_many(const std::vector<int>& in, int z0);
+    bool ls_fits();  // room for the line-search setup's fields in slab mode
     void release_io_buffers();      // drop lazily allocated work buffers (state and twiddles stay)
     cpx<T>* xsbuf(int i);                 // [n][n][nxcap]
     cpx<T>* ysbuf(int i);                 // [n][nbcap][nxcap]
@@ -217,7 +223,7 @@ class Engine : public EngineBase {
     // Line search along phi = u + tau d when q = 4 (|u|^{q-4} = 1): the
     // setup forms the tau-coefficient fields once; a trial is then one
     // forward transform of g(tau)^2 plus polynomial evaluations.
-    bool ls_ok() const { return !use_e_u && P.q == 4.0 && !slab_; }
+    bool ls_ok() const { return !use_e_u && P.q == 4.0; }
     void ls_setup(const double2* u, const double2* d);
     void ls_trial(double tau, double out[3], double* lqq);
     double ls_r2_[5] = {0}, ls_r3_[6] = {0};

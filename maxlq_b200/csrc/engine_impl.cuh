@@ -864,8 +864,7 @@ void Engine<T>::pointwise(const F& f, const std::vector<int>& in, const std::vec
         a.npts = (long)zs_ * n * n;
         const int grid = grid_for(a.npts, RED_THREADS, 148 * 8);
         for (int z0 = 0; z0 < n; z0 += zs_) {
-            std::vector<const T*> ptr(uniq.size());
-            for (size_t k = 0; k < uniq.size(); ++k) ptr[k] = expand(uniq[k], z0, (int)k);
+            const std::vector<const T*> ptr = expand_many(uniq, z0);
             for (int i = 0; i < F::NIN; ++i) a.in[i] = ptr[which[i]];
             ensure_partials((long)grid * std::max(F::NRED, 1));
             a.partials = d_partials;
@@ -899,8 +898,82 @@ typename Engine<T>::PSlot& Engine<T>::slot(int i) {
 template <typename T>
 cpx<T>* Engine<T>::slot_ys(int i) {
     if ((int)slot_ys_.size() <= i) slot_ys_.resize(i + 1, nullptr);
-    if (!slot_ys_[i]) slot_ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * nxcap * sizeof(cpx<T>));
+    if (!slot_ys_[i]) {
+        if (!slot_pool_.empty()) {
+            slot_ys_[i] = slot_pool_.back();
+            slot_pool_.pop_back();
+        } else {
+            slot_ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * nxcap * sizeof(cpx<T>));
+        }
+    }
     return slot_ys_[i];
+}
+
+template <typename T>
+void Engine<T>::release_slots(int lo, int hi) {
+    for (int i = lo; i < hi && i < (int)slot_ys_.size(); ++i)
+        if (slot_ys_[i]) {
+            slot_pool_.push_back(slot_ys_[i]);
+            slot_ys_[i] = nullptr;
+        }
+    for (int i = lo; i < hi && i < (int)slot_.size(); ++i)
+        if (slot_[i].kind != PSlot::FULL) slot_[i] = PSlot{};
+}
+
+template <typename T>
+std::vector<const T*> Engine<T>::expand_many(const std::vector<int>& in, int z0) {
+    std::vector<const T*> ptr(in.size(), nullptr);
+    std::vector<int> batch;  // y-stage slots waiting for a shared launch
+    Band bb{};
+    auto flush = [&]() {
+        if (batch.empty()) return;
+        YArgs<T> ya{};
+        ya.n = n;
+        ya.nx = bb.nx;
+        ya.band = bb;
+        ya.nz = zs_;
+        XInvArgs<T> xa{};
+        xa.n = n;
+        xa.nx_in = bb.nx;
+        xa.nlines = (long)zs_ * n;
+        xa.plan_half = plan(n / 2);
+        xa.tw = d_tw;
+        for (size_t j = 0; j < batch.size(); ++j) {
+            ya.in[j] = slot_ys_[in[batch[j]]] + (long)z0 * bb.nb * bb.nx;
+            ya.out[j] = xslab(MAX_ARR + (int)j);
+            xa.in[j] = xslab(MAX_ARR + (int)j);
+            xa.out[j] = slab_buf(batch[j]);
+        }
+        launch_y(ya, +1, (int)batch.size(), bb);
+        launch_xinv(xa, (int)batch.size(), bb);
+        for (int k : batch) ptr[k] = slab_buf(k);
+        batch.clear();
+    };
+    for (size_t k = 0; k < in.size(); ++k) {
+        const PSlot& s = slot(in[k]);
+        if (s.kind != PSlot::YS) continue;
+        if (!batch.empty() && (s.band.cut != bb.cut || (int)batch.size() == MAX_ARR)) flush();
+        bb = s.band;
+        batch.push_back((int)k);
+    }
+    flush();
+    for (size_t k = 0; k < in.size(); ++k)
+        if (!ptr[k]) ptr[k] = expand(in[k], z0, (int)k);
+    return ptr;
+}
+
+// the line-search setup holds 39 y-stage slots; program slots (0..59) are
+// released first, so it needs 39 blocks minus what the pool already holds
+template <typename T>
+bool Engine<T>::ls_fits() {
+    if (!slab_) return true;
+    size_t fr = 0, tot = 0;
+    MLQ_CUDA(cudaMemGetInfo(&fr, &tot));
+    long held = (long)slot_pool_.size();
+    for (int i = 0; i < 60 && i < (int)slot_ys_.size(); ++i) held += slot_ys_[i] ? 1 : 0;
+    for (int i = 60; i < (int)slot_ys_.size(); ++i) held += slot_ys_[i] ? 1 : 0;
+    const double blk = (double)n * nbcap * nxcap * sizeof(cpx<T>);
+    return (39.0 - (double)held) * blk < 0.9 * (double)fr;
 }
 
 template <typename T>
@@ -996,8 +1069,7 @@ void Engine<T>::fwd_slab(const Band& b, const F& f, const std::vector<int>& in, 
     ya.band = b;
     ya.nz = zs_;
     for (int z0 = 0; z0 < n; z0 += zs_) {
-        std::vector<const T*> ptr(uniq.size());
-        for (size_t k = 0; k < uniq.size(); ++k) ptr[k] = expand(uniq[k], z0, (int)k);
+        const std::vector<const T*> ptr = expand_many(uniq, z0);
         for (int i = 0; i < F::NIN; ++i) xa.in[i] = ptr[which[i]];
         launch_xfwd(xa, f, NOUT, b);
         if (F::NRED > 0 && fred_dst >= 0) finalize((int)last_xblocks_, F::NRED, 1.0 / (double)n3, fred_dst, z0 > 0);
@@ -1020,12 +1092,13 @@ void Engine<T>::release_io_buffers() {
             p = nullptr;
         }
     }
-    for (auto* v : {&xs_, &ys_, &ws_, &slot_ys_, &xslab_}) {
+    for (auto* v : {&xs_, &ys_, &ws_, &slot_ys_, &xslab_, &slot_pool_}) {
         for (auto*& p : *v) {
             if (p) free_dev(p);
             p = nullptr;
         }
     }
+    slot_pool_.clear();
     for (auto*& p : slab_bufs_) {
         if (p) free_dev(p);
         p = nullptr;
@@ -1654,6 +1727,7 @@ enum : int {
 template <typename T>
 void Engine<T>::ls_setup(const double2* u, const double2* d) {
     const long nc = spec_ncomp();
+    if (slab_) release_slots(0, LU);  // the programs' fields are rebuilt by the next program
     // phi's pieces: u, d and their gradients (function_ops.f90:3147-3195)
     std::vector<InvOut> io;
     for (int f = 0; f < 2; ++f)
@@ -1709,6 +1783,10 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     for (int i = 0; i < 6; ++i) rin.push_back(ud[i]);
     pointwise(FLSRed{}, rin, {}, 100);
     fetch_results();
+    if (slab_) {  // the trials read only S_a
+        release_slots(LU, LS);
+        release_slots(LV, LP + 3);
+    }
     const double* r = h_results + 100;
     const double M[3][3] = {{r[0], r[1], r[2]}, {r[1], r[3], r[4]}, {r[2], r[4], r[5]}};
     for (int k = 0; k < 5; ++k) ls_r2_[k] = 0.0;
@@ -1996,12 +2074,13 @@ void Engine<T>::widen_to(const Band& b) {
         }
     // slab-mode storage is sized by the caps too (slot contents are dropped:
     // callers widen before a pipeline, never between its steps)
-    for (auto* v : {&slot_ys_, &xslab_})
+    for (auto* v : {&slot_ys_, &xslab_, &slot_pool_})
         for (auto& p : *v)
             if (p) {
                 free_dev(p);
                 p = nullptr;
             }
+    slot_pool_.clear();
     for (auto& sl : slot_)
         if (sl.kind == PSlot::YS) sl.kind = PSlot::NONE;
     nxcap = std::max(nxcap, b.nx);

@@ -90,7 +90,7 @@ class Solver : public SolverBase {
     void ls_begin(const double2* base, const double2* dir) {
         trials.clear();
         ls_ready = false;
-        if (e.ls_ok() && dir) {
+        if (e.ls_ok() && dir && e.ls_fits()) {
             e.ls_setup(base, dir);
             ls_ready = true;
         }
