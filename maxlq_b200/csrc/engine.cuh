@@ -227,6 +227,13 @@ class Engine : public EngineBase {
     void ls_setup(const double2* u, const double2* d);
     void ls_trial(double tau, double out[3], double* lqq);
     double ls_r2_[5] = {0}, ls_r3_[6] = {0};
+    // Where S(tau) = S0 + tau S1 + tau^2 S2 (the dealiased |phi|^2) is >= 0 at
+    // every point, the clamp of calc_uk is inactive and P2(g^2) = S(tau): a
+    // trial in [ls_tlo_, ls_thi_] is then a polynomial in tau of the Parseval
+    // products <S_i, X_a> (X_a: coefficients of P2|grad phi|^2) and <S_i, S_j>.
+    double ls_tlo_ = 0.0, ls_thi_ = 0.0;
+    double ls_sx_[3][3] = {{0}}, ls_ss_[3][3] = {{0}};
+    long long ls_poly_trials_ = 0, ls_fft_trials_ = 0;
 
     // ---- state <-> host ----
     // Forward transform of a host FP64 vector field into state spectra.

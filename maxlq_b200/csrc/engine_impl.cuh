@@ -222,6 +222,8 @@ std::string Engine<T>::kernel_config() const {
     const char* fam = cfft_ok_ ? "compile-time" : (reg_ok_ ? "register" : "shared-memory");
     std::string r = std::string("{\"precision\": \"") + (sizeof(T) == 4 ? "fp32" : "fp64") +
                     "\", \"pass_kernels\": \"" + fam + "\", \"slab_planes\": " + std::to_string(slab_ ? zs_ : 0) +
+                    ", \"line_search_trials_polynomial\": " + std::to_string(ls_poly_trials_) +
+                    ", \"line_search_trials_transform\": " + std::to_string(ls_fft_trials_) +
                     ", \"yz_variants\": \"" + (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
     return r;
 }
@@ -1721,8 +1723,95 @@ enum : int {
     LV = 87,    // V_aj = P2 coefficients of W_j at 87+3a+j
     LP = 96,    // p_a (3)
     WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
+    WLS = 43,   // work spectra: S_a (3)
 };
 }  // namespace
+
+// Per block: the largest lower end and the smallest upper end, over its
+// points, of the interval around tau = 0 on which s0 + tau s1 + tau^2 s2 >= 0
+// (empty when s0 < 0), as (lo, hi) pairs.
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+    ls_interval_kernel(const T* __restrict__ s0, const T* __restrict__ s1, const T* __restrict__ s2, long npts,
+                       double* __restrict__ out) {
+    const double inf = 1e300;
+    double lo = -inf, hi = inf;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long)gridDim.x * blockDim.x) {
+        const double a = (double)s2[i], b = (double)s1[i], c = (double)s0[i];
+        if (c < 0.0) {
+            lo = inf;
+            hi = -inf;
+            continue;
+        }
+        if (a == 0.0) {
+            if (b > 0.0) lo = fmax(lo, -c / b);
+            if (b < 0.0) hi = fmin(hi, -c / b);
+            continue;
+        }
+        const double disc = b * b - 4.0 * a * c;
+        if (disc < 0.0) continue;  // a > 0: positive everywhere
+        const double sq = sqrt(disc);
+        const double qq = -0.5 * (b + (b >= 0.0 ? sq : -sq));
+        double r1 = qq / a, r2 = qq != 0.0 ? c / qq : 0.0;
+        if (r1 > r2) {
+            const double t = r1;
+            r1 = r2;
+            r2 = t;
+        }
+        if (a < 0.0) {  // non-negative between the roots
+            lo = fmax(lo, r1);
+            hi = fmin(hi, r2);
+        } else if (r2 <= 0.0) {  // opens up: the side of 0
+            lo = fmax(lo, r2);
+        } else if (r1 >= 0.0) {
+            hi = fmin(hi, r1);
+        } else {
+            lo = fmax(lo, 0.0);
+            hi = fmin(hi, 0.0);
+        }
+    }
+    __shared__ double slo[RED_THREADS / 32], shi[RED_THREADS / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmax(lo, __shfl_down_sync(0xffffffffu, lo, o));
+        hi = fmin(hi, __shfl_down_sync(0xffffffffu, hi, o));
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+        slo[warp] = lo;
+        shi[warp] = hi;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+            lo = fmax(lo, slo[w]);
+            hi = fmin(hi, shi[w]);
+        }
+        out[2 * blockIdx.x] = lo;
+        out[2 * blockIdx.x + 1] = hi;
+    }
+}
+
+// Per block: the minimum over its points of s0 + tau (s1 + tau s2), evaluated
+// exactly as the trial functor FLSA does (precision T).
+template <typename T>
+__global__ void __launch_bounds__(RED_THREADS)
+    ls_min_kernel(const T* __restrict__ s0, const T* __restrict__ s1, const T* __restrict__ s2, long npts, double tau,
+                  double* __restrict__ out) {
+    const T t = (T)tau;
+    T m = T(1e30);
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long)gridDim.x * blockDim.x)
+        m = fmin(m, s0[i] + t * (s1[i] + t * s2[i]));
+    __shared__ T sm[RED_THREADS / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fmin(m, sm[w]);
+        out[blockIdx.x] = (double)m;
+    }
+}
 
 template <typename T>
 void Engine<T>::ls_setup(const double2* u, const double2* d) {
@@ -1752,7 +1841,11 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333)
     {
         FwdOut o[3];
-        for (int a = 0; a < 3; ++a) o[a].phys_out = LS + a;
+        for (int a = 0; a < 3; ++a) {
+            o[a].phys_out = LS + a;
+            o[a].spec = wspec(WLS + a);
+            o[a].spec_f64 = wf64<T>();
+        }
         fwd(b2, FLSS{}, ud, {o[0], o[1], o[2]});
     }
     // P2 of the coefficients of W_j (calc_vgraduvgradu / calc_vvgradu, v = phi)
@@ -1796,11 +1889,109 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     for (int a = 0; a < 3; ++a)
         for (int cc = 0; cc < 2; ++cc)
             for (int b = 0; b < 3; ++b) ls_r3_[a + cc + b] += r[6 + 3 * (2 * a + cc) + b];
+    // Parseval products for the transform-free trials
+    {
+        std::vector<std::pair<const cpx<T>*, const cpx<T>*>> p1, p2, p3;
+        for (int i = 0; i < 3; ++i)
+            for (int a = 0; a < 3; ++a) (i < 2 ? p1 : p2).push_back({wspec(WLS + i), wspec(WLG + a)});
+        for (int i = 0; i < 3; ++i)
+            for (int j = i; j < 3; ++j) (p2.size() < 6 ? p2 : p3).push_back({wspec(WLS + i), wspec(WLS + j)});
+        sdots(*this, p1, 140);
+        sdots(*this, p2, 146);
+        sdots(*this, p3, 152);
+    }
+    // the interval of tau around 0 on which S(tau) >= 0 everywhere
+    {
+        const long npts = slab_ ? (long)zs_ * n * n : n3;
+        const int grid = grid_for(npts, RED_THREADS, 148 * 4);
+        ensure_partials((long)grid * 2);
+        std::vector<double> h((size_t)grid * 2);
+        double lo = -1e300, hi = 1e300;
+        for (int z0 = 0; z0 < n; z0 += (slab_ ? zs_ : n)) {
+            const T* s[3];
+            if (slab_) {
+                const std::vector<const T*> p = expand_many({LS, LS + 1, LS + 2}, z0);
+                for (int a = 0; a < 3; ++a) s[a] = p[a];
+            } else {
+                for (int a = 0; a < 3; ++a) s[a] = phys(LS + a);
+            }
+            ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(s[0], s[1], s[2], npts, d_partials);
+            launched();
+            MLQ_CUDA(cudaMemcpyAsync(h.data(), d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            MLQ_CUDA(cudaStreamSynchronize(stream));
+            for (int g = 0; g < grid; ++g) {
+                lo = std::max(lo, h[2 * g]);
+                hi = std::min(hi, h[2 * g + 1]);
+            }
+        }
+        // stay clear of the ends, where the T-precision trial may round either way
+        ls_tlo_ = lo <= 0.0 ? lo * (1.0 - 1e-6) : 1.0;
+        ls_thi_ = hi >= 0.0 ? hi * (1.0 - 1e-6) : -1.0;
+    }
+    fetch_results();
+    {
+        const double* q1 = h_results + 140;
+        int k = 0;
+        for (int i = 0; i < 3; ++i)
+            for (int a = 0; a < 3; ++a) ls_sx_[i][a] = q1[k++];  // slots 140..148 (146.. holds i = 2)
+        const double* q2 = h_results + 149;
+        k = 0;
+        for (int i = 0; i < 3; ++i)
+            for (int j = i; j < 3; ++j) {
+                ls_ss_[i][j] = ls_ss_[j][i] = q2[k++];
+            }
+    }
 }
 
 template <typename T>
 void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
     const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
+    bool clamp_off = tau >= ls_tlo_ && tau <= ls_thi_;
+    if (!clamp_off) {
+        // outside the interval: one read of S_0..2 decides for this tau
+        const long npts = slab_ ? (long)zs_ * n * n : n3;
+        const int grid = grid_for(npts, RED_THREADS, 148 * 4);
+        ensure_partials(grid);
+        std::vector<double> h(grid);
+        double mn = 1e300;
+        for (int z0 = 0; z0 < n; z0 += (slab_ ? zs_ : n)) {
+            const T* sp[3];
+            if (slab_) {
+                const std::vector<const T*> p = expand_many({LS, LS + 1, LS + 2}, z0);
+                for (int a = 0; a < 3; ++a) sp[a] = p[a];
+            } else {
+                for (int a = 0; a < 3; ++a) sp[a] = phys(LS + a);
+            }
+            cudaEvent_t ev = prof_mark();
+            ls_min_kernel<T><<<grid, RED_THREADS, 0, stream>>>(sp[0], sp[1], sp[2], npts, tau, d_partials);
+            launched("ls_min", 3.0 * npts * sizeof(T), ev);
+            MLQ_CUDA(cudaMemcpyAsync(h.data(), d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            MLQ_CUDA(cudaStreamSynchronize(stream));
+            for (double v : h) mn = std::min(mn, v);
+        }
+        clamp_off = mn >= 0.0;
+    }
+    if (clamp_off) {
+        // S(tau) >= 0 everywhere: P2(g^2) = S(tau), every product is a polynomial
+        ++ls_poly_trials_;
+        const double tp[5] = {1.0, tau, tau * tau, tau * tau * tau, tau * tau * tau * tau};
+        double ra[3] = {0, 0, 0}, r0 = 0.0;
+        for (int i = 0; i < 3; ++i)
+            for (int a = 0; a < 3; ++a) ra[a] += tp[i] * ls_sx_[i][a];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) r0 += tp[i + j] * ls_ss_[i][j];
+        const double I1 = ra[0] + tau * (ra[1] + tau * ra[2]);
+        double I2 = 0.0, I3 = 0.0;
+        for (int k = 4; k >= 0; --k) I2 = I2 * tau + ls_r2_[k];
+        for (int k = 5; k >= 0; --k) I3 = I3 * tau + ls_r3_[k];
+        const double R1 = -cv * I1, R2 = -cv * (q - 2.0) * I2, R3 = cp * (q - 2.0) * I3;
+        out[0] = R1 + R2 + R3;
+        out[1] = R1 + R2;
+        out[2] = R3;
+        if (lqq) *lqq = r0;
+        return;
+    }
+    ++ls_fft_trials_;
     // A(tau) = P2(g^2) with its Parseval products: ||A||^2 (= ||phi||_4^4) and
     // <A, P2(|grad phi|^2)_a>, a = 0..2
     FwdOut o;
