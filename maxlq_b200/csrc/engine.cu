@@ -191,6 +191,7 @@ std::string EngineBase::prof_report(bool reset) {
 
 void EngineBase::lincomb(double2* out, double a, const double2* x, double b, const double2* y, double c,
                          const double2* z) {
+    state_written(out);
     SpecGeom g = geom(b2);
     cudaEvent_t ev = prof_mark();
     spec_lincomb_kernel<<<grid_for(3 * g.ncomp, 256), 256, 0, stream>>>(g, out, a, x, b, y, c, z);
@@ -198,6 +199,7 @@ void EngineBase::lincomb(double2* out, double a, const double2* x, double b, con
 }
 
 void EngineBase::hilbert(double2* f, double order) {
+    state_written(f);
     SpecGeom g = geom(b2);
     cudaEvent_t ev = prof_mark();
     spec_hilbert_kernel<<<grid_for(g.ncomp, 256), 256, 0, stream>>>(g, f, P.lambda1, 2.0 * order);
@@ -205,6 +207,7 @@ void EngineBase::hilbert(double2* f, double order) {
 }
 
 void EngineBase::leray(double2* f) {
+    state_written(f);
     SpecGeom g = geom(b2);
     cudaEvent_t ev = prof_mark();
     spec_leray_kernel<<<grid_for(g.ncomp, 256), 256, 0, stream>>>(g, f);

@@ -80,6 +80,14 @@ class EngineBase {
     void zeroth(const double2* f, double out[3]);
 
     void finalize(int nblocks, int nr, double scale, int dst, bool accumulate = false);
+    // The state spectrum whose u and grad u the physical fields 0..11 hold
+    // (set by the gradient program; cleared by any write to that spectrum or
+    // to those fields), so the line-search setup of the same iteration can
+    // reuse them instead of transforming again.
+    const void* pu_of_ = nullptr;
+    void state_written(const void* p) {
+        if (p == pu_of_) pu_of_ = nullptr;
+    }
     void ensure_partials(long n);
     // Count a launch and surface launch-configuration errors immediately.
     // With profiling on, `a` is the event recorded before the launch; the

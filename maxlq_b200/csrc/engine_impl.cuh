@@ -1088,6 +1088,7 @@ void Engine<T>::fwd_slab(const Band& b, const F& f, const std::vector<int>& in, 
 
 template <typename T>
 void Engine<T>::release_io_buffers() {
+    pu_of_ = nullptr;
     for (auto* v : {&phys_}) {
         for (auto*& p : *v) {
             if (p) free_dev(p);
@@ -1317,6 +1318,7 @@ static void sdots(Engine<T>& e, const std::vector<std::pair<const cpx<T>*, const
 // on the band instead of by a round trip (the projection is self-adjoint).
 template <typename T>
 void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double out[3], double* lqq) {
+    pu_of_ = nullptr;
     const Band& b = b2;
     const long nc = spec_ncomp();
     const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
@@ -1442,6 +1444,7 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
 // is linear), the fifth term nu Lap P2(|u|^{q-2}u) is added in the spectrum.
 template <typename T>
 void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
+    pu_of_ = nullptr;
     const Band& b = b2;
     const long nc = spec_ncomp();
     const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
@@ -1464,6 +1467,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
         io.push_back(o);
     }
     inv(b, io);
+    if (!slab_) pu_of_ = u;  // PU, PD hold u and grad u until the next program
     std::vector<int> uin;
     for (int i = 0; i < 3; ++i) uin.push_back(PU + i);
     for (int i = 0; i < 9; ++i) uin.push_back(PD + i);
@@ -1593,6 +1597,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
 // ||u + tau d||_q^q (calc_global_Lq_norm)
 template <typename T>
 double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
+    pu_of_ = nullptr;
     const long nc = spec_ncomp();
     chain_reset();
     std::vector<InvOut> io;
@@ -1625,6 +1630,7 @@ double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
 template <typename T>
 double Engine<T>::transport_pieces(const double2* u, const double2* d, double tau, const double2* const* xi,
                                    int nxi, double* ir) {
+    pu_of_ = nullptr;
     const long nc = spec_ncomp();
     const double q = P.q;
     chain_reset();
@@ -1682,6 +1688,7 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
 // calc_uk (function_ops.f90:2324-2343) of the state u into phys(dst)
 template <typename T>
 void Engine<T>::calc_uk(const double2* u, double k, int dst) {
+    pu_of_ = nullptr;
     const long nc = spec_ncomp();
     chain_reset();
     std::vector<InvOut> io;
@@ -1816,10 +1823,14 @@ __global__ void __launch_bounds__(RED_THREADS)
 template <typename T>
 void Engine<T>::ls_setup(const double2* u, const double2* d) {
     const long nc = spec_ncomp();
+    // u and grad u are still in PU, PD when the gradient program of this
+    // iteration transformed the same spectrum
+    const bool reuse_u = !slab_ && pu_of_ == (const void*)u;
     if (slab_) release_slots(0, LU);  // the programs' fields are rebuilt by the next program
+    const int iu = reuse_u ? PU : LU, idu = reuse_u ? PD : LDU;
     // phi's pieces: u, d and their gradients (function_ops.f90:3147-3195)
     std::vector<InvOut> io;
-    for (int f = 0; f < 2; ++f)
+    for (int f = reuse_u ? 1 : 0; f < 2; ++f)
         for (int i = 0; i < 3; ++i)
             for (int j = -1; j < 3; ++j) {
                 InvOut o;
@@ -1829,14 +1840,14 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
                 io.push_back(o);
             }
     inv(b2, io);
-    std::vector<int> ud = {LU, LU + 1, LU + 2, LD, LD + 1, LD + 2};
+    std::vector<int> ud = {iu, iu + 1, iu + 2, LD, LD + 1, LD + 2};
     std::vector<int> all;
-    for (int i = 0; i < 3; ++i) all.push_back(LU + i);
-    for (int i = 0; i < 9; ++i) all.push_back(LDU + i);
+    for (int i = 0; i < 3; ++i) all.push_back(iu + i);
+    for (int i = 0; i < 9; ++i) all.push_back(idu + i);
     for (int i = 0; i < 3; ++i) all.push_back(LD + i);
     for (int i = 0; i < 9; ++i) all.push_back(LDD + i);
     std::vector<int> grads;
-    for (int i = 0; i < 9; ++i) grads.push_back(LDU + i);
+    for (int i = 0; i < 9; ++i) grads.push_back(idu + i);
     for (int i = 0; i < 9; ++i) grads.push_back(LDD + i);
     // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333)
     {

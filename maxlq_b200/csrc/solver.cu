@@ -74,6 +74,7 @@ class Solver : public SolverBase {
     // load a host vector field, refusing fields with modes outside the band
     void load(const double* host, double2* spec) {
         MLQ_CUDA(cudaStreamSynchronize(e.stream));
+        e.state_written(spec);
         const double rel = io().load_vec(host, spec);
         trim_io();
         const double tol = 1e-24;  // relative energy; FP64 FFT round-trip noise is ~1e-32
