@@ -51,9 +51,12 @@ EngineBase::EngineBase(const mlq_params& p) : P(p) {
     d_results = (double*)dev_alloc(NRES * sizeof(double));
     MLQ_CUDA(cudaMemset(d_results, 0, NRES * sizeof(double)));
     ensure_partials(1 << 20);
+    if (const char* e = std::getenv("MLQ_GRAPHS")) graphs_on_ = std::string(e) != "0";
 }
 
 EngineBase::~EngineBase() {
+    for (auto& kv : graphs_)
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     for (void* p : allocs_) cudaFree(p);
     if (stream) cudaStreamDestroy(stream);
 }
@@ -101,6 +104,7 @@ void* EngineBase::dev_alloc(size_t b) {
 void EngineBase::free_dev(void* p) {
     auto it = std::find(allocs_.begin(), allocs_.end(), p);
     if (it != allocs_.end()) {
+        ++graph_gen_;  // captured graphs may reference the freed block
         allocs_.erase(it);
         cudaFree(p);
     }

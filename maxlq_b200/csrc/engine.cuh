@@ -96,6 +96,28 @@ class EngineBase {
     void launched(const char* name = nullptr, double alg_bytes = 0.0, cudaEvent_t a = nullptr);
     cudaEvent_t prof_mark();
     bool prof_on = false;
+
+    // ---- CUDA graphs of fixed launch sequences ----
+    // as_graph(name, key, body): the first call with a key runs body() as is
+    // (lazy allocations, attributes), the second captures it into a graph,
+    // later calls with the same key launch the graph.  body() may issue only
+    // stream-ordered work.  Freeing device memory drops every graph (they may
+    // hold the pointers); profiling runs bodies directly.  MLQ_GRAPHS=0 turns
+    // graphs off.
+    struct ProgGraph {
+        std::vector<const void*> key;
+        long gen = -1;
+        int seen = 0;
+        bool disabled = false;
+        long long nlaunch = 0;
+        cudaGraphExec_t exec = nullptr;
+    };
+    std::map<std::string, ProgGraph> graphs_;
+    long graph_gen_ = 0;
+    bool graphs_on_ = true;
+    long long graph_launches_ = 0;  // graphs launched (replays)
+    template <class Fn>
+    void as_graph(const std::string& name, const std::vector<const void*>& key, Fn&& body);
     bool prof_detail = false;  // x-stage launches keyed by functor as well
     struct KStat {
         long long n = 0;
@@ -120,6 +142,71 @@ class EngineBase {
 
     std::vector<void*> allocs_;
 };
+
+template <class Fn>
+void EngineBase::as_graph(const std::string& name, const std::vector<const void*>& key, Fn&& body) {
+    if (!graphs_on_ || prof_on) {
+        body();
+        return;
+    }
+    // one cached graph per (name, key): callers alternate between buffers
+    std::string id = name;
+    for (const void* k : key) id += ":" + std::to_string(reinterpret_cast<uintptr_t>(k));
+    if (graphs_.size() > 32 && !graphs_.count(id)) {
+        for (auto& kv : graphs_)
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        graphs_.clear();
+    }
+    ProgGraph& g = graphs_[id];
+    if (g.key != key || g.gen != graph_gen_) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+        g.key = key;
+        g.gen = graph_gen_;
+        g.seen = 0;
+    }
+    if (g.exec) {
+        MLQ_CUDA(cudaGraphLaunch(g.exec, stream));
+        launches += g.nlaunch;
+        ++graph_launches_;
+        return;
+    }
+    if (g.disabled || g.seen++ == 0) {
+        body();
+        return;
+    }
+    const long long l0 = launches;
+    MLQ_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    bool ok = true;
+    try {
+        body();
+    } catch (...) {
+        ok = false;
+    }
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(stream, &gr);
+    if (ok && ec == cudaSuccess && gr) {
+        const cudaError_t ei = cudaGraphInstantiate(&g.exec, gr, 0);
+        cudaGraphDestroy(gr);
+        if (ei == cudaSuccess && g.gen == graph_gen_) {
+            g.nlaunch = launches - l0;
+            launches = l0;
+            MLQ_CUDA(cudaGraphLaunch(g.exec, stream));
+            launches += g.nlaunch;
+            ++graph_launches_;
+            return;
+        }
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    } else if (gr) {
+        cudaGraphDestroy(gr);
+    }
+    // capture failed (for instance an allocation inside body): run directly
+    cudaGetLastError();
+    g.disabled = true;
+    launches = l0;
+    body();
+}
 
 // A physical-space power field |u|^k as computed by calc_uk.
 struct PowField {
@@ -220,6 +307,8 @@ class Engine : public EngineBase {
     // dealiased |u|^{q-2} u spectra (for calcConstraintDerivativeL2) into
     // c (FP64, may be null) and ||u||_q^q.
     void grad_l2(const double2* u, double2* v, double2* c, double* lqq);
+    void grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq);
+    int grad_lq_slot_ = 0;
     // vectorTransport pieces at w = u + tau*d: ir[i] = <P2(|w|^{q-2} w), xi_i>,
     // returns ||w||_q^q.
     double transport_pieces(const double2* u, const double2* d, double tau, const double2* const* xi, int nxi,

@@ -68,6 +68,7 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
             }
             slab_ = true;
             zs_ = zs;
+            graphs_on_ = false;  // slot storage moves between fields from one call to the next
         }
     }
 }
@@ -222,6 +223,7 @@ std::string Engine<T>::kernel_config() const {
     const char* fam = cfft_ok_ ? "compile-time" : (reg_ok_ ? "register" : "shared-memory");
     std::string r = std::string("{\"precision\": \"") + (sizeof(T) == 4 ? "fp32" : "fp64") +
                     "\", \"pass_kernels\": \"" + fam + "\", \"slab_planes\": " + std::to_string(slab_ ? zs_ : 0) +
+                    ", \"graph_replays\": " + std::to_string(graph_launches_) +
                     ", \"line_search_trials_polynomial\": " + std::to_string(ls_poly_trials_) +
                     ", \"line_search_trials_transform\": " + std::to_string(ls_fft_trials_) +
                     ", \"yz_variants\": \"" + (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
@@ -1444,11 +1446,22 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
 // is linear), the fifth term nu Lap P2(|u|^{q-2}u) is added in the spectrum.
 template <typename T>
 void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
+    if (!c) throw CudaError("grad_l2 needs a spectrum buffer for |u|^{q-2}u", MLQ_ERR_BADARG);
+    // the same launches every CG iteration: a CUDA graph after the first two
+    as_graph("grad_l2", {u, v, c, lqq ? (const void*)v : nullptr}, [&] { grad_l2_body(u, v, c, lqq != nullptr); });
+    if (!slab_) pu_of_ = u;  // PU, PD hold u and grad u until the next program
+    if (lqq) {
+        fetch_results();
+        *lqq = h_results[grad_lq_slot_];
+    }
+}
+
+template <typename T>
+void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq) {
     pu_of_ = nullptr;
     const Band& b = b2;
     const long nc = spec_ncomp();
     const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
-    if (!c) throw CudaError("grad_l2 needs a spectrum buffer for |u|^{q-2}u", MLQ_ERR_BADARG);
     chain_reset();
     // 1. u, grad u, Lap u
     std::vector<InvOut> io;
@@ -1467,7 +1480,6 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
         io.push_back(o);
     }
     inv(b, io);
-    if (!slab_) pu_of_ = u;  // PU, PD hold u and grad u until the next program
     std::vector<int> uin;
     for (int i = 0; i < 3; ++i) uin.push_back(PU + i);
     for (int i = 0; i < 9; ++i) uin.push_back(PD + i);
@@ -1580,16 +1592,14 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
             fwd(b, f, in3, {o[0], o[1], o[2]});
         }
     }
-    if (lqq) {
+    if (want_lq) {
         if (ah.kind == PowField::RAW || ah.spec < 0) {
             pointwise(FSqRed{}, {ah.phys}, {}, 20);
-            fetch_results();
-            *lqq = h_results[20];
+            grad_lq_slot_ = 20;
         } else {
             ensure_p2_spec(ah);
             sdots(*this, {{wspec(ah.spec), wspec(ah.spec)}}, 0);
-            fetch_results();
-            *lqq = h_results[0];
+            grad_lq_slot_ = 0;
         }
     }
 }

@@ -77,3 +77,18 @@ def test_compile_time_kernels_match_runtime_plan_kernels(n, precision, tol, monk
         assert r1["n_evals"] == r0["n_evals"]  # FP32 roundoff may move Brent by an evaluation
     assert r1["J1"] == pytest.approx(r0["J1"], rel=tol)
     assert r1["tau"] == pytest.approx(r0["tau"], rel=1e-3 if precision == "mixed" else 1e-9)
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_gradient_graph_replay_matches_direct_launches(prec, monkeypatch):
+    """The gradient program replayed as a CUDA graph gives the same CG
+    trajectory, bit for bit, as the same launches issued one by one."""
+    runs = {}
+    for graphs in ("0", "1"):
+        monkeypatch.setenv("MLQ_GRAPHS", graphs)
+        with mlq.MaxLq(64, 4.0, 1.0, precision=prec, optim_tol=1e-14) as c:
+            c.state_load(c.seed_field(2, 2.0, 4.0))
+            _, st, rec = c.state_iterate(5)
+            runs[graphs] = ([r["J1"] for r in rec], [r["tau"] for r in rec], c.kernel_config()["graph_replays"])
+    assert runs["0"][0] == runs["1"][0] and runs["0"][1] == runs["1"][1]
+    assert runs["0"][2] == 0 and runs["1"][2] >= 3
