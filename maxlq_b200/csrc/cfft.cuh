@@ -291,13 +291,17 @@ struct CShape {
 template <int N, typename T, int V>
 struct YShape {
     static constexpr bool F32 = sizeof(T) == 4;
-    static constexpr int EY = V == 0 ? CShape<N, T>::EY : (V == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8));
-    static constexpr int TX = V == 0 ? CShape<N, T>::TX : (V == 1 ? 8 : (F32 ? 16 : 4));
+    // V: 0 default; 1 the other element count; 2 the other tile width;
+    // 3 and 4 as 0 and 1 with the stage twiddles held in registers
+    static constexpr int VB = V >= 3 ? V - 3 : V;
+    static constexpr int EY = VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8));
+    static constexpr int TX = VB == 0 ? CShape<N, T>::TX : (VB == 1 ? 8 : (F32 ? 16 : 4));
+    static constexpr bool TWREG = V >= 3;
     static constexpr int TPLY = N / EY;
     static constexpr int YTHREADS = TX * TPLY;
     // resident blocks the register budget aims at (8 elements per thread in
     // FP32 leave room for two 512-thread blocks: 64 registers)
-    static constexpr int YMINB = YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1);
+    static constexpr int YMINB = TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1));
     // two tiles (the staged next item, and the current item's exchange
     // buffer) + the twiddle table; the z stage adds the K table
     static constexpr size_t YSMEM = ((size_t)2 * N * TX + N) * sizeof(cpx<T>);
@@ -305,8 +309,20 @@ struct YShape {
     static constexpr size_t ZISMEM = ((size_t)N * TX + N) * sizeof(cpx<T>) + 2 * N * sizeof(T);  // z inverse: one tile
     static constexpr bool valid =
         V == 0 || (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
-                   (EY != CShape<N, T>::EY || TX != CShape<N, T>::TX));
+                   (V >= 3 || EY != CShape<N, T>::EY || TX != CShape<N, T>::TX) && (V != 4 || F32));
     static_assert(V != 0 || ZSMEM <= 200 * 1024, "default y/z tile fits the shared-memory limit");
+};
+
+// stage twiddles of a y/z column thread: a broadcast shared table, or registers
+template <int N, int E, typename T, bool REG>
+struct YTw;
+template <int N, int E, typename T>
+struct YTw<N, E, T, false> : TwTab<N, E, T> {
+    __device__ __forceinline__ YTw(const cpx<T>* stw, const cpx<T>*, int) { this->tab = stw; }
+};
+template <int N, int E, typename T>
+struct YTw<N, E, T, true> : TwReg<N, E, T> {
+    __device__ __forceinline__ YTw(const cpx<T>*, const cpx<T>* __restrict__ gtab, int t) { this->load(gtab, t); }
 };
 
 // block-wide deterministic reduction of NR accumulators into partials[slot]
@@ -530,8 +546,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     cpx<T>* stw = buf1 + N * TX;
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
     __syncthreads();
-    const TwTab<N, E, T> tw{stw};
     const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const YTw<N, E, T, S::TWREG> tw(stw, twN, t);
     const ColMap<TX> map{l};
     const int nx = a.nx, nb = a.band.nb;
     const int ntile = (nx + TX - 1) / TX;
@@ -723,8 +739,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
     fill_k_table<N>(kt);
     __syncthreads();
-    const TwTab<N, E, T> tw{stw};
     const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const YTw<N, E, T, S::TWREG> tw(stw, twN, t);
     const ColMap<TX> map{l};
     const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
     const int ntile = (nx + TX - 1) / TX;
@@ -869,8 +885,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
     fill_k_table<N>(kt);
     __syncthreads();
-    const TwTab<N, E, T> tw{stw};
     const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const YTw<N, E, T, S::TWREG> tw(stw, twN, t);
     const ColMap<TX> map{l};
     const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
     const int ntile = (nx + TX - 1) / TX;

@@ -47,9 +47,14 @@ EngineBase::EngineBase(const mlq_params& p) : P(p) {
         }
     }
     d_tw = (cpx<double>*)dev_alloc(pool.size() * sizeof(cpx<double>));
-    MLQ_CUDA(cudaMemcpy(d_tw, pool.data(), pool.size() * sizeof(cpx<double>), cudaMemcpyHostToDevice));
+    // stream-ordered and complete before the first kernel that reads it (a
+    // pageable cudaMemcpy may return before its DMA lands, and the engine's
+    // stream does not wait for the legacy stream)
+    MLQ_CUDA(cudaMemcpyAsync(d_tw, pool.data(), pool.size() * sizeof(cpx<double>), cudaMemcpyHostToDevice, stream));
+    MLQ_CUDA(cudaStreamSynchronize(stream));
     d_results = (double*)dev_alloc(NRES * sizeof(double));
-    MLQ_CUDA(cudaMemset(d_results, 0, NRES * sizeof(double)));
+    MLQ_CUDA(cudaMemsetAsync(d_results, 0, NRES * sizeof(double), stream));
+    MLQ_CUDA(cudaStreamSynchronize(stream));
     ensure_partials(1 << 20);
     if (const char* e = std::getenv("MLQ_GRAPHS")) graphs_on_ = std::string(e) != "0";
 }
@@ -202,11 +207,49 @@ void EngineBase::lincomb(double2* out, double a, const double2* x, double b, con
     launched("spec_lincomb", 48.0 * g.ncomp * (2 + (y ? 1 : 0) + (z ? 1 : 0)), ev);
 }
 
+// K = 2 pi j: |K|^2 of a mode with |j|^2 = jsq
+static double ksq_of(long jsq) {
+    const double twopi = 2.0 * PI_REF;
+    return twopi * twopi * (double)jsq;
+}
+
+const double* EngineBase::hilbert_table(double order) {
+    auto it = htab_.find(order);
+    if (it != htab_.end()) return it->second;
+    const long m = 3L * b2.cut * b2.cut + 1;
+    std::vector<double> h(m);
+    for (long j = 0; j < m; ++j) h[j] = 1.0 / (1.0 + std::pow(P.lambda1 * std::sqrt(ksq_of(j)), 2.0 * order));
+    double* d = (double*)dev_alloc(m * sizeof(double));
+    MLQ_CUDA(cudaMemcpyAsync(d, h.data(), m * sizeof(double), cudaMemcpyHostToDevice, stream));
+    MLQ_CUDA(cudaStreamSynchronize(stream));
+    htab_[order] = d;
+    return d;
+}
+
+const double* EngineBase::hweight_table(double order) {
+    auto it = hwtab_.find(order);
+    if (it != hwtab_.end()) return it->second;
+    const long m = 3L * b2.cut * b2.cut + 1;
+    std::vector<double> h(m);
+    for (long j = 0; j < m; ++j) {
+        const double f = 1.0 + std::pow(P.lambda1 * std::sqrt(ksq_of(j)), order);
+        h[j] = f * f;
+    }
+    double* d = (double*)dev_alloc(m * sizeof(double));
+    MLQ_CUDA(cudaMemcpyAsync(d, h.data(), m * sizeof(double), cudaMemcpyHostToDevice, stream));
+    MLQ_CUDA(cudaStreamSynchronize(stream));
+    hwtab_[order] = d;
+    return d;
+}
+
+static int spec_rows_grid(const SpecGeom& g) { return std::max(1, std::min(g.nb * g.nb, 148 * 16)); }
+
 void EngineBase::hilbert(double2* f, double order) {
     state_written(f);
     SpecGeom g = geom(b2);
+    const double* t = hilbert_table(order);
     cudaEvent_t ev = prof_mark();
-    spec_hilbert_kernel<<<grid_for(g.ncomp, 256), 256, 0, stream>>>(g, f, P.lambda1, 2.0 * order);
+    spec_hilbert_leray_kernel<<<spec_rows_grid(g), 128, 0, stream>>>(g, f, t, 1.0, 0);
     launched("spec_hilbert", 96.0 * g.ncomp, ev);
 }
 
@@ -214,8 +257,17 @@ void EngineBase::leray(double2* f) {
     state_written(f);
     SpecGeom g = geom(b2);
     cudaEvent_t ev = prof_mark();
-    spec_leray_kernel<<<grid_for(g.ncomp, 256), 256, 0, stream>>>(g, f);
+    spec_hilbert_leray_kernel<<<spec_rows_grid(g), 128, 0, stream>>>(g, f, nullptr, 1.0, 1);
     launched("spec_leray", 96.0 * g.ncomp, ev);
+}
+
+void EngineBase::hilbert_leray(double2* f, double order, double scale) {
+    state_written(f);
+    SpecGeom g = geom(b2);
+    const double* t = hilbert_table(order);
+    cudaEvent_t ev = prof_mark();
+    spec_hilbert_leray_kernel<<<spec_rows_grid(g), 128, 0, stream>>>(g, f, t, scale, 1);
+    launched("spec_hilbert_leray", 96.0 * g.ncomp, ev);
 }
 
 void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
@@ -223,8 +275,9 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
     a.g = geom(b2);
     for (int i = 0; i < np; ++i) a.pr[i] = pairs[i];
     a.npairs = np;
-    a.lambda1 = P.lambda1;
-    a.order = 1.5 - 1.0 / P.q;  // (3/2)-(1/q), function_ops.f90:3467
+    bool need_h = false;
+    for (int i = 0; i < np; ++i) need_h |= pairs[i].kind == 1;
+    a.hwtab = need_h ? hweight_table(1.5 - 1.0 / P.q) : nullptr;  // (3/2)-(1/q), function_ops.f90:3467
     a.partials = d_partials;
     const int grid = grid_for(a.g.ncomp, RED_THREADS, 148 * 4);
     cudaEvent_t ev = prof_mark();

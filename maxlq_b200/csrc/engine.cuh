@@ -75,6 +75,12 @@ class EngineBase {
                  const double2* z = nullptr);
     void hilbert(double2* f, double order);
     void leray(double2* f);
+    // f <- leray(hilbert(scale * f, order)) in one pass
+    void hilbert_leray(double2* f, double order, double scale = 1.0);
+    // tables over |j|^2 of the band b2: Hilbert symbol and H_l inner-product weight
+    std::map<double, double*> htab_, hwtab_;
+    const double* hilbert_table(double order);
+    const double* hweight_table(double order);
     // up to 6 vector inner products; kinds 0 L2, 1 H_l, 2 div energy
     void dots(const SpecDotPair* pairs, int np, double* out);
     void zeroth(const double2* f, double out[3]);

@@ -40,10 +40,12 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
     } else {
         d_twT_ = (cpx<T>*)dev_alloc(ntw * sizeof(cpx<T>));
         std::vector<cpx<double>> h(ntw);
-        MLQ_CUDA(cudaMemcpy(h.data(), d_tw, ntw * sizeof(cpx<double>), cudaMemcpyDeviceToHost));
+        MLQ_CUDA(cudaMemcpyAsync(h.data(), d_tw, ntw * sizeof(cpx<double>), cudaMemcpyDeviceToHost, stream));
+        MLQ_CUDA(cudaStreamSynchronize(stream));
         std::vector<cpx<T>> hf(ntw);
         for (long i = 0; i < ntw; ++i) hf[i] = mk<T>((T)h[i].x, (T)h[i].y);
-        MLQ_CUDA(cudaMemcpy(d_twT_, hf.data(), ntw * sizeof(cpx<T>), cudaMemcpyHostToDevice));
+        MLQ_CUDA(cudaMemcpyAsync(d_twT_, hf.data(), ntw * sizeof(cpx<T>), cudaMemcpyHostToDevice, stream));
+        MLQ_CUDA(cudaStreamSynchronize(stream));
     }
     tune_yz();
     // z-slab streaming when the physical fields the programs keep resident
@@ -196,6 +198,12 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
     if constexpr (YShape<NN, T, 2>::valid) {
         if (v == 2) return f(std::integral_constant<int, 2>{});
     }
+    if constexpr (YShape<NN, T, 3>::valid) {
+        if (v == 3) return f(std::integral_constant<int, 3>{});
+    }
+    if constexpr (YShape<NN, T, 4>::valid) {
+        if (v == 4) return f(std::integral_constant<int, 4>{});
+    }
     f(std::integral_constant<int, 0>{});
 }
 
@@ -243,7 +251,7 @@ void Engine<T>::tune_yz() {
     bool any = false;
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
-        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid;
+        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid || YShape<NN, T, 3>::valid;
     });
     if (!any) return;
     if (const char* e = std::getenv("MLQ_YZ_VARIANT")) {  // fixed variant (measurement runs)
@@ -251,7 +259,8 @@ void Engine<T>::tune_yz() {
         bool ok = v == 0;
         dispatch_n(n, [&](auto nc) {
             constexpr int NN = decltype(nc)::value;
-            ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid);
+            ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid) ||
+                 (v == 3 && YShape<NN, T, 3>::valid) || (v == 4 && YShape<NN, T, 4>::valid);
         });
         if (ok)
             for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
@@ -314,15 +323,18 @@ void Engine<T>::tune_yz() {
         });
         MLQ_CUDA(cudaGetLastError());
     };
-    bool valid[3] = {true, false, false};
+    constexpr int NV = 5;
+    bool valid[NV] = {true, false, false, false, false};
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         valid[1] = YShape<NN, T, 1>::valid;
         valid[2] = YShape<NN, T, 2>::valid;
+        valid[3] = YShape<NN, T, 3>::valid;
+        valid[4] = YShape<NN, T, 4>::valid;
     });
     // every variant of every kind once first (clocks, attributes, page-in)
     for (int kind = 0; kind < YV_KINDS; ++kind)
-        for (int v = 0; v < 3; ++v)
+        for (int v = 0; v < NV; ++v)
             if (valid[v]) {
                 yvar_[kind] = v;
                 launch(kind);
@@ -331,9 +343,9 @@ void Engine<T>::tune_yz() {
     // replaces variant 0 only when it is at least 3 % faster
     std::string rep;
     for (int kind = 0; kind < YV_KINDS; ++kind) {
-        float best_ms[3] = {1e30f, 1e30f, 1e30f};
+        float best_ms[NV] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
         for (int r = 0; r < 5; ++r)
-            for (int v = 0; v < 3; ++v) {
+            for (int v = 0; v < NV; ++v) {
                 if (!valid[v]) continue;
                 yvar_[kind] = v;
                 MLQ_CUDA(cudaEventRecord(e0, stream));
@@ -346,7 +358,7 @@ void Engine<T>::tune_yz() {
             }
         int bestv = 0;
         std::string times;
-        for (int v = 0; v < 3; ++v) {
+        for (int v = 0; v < NV; ++v) {
             if (!valid[v]) continue;
             times += (times.empty() ? "" : " ") + std::to_string(v) + ":" + std::to_string(best_ms[v]);
             if (best_ms[v] < 0.97f * best_ms[bestv]) bestv = v;

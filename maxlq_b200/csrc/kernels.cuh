@@ -559,41 +559,61 @@ static __global__ void spec_lincomb_kernel(SpecGeom g, double2* out, double a, c
     }
 }
 
-// Hilbert gradient symbol 1/(1+(lambda1|K|)^(2 order)) (function_ops.f90:3611)
-static __global__ void spec_hilbert_kernel(SpecGeom g, double2* f, double lambda1, double order2) {
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
-        int fx, fy, fz;
-        spec_coords(g, i, fx, fy, fz);
-        const Kvec k = make_k(g.n, fx, fy, fz);
-        const double s = 1.0 / (1.0 + pow(lambda1 * sqrt(k.ksq), order2));
-        for (int c = 0; c < 3; ++c) {
-            double2 v = f[c * g.ncomp + i];
-            f[c * g.ncomp + i] = make_double2(v.x * s, v.y * s);
-        }
+// Row-structured walk over a band spectrum [nb][nb][nx]: block b takes rows
+// r = b, b + gridDim.x, ... (r = cz*nb + cy), threads take kx; no division per
+// element.  Signed indices and |j|^2 of a mode give the wavenumbers exactly
+// as make_k does (K = 2 pi j).
+struct SpecRow {
+    int cz, cy, jy, jz;
+    __device__ __forceinline__ SpecRow(const SpecGeom& g, int r) {
+        cz = r / g.nb;
+        cy = r - cz * g.nb;
+        jy = signed_j(g.n, band_fft_index(g.band, cy));
+        jz = signed_j(g.n, band_fft_index(g.band, cz));
     }
-}
+};
 
-// divAvg_free (function_ops.f90:2843-2918): u - K(K.u)/|K|^2 with the odd
-// (first-derivative) factors of the divergence/gradient round trip, k=0 -> 0.
-static __global__ void spec_leray_kernel(SpecGeom g, double2* f) {
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
-        int fx, fy, fz;
-        spec_coords(g, i, fx, fy, fz);
-        const Kvec k = make_k(g.n, fx, fy, fz);
-        double2 u0 = f[i], u1 = f[g.ncomp + i], u2 = f[2 * g.ncomp + i];
-        if (k.ksq > MACH_EPSILON) {
-            const double dr = k.ox * u0.x + k.oy * u1.x + k.oz * u2.x;
-            const double di = k.ox * u0.y + k.oy * u1.y + k.oz * u2.y;
-            const double s = 1.0 / k.ksq;
-            u0.x -= k.ox * dr * s; u0.y -= k.ox * di * s;
-            u1.x -= k.oy * dr * s; u1.y -= k.oy * di * s;
-            u2.x -= k.oz * dr * s; u2.y -= k.oz * di * s;
-        } else {
-            u0 = u1 = u2 = make_double2(0.0, 0.0);
+// f <- Leray(s(K) * scale * f) over a band spectrum, either part optional:
+// the Hilbert gradient symbol s = 1/(1+(lambda1|K|)^(2 order))
+// (function_ops.f90:3611) read from a table indexed by |j|^2, and divAvg_free
+// (2843-2918): u - K(K.u)/|K|^2 (odd factors), k = 0 -> 0.
+static __global__ void spec_hilbert_leray_kernel(SpecGeom g, double2* f, const double* __restrict__ htab,
+                                                 double scale, int do_leray) {
+    const double twopi = 2.0 * 3.14159265358979311600;
+    const int nrows = g.nb * g.nb;
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const SpecRow row(g, r);
+        const long base = (long)r * g.nx;
+        const double ky = twopi * (double)row.jy, kz = twopi * (double)row.jz;
+        for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
+            const long i = base + fx;
+            double2 u0 = f[i], u1 = f[g.ncomp + i], u2 = f[2 * g.ncomp + i];
+            double s = scale;
+            if (htab) s *= htab[fx * fx + row.jy * row.jy + row.jz * row.jz];
+            u0.x *= s; u0.y *= s;
+            u1.x *= s; u1.y *= s;
+            u2.x *= s; u2.y *= s;
+            if (do_leray) {
+                const double kx = twopi * (double)fx;
+                const double ox = (2 * fx == g.n) ? 0.0 : kx;
+                const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
+                const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
+                const double ksq = kx * kx + ky * ky + kz * kz;
+                if (ksq > MACH_EPSILON) {
+                    const double dr = ox * u0.x + oy * u1.x + oz * u2.x;
+                    const double di = ox * u0.y + oy * u1.y + oz * u2.y;
+                    const double is = 1.0 / ksq;
+                    u0.x -= ox * dr * is; u0.y -= ox * di * is;
+                    u1.x -= oy * dr * is; u1.y -= oy * di * is;
+                    u2.x -= oz * dr * is; u2.y -= oz * di * is;
+                } else {
+                    u0 = u1 = u2 = make_double2(0.0, 0.0);
+                }
+            }
+            f[i] = u0;
+            f[g.ncomp + i] = u1;
+            f[2 * g.ncomp + i] = u2;
         }
-        f[i] = u0;
-        f[g.ncomp + i] = u1;
-        f[2 * g.ncomp + i] = u2;
     }
 }
 
@@ -609,43 +629,43 @@ struct SpecDotArgs {
     SpecGeom g;
     SpecDotPair pr[6];
     int npairs;
-    double lambda1, order;
+    const double* hwtab;  // H_l weight (1+(lambda1|K|)^order)^2 by |j|^2 (function_ops.f90:3472), or null
     double* partials;
 };
 
 static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
     double acc[6] = {0, 0, 0, 0, 0, 0};
     const SpecGeom& g = a.g;
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
-        int fx, fy, fz;
-        spec_coords(g, i, fx, fy, fz);
-        const Kvec k = make_k(g.n, fx, fy, fz);
-        const double wgt = kx_weight(g.n, fx);
-        double hw = 1.0;
-        bool need_h = false;
-        for (int p = 0; p < a.npairs; ++p) need_h |= a.pr[p].kind == 1;
-        if (need_h) {
-            const double f = 1.0 + pow(a.lambda1 * sqrt(k.ksq), a.order);
-            hw = f * f;
-        }
-        for (int p = 0; p < a.npairs; ++p) {
-            const SpecDotPair& q = a.pr[p];
-            if (q.kind == 2) {
-                double dr = 0.0, di = 0.0;
-                const double o[3] = {k.ox, k.oy, k.oz};
-                for (int c = 0; c < 3; ++c) {
-                    const double2 v = q.a[c * g.ncomp + i];
-                    dr += o[c] * v.x;
-                    di += o[c] * v.y;
+    const double twopi = 2.0 * 3.14159265358979311600;
+    const int nrows = g.nb * g.nb;
+    // 32 threads per row: RED_THREADS / 32 rows per block pass
+    const int lane = threadIdx.x & 31, wrow = threadIdx.x >> 5, rows_per = blockDim.x >> 5;
+    for (int r = blockIdx.x * rows_per + wrow; r < nrows; r += gridDim.x * rows_per) {
+        const SpecRow row(g, r);
+        const long base = (long)r * g.nx;
+        const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : twopi * (double)row.jy;
+        const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : twopi * (double)row.jz;
+        const int jyz = row.jy * row.jy + row.jz * row.jz;
+        for (int fx = lane; fx < g.nx; fx += 32) {
+            const long i = base + fx;
+            const double wgt = kx_weight(g.n, fx);
+            const double hw = a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0;
+            const double ox = (2 * fx == g.n) ? 0.0 : twopi * (double)fx;
+            for (int p = 0; p < a.npairs; ++p) {
+                const SpecDotPair& q = a.pr[p];
+                if (q.kind == 2) {
+                    const double2 v0 = q.a[i], v1 = q.a[g.ncomp + i], v2 = q.a[2 * g.ncomp + i];
+                    const double dr = ox * v0.x + oy * v1.x + oz * v2.x;
+                    const double di = ox * v0.y + oy * v1.y + oz * v2.y;
+                    acc[p] += wgt * (dr * dr + di * di);
+                } else {
+                    double s = 0.0;
+                    for (int c = 0; c < 3; ++c) {
+                        const double2 u = q.a[c * g.ncomp + i], v = q.b[c * g.ncomp + i];
+                        s += u.x * v.x + u.y * v.y;
+                    }
+                    acc[p] += wgt * (q.kind == 1 ? hw : 1.0) * s;
                 }
-                acc[p] += wgt * (dr * dr + di * di);
-            } else {
-                double s = 0.0;
-                for (int c = 0; c < 3; ++c) {
-                    const double2 u = q.a[c * g.ncomp + i], v = q.b[c * g.ncomp + i];
-                    s += u.x * v.x + u.y * v.y;
-                }
-                acc[p] += wgt * (q.kind == 1 ? hw : 1.0) * s;
             }
         }
     }

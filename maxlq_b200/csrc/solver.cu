@@ -301,13 +301,10 @@ class Solver : public SolverBase {
         double2* g1 = gu1;
         double lqq_u = 0;
         e.grad_l2(u, g1, c, &lqq_u);  // 146
-        e.hilbert(g1, s);             // 151
-        e.leray(g1);                  // 153
+        e.hilbert_leray(g1, s);       // 151, 153
         // normal of the tangent space: ||u||_q^{1-q} P2(|u|^{q-2} u) (162)
         const double unorm = std::pow(lqq_u, 1.0 / qq);
-        e.lincomb(c, std::pow(unorm, 1.0 - qq), c);
-        e.hilbert(c, s);  // 164
-        e.leray(c);       // 169
+        e.hilbert_leray(c, s, std::pow(unorm, 1.0 - qq));  // 162, 164, 169
         double dd[6];
         {
             SpecDotPair p[2] = {{c, g1, 1}, {c, c, 1}};
