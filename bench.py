@@ -230,6 +230,11 @@ def cpu_reference_sample(n, q, n_evals, workers):
     return dt / 2.0
 
 
+def workload_name(n, q):
+    return (f"maxdLqdt CG iteration, N={n}^3, q={q:g}, B=1, seeded spectrum |j|^-2 exp(-(|j|/{n / 32.0:g})^2), "
+            "one independent replica per GPU")
+
+
 def bench_reference(args, dist):
     """--impl reference: the reference algorithm (reference-order CPU
     transcription, scipy pocketfft on all host threads) on the host cores."""
@@ -253,7 +258,7 @@ def bench_reference(args, dist):
             "warmup": args.warmup, "ms_per_step": 1000.0 * tot / len(per_iter), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": f"maxdLqdt CG iteration, N={n}^3, q={q:g}, B=1", "n": n, "q": q},
+            "config": {"workload": workload_name(n, q), "n": n, "q": q},
             "cpu_baseline": {"value": value, "unit": "iters/s", "cores": workers, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -582,8 +587,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": dist.world, "steps": K, "warmup": W,
             "ms_per_step": 1000.0 * t_m / max(res_m["iters"], 1), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32/f64", "data": "synthetic",
-            "config": {"workload": f"maxdLqdt CG iteration, N={n}^3, q={q:g}, B=1, seeded spectrum "
-                                   f"|j|^-2 exp(-(|j|/{k0:g})^2), one independent replica per GPU",
+            "config": {"workload": workload_name(n, q),
                        "n": n, "q": q, "precision": "mixed: FP32 fields and FFTs, FP64 state/reductions/control",
                        "fp64_iters_per_s": fp64_value,
                        "mixed_over_fp64": (value / fp64_value) if fp64_value else None,

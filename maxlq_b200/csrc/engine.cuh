@@ -142,9 +142,10 @@ class EngineBase {
     };
     std::vector<Pend> pend_;
     std::vector<cudaEvent_t> evpool_;
-    cudaEvent_t ev_take();
 
    public:
+    cudaEvent_t ev_take();  // from the engine's pool of events
+    void ev_give(cudaEvent_t e) { evpool_.push_back(e); }
 
     std::vector<void*> allocs_;
 };

@@ -2055,34 +2055,85 @@ void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
 // ----------------------------------------------------------------------------
 // state <-> host
 // ----------------------------------------------------------------------------
+// Host copies of transfers run on several threads, and are pipelined with
+// the DMA in chunks through two pinned staging buffers.
+template <class Fn>
+static void par_range(long count, Fn&& fn) {
+    const long nt = std::max(1L, std::min<long>(16, (long)std::thread::hardware_concurrency() / 2));
+    if (nt == 1 || count < (1L << 20)) {
+        fn(0L, count);
+        return;
+    }
+    std::vector<std::thread> th;
+    const long per = (count + nt - 1) / nt;
+    for (long t = 0; t < nt; ++t) {
+        const long a = t * per, b = std::min(count, a + per);
+        if (a < b) th.emplace_back([&fn, a, b] { fn(a, b); });
+    }
+    for (auto& x : th) x.join();
+}
+
+static constexpr long XFER_CHUNK = 1L << 25;  // elements per pipelined chunk
+
 template <typename T>
 void Engine<T>::load_scalar_phys(const double* host, int dst) {
-    T* st = (T*)stage(n3 * sizeof(T));
-    if (sizeof(T) == 8)
-        std::memcpy(st, host, n3 * sizeof(double));
-    else
-        for (long i = 0; i < n3; ++i) st[i] = (T)host[i];
-    MLQ_CUDA(cudaMemcpyAsync(phys(dst), st, n3 * sizeof(T), cudaMemcpyHostToDevice, stream));
+    const long ch = std::min(n3, XFER_CHUNK);
+    T* buf[2];
+    buf[0] = (T*)stage(2 * ch * sizeof(T));
+    buf[1] = buf[0] + ch;
+    cudaEvent_t done[2] = {ev_take(), ev_take()};
+    T* d = phys(dst);
+    long k = 0;
+    for (long off = 0; off < n3; off += ch, ++k) {
+        const long cnt = std::min(ch, n3 - off);
+        T* b = buf[k & 1];
+        if (k >= 2) MLQ_CUDA(cudaEventSynchronize(done[k & 1]));  // that buffer's DMA has finished
+        par_range(cnt, [&](long a, long e) {
+            if (sizeof(T) == 8)
+                std::memcpy(b + a, host + off + a, (e - a) * sizeof(double));
+            else
+                for (long i = a; i < e; ++i) b[i] = (T)host[off + i];
+        });
+        MLQ_CUDA(cudaMemcpyAsync(d + off, b, cnt * sizeof(T), cudaMemcpyHostToDevice, stream));
+        MLQ_CUDA(cudaEventRecord(done[k & 1], stream));
+    }
     MLQ_CUDA(cudaStreamSynchronize(stream));
+    ev_give(done[0]);
+    ev_give(done[1]);
     if (slab_) slot(dst).kind = PSlot::FULL;
 }
 
 template <typename T>
 void Engine<T>::store_scalar_phys(int src, double* host) {
-    T* st = (T*)stage(n3 * sizeof(T));
-    if (slab_) {
-        const long per = (long)zs_ * n * n;
-        for (int z0 = 0; z0 < n; z0 += zs_)
-            MLQ_CUDA(cudaMemcpyAsync(st + (long)z0 * n * n, expand(src, z0, 0), per * sizeof(T), cudaMemcpyDeviceToHost,
-                                     stream));
-    } else {
-        MLQ_CUDA(cudaMemcpyAsync(st, phys(src), n3 * sizeof(T), cudaMemcpyDeviceToHost, stream));
+    // chunks of whole slabs in slab mode (each expanded just before its copy)
+    const long ch = slab_ ? (long)zs_ * n * n : std::min(n3, XFER_CHUNK);
+    T* buf[2];
+    buf[0] = (T*)stage(2 * ch * sizeof(T));
+    buf[1] = buf[0] + ch;
+    cudaEvent_t done[2] = {ev_take(), ev_take()};
+    auto issue = [&](long k) {
+        const long off = k * ch, cnt = std::min(ch, n3 - off);
+        const T* d = slab_ ? expand(src, (int)(off / ((long)n * n)), 0) : phys(src) + off;
+        MLQ_CUDA(cudaMemcpyAsync(buf[k & 1], d, cnt * sizeof(T), cudaMemcpyDeviceToHost, stream));
+        MLQ_CUDA(cudaEventRecord(done[k & 1], stream));
+    };
+    const long nk = (n3 + ch - 1) / ch;
+    for (long k = 0; k < std::min(nk, 2L); ++k) issue(k);
+    for (long k = 0; k < nk; ++k) {
+        const long off = k * ch, cnt = std::min(ch, n3 - off);
+        MLQ_CUDA(cudaEventSynchronize(done[k & 1]));
+        const T* b = buf[k & 1];
+        par_range(cnt, [&](long a, long e) {
+            if (sizeof(T) == 8)
+                std::memcpy(host + off + a, b + a, (e - a) * sizeof(double));
+            else
+                for (long i = a; i < e; ++i) host[off + i] = (double)b[i];
+        });
+        if (k + 2 < nk) issue(k + 2);
     }
     MLQ_CUDA(cudaStreamSynchronize(stream));
-    if (sizeof(T) == 8)
-        std::memcpy(host, st, n3 * sizeof(double));
-    else
-        for (long i = 0; i < n3; ++i) host[i] = (double)st[i];
+    ev_give(done[0]);
+    ev_give(done[1]);
 }
 
 // Forward transform of a host vector field into band-b2 state spectra.  The
