@@ -292,25 +292,52 @@ template <int N, typename T, int V>
 struct YShape {
     static constexpr bool F32 = sizeof(T) == 4;
     // V: 0 default; 1 the other element count; 2 the other tile width;
-    // 3 and 4 as 0 and 1 with the stage twiddles held in registers
-    static constexpr int VB = V >= 3 ? V - 3 : V;
-    static constexpr int EY = VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8));
-    static constexpr int TX = VB == 0 ? CShape<N, T>::TX : (VB == 1 ? 8 : (F32 ? 16 : 4));
-    static constexpr bool TWREG = V >= 3;
+    // 3 and 4 as 0 and 1 with the stage twiddles held in registers;
+    // 5 and 6 column-per-warp (CW): one warp transforms one column, 32
+    // threads x N/32 elements, tiles of 8 or 16 (FP32) / 4 or 2 (FP64) columns
+    static constexpr bool CW = V >= 5;
+    static constexpr int VB = CW ? 0 : (V >= 3 ? V - 3 : V);
+    static constexpr int EY = CW ? N / 32 : (VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8)));
+    static constexpr int TX = CW ? (V == 5 ? (F32 ? 8 : 4) : (F32 ? 16 : 2))
+                                 : (VB == 0 ? CShape<N, T>::TX : (VB == 1 ? 8 : (F32 ? 16 : 4)));
+    static constexpr bool TWREG = V == 3 || V == 4;
     static constexpr int TPLY = N / EY;
     static constexpr int YTHREADS = TX * TPLY;
-    // resident blocks the register budget aims at (8 elements per thread in
-    // FP32 leave room for two 512-thread blocks: 64 registers)
-    static constexpr int YMINB = TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1));
+    // CW: the per-warp exchange row (one pad element every EY)
+    static constexpr int WPITCH = N + N / EY;
     // two tiles (the staged next item, and the current item's exchange
-    // buffer) + the twiddle table; the z stage adds the K table
-    static constexpr size_t YSMEM = ((size_t)2 * N * TX + N) * sizeof(cpx<T>);
+    // buffer) + the twiddle table; the z stage adds the K table.  CW adds
+    // the warps' exchange rows and uses two tiles in every pass.
+    static constexpr size_t YSMEM =
+        ((size_t)2 * N * TX + (CW ? (size_t)TX * WPITCH : 0) + N) * sizeof(cpx<T>);
     static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);
-    static constexpr size_t ZISMEM = ((size_t)N * TX + N) * sizeof(cpx<T>) + 2 * N * sizeof(T);  // z inverse: one tile
+    static constexpr size_t ZISMEM =
+        CW ? ZSMEM : ((size_t)N * TX + N) * sizeof(cpx<T>) + 2 * N * sizeof(T);  // z inverse: one tile
+    // resident blocks the register budget aims at (8 elements per thread in
+    // FP32 leave room for two 512-thread blocks: 64 registers); CW: as many
+    // blocks as the shared memory holds, keeping at least 96 registers
+    static constexpr int CW_SMB = (int)((228 * 1024) / (ZSMEM + 1024));
+    static constexpr int CW_RGB = 65536 / (YTHREADS * 96);
+    static constexpr int CW_MINB = CW_SMB < CW_RGB ? CW_SMB : CW_RGB;
+    static constexpr int YMINB = CW ? (CW_MINB < 1 ? 1 : CW_MINB)
+                                    : (TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1)));
     static constexpr bool valid =
-        V == 0 || (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
-                   (V >= 3 || EY != CShape<N, T>::EY || TX != CShape<N, T>::TX) && (V != 4 || F32));
+        V == 0 ||
+        (CW ? (N >= 256 && EY >= 2 && EY <= 16 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 227 * 1024)
+            : (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
+               (V >= 3 || EY != CShape<N, T>::EY || TX != CShape<N, T>::TX) && (V != 4 || F32)));
     static_assert(V != 0 || ZSMEM <= 200 * 1024, "default y/z tile fits the shared-memory limit");
+};
+
+// Column tile of TX columns x N rows for the CW variants: rows of TX
+// elements, the column index XOR-swizzled by the row so that a warp reading
+// one column (32 consecutive rows) and the staging threads writing whole rows
+// both hit distinct banks.
+template <int TX, typename T>
+struct TileMap {
+    static constexpr int W = (int)sizeof(cpx<T>) / 4;            // 32-bit words per element
+    static constexpr int R = TX * W >= 32 ? 1 : 32 / (TX * W);   // rows per bank period
+    __device__ __forceinline__ static int at(int p, int l) { return p * TX + (l ^ ((p / R) & (TX - 1))); }
 };
 
 // stage twiddles of a y/z column thread: a broadcast shared table, or registers
@@ -721,6 +748,90 @@ struct ZCol {
     }
 };
 
+// Spectral side of a z-forward item, on the column elements Y[m] (z position
+// t + TPL m, forward-transformed): the main symbol (the 1/N^3 folded in), the
+// optional added term, the reductions and the optional pruned-spectrum store.
+// Y is left holding the spectrum (zero outside the band).
+struct ZAcc {
+    double self = 0.0, w[3] = {0.0, 0.0, 0.0};
+};
+template <int N, int E, int TPL, typename C>
+__device__ __forceinline__ void zfwd_spectral(const ZFwdOp& op, const SymD<C>& dmain, const SymD<C>& dadd,
+                                              const C* kt, const ZCol<N, TPL>& idx, int fy, int kxc, double wgt,
+                                              cpx<C> (&Y)[E], ZAcc& acc) {
+    constexpr int CH = E < 8 ? E : 8;
+    const C ox = kt[N + kxc], oy = kt[N + fy];
+    const C kxy2 = kt[kxc] * kt[kxc] + kt[fy] * kt[fy];
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int fz = idx.t + TPL * m;
+        const C kz = kt[fz], oz = kt[N + fz];
+        const C ksq = kxy2 + kz * kz;
+        const C ri = dmain.inv ? rinv_of(ksq) : C(0);
+        Y[m] = idx.valid(m) ? sym_apply(dmain, ox, oy, oz, ksq, ri, Y[m]) : mk(C(0), C(0));
+    }
+    if (op.add) {
+#pragma unroll
+        for (int m0 = 0; m0 < E; m0 += CH) {
+            cpx<C> A[CH];
+            ld_chunk<CH>(op.add, op.add_f64, idx, m0, A);
+#pragma unroll
+            for (int j = 0; j < CH; ++j) {
+                const int fz = idx.t + TPL * (m0 + j);
+                const C kz = kt[fz], oz = kt[N + fz];
+                const C ksq = kxy2 + kz * kz;
+                const C ri = dadd.inv ? rinv_of(ksq) : C(0);
+                if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(dadd, ox, oy, oz, ksq, ri, A[j]);
+            }
+        }
+    }
+    if (op.red_self >= 0) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const double yx = (double)Y[m].x, yy = (double)Y[m].y;
+            acc.self += wgt * (yx * yx + yy * yy);  // zero outside the band
+        }
+    }
+#pragma unroll 1
+    for (int r = 0; r < 3; ++r) {
+        if (!op.red_with[r]) continue;
+        double s = 0.0;
+#pragma unroll
+        for (int m0 = 0; m0 < E; m0 += CH) {
+            cpx<double> W[CH];
+            ld_chunk<CH>(op.red_with[r], op.red_with_f64[r], idx, m0, W);
+#pragma unroll
+            for (int j = 0; j < CH; ++j) s += (double)Y[m0 + j].x * W[j].x + (double)Y[m0 + j].y * W[j].y;
+        }
+        acc.w[r] += wgt * s;
+    }
+    if (op.spec_out) {
+#pragma unroll
+        for (int m = 0; m < E; ++m)
+            if (idx.valid(m)) st_spec_c(op.spec_out, op.spec_f64, idx(m), Y[m]);
+    }
+}
+
+// one reduction record of MAX_RED partials per block from the accumulators
+__device__ __forceinline__ void zfwd_partials(const ZFwdOp& op, const ZAcc& acc, double* part) {
+    const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
+    if (any_red) {
+        double acc4[4] = {acc.self, acc.w[0], acc.w[1], acc.w[2]};
+        __shared__ double part4[4];
+        block_reduce_to<4>(acc4, part4);
+        __syncthreads();
+        if (threadIdx.x < MAX_RED) {
+            double s = 0.0;
+            if ((int)threadIdx.x == op.red_self) s += part4[0];
+            for (int r = 0; r < 3; ++r)
+                if (op.red_with[r] && (int)threadIdx.x == op.red_with_slot[r]) s += part4[1 + r];
+            part[threadIdx.x] = s;
+        }
+    } else if (threadIdx.x < MAX_RED) {
+        part[threadIdx.x] = 0.0;
+    }
+}
+
 // ----------------------------------------------------------------------------
 // z stage, forward (+ optional round trip).  grid = (G, narr); items (cy, tile).
 // One reduction record of MAX_RED partials per block.
@@ -730,7 +841,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     zfwd_c_kernel(ZFwdArgs<T> a, const cpx<T>* __restrict__ twN) {
     using S = YShape<N, T, V>;
     using C = T;
-    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     cpx<T>* buf0 = reinterpret_cast<cpx<T>*>(smem_raw);
     cpx<T>* buf1 = buf0 + N * TX;
@@ -751,8 +862,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
     const SymD<C> dmain = make_symd<C>(op.sym, op.sym_ab, a.norm);  // the 1/N^3 folded in
     const SymD<C> dadd = make_symd<C>(op.add_sym, op.add_ab, op.add_coef);
-    const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
-    double acc_self = 0.0, acc_w0 = 0.0, acc_w1 = 0.0, acc_w2 = 0.0;
+    ZAcc acc;
     // stage the ys column tile of item `it` into buffer b, asynchronously
     auto stage = [&](long it, cpx<T>* b) {
         const int cy = (int)(it / ntile);
@@ -782,64 +892,11 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         cfft<N, E, -1, SyncBlock>(v, t, sm, map, tw);
         const int fy = band_fft_index(a.band, cy);
         const int kxc = col - cy * nx;
-        const C kxv = kt[kxc], ox = kt[N + kxc], kyv = kt[fy], oy = kt[N + fy];
-        const C kxy2 = kxv * kxv + kyv * kyv;
-        const double wgt = kx_weight(N, kx);
         const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
         cpx<C> Y[E];
 #pragma unroll
-        for (int m = 0; m < E; ++m) {
-            const int fz = t + TPL * m;
-            const C kz = kt[fz], oz = kt[N + fz];
-            const C ksq = kxy2 + kz * kz;
-            const C ri = dmain.inv ? rinv_of(ksq) : C(0);
-            Y[m] = idx.valid(m) ? sym_apply(dmain, ox, oy, oz, ksq, ri, mk((C)v[m].x, (C)v[m].y)) : mk(C(0), C(0));
-        }
-        if (op.add) {
-#pragma unroll
-            for (int m0 = 0; m0 < E; m0 += CH) {
-                cpx<C> A[CH];
-                ld_chunk<CH>(op.add, op.add_f64, idx, m0, A);
-#pragma unroll
-                for (int j = 0; j < CH; ++j) {
-                    const int fz = t + TPL * (m0 + j);
-                    const C kz = kt[fz], oz = kt[N + fz];
-                    const C ksq = kxy2 + kz * kz;
-                    const C ri = dadd.inv ? rinv_of(ksq) : C(0);
-                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(dadd, ox, oy, oz, ksq, ri, A[j]);
-                }
-            }
-        }
-        if (op.red_self >= 0) {
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const double yx = (double)Y[m].x, yy = (double)Y[m].y;
-                acc_self += wgt * (yx * yx + yy * yy);  // zero outside the band
-            }
-        }
-#pragma unroll 1
-        for (int r = 0; r < 3; ++r) {
-            if (!op.red_with[r]) continue;
-            double s = 0.0;
-#pragma unroll
-            for (int m0 = 0; m0 < E; m0 += CH) {
-                cpx<double> W[CH];
-                ld_chunk<CH>(op.red_with[r], op.red_with_f64[r], idx, m0, W);
-#pragma unroll
-                for (int j = 0; j < CH; ++j) s += (double)Y[m0 + j].x * W[j].x + (double)Y[m0 + j].y * W[j].y;
-            }
-            if (r == 0)
-                acc_w0 += wgt * s;
-            else if (r == 1)
-                acc_w1 += wgt * s;
-            else
-                acc_w2 += wgt * s;
-        }
-        if (op.spec_out) {
-#pragma unroll
-            for (int m = 0; m < E; ++m)
-                if (idx.valid(m)) st_spec_c(op.spec_out, op.spec_f64, idx(m), Y[m]);
-        }
+        for (int m = 0; m < E; ++m) Y[m] = mk((C)v[m].x, (C)v[m].y);
+        zfwd_spectral<N, E, TPL>(op, dmain, dadd, kt, idx, fy, kxc, kx_weight(N, kx), Y, acc);
         if (yout) {
 #pragma unroll
             for (int m = 0; m < E; ++m) v[m] = mk((T)Y[m].x, (T)Y[m].y);
@@ -850,23 +907,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
             }
         }
     }
-    const int block_lin = blockIdx.y * gridDim.x + blockIdx.x;
-    double* part = a.partials + (long)block_lin * MAX_RED;
-    if (any_red) {
-        double acc4[4] = {acc_self, acc_w0, acc_w1, acc_w2};
-        __shared__ double part4[4];
-        block_reduce_to<4>(acc4, part4);
-        __syncthreads();
-        if (threadIdx.x < MAX_RED) {
-            double s = 0.0;
-            if ((int)threadIdx.x == op.red_self) s += part4[0];
-            for (int r = 0; r < 3; ++r)
-                if (op.red_with[r] && (int)threadIdx.x == op.red_with_slot[r]) s += part4[1 + r];
-            part[threadIdx.x] = s;
-        }
-    } else if (threadIdx.x < MAX_RED) {
-        part[threadIdx.x] = 0.0;
-    }
+    zfwd_partials(op, acc, a.partials + (long)(blockIdx.y * gridDim.x + blockIdx.x) * MAX_RED);
 }
 
 // ----------------------------------------------------------------------------
@@ -934,6 +975,267 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         if (ok) {
 #pragma unroll
             for (int m = 0; m < E; ++m) dst[(t + TPL * m) * plane + col] = v[m];
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Column-per-warp (CW) y/z passes, variants V = 5, 6 of YShape.  A block holds
+// a tile of TX columns x N rows in shared memory (TileMap).  Global memory is
+// read and written in the staging mapping (thread = column ls of row
+// ts + 32 m, so a warp covers whole 64-128-byte rows); each warp then
+// transforms one column held as 32 threads x N/32 elements, exchanging
+// through its own padded row with __syncwarp only.  Two block barriers per
+// item (four for a z round trip) instead of two per FFT stage.
+// ----------------------------------------------------------------------------
+template <int N, int V, typename T>
+struct CWGeom {
+    using S = YShape<N, T, V>;
+    static_assert(S::CW && S::TPLY == 32 && S::YTHREADS / S::TX == 32, "CW shape: one warp per column");
+    static constexpr int E = S::EY, TX = S::TX, SR = 32;
+    using TM = TileMap<TX, T>;
+    int lane, w, ls, ts;
+    __device__ __forceinline__ CWGeom()
+        : lane(threadIdx.x & 31), w(threadIdx.x >> 5), ls(threadIdx.x % TX), ts(threadIdx.x / TX) {}
+    // the warp's column of a tile into / out of registers (position lane + 32 m)
+    __device__ __forceinline__ void col_load(const cpx<T>* tile, cpx<T> (&v)[E]) const {
+#pragma unroll
+        for (int m = 0; m < E; ++m) v[m] = tile[TM::at(lane + 32 * m, w)];
+    }
+    __device__ __forceinline__ void col_store(cpx<T>* tile, const cpx<T> (&v)[E]) const {
+#pragma unroll
+        for (int m = 0; m < E; ++m) tile[TM::at(lane + 32 * m, w)] = v[m];
+    }
+    // slot of staging element m (row ts + 32 m, column ls)
+    __device__ __forceinline__ int slot(int m) const { return TM::at(ts + SR * m, ls); }
+};
+
+template <int N, int V, int SIGN, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
+    ypass_cw_kernel(YArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = YShape<N, T, V>;
+    using G = CWGeom<N, V, T>;
+    constexpr int E = G::E, TX = G::TX, SR = G::SR;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* tile0 = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* tile1 = tile0 + N * TX;
+    cpx<T>* xch = tile1 + N * TX;
+    cpx<T>* stw = xch + TX * S::WPITCH;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    __syncthreads();
+    const G g;
+    const TwTab<N, E, T> tw{stw};
+    const RowMap<E> xmap{g.w * S::WPITCH};
+    const int nx = a.nx, nb = a.band.nb;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)a.nz * ntile;
+    const cpx<T>* __restrict__ src = a.in[blockIdx.y];
+    cpx<T>* __restrict__ dst = a.out[blockIdx.y];
+    auto stage = [&](long it, cpx<T>* b) {
+        const int z = (int)(it / ntile);
+        const int kx = (int)(it - (long)z * ntile) * TX + g.ls;
+        const bool ok = kx < nx;
+        const int kxc = ok ? kx : nx - 1;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int p = g.ts + SR * m;
+            if constexpr (SIGN < 0) {
+                cp_async_elem(b + g.slot(m), src + ((long)z * N + p) * nx + kxc, ok);
+            } else {
+                const int ci = band_compact_index(a.band, p);
+                cp_async_elem(b + g.slot(m), src + ((long)z * nb + (ci >= 0 ? ci : 0)) * nx + kxc, ok && ci >= 0);
+            }
+        }
+        cp_async_commit();
+    };
+    long it = blockIdx.x;
+    if (it < items) stage(it, tile0);
+    for (int k = 0; it < items; it += gridDim.x, k ^= 1) {
+        cpx<T>* cur = k ? tile1 : tile0;
+        cpx<T>* nxt = k ? tile0 : tile1;
+        cp_async_wait_all();
+        // the tile is complete, and every thread is done storing the item
+        // that last used nxt
+        __syncthreads();
+        if (it + gridDim.x < items) stage(it + gridDim.x, nxt);
+        cpx<T> v[E];
+        g.col_load(cur, v);
+        cfft<N, E, SIGN, SyncWarp>(v, g.lane, xch, xmap, tw);
+        g.col_store(cur, v);
+        __syncthreads();
+        const int z = (int)(it / ntile);
+        const int kx = (int)(it - (long)z * ntile) * TX + g.ls;
+        if (kx < nx) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int p = g.ts + SR * m;
+                if constexpr (SIGN < 0) {
+                    const int ci = band_compact_index(a.band, p);
+                    if (ci >= 0) dst[((long)z * nb + ci) * nx + kx] = cur[g.slot(m)];
+                } else {
+                    dst[((long)z * N + p) * nx + kx] = cur[g.slot(m)];
+                }
+            }
+        }
+    }
+}
+
+template <int N, int V, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
+    zfwd_cw_kernel(ZFwdArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = YShape<N, T, V>;
+    using G = CWGeom<N, V, T>;
+    using C = T;
+    constexpr int E = G::E, TX = G::TX, SR = G::SR;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* tile0 = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* tile1 = tile0 + N * TX;
+    cpx<T>* xch = tile1 + N * TX;
+    cpx<T>* stw = xch + TX * S::WPITCH;
+    C* kt = reinterpret_cast<C*>(stw + N);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    fill_k_table<N>(kt);
+    __syncthreads();
+    const G g;
+    const TwTab<N, E, T> tw{stw};
+    const RowMap<E> xmap{g.w * S::WPITCH};
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)nb * ntile;
+    const ZFwdOp& op = a.op[blockIdx.y];
+    const int plane = nb * nx;
+    const cpx<T>* __restrict__ src = reinterpret_cast<const cpx<T>*>(op.in);
+    cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
+    const SymD<C> dmain = make_symd<C>(op.sym, op.sym_ab, a.norm);  // the 1/N^3 folded in
+    const SymD<C> dadd = make_symd<C>(op.add_sym, op.add_ab, op.add_coef);
+    ZAcc acc;
+    auto stage = [&](long it, cpx<T>* b) {
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + g.ls;
+        const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);
+#pragma unroll
+        for (int m = 0; m < E; ++m) cp_async_elem(b + g.slot(m), src + (g.ts + SR * m) * plane + col, ok);
+        cp_async_commit();
+    };
+    long it0 = blockIdx.x;
+    if (it0 < items) stage(it0, tile0);
+    int kbuf = 0;
+    for (long it = it0; it < items; it += gridDim.x, kbuf ^= 1) {
+        cpx<T>* cur = kbuf ? tile1 : tile0;
+        cpx<T>* nxt = kbuf ? tile0 : tile1;
+        cp_async_wait_all();
+        __syncthreads();
+        if (it + gridDim.x < items) stage(it + gridDim.x, nxt);
+        cpx<T> v[E];
+        g.col_load(cur, v);
+        cfft<N, E, -1, SyncWarp>(v, g.lane, xch, xmap, tw);
+        g.col_store(cur, v);
+        __syncthreads();
+        // spectral side in the staging mapping (coalesced spectrum accesses)
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + g.ls;
+        const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
+        const ZCol<N, SR> idx{g.ts, cut, nb, plane, col, ok};
+        cpx<C> Y[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const cpx<T> y = cur[g.slot(m)];
+            Y[m] = mk((C)y.x, (C)y.y);
+        }
+        zfwd_spectral<N, E, SR>(op, dmain, dadd, kt, idx, band_fft_index(a.band, cy), col - cy * nx,
+                                kx_weight(N, kx), Y, acc);
+        if (yout) {  // uniform over the block
+#pragma unroll
+            for (int m = 0; m < E; ++m) cur[g.slot(m)] = mk((T)Y[m].x, (T)Y[m].y);
+            __syncthreads();
+            g.col_load(cur, v);
+            cfft<N, E, +1, SyncWarp>(v, g.lane, xch, xmap, tw);
+            g.col_store(cur, v);
+            __syncthreads();
+            if (ok) {
+#pragma unroll
+                for (int m = 0; m < E; ++m) yout[(g.ts + SR * m) * plane + col] = cur[g.slot(m)];
+            }
+        }
+    }
+    zfwd_partials(op, acc, a.partials + (long)(blockIdx.y * gridDim.x + blockIdx.x) * MAX_RED);
+}
+
+template <int N, int V, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
+    zinv_cw_kernel(ZInvArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = YShape<N, T, V>;
+    using G = CWGeom<N, V, T>;
+    using C = T;
+    constexpr int E = G::E, TX = G::TX, SR = G::SR, CH = E < 8 ? E : 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* tile0 = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* tile1 = tile0 + N * TX;
+    cpx<T>* xch = tile1 + N * TX;
+    cpx<T>* stw = xch + TX * S::WPITCH;
+    C* kt = reinterpret_cast<C*>(stw + N);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    fill_k_table<N>(kt);
+    __syncthreads();
+    const G g;
+    const TwTab<N, E, T> tw{stw};
+    const RowMap<E> xmap{g.w * S::WPITCH};
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)nb * ntile;
+    const ZInvOp& op = a.op[blockIdx.y];
+    const int plane = nb * nx;
+    const int nsrc = op.nsrc;
+    cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out);
+    int kbuf = 0;
+    for (long it = blockIdx.x; it < items; it += gridDim.x, kbuf ^= 1) {
+        // two tiles alternate, so this item's staging writes never meet the
+        // previous item's stores (the barrier after them orders the one before)
+        cpx<T>* cur = kbuf ? tile1 : tile0;
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + g.ls;
+        const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
+        const int fy = band_fft_index(a.band, cy);
+        const int kxc = col - cy * nx;
+        const C ox = kt[N + kxc], oy = kt[N + fy];
+        const C kxy2 = kt[kxc] * kt[kxc] + kt[fy] * kt[fy];
+        const ZCol<N, SR> idx{g.ts, cut, nb, plane, col, ok};
+        cpx<C> Y[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) Y[m] = mk(C(0), C(0));
+#pragma unroll 1
+        for (int s = 0; s < nsrc; ++s) {
+            const void* spec = op.src[s].spec;
+            const int f64 = op.src[s].f64;
+            const SymD<C> d = make_symd<C>(op.src[s].sym, op.src[s].ab, op.src[s].coef);
+#pragma unroll
+            for (int m0 = 0; m0 < E; m0 += CH) {
+                cpx<C> Vv[CH];
+                ld_chunk<CH>(spec, f64, idx, m0, Vv);
+#pragma unroll
+                for (int j = 0; j < CH; ++j) {
+                    const int fz = g.ts + SR * (m0 + j);
+                    const C kz = kt[fz], oz = kt[N + fz];
+                    const C ksq = kxy2 + kz * kz;
+                    const C ri = d.inv ? rinv_of(ksq) : C(0);
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(d, ox, oy, oz, ksq, ri, Vv[j]);
+                }
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < E; ++m) cur[g.slot(m)] = mk((T)Y[m].x, (T)Y[m].y);
+        __syncthreads();
+        cpx<T> v[E];
+        g.col_load(cur, v);
+        cfft<N, E, +1, SyncWarp>(v, g.lane, xch, xmap, tw);
+        g.col_store(cur, v);
+        __syncthreads();
+        if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) dst[(g.ts + SR * m) * plane + col] = cur[g.slot(m)];
         }
     }
 }

@@ -45,7 +45,15 @@ static void allow_smem(K kernel) {
     const void* key = reinterpret_cast<const void*>(kernel);
     std::lock_guard<std::mutex> lock(smem_attr_mutex());
     if (done.insert(key).second) {
-        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        // the opt-in per-block limit less the kernel's static shared memory
+        int dev = 0, optin = 0;
+        cudaFuncAttributes fa{};
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, kernel);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     optin - (int)fa.sharedSizeBytes);
         if (e != cudaSuccess) throw CudaError(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e), MLQ_ERR_CUDA);
     }
 }

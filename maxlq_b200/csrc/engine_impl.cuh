@@ -152,10 +152,17 @@ void Engine<T>::y_cv(YArgs<T>& ya, int sign, int narr) {
         dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
         kern<<<grid, S::YTHREADS, smem, stream>>>(ya, d_twT_ + tw_off.at(NN));
     };
-    if (sign < 0)
-        run(ypass_c_kernel<NN, V, -1, T>);
-    else
-        run(ypass_c_kernel<NN, V, +1, T>);
+    if constexpr (S::CW) {
+        if (sign < 0)
+            run(ypass_cw_kernel<NN, V, -1, T>);
+        else
+            run(ypass_cw_kernel<NN, V, +1, T>);
+    } else {
+        if (sign < 0)
+            run(ypass_c_kernel<NN, V, -1, T>);
+        else
+            run(ypass_c_kernel<NN, V, +1, T>);
+    }
 }
 
 template <typename T>
@@ -164,14 +171,19 @@ void Engine<T>::zfwd_cv(ZFwdArgs<T>& za, int narr) {
     using S = YShape<NN, T, V>;
     const size_t smem = S::ZSMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
-    auto kern = zfwd_c_kernel<NN, V, T>;
-    allow_smem(kern);
-    const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
-    dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
-    last_zblocks_ = (long)grid.x * narr;
-    ensure_partials(last_zblocks_ * MAX_RED);
-    za.partials = d_partials;
-    kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+    auto run = [&](auto kern) {
+        allow_smem(kern);
+        const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
+        dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
+        last_zblocks_ = (long)grid.x * narr;
+        ensure_partials(last_zblocks_ * MAX_RED);
+        za.partials = d_partials;
+        kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+    };
+    if constexpr (S::CW)
+        run(zfwd_cw_kernel<NN, V, T>);
+    else
+        run(zfwd_c_kernel<NN, V, T>);
 }
 
 template <typename T>
@@ -180,11 +192,16 @@ void Engine<T>::zinv_cv(ZInvArgs<T>& za, int narr) {
     using S = YShape<NN, T, V>;
     const size_t smem = S::ZISMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
-    auto kern = zinv_c_kernel<NN, V, T>;
-    allow_smem(kern);
-    const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
-    dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
-    kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+    auto run = [&](auto kern) {
+        allow_smem(kern);
+        const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
+        dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
+        kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+    };
+    if constexpr (S::CW)
+        run(zinv_cw_kernel<NN, V, T>);
+    else
+        run(zinv_c_kernel<NN, V, T>);
 }
 
 // f(std::integral_constant<int, V>) for the variant chosen for pass `kind`
@@ -203,6 +220,12 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
     }
     if constexpr (YShape<NN, T, 4>::valid) {
         if (v == 4) return f(std::integral_constant<int, 4>{});
+    }
+    if constexpr (YShape<NN, T, 5>::valid) {
+        if (v == 5) return f(std::integral_constant<int, 5>{});
+    }
+    if constexpr (YShape<NN, T, 6>::valid) {
+        if (v == 6) return f(std::integral_constant<int, 6>{});
     }
     f(std::integral_constant<int, 0>{});
 }
@@ -251,7 +274,8 @@ void Engine<T>::tune_yz() {
     bool any = false;
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
-        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid || YShape<NN, T, 3>::valid;
+        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid || YShape<NN, T, 3>::valid ||
+              YShape<NN, T, 5>::valid || YShape<NN, T, 6>::valid;
     });
     if (!any) return;
     if (const char* e = std::getenv("MLQ_YZ_VARIANT")) {  // fixed variant (measurement runs)
@@ -260,7 +284,8 @@ void Engine<T>::tune_yz() {
         dispatch_n(n, [&](auto nc) {
             constexpr int NN = decltype(nc)::value;
             ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid) ||
-                 (v == 3 && YShape<NN, T, 3>::valid) || (v == 4 && YShape<NN, T, 4>::valid);
+                 (v == 3 && YShape<NN, T, 3>::valid) || (v == 4 && YShape<NN, T, 4>::valid) ||
+                 (v == 5 && YShape<NN, T, 5>::valid) || (v == 6 && YShape<NN, T, 6>::valid);
         });
         if (ok)
             for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
@@ -323,14 +348,16 @@ void Engine<T>::tune_yz() {
         });
         MLQ_CUDA(cudaGetLastError());
     };
-    constexpr int NV = 5;
-    bool valid[NV] = {true, false, false, false, false};
+    constexpr int NV = 7;
+    bool valid[NV] = {true, false, false, false, false, false, false};
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         valid[1] = YShape<NN, T, 1>::valid;
         valid[2] = YShape<NN, T, 2>::valid;
         valid[3] = YShape<NN, T, 3>::valid;
         valid[4] = YShape<NN, T, 4>::valid;
+        valid[5] = YShape<NN, T, 5>::valid;
+        valid[6] = YShape<NN, T, 6>::valid;
     });
     // every variant of every kind once first (clocks, attributes, page-in)
     for (int kind = 0; kind < YV_KINDS; ++kind)
@@ -343,7 +370,8 @@ void Engine<T>::tune_yz() {
     // replaces variant 0 only when it is at least 3 % faster
     std::string rep;
     for (int kind = 0; kind < YV_KINDS; ++kind) {
-        float best_ms[NV] = {1e30f, 1e30f, 1e30f, 1e30f, 1e30f};
+        float best_ms[NV];
+        std::fill(best_ms, best_ms + NV, 1e30f);
         for (int r = 0; r < 5; ++r)
             for (int v = 0; v < NV; ++v) {
                 if (!valid[v]) continue;

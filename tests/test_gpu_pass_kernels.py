@@ -92,3 +92,51 @@ def test_gradient_graph_replay_matches_direct_launches(prec, monkeypatch):
             runs[graphs] = ([r["J1"] for r in rec], [r["tau"] for r in rec], c.kernel_config()["graph_replays"])
     assert runs["0"][0] == runs["1"][0] and runs["0"][1] == runs["1"][1]
     assert runs["0"][2] == 0 and runs["1"][2] >= 3
+
+
+def _variant_run(n, precision, variant, monkeypatch):
+    monkeypatch.setenv("MLQ_YZ_VARIANT", str(variant))
+    with mlq.MaxLq(n, 4.0, 1.0, precision=precision, optim_tol=1e-14) as c:
+        assert c.kernel_config()["yz_variants"] == f"fixed by MLQ_YZ_VARIANT={variant}"
+        u = c.seed_field(1, 2.0, n / 16)
+        g = c.GradL2ForLq(u)
+        out = {"g": g, "uk": c.calc_uk(u, 2.0), "vt": c.vectorTransport(u, 4.0, 1.0, 0.01 * g, g)}
+        f = np.random.default_rng(3).standard_normal((n, n, n))
+        out["dealias"] = c.dealias_scalar(f, 2.0)
+        c.state_load(u)
+        out["R"] = c.state_R()[0]
+        _, _, rec = c.state_iterate(2)
+        out["J1"] = [r["J1"] for r in rec]
+    return out
+
+
+_VARIANT0 = {}
+
+
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("n,precision,tol", [(256, "fp64", 1e-12), (256, "mixed", 2e-6)])
+def test_yz_tile_variants_match_default(n, precision, tol, variant, monkeypatch):
+    """Every y/z tile-shape variant the autotuner may pick (including the
+    column-per-warp kernels, variants 5 and 6) computes what variant 0 does:
+    y and z passes both ways, z round trips, symbols and reductions."""
+    if (n, precision) not in _VARIANT0:
+        _VARIANT0[(n, precision)] = _variant_run(n, precision, 0, monkeypatch)
+    a = _VARIANT0[(n, precision)]
+    b = _variant_run(n, precision, variant, monkeypatch)
+    for k in ("uk", "dealias", "R"):
+        assert rel(b[k], a[k]) < tol, k
+    # the gradient and the transported vector end in cancelling differences:
+    # a different radix order moves them by more than the fields' roundoff
+    for k in ("g", "vt"):
+        assert rel(b[k], a[k]) < (1e-10 if precision == "fp64" else 1e-4), k
+    assert b["J1"] == pytest.approx(a["J1"], rel=1e-10 if precision == "fp64" else 1e-5)
+
+
+@pytest.mark.parametrize("variant", [5, 6])
+def test_column_per_warp_variants_512_mixed(variant, monkeypatch):
+    a = _state_run(512, "mixed", "compile-time", monkeypatch)
+    monkeypatch.setenv("MLQ_YZ_VARIANT", str(variant))
+    b = _state_run(512, "mixed", "compile-time", monkeypatch)
+    assert rel(b[0], a[0]) < 2e-6
+    assert b[1] == pytest.approx(a[1], rel=2e-6)
+    assert b[3]["J1"] == pytest.approx(a[3]["J1"], rel=2e-6)
