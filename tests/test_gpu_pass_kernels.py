@@ -128,7 +128,7 @@ def test_yz_tile_variants_match_default(n, precision, tol, variant, monkeypatch)
     # the gradient and the transported vector end in cancelling differences:
     # a different radix order moves them by more than the fields' roundoff
     for k in ("g", "vt"):
-        assert rel(b[k], a[k]) < (1e-10 if precision == "fp64" else 1e-4), k
+        assert rel(b[k], a[k]) < (1e-10 if precision == "fp64" else 1e-3), k
     assert b["J1"] == pytest.approx(a["J1"], rel=1e-10 if precision == "fp64" else 1e-5)
 
 
