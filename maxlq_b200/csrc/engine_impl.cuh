@@ -1909,15 +1909,33 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
         }
         fwd(b2, FLSS{}, ud, {o[0], o[1], o[2]});
     }
-    // P2 of the coefficients of W_j (calc_vgraduvgradu / calc_vvgradu, v = phi)
-    {
+    // P2 of the coefficients of W_j = sum_i phi_i d_j phi_i (calc_vgraduvgradu /
+    // calc_vvgradu, v = phi).  W_j = (1/2) d_j |phi|^2, and when the cut c
+    // satisfies 3c < N the dealiased grid product of two band-limited fields
+    // is the band truncation of their exact product (its aliases land beyond
+    // the cut), so P2(W_j) = (1/2) d_j P2(|phi|^2): the derivatives of the
+    // S_a spectra just formed.  For 3c >= N (N divisible by 3) the products
+    // are formed and dealiased as the reference does.
+    if (3 * b2.cut < n) {
+        std::vector<InvOut> g;
+        for (int a = 0; a < 3; ++a)
+            for (int j = 0; j < 3; ++j) {
+                InvOut o;
+                o.nsrc = 1;
+                o.src[0] = ZSrc{wspec(WLS + a), wf64<T>(), SYM_IKX + j, 0, 0.5};
+                o.phys_out = LV + 3 * a + j;
+                g.push_back(o);
+            }
+        inv(b2, g);
+    } else {
+        std::vector<int> uself(all.begin(), all.begin() + 12), dself(all.begin() + 12, all.end());
         FwdOut o[3];
         for (int j = 0; j < 3; ++j) o[j].phys_out = LV + j;
-        fwd(b2, FLSW<0>{}, all, {o[0], o[1], o[2]});
+        fwd(b2, FLSW<0>{}, uself, {o[0], o[1], o[2]});
         for (int j = 0; j < 3; ++j) o[j].phys_out = LV + 3 + j;
         fwd(b2, FLSW<1>{}, all, {o[0], o[1], o[2]});
         for (int j = 0; j < 3; ++j) o[j].phys_out = LV + 6 + j;
-        fwd(b2, FLSW<2>{}, all, {o[0], o[1], o[2]});
+        fwd(b2, FLSW<0>{}, dself, {o[0], o[1], o[2]});
     }
     // p_a = -Lap^-1 P2(Q_a) and the spectra of P2(|grad phi|^2)_a
     {

@@ -303,24 +303,25 @@ struct FLSS {
     }
 };
 
-// tau^A coefficient of W_j = sum_i phi_i d_j phi_i.  inputs u(3), Du(9), d(3), Dd(9)
+// Coefficients of W_j = sum_i phi_i d_j phi_i in tau.  A = 0: v_i d_j v_i,
+// inputs v(3), Dv(9) (the tau^0 term with v = u, the tau^2 term with v = d);
+// A = 1: the tau^1 term u_i d_j d_i + d_i d_j u_i, inputs u(3), Du(9), d(3), Dd(9).
 template <int A>
 struct FLSW {
-    static constexpr int NIN = 24, NOUT = 3, NRED = 0;
+    static constexpr int NIN = A == 1 ? 24 : 12, NOUT = 3, NRED = 0;
     template <typename T>
     __device__ void operator()(const T* in, T* out, double*) const {
         const T* u = in;
         const T* du = in + 3;
-        const T* d = in + 12;
-        const T* dd = in + 15;
 #pragma unroll
         for (int j = 0; j < 3; ++j) {
             T w = 0;
 #pragma unroll
             for (int i = 0; i < 3; ++i) {
-                if (A == 0) w += u[i] * du[3 * i + j];
-                if (A == 1) w += u[i] * dd[3 * i + j] + d[i] * du[3 * i + j];
-                if (A == 2) w += d[i] * dd[3 * i + j];
+                if constexpr (A == 1)
+                    w += u[i] * in[15 + 3 * i + j] + in[12 + i] * du[3 * i + j];
+                else
+                    w += u[i] * du[3 * i + j];
             }
             out[j] = w;
         }
