@@ -244,6 +244,18 @@ const double* EngineBase::hweight_table(double order) {
 
 static int spec_rows_grid(const SpecGeom& g) { return std::max(1, std::min(g.nb * g.nb, 148 * 16)); }
 
+void EngineBase::retract(double2* u, double cs, double tau, const double2* d) {
+    const PhysMemo keep = pm_;
+    lincomb(u, cs, u, cs * tau, d);
+    if (keep.tr && keep.u == (const void*)u && keep.d == (const void*)d && keep.tau == tau) {
+        pm_ = keep;
+        pm_.u = nullptr;  // the fields describe the old u, no longer stored
+        pm_.ls = false;
+        pm_.next = u;
+        pm_.cs = cs;
+    }
+}
+
 void EngineBase::hilbert(double2* f, double order) {
     state_written(f);
     SpecGeom g = geom(b2);

@@ -91,9 +91,31 @@ class EngineBase {
     // to those fields), so the line-search setup of the same iteration can
     // reuse them instead of transforming again.
     const void* pu_of_ = nullptr;
+    // Physical fields the line search leaves for the transport and the next
+    // gradient program (resident mode).  ls: after the line-search setup,
+    // phys(iu..iu+2) = u, phys(idu..idu+8) = grad u, and the fields 63..65,
+    // 75..83 hold d and grad d, for the spectra u, d.  tr: after a transport
+    // (or Lq norm) at w = u + tau d formed from them, phys 0..2 = w while
+    // idu and 75..83 still hold grad u and grad d.  retract() then records
+    // that the state spectrum `next` holds cs * w, and the next gradient
+    // program forms u and grad u pointwise instead of transforming them.
+    // Cleared by a write to physical fields 0..11 or 60..83 and by a write
+    // to any of the spectra.
+    struct PhysMemo {
+        const void* u = nullptr;
+        const void* d = nullptr;
+        const void* next = nullptr;
+        int iu = -1, idu = -1;
+        bool ls = false, tr = false;
+        double tau = 0.0, cs = 0.0;
+    } pm_;
     void state_written(const void* p) {
         if (p == pu_of_) pu_of_ = nullptr;
+        if (p && (p == pm_.u || p == pm_.d || p == pm_.next)) pm_ = PhysMemo{};
     }
+    // u <- cs (u + tau d), keeping the transport's physical fields of
+    // u + tau d for the next gradient program
+    void retract(double2* u, double cs, double tau, const double2* d);
     void ensure_partials(long n);
     // Count a launch and surface launch-configuration errors immediately.
     // With profiling on, `a` is the event recorded before the launch; the
@@ -314,7 +336,7 @@ class Engine : public EngineBase {
     // dealiased |u|^{q-2} u spectra (for calcConstraintDerivativeL2) into
     // c (FP64, may be null) and ||u||_q^q.
     void grad_l2(const double2* u, double2* v, double2* c, double* lqq);
-    void grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq);
+    void grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq, bool from_retraction);
     int grad_lq_slot_ = 0;
     // vectorTransport pieces at w = u + tau*d: ir[i] = <P2(|w|^{q-2} w), xi_i>,
     // returns ||w||_q^q.
@@ -362,6 +384,9 @@ class Engine : public EngineBase {
     void widen_to(const Band& b);
 
     double2* c_tmp_ = nullptr;  // FP64 spectra of P2(|w|^{q-2} w) for the transport
+    double* d_coef_ = nullptr;  // cs, tau of the retraction (read by a captured launch)
+    void phys_written(int idx);  // clears the physical-field memo when it covers idx
+    bool w_from_memo(const double2* u, const double2* d, double tau);
 
     // register-resident FFT kernels (power-of-two n >= 64); E elements per thread
     int ereg_ = 8;  // elements per thread: 8 up to n = 512, 16 above

@@ -829,6 +829,7 @@ void Engine<T>::yx_inverse(const Band& b, const std::vector<cpx<T>*>& ys, const 
     for (int i = 0; i < k; ++i) {
         xa.in[i] = xs[i];
         xa.out[i] = phys(phys_out[i]);
+        phys_written(phys_out[i]);
     }
     xa.plan_half = plan(n / 2);
     xa.tw = d_tw;
@@ -922,7 +923,10 @@ void Engine<T>::pointwise(const F& f, const std::vector<int>& in, const std::vec
     PArgs<T> a;
     a.npts = n3;
     for (int i = 0; i < F::NIN; ++i) a.in[i] = phys(in[i]);
-    for (int o = 0; o < F::NOUT; ++o) a.out[o] = phys(out[o]);
+    for (int o = 0; o < F::NOUT; ++o) {
+        a.out[o] = phys(out[o]);
+        phys_written(out[o]);
+    }
     const int grid = grid_for(n3, RED_THREADS, 148 * 8);
     ensure_partials((long)grid * std::max(F::NRED, 1));
     a.partials = d_partials;
@@ -1131,6 +1135,7 @@ void Engine<T>::fwd_slab(const Band& b, const F& f, const std::vector<int>& in, 
 template <typename T>
 void Engine<T>::release_io_buffers() {
     pu_of_ = nullptr;
+    pm_ = PhysMemo{};
     for (auto* v : {&phys_}) {
         for (auto*& p : *v) {
             if (p) free_dev(p);
@@ -1175,6 +1180,46 @@ enum : int {
 // work spectra (band b2)
 enum : int { WG2 = 0, WA = 1, WP = 2, WT = 3 /*3..5*/, WONE = 6, WCH = 7 /*7..*/ };
 }  // namespace
+// line search along phi = u + tau d (q = 4): physical fields and work spectra
+namespace {
+enum : int {
+    LU = 60,    // u (3)
+    LD = 63,    // d (3)
+    LDU = 66,   // d_j u_i at 66+3i+j
+    LDD = 75,   // d_j d_i at 75+3i+j
+    LS = 84,    // S_a = P2 coefficients of |phi|^2 (3)
+    LV = 87,    // V_aj = P2 coefficients of W_j at 87+3a+j
+    LP = 96,    // p_a (3)
+    WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
+    WLS = 43,   // work spectra: S_a (3)
+};
+}  // namespace
+
+// the physical-field memo covers u, grad u (0..11) and the line search's u, d
+// and their gradients (60..83)
+template <typename T>
+void Engine<T>::phys_written(int idx) {
+    if ((idx >= PU && idx < PL) || (idx >= LU && idx < LS)) pm_ = PhysMemo{};
+}
+
+// PU <- u + tau d from the line search's physical fields of u and d, when the
+// memo holds them; records the transport fields (tr) for the next gradient
+template <typename T>
+bool Engine<T>::w_from_memo(const double2* u, const double2* d, double tau) {
+    if (slab_ || !d || !pm_.ls || pm_.u != (const void*)u || pm_.d != (const void*)d) {
+        pm_ = PhysMemo{};
+        return false;
+    }
+    const PhysMemo m = pm_;
+    FAxpy3 f;
+    f.tau = tau;
+    pointwise(f, {m.iu, m.iu + 1, m.iu + 2, LD, LD + 1, LD + 2}, {PU, PU + 1, PU + 2});
+    pm_ = m;
+    pm_.ls = false;
+    pm_.tr = true;
+    pm_.tau = tau;
+    return true;
+}
 
 template <typename T>
 static constexpr int wf64() {
@@ -1487,8 +1532,19 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
 template <typename T>
 void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
     if (!c) throw CudaError("grad_l2 needs a spectrum buffer for |u|^{q-2}u", MLQ_ERR_BADARG);
+    // u = cs w from the last line search's transport: u and grad u pointwise
+    const bool rt = !slab_ && pm_.tr && pm_.next == (const void*)u;
+    if (rt) {
+        if (!d_coef_) d_coef_ = (double*)dev_alloc(2 * sizeof(double));
+        const double h[2] = {pm_.cs, pm_.tau};
+        MLQ_CUDA(cudaMemcpyAsync(d_coef_, h, sizeof(h), cudaMemcpyHostToDevice, stream));
+    }
     // the same launches every CG iteration: a CUDA graph after the first two
-    as_graph("grad_l2", {u, v, c, lqq ? (const void*)v : nullptr}, [&] { grad_l2_body(u, v, c, lqq != nullptr); });
+    // (one per path: the physical fields the retraction reads are in the key)
+    as_graph(rt ? "grad_l2_rt" : "grad_l2",
+             {u, v, c, lqq ? (const void*)v : nullptr, rt ? (const void*)phys(pm_.idu) : nullptr},
+             [&] { grad_l2_body(u, v, c, lqq != nullptr, rt); });
+    pm_ = PhysMemo{};        // a replayed graph runs no host code: clear here
     if (!slab_) pu_of_ = u;  // PU, PD hold u and grad u until the next program
     if (lqq) {
         fetch_results();
@@ -1497,7 +1553,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
 }
 
 template <typename T>
-void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq) {
+void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq, bool from_retraction) {
     pu_of_ = nullptr;
     const Band& b = b2;
     const long nc = spec_ncomp();
@@ -1505,8 +1561,23 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
     chain_reset();
     // 1. u, grad u, Lap u
     std::vector<InvOut> io;
+    if (from_retraction) {
+        // u = cs w and grad u = cs (grad u_prev + tau grad d) from the physical
+        // fields of the line search (linear in the spectra, so equal to the
+        // transforms up to rounding); only Lap u is transformed
+        const int idu = pm_.idu;
+        pm_ = PhysMemo{};
+        std::vector<int> in, out;
+        for (int i = 0; i < 3; ++i) in.push_back(PU + i);
+        for (int k = 0; k < 9; ++k) in.push_back(idu + k);
+        for (int k = 0; k < 9; ++k) in.push_back(LDD + k);
+        for (int i = 0; i < 12; ++i) out.push_back(PU + i);
+        FRetract f;
+        f.coef = d_coef_;
+        pointwise(f, in, out);
+    }
     for (int i = 0; i < 3; ++i) {
-        for (int j = -1; j < 3; ++j) {
+        for (int j = -1; j < 3 && !from_retraction; ++j) {
             InvOut o;
             o.nsrc = 1;
             o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
@@ -1650,16 +1721,18 @@ double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
     pu_of_ = nullptr;
     const long nc = spec_ncomp();
     chain_reset();
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i) {
-        InvOut o;
-        o.nsrc = d ? 2 : 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-        if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
-        o.phys_out = PU + i;
-        io.push_back(o);
+    if (!w_from_memo(u, d, tau)) {
+        std::vector<InvOut> io;
+        for (int i = 0; i < 3; ++i) {
+            InvOut o;
+            o.nsrc = d ? 2 : 1;
+            o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
+            if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
+            o.phys_out = PU + i;
+            io.push_back(o);
+        }
+        inv(b2, io);
     }
-    inv(b2, io);
     FwdOut oS;
     oS.phys_out = PS;
     fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
@@ -1684,16 +1757,18 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
     const long nc = spec_ncomp();
     const double q = P.q;
     chain_reset();
-    std::vector<InvOut> io;
-    for (int i = 0; i < 3; ++i) {
-        InvOut o;
-        o.nsrc = d ? 2 : 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-        if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
-        o.phys_out = PU + i;
-        io.push_back(o);
+    if (!w_from_memo(u, d, tau)) {
+        std::vector<InvOut> io;
+        for (int i = 0; i < 3; ++i) {
+            InvOut o;
+            o.nsrc = d ? 2 : 1;
+            o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
+            if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
+            o.phys_out = PU + i;
+            io.push_back(o);
+        }
+        inv(b2, io);
     }
-    inv(b2, io);
     FwdOut oS;
     oS.phys_out = PS;
     fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
@@ -1770,19 +1845,6 @@ void Engine<T>::calc_uk(const double2* u, double k, int dst) {
 // ----------------------------------------------------------------------------
 // line search along phi = u + tau d at q = 4
 // ----------------------------------------------------------------------------
-namespace {
-enum : int {
-    LU = 60,    // u (3)
-    LD = 63,    // d (3)
-    LDU = 66,   // d_j u_i at 66+3i+j
-    LDD = 75,   // d_j d_i at 75+3i+j
-    LS = 84,    // S_a = P2 coefficients of |phi|^2 (3)
-    LV = 87,    // V_aj = P2 coefficients of W_j at 87+3a+j
-    LP = 96,    // p_a (3)
-    WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
-    WLS = 43,   // work spectra: S_a (3)
-};
-}  // namespace
 
 // Per block: the largest lower end and the smallest upper end, over its
 // points, of the interval around tau = 0 on which s0 + tau s1 + tau^2 s2 >= 0
@@ -1890,6 +1952,14 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
                 io.push_back(o);
             }
     inv(b2, io);
+    if (!slab_) {
+        pm_ = PhysMemo{};
+        pm_.u = u;
+        pm_.d = d;
+        pm_.iu = iu;
+        pm_.idu = idu;
+        pm_.ls = true;
+    }
     std::vector<int> ud = {iu, iu + 1, iu + 2, LD, LD + 1, LD + 2};
     std::vector<int> all;
     for (int i = 0; i < 3; ++i) all.push_back(iu + i);

@@ -277,6 +277,35 @@ struct FC3 {
     }
 };
 
+// w = x + tau y for three components (a point of the line search from the
+// physical fields of u and d).  inputs x(3), y(3)
+struct FAxpy3 {
+    static constexpr int NIN = 6, NOUT = 3, NRED = 0;
+    double tau;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[i] = in[i] + (T)tau * in[3 + i];
+    }
+};
+
+// The retracted state u' = cs w, w = u + tau d, and its gradient
+// cs (grad u + tau grad d).  inputs w(3), Du(9), Dd(9); outputs u'(3), Du'(9).
+// cs and tau are read from device memory (coef[0], coef[1]), so a captured
+// launch stays valid from one iteration to the next.
+struct FRetract {
+    static constexpr int NIN = 21, NOUT = 12, NRED = 0;
+    const double* coef;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        const T cs = (T)coef[0], ctau = (T)(coef[0] * coef[1]);
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[i] = cs * in[i];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) out[3 + k] = cs * in[3 + k] + ctau * in[12 + k];
+    }
+};
+
 // sum (a-b)^2 and sum a^2: energy of a field outside its band projection
 struct FDiffSq {
     static constexpr int NIN = 2, NOUT = 0, NRED = 2;

@@ -402,7 +402,7 @@ class Solver : public SolverBase {
         const Trial tr = trial(u, d1, tau1);
         const double cs = Bc / std::pow(tr.lqq, 1.0 / qq);
         const double R12n = std::pow(cs, qq) * tr.R[1], R3n = std::pow(cs, qq + 1.0) * tr.R[2];
-        e.lincomb(u, Bc / ln, u, Bc / ln * tau1, d1);
+        e.retract(u, Bc / ln, tau1, d1);
         trials.clear();
         const double J1 = R12n + R3n;
         const double deltaJ = (J1 - J0) / std::fabs(J0);
