@@ -884,6 +884,9 @@ __global__ void fill_kernel(T* p, long cnt, T v) {
 template <typename T>
 template <class F>
 void Engine<T>::pointwise(const F& f, const std::vector<int>& in, const std::vector<int>& out, int fred_dst) {
+    static_assert(F::NIN <= PArgs<T>::MAX_IN && F::NOUT <= PArgs<T>::MAX_OUT, "pointwise arity");
+    if ((int)in.size() != F::NIN || (int)out.size() != F::NOUT)
+        throw CudaError("pointwise: argument count does not match the functor", MLQ_ERR_BADARG);
     if (slab_) {
         if constexpr (F::NOUT > 0) {
             // the only pointwise outputs are the |u|^k powers of the calc_uk

@@ -129,9 +129,10 @@ __global__ void __launch_bounds__(256) xfwd_kernel(XFwdArgs<T> a, F f) {
 // ----------------------------------------------------------------------------
 template <typename T>
 struct PArgs {
+    static constexpr int MAX_IN = 24, MAX_OUT = 12;
     long npts;
-    const T* in[24];
-    T* out[MAX_ARR];
+    const T* in[MAX_IN];
+    T* out[MAX_OUT];
     double* partials;
 };
 
