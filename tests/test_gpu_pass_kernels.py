@@ -88,7 +88,7 @@ def test_gradient_graph_replay_matches_direct_launches(prec, monkeypatch):
         monkeypatch.setenv("MLQ_GRAPHS", graphs)
         with mlq.MaxLq(64, 4.0, 1.0, precision=prec, optim_tol=1e-14) as c:
             c.state_load(c.seed_field(2, 2.0, 4.0))
-            _, st, rec = c.state_iterate(5)
+            _, st, rec = c.state_iterate(8)
             runs[graphs] = ([r["J1"] for r in rec], [r["tau"] for r in rec], c.kernel_config()["graph_replays"])
     assert runs["0"][0] == runs["1"][0] and runs["0"][1] == runs["1"][1]
     assert runs["0"][2] == 0 and runs["1"][2] >= 3
