@@ -139,10 +139,30 @@ struct PArgs {
 template <typename T, class F>
 __global__ void __launch_bounds__(RED_THREADS) pointwise_kernel(PArgs<T> a, F f) {
     constexpr int NIN = F::NIN, NOUT = F::NOUT, NR = F::NRED;
+    using T2 = cpx<T>;  // two consecutive points per load and store
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
     for (int r = 0; r < (NR > 0 ? NR : 1); ++r) acc[r] = 0.0;
-    for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < a.npts; g += (long)gridDim.x * blockDim.x) {
+    const long npairs = a.npts / 2;
+    for (long g = (long)blockIdx.x * blockDim.x + threadIdx.x; g < npairs; g += (long)gridDim.x * blockDim.x) {
+        T2 vin[NIN > 0 ? NIN : 1];
+#pragma unroll
+        for (int i = 0; i < NIN; ++i) vin[i] = reinterpret_cast<const T2*>(a.in[i])[g];
+        T in0[NIN > 0 ? NIN : 1], in1[NIN > 0 ? NIN : 1];
+#pragma unroll
+        for (int i = 0; i < NIN; ++i) {
+            in0[i] = vin[i].x;
+            in1[i] = vin[i].y;
+        }
+        T o0[NOUT > 0 ? NOUT : 1], o1[NOUT > 0 ? NOUT : 1];
+        f(in0, o0, acc);
+        f(in1, o1, acc);
+#pragma unroll
+        for (int o = 0; o < NOUT; ++o) reinterpret_cast<T2*>(a.out[o])[g] = mk(o0[o], o1[o]);
+    }
+    // an odd last point
+    if ((a.npts & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const long g = a.npts - 1;
         T vin[NIN > 0 ? NIN : 1];
 #pragma unroll
         for (int i = 0; i < NIN; ++i) vin[i] = a.in[i][g];
