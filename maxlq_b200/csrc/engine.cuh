@@ -99,14 +99,17 @@ class EngineBase {
     // idu and 75..83 still hold grad u and grad d.  retract() then records
     // that the state spectrum `next` holds cs * w, and the next gradient
     // program forms u and grad u pointwise instead of transforming them.
-    // Cleared by a write to physical fields 0..11 or 60..83 and by a write
-    // to any of the spectra.
+    // sac: the transport also left P2(|w|^2), P2(g^2) (physical 18, 19 and
+    // work spectrum 1) and P2(|w|^2 w) (c_tmp_) at q = 4, which the gradient
+    // program at cs w scales by cs^2 and cs^3.  Cleared by a write to
+    // physical fields 0..11, 18, 19 or 60..83 and by a write to any of the
+    // spectra.
     struct PhysMemo {
         const void* u = nullptr;
         const void* d = nullptr;
         const void* next = nullptr;
         int iu = -1, idu = -1;
-        bool ls = false, tr = false;
+        bool ls = false, tr = false, sac = false;
         double tau = 0.0, cs = 0.0;
     } pm_;
     void state_written(const void* p) {

@@ -1198,11 +1198,11 @@ enum : int {
 };
 }  // namespace
 
-// the physical-field memo covers u, grad u (0..11) and the line search's u, d
-// and their gradients (60..83)
+// the physical-field memo covers u, grad u (0..11), S and A (18, 19) and the
+// line search's u, d and their gradients (60..83)
 template <typename T>
 void Engine<T>::phys_written(int idx) {
-    if ((idx >= PU && idx < PL) || (idx >= LU && idx < LS)) pm_ = PhysMemo{};
+    if ((idx >= PU && idx < PL) || idx == PS || idx == PA || (idx >= LU && idx < LS)) pm_ = PhysMemo{};
 }
 
 // PU <- u + tau d from the line search's physical fields of u and d, when the
@@ -1544,7 +1544,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
     }
     // the same launches every CG iteration: a CUDA graph after the first two
     // (one per path: the physical fields the retraction reads are in the key)
-    as_graph(rt ? "grad_l2_rt" : "grad_l2",
+    as_graph(rt ? (pm_.sac ? "grad_l2_rts" : "grad_l2_rt") : "grad_l2",
              {u, v, c, lqq ? (const void*)v : nullptr, rt ? (const void*)phys(pm_.idu) : nullptr},
              [&] { grad_l2_body(u, v, c, lqq != nullptr, rt); });
     pm_ = PhysMemo{};        // a replayed graph runs no host code: clear here
@@ -1558,6 +1558,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
 template <typename T>
 void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq, bool from_retraction) {
     pu_of_ = nullptr;
+    const bool sac = from_retraction && pm_.sac;
     const Band& b = b2;
     const long nc = spec_ncomp();
     const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
@@ -1575,9 +1576,28 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         for (int k = 0; k < 9; ++k) in.push_back(idu + k);
         for (int k = 0; k < 9; ++k) in.push_back(LDD + k);
         for (int i = 0; i < 12; ++i) out.push_back(PU + i);
-        FRetract f;
-        f.coef = d_coef_;
-        pointwise(f, in, out);
+        if (sac) {
+            // S and A of the transport, scaled by cs^2; A's spectrum too, and
+            // c = P2(A u) = cs^3 P2(A_w w) from the transport's c_tmp_
+            in.push_back(PS);
+            in.push_back(PA);
+            out.push_back(PS);
+            out.push_back(PA);
+            FRetract<true> f;
+            f.coef = d_coef_;
+            pointwise(f, in, out);
+            const long nsp = (long)b.nb * b.nb * b.nx;
+            cudaEvent_t ev = prof_mark();
+            spec_scale_pow_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(wspec(WA), wspec(WA), nsp, d_coef_, 2);
+            launched("spec_scale", 2.0 * nsp * sizeof(cpx<T>), ev);
+            ev = prof_mark();
+            spec_scale_pow_kernel<double2><<<grid_for(3 * nc, 256), 256, 0, stream>>>(c, c_tmp_, 3 * nc, d_coef_, 3);
+            launched("spec_scale", 2.0 * 3 * nc * sizeof(double2), ev);
+        } else {
+            FRetract<false> f;
+            f.coef = d_coef_;
+            pointwise(f, in, out);
+        }
     }
     for (int i = 0; i < 3; ++i) {
         for (int j = -1; j < 3 && !from_retraction; ++j) {
@@ -1604,7 +1624,10 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         oQ.sym = SYM_INV_KSQ;
         oQ.spec = wspec(WP);
         oQ.spec_f64 = wf64<T>();
-        fwd(b, FG1{}, uin, {oS, oQ});
+        if (sac)
+            fwd(b, FG1Q{}, std::vector<int>(uin.begin() + 3, uin.end()), {oQ});
+        else
+            fwd(b, FG1{}, uin, {oS, oQ});
     }
     // 3. grad p (1109)
     {
@@ -1619,7 +1642,7 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         inv(b, g);
     }
     // 4. |u|^k fields
-    A_and_S(true);
+    if (!sac) A_and_S(true);
     PowField a2 = chain(q - 2.0);
     PowField a4;
     if (!use_e_u) a4 = chain(q - 4.0);
@@ -1638,7 +1661,12 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         for (int i = 0; i < 3; ++i) in2.push_back(PL + i);
         for (int i = 0; i < 3; ++i) in2.push_back(PGP + i);
         in2.push_back(a2.phys);
-        if (!use_e_u) {
+        if (sac) {
+            FG2T f;
+            f.cvisc = cv;
+            f.cpress = cp;
+            fwd(b, f, std::vector<int>(in2.begin(), in2.begin() + 9), {oT});
+        } else if (!use_e_u) {
             FG2 f;
             f.cvisc = cv;
             f.cpress = cp;
@@ -1760,7 +1788,8 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
     const long nc = spec_ncomp();
     const double q = P.q;
     chain_reset();
-    if (!w_from_memo(u, d, tau)) {
+    const bool memo = w_from_memo(u, d, tau);
+    if (!memo) {
         std::vector<InvOut> io;
         for (int i = 0; i < 3; ++i) {
             InvOut o;
@@ -1772,6 +1801,7 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
         }
         inv(b2, io);
     }
+    const PhysMemo m = pm_;  // this program's own writes below keep it
     FwdOut oS;
     oS.phys_out = PS;
     fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
@@ -1789,6 +1819,11 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
             o[i].spec_f64 = 1;
         }
         fwd(b2, FC3{}, {a2.phys, PU, PU + 1, PU + 2}, {o[0], o[1], o[2]});
+        if (memo) {
+            pm_ = m;
+            // at q = 4 (no e_u) the gradient's S, A = |u|^{q-2} and c are these
+            pm_.sac = q == 4.0 && !use_e_u && a2.phys == PA && a2.spec == WA;
+        }
     } else {
         if (a2.kind != PowField::ONE) throw CudaError("vectorTransport with 2 < q < 2+eps", MLQ_ERR_BADARG);
         lincomb(cbuf, 1.0, u, d ? tau : 0.0, d, 0.0, nullptr);

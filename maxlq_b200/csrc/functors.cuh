@@ -289,12 +289,14 @@ struct FAxpy3 {
     }
 };
 
-// The retracted state u' = cs w, w = u + tau d, and its gradient
-// cs (grad u + tau grad d).  inputs w(3), Du(9), Dd(9); outputs u'(3), Du'(9).
-// cs and tau are read from device memory (coef[0], coef[1]), so a captured
-// launch stays valid from one iteration to the next.
+// The retracted state u' = cs w, w = u + tau d, its gradient
+// cs (grad u + tau grad d), and (with S) P2(|u'|^2) = cs^2 P2(|w|^2) and
+// P2(g'^2) = cs^2 P2(g^2).  inputs w(3), Du(9), Dd(9)[, S, A]; outputs u'(3),
+// Du'(9)[, S', A'].  cs and tau are read from device memory (coef[0],
+// coef[1]), so a captured launch stays valid from one iteration to the next.
+template <bool S>
 struct FRetract {
-    static constexpr int NIN = 21, NOUT = 12, NRED = 0;
+    static constexpr int NIN = S ? 23 : 21, NOUT = S ? 14 : 12, NRED = 0;
     const double* coef;
     template <typename T>
     __device__ void operator()(const T* in, T* out, double*) const {
@@ -303,6 +305,38 @@ struct FRetract {
         for (int i = 0; i < 3; ++i) out[i] = cs * in[i];
 #pragma unroll
         for (int k = 0; k < 9; ++k) out[3 + k] = cs * in[3 + k] + ctau * in[12 + k];
+        if constexpr (S) {
+            const T cs2 = (T)(coef[0] * coef[0]);
+            out[12] = cs2 * in[21];
+            out[13] = cs2 * in[22];
+        }
+    }
+};
+
+// Q = d_j u_i d_i u_j alone (FG1 without S).  inputs D(9), D[3i+j] = d_j u_i
+struct FG1Q {
+    static constexpr int NIN = 9, NOUT = 1, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        T q = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) q += in[3 * j + i] * in[3 * i + j];
+        out[0] = q;
+    }
+};
+
+// T of FG2 alone (c given).  inputs u(3), Lu(3), Gp(3)
+struct FG2T {
+    static constexpr int NIN = 9, NOUT = 1, NRED = 0;
+    double cvisc, cpress;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        T t = 0;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) t += in[i] * ((T)cvisc * in[3 + i] - (T)cpress * in[6 + i]);
+        out[0] = t;
     }
 };
 

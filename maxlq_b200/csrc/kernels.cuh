@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256) xfwd_kernel(XFwdArgs<T> a, F f) {
 // ----------------------------------------------------------------------------
 template <typename T>
 struct PArgs {
-    static constexpr int MAX_IN = 24, MAX_OUT = 12;
+    static constexpr int MAX_IN = 24, MAX_OUT = 14;
     long npts;
     const T* in[MAX_IN];
     T* out[MAX_OUT];
@@ -577,6 +577,18 @@ static __global__ void spec_lincomb_kernel(SpecGeom g, double2* out, double a, c
             r.y += c * w.y;
         }
         out[i] = r;
+    }
+}
+
+// out = coef[0]^pw * in over n elements of type C (complex float / double),
+// the factor read from device memory (stays valid in a replayed graph)
+template <typename C>
+__global__ void spec_scale_pow_kernel(C* out, const C* in, long n, const double* coef, int pw) {
+    double f = 1.0;
+    for (int k = 0; k < pw; ++k) f *= coef[0];
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const C v = in[i];
+        out[i] = C{(decltype(v.x))(f * v.x), (decltype(v.y))(f * v.y)};
     }
 }
 
