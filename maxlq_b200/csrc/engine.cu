@@ -283,6 +283,7 @@ void EngineBase::hilbert_leray(double2* f, double order, double scale) {
 }
 
 void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
+    if (np < 1 || np > 8) throw CudaError("dots: 1 to 8 pairs per call", MLQ_ERR_BADARG);
     SpecDotArgs a;
     a.g = geom(b2);
     for (int i = 0; i < np; ++i) a.pr[i] = pairs[i];
@@ -290,8 +291,18 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
     bool need_h = false;
     for (int i = 0; i < np; ++i) need_h |= pairs[i].kind == 1;
     a.hwtab = need_h ? hweight_table(1.5 - 1.0 / P.q) : nullptr;  // (3/2)-(1/q), function_ops.f90:3467
+    // as many blocks as are resident at once: the reduction is latency-bound
+    // (thread-safe one-time initialisation; every device here is a B200)
+    static const int resident = [] {
+        int per_sm = 0, dev = 0, sms = 0;
+        MLQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spec_dot_kernel, RED_THREADS, 0));
+        MLQ_CUDA(cudaGetDevice(&dev));
+        MLQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        return std::max(1, per_sm) * sms;
+    }();
+    const int grid = grid_for(a.g.ncomp, RED_THREADS, resident);
+    ensure_partials((long)grid * 8);
     a.partials = d_partials;
-    const int grid = grid_for(a.g.ncomp, RED_THREADS, 148 * 4);
     cudaEvent_t ev = prof_mark();
     spec_dot_kernel<<<grid, RED_THREADS, 0, stream>>>(a);
     {
@@ -302,7 +313,7 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
         }
         launched("spec_dot", 48.0 * a.g.ncomp * uniq.size(), ev);
     }
-    finalize(grid, 6, 1.0, 200);
+    finalize(grid, 8, 1.0, 200);
     fetch_results();
     for (int i = 0; i < np; ++i) out[i] = h_results[200 + i];
 }

@@ -660,18 +660,20 @@ struct SpecDotPair {
 };
 struct SpecDotArgs {
     SpecGeom g;
-    SpecDotPair pr[6];
+    SpecDotPair pr[8];
     int npairs;
     const double* hwtab;  // H_l weight (1+(lambda1|K|)^order)^2 by |j|^2 (function_ops.f90:3472), or null
     double* partials;
 };
 
 static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
-    double acc[6] = {0, 0, 0, 0, 0, 0};
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const SpecGeom& g = a.g;
     const double twopi = 2.0 * 3.14159265358979311600;
     const int nrows = g.nb * g.nb;
-    // 32 threads per row: RED_THREADS / 32 rows per block pass
+    // 32 threads per row: RED_THREADS / 32 rows per block pass; each thread
+    // takes kx = fx and fx + 32 together, so a pair's loads for both are in
+    // flight at once (the second is a weight-0 repeat of the first past nx)
     const int lane = threadIdx.x & 31, wrow = threadIdx.x >> 5, rows_per = blockDim.x >> 5;
     for (int r = blockIdx.x * rows_per + wrow; r < nrows; r += gridDim.x * rows_per) {
         const SpecRow row(g, r);
@@ -679,30 +681,48 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
         const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : twopi * (double)row.jy;
         const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : twopi * (double)row.jz;
         const int jyz = row.jy * row.jy + row.jz * row.jz;
-        for (int fx = lane; fx < g.nx; fx += 32) {
-            const long i = base + fx;
-            const double wgt = kx_weight(g.n, fx);
-            const double hw = a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0;
-            const double ox = (2 * fx == g.n) ? 0.0 : twopi * (double)fx;
+        for (int fx = lane; fx < g.nx; fx += 64) {
+            const bool two = fx + 32 < g.nx;
+            const int fx1 = two ? fx + 32 : fx;
+            const long i[2] = {base + fx, base + fx1};
+            const double wgt[2] = {kx_weight(g.n, fx), two ? kx_weight(g.n, fx1) : 0.0};
+            const double hw[2] = {a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0, a.hwtab ? a.hwtab[fx1 * fx1 + jyz] : 1.0};
+            const double ox[2] = {(2 * fx == g.n) ? 0.0 : twopi * (double)fx, (2 * fx1 == g.n) ? 0.0 : twopi * (double)fx1};
             for (int p = 0; p < a.npairs; ++p) {
                 const SpecDotPair& q = a.pr[p];
                 if (q.kind == 2) {
-                    const double2 v0 = q.a[i], v1 = q.a[g.ncomp + i], v2 = q.a[2 * g.ncomp + i];
-                    const double dr = ox * v0.x + oy * v1.x + oz * v2.x;
-                    const double di = ox * v0.y + oy * v1.y + oz * v2.y;
-                    acc[p] += wgt * (dr * dr + di * di);
-                } else {
-                    double s = 0.0;
-                    for (int c = 0; c < 3; ++c) {
-                        const double2 u = q.a[c * g.ncomp + i], v = q.b[c * g.ncomp + i];
-                        s += u.x * v.x + u.y * v.y;
+                    double2 v[2][3];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) v[e][c] = q.a[c * g.ncomp + i[e]];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const double dr = ox[e] * v[e][0].x + oy * v[e][1].x + oz * v[e][2].x;
+                        const double di = ox[e] * v[e][0].y + oy * v[e][1].y + oz * v[e][2].y;
+                        acc[p] += wgt[e] * (dr * dr + di * di);
                     }
-                    acc[p] += wgt * (q.kind == 1 ? hw : 1.0) * s;
+                } else {
+                    double2 u[2][3], v[2][3];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            u[e][c] = q.a[c * g.ncomp + i[e]];
+                            v[e][c] = q.b[c * g.ncomp + i[e]];
+                        }
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        double s = 0.0;
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) s += u[e][c].x * v[e][c].x + u[e][c].y * v[e][c].y;
+                        acc[p] += wgt[e] * (q.kind == 1 ? hw[e] : 1.0) * s;
+                    }
                 }
             }
         }
     }
-    block_reduce_store<6>(acc, a.partials, blockIdx.x);
+    block_reduce_store<8>(acc, a.partials, blockIdx.x);
 }
 
 // Fourier coefficients of a physical scalar restricted to a band, full-band

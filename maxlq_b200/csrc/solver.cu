@@ -313,28 +313,33 @@ class Solver : public SolverBase {
         const double alpha = dd[0] / dd[1];  // 170-171
         info.alpha = alpha;
         e.lincomb(g1, 1.0, g1, -alpha, c);  // gradJproj (177), kept in gu1
-        {
-            // 180-193: orthogonality and divergence checks
-            e.lincomb(tmp, 1.0, g1, 1.0, c);
-            SpecDotPair p[4] = {{g1, c, 1}, {tmp, tmp, 1}, {g1, nullptr, 2}, {g1, g1, 1}};
-            e.dots(p, 4, dd);
-            info.ortho_check = std::fabs(dd[0] / dd[1]);
-            info.div_check = dd[2] / dd[3];
-        }
         if (!e.P.use_tangential_gradient) throw CudaError("useTangentialGradient=.false. is not supported",
                                                           MLQ_ERR_BADARG);
-        if (e.P.normalize_gradient) {
-            SpecDotPair p[2] = {{u, u, 1}, {g1, g1, 1}};
-            e.dots(p, 2, dd);
-            e.lincomb(g1, std::sqrt(dd[0] / dd[1]), g1);  // 213
+        // Every inner product the rest of the update needs, in one pass.  The
+        // reference forms g + c (180-193) and g - T g0 (223-226) and the norm
+        // of d1 only to take inner products of them; those are expanded here
+        // into products of g, c, u, T g0, g0, T d0 (bilinearity), which
+        // saves two state-vector temporaries and four reductions.
+        const double cc = dd[1];  // <c, c>
+        enum { GC, GDIV, GG, UU, GTG, G0G0, GTD, TDTD };
+        double ip[8];
+        {
+            SpecDotPair p[8] = {{g1, c, 1},    {g1, nullptr, 2}, {g1, g1, 1},   {u, u, 1},
+                                {g1, vtg0, 1}, {gu0, gu0, 1},    {g1, vtd0, 1}, {vtd0, vtd0, 1}};
+            e.dots(p, 8, ip);
         }
+        info.ortho_check = std::fabs(ip[GC] / (ip[GG] + 2.0 * ip[GC] + cc));  // <g,c> / <g+c, g+c>
+        info.div_check = ip[GDIV] / ip[GG];
+        double sg = 1.0;  // gradient normalisation (213)
+        if (e.P.normalize_gradient) {
+            sg = std::sqrt(ip[UU] / ip[GG]);
+            e.lincomb(g1, sg, g1);
+        }
+        const double gg = sg * sg * ip[GG], gtd = sg * ip[GTD];  // <g', g'>, <g', T d0>
         double beta = 0.0;
         if (e.P.use_conjugate_gradient) {
-            e.lincomb(tmp, 1.0, g1, -1.0, vtg0);
-            SpecDotPair p[2] = {{g1, tmp, 1}, {gu0, gu0, 1}};
-            e.dots(p, 2, dd);
-            beta = dd[0];  // 226
-            const double g0n = dd[1];  // 227
+            beta = gg - sg * ip[GTG];  // <g', g' - T g0> (226)
+            const double g0n = ip[G0G0];  // 227
             if (g0n < MACH_EPSILON || beta < MACH_EPSILON)
                 beta = 0.0;
             else
@@ -345,13 +350,9 @@ class Solver : public SolverBase {
             e.lincomb(d1, 1.0, g1);
         }
         info.beta = beta;
-        {
-            SpecDotPair p[3] = {{g1, g1, 1}, {vtd0, vtd0, 1}, {d1, d1, 1}};
-            e.dots(p, 3, dd);
-            info.norm_grad = std::sqrt(dd[0]);
-            info.norm_td0 = std::sqrt(dd[1]);
-            info.norm_d1 = std::sqrt(dd[2]);
-        }
+        info.norm_grad = std::sqrt(gg);
+        info.norm_td0 = std::sqrt(ip[TDTD]);
+        info.norm_d1 = std::sqrt(std::max(0.0, gg + 2.0 * beta * gtd + beta * beta * ip[TDTD]));
         e.zeroth(d1, info.mean_d1);  // 251
         e.zeroth(u, info.mean_u);    // 257
         // line search (269-318)
