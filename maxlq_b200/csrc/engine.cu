@@ -256,6 +256,28 @@ void EngineBase::retract(double2* u, double cs, double tau, const double2* d) {
     }
 }
 
+void EngineBase::transport_retract(double2* tg, double2* td, const double2* g, const double2* d, double2* u,
+                                   double ag, double bg, double cg, double ad, double bd, double cd, double cs,
+                                   double tau) {
+    const PhysMemo keep = pm_;
+    state_written(tg);
+    state_written(td);
+    state_written(u);
+    SpecGeom geo = geom(b2);
+    const long nt = 3 * geo.ncomp;
+    cudaEvent_t ev = prof_mark();
+    spec_transport_kernel<<<grid_for(nt, 256), 256, 0, stream>>>(nt, g, d, u, tg, td, ag, bg, cg, ad, bd, cd, cs,
+                                                                cs * tau);
+    launched("spec_lincomb", 16.0 * nt * 6, ev);
+    if (keep.tr && keep.u == (const void*)u && keep.d == (const void*)d && keep.tau == tau) {
+        pm_ = keep;
+        pm_.u = nullptr;  // the fields describe the old u, no longer stored
+        pm_.ls = false;
+        pm_.next = u;
+        pm_.cs = cs;
+    }
+}
+
 void EngineBase::hilbert(double2* f, double order) {
     state_written(f);
     SpecGeom g = geom(b2);

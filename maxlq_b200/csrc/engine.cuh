@@ -119,6 +119,10 @@ class EngineBase {
     // u <- cs (u + tau d), keeping the transport's physical fields of
     // u + tau d for the next gradient program
     void retract(double2* u, double cs, double tau, const double2* d);
+    // the vector transport's outputs tg = ag g + bg u + cg d, td = ad d + bd u
+    // + cd d and then the retraction u <- cs (u + tau d), in one pass
+    void transport_retract(double2* tg, double2* td, const double2* g, const double2* d, double2* u, double ag,
+                           double bg, double cg, double ad, double bd, double cd, double cs, double tau);
     void ensure_partials(long n);
     // Count a launch and surface launch-configuration errors immediately.
     // With profiling on, `a` is the event recorded before the launch; the
@@ -390,6 +394,7 @@ class Engine : public EngineBase {
     double* d_coef_ = nullptr;  // cs, tau of the retraction (read by a captured launch)
     void phys_written(int idx);  // clears the physical-field memo when it covers idx
     bool w_from_memo(const double2* u, const double2* d, double tau);
+    bool ls_clamp_free(double tau);  // S(tau) >= 0 at every point (the interval, else one check)
 
     // register-resident FFT kernels (power-of-two n >= 64); E elements per thread
     int ereg_ = 8;  // elements per thread: 8 up to n = 512, 16 above

@@ -1195,6 +1195,7 @@ enum : int {
     LP = 96,    // p_a (3)
     WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
     WLS = 43,   // work spectra: S_a (3)
+    WLQ = 46,   // work spectra: -Lap^-1 P2(Q_a) (3), read by the next gradient
 };
 }  // namespace
 
@@ -1624,10 +1625,18 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         oQ.sym = SYM_INV_KSQ;
         oQ.spec = wspec(WP);
         oQ.spec_f64 = wf64<T>();
-        if (sac)
-            fwd(b, FG1Q{}, std::vector<int>(uin.begin() + 3, uin.end()), {oQ});
-        else
+        if (from_retraction) {
+            // Q of u = cs (u_prev + tau d) is cs^2 (Q_0 + tau Q_1 + tau^2 Q_2),
+            // the line search's coefficient spectra (same symbol)
+            const long nsp = (long)b.nb * b.nb * b.nx;
+            cudaEvent_t ev = prof_mark();
+            spec_poly3_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(
+                wspec(WP), wspec(WLQ), wspec(WLQ + 1), wspec(WLQ + 2), nsp, 0.0, 0.0, 0.0, d_coef_);
+            launched("spec_poly", 4.0 * nsp * sizeof(cpx<T>), ev);
+            if (!sac) fwd(b, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
+        } else {
             fwd(b, FG1{}, uin, {oS, oQ});
+        }
     }
     // 3. grad p (1109)
     {
@@ -1802,10 +1811,23 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
         inv(b2, io);
     }
     const PhysMemo m = pm_;  // this program's own writes below keep it
-    FwdOut oS;
-    oS.phys_out = PS;
-    fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
-    A_and_S(true);
+    if (memo && q == 4.0 && !use_e_u && ls_clamp_free(tau)) {
+        // |w|^2 = S_0 + tau S_1 + tau^2 S_2 (the line search's coefficient
+        // fields, P2 linear) is >= 0 at every point, so A = P2(max(S, 0)) = S
+        FPolyS f;
+        f.tau = tau;
+        pointwise(f, {LS, LS + 1, LS + 2}, {PS, PA});
+        const long nsp = (long)b2.nb * b2.nb * b2.nx;
+        cudaEvent_t ev = prof_mark();
+        spec_poly3_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(
+            wspec(WA), wspec(WLS), wspec(WLS + 1), wspec(WLS + 2), nsp, 1.0, tau, tau * tau, nullptr);
+        launched("spec_poly", 4.0 * nsp * sizeof(cpx<T>), ev);
+    } else {
+        FwdOut oS;
+        oS.phys_out = PS;
+        fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
+        A_and_S(true);
+    }
     PowField a2 = chain(q - 2.0);
     PowField ah = chain(q / 2.0);
     if (!c_tmp_) c_tmp_ = alloc_state();
@@ -2051,6 +2073,10 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
         for (int a = 0; a < 3; ++a) {
             o[a].sym = SYM_INV_KSQ;
             o[a].phys_out = LP + a;
+            if (!slab_) {  // the next gradient's pressure source is a polynomial in tau of these
+                o[a].spec = wspec(WLQ + a);
+                o[a].spec_f64 = wf64<T>();
+            }
             o[3 + a].spec = wspec(WLG + a);
             o[3 + a].spec_f64 = wf64<T>();
         }
@@ -2131,8 +2157,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
 }
 
 template <typename T>
-void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
-    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
+bool Engine<T>::ls_clamp_free(double tau) {
     bool clamp_off = tau >= ls_tlo_ && tau <= ls_thi_;
     if (!clamp_off) {
         // outside the interval: one read of S_0..2 decides for this tau
@@ -2158,7 +2183,13 @@ void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
         }
         clamp_off = mn >= 0.0;
     }
-    if (clamp_off) {
+    return clamp_off;
+}
+
+template <typename T>
+void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
+    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
+    if (ls_clamp_free(tau)) {
         // S(tau) >= 0 everywhere: P2(g^2) = S(tau), every product is a polynomial
         ++ls_poly_trials_;
         const double tp[5] = {1.0, tau, tau * tau, tau * tau * tau, tau * tau * tau * tau};

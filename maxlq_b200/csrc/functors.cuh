@@ -313,20 +313,6 @@ struct FRetract {
     }
 };
 
-// Q = d_j u_i d_i u_j alone (FG1 without S).  inputs D(9), D[3i+j] = d_j u_i
-struct FG1Q {
-    static constexpr int NIN = 9, NOUT = 1, NRED = 0;
-    template <typename T>
-    __device__ void operator()(const T* in, T* out, double*) const {
-        T q = 0;
-#pragma unroll
-        for (int i = 0; i < 3; ++i)
-#pragma unroll
-            for (int j = 0; j < 3; ++j) q += in[3 * j + i] * in[3 * i + j];
-        out[0] = q;
-    }
-};
-
 // T of FG2 alone (c given).  inputs u(3), Lu(3), Gp(3)
 struct FG2T {
     static constexpr int NIN = 9, NOUT = 1, NRED = 0;
@@ -337,6 +323,21 @@ struct FG2T {
 #pragma unroll
         for (int i = 0; i < 3; ++i) t += in[i] * ((T)cvisc * in[3 + i] - (T)cpress * in[6 + i]);
         out[0] = t;
+    }
+};
+
+// S(tau) = s0 + tau s1 + tau^2 s2 from the line search's coefficient fields,
+// written twice (S and, where S >= 0 everywhere, A = P2(max(S, 0)) = S).
+// inputs s0, s1, s2
+struct FPolyS {
+    static constexpr int NIN = 3, NOUT = 2, NRED = 0;
+    double tau;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        const T t = (T)tau;
+        const T v = in[0] + t * (in[1] + t * in[2]);
+        out[0] = v;
+        out[1] = v;
     }
 };
 

@@ -592,6 +592,38 @@ __global__ void spec_scale_pow_kernel(C* out, const C* in, long n, const double*
     }
 }
 
+// out = c0 a + c1 b + c2 c over n elements of type C (a polynomial in tau of
+// three coefficient spectra); with coef non-null the coefficients are
+// cs^2 (1, tau, tau^2) for cs = coef[0], tau = coef[1], read from device
+// memory (stays valid in a replayed graph)
+template <typename C>
+__global__ void spec_poly3_kernel(C* out, const C* a, const C* b, const C* c, long n, double c0, double c1,
+                                  double c2, const double* coef) {
+    if (coef) {
+        c0 = coef[0] * coef[0];
+        c1 = c0 * coef[1];
+        c2 = c1 * coef[1];
+    }
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const C x = a[i], y = b[i], z = c[i];
+        out[i] = C{(decltype(x.x))(c0 * x.x + c1 * y.x + c2 * z.x), (decltype(x.y))(c0 * x.y + c1 * y.y + c2 * z.y)};
+    }
+}
+
+// The vector transport's two outputs and the retraction in one pass over the
+// state (function_ops.f90:1716-1768 with optimization.f90:324-338):
+//   tg = ag g + bg u + cg d,  td = ad d + bd u + cd d,  u <- cs u + ct d
+static __global__ void spec_transport_kernel(long nt, const double2* g, const double2* d, double2* u, double2* tg,
+                                             double2* td, double ag, double bg, double cg, double ad, double bd,
+                                             double cd, double cs, double ct) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += (long)gridDim.x * blockDim.x) {
+        const double2 gv = g[i], dv = d[i], uv = u[i];
+        tg[i] = make_double2(ag * gv.x + bg * uv.x + cg * dv.x, ag * gv.y + bg * uv.y + cg * dv.y);
+        td[i] = make_double2(ad * dv.x + bd * uv.x + cd * dv.x, ad * dv.y + bd * uv.y + cd * dv.y);
+        u[i] = make_double2(cs * uv.x + ct * dv.x, cs * uv.y + ct * dv.y);
+    }
+}
+
 // Row-structured walk over a band spectrum [nb][nb][nx]: block b takes rows
 // r = b, b + gridDim.x, ... (r = cz*nb + cy), threads take kx; no division per
 // element.  Signed indices and |j|^2 of a mode give the wavenumbers exactly

@@ -390,20 +390,21 @@ class Solver : public SolverBase {
         else
             lqw = e.lq_pow(u, d1, tau1);
         const double ln = std::pow(lqw, 1.0 / qq);
-        if (e.P.use_riemannian_geometry) {
-            const double f = std::pow(ln, -qq);
-            e.lincomb(vtg0, Bc / ln, g1, -Bc / ln * f * ir[0], u, -Bc / ln * f * ir[0] * tau1, d1);
-            e.lincomb(vtd0, Bc / ln, d1, -Bc / ln * f * ir[1], u, -Bc / ln * f * ir[1] * tau1, d1);
-        } else {
-            e.lincomb(vtg0, 1.0, g1);
-            e.lincomb(vtd0, 1.0, d1);
-        }
         // R at the retracted point from the accepted trial (homogeneity), as
         // eval_J(Uvec, "maxdLqdt") after rescaleLqNorm (344-349)
         const Trial tr = trial(u, d1, tau1);
         const double cs = Bc / std::pow(tr.lqq, 1.0 / qq);
         const double R12n = std::pow(cs, qq) * tr.R[1], R3n = std::pow(cs, qq + 1.0) * tr.R[2];
-        e.retract(u, Bc / ln, tau1, d1);
+        if (e.P.use_riemannian_geometry) {
+            // transported gradient and direction (324-328), then u <- (B/ln) w
+            const double f = std::pow(ln, -qq);
+            e.transport_retract(vtg0, vtd0, g1, d1, u, Bc / ln, -Bc / ln * f * ir[0], -Bc / ln * f * ir[0] * tau1,
+                                Bc / ln, -Bc / ln * f * ir[1], -Bc / ln * f * ir[1] * tau1, Bc / ln, tau1);
+        } else {
+            e.lincomb(vtg0, 1.0, g1);
+            e.lincomb(vtd0, 1.0, d1);
+            e.retract(u, Bc / ln, tau1, d1);
+        }
         trials.clear();
         const double J1 = R12n + R3n;
         const double deltaJ = (J1 - J0) / std::fabs(J0);
