@@ -62,7 +62,7 @@ EngineBase::EngineBase(const mlq_params& p) : P(p) {
 EngineBase::~EngineBase() {
     for (auto& kv : graphs_)
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    for (void* p : allocs_) cudaFree(p);
+    for (auto& a : allocs_) cudaFree(a.first);
     if (stream) cudaStreamDestroy(stream);
 }
 
@@ -101,15 +101,17 @@ void* EngineBase::dev_alloc(size_t b) {
         throw CudaError("cudaMalloc of " + std::to_string(b) + " bytes failed: " + cudaGetErrorString(e),
                         MLQ_ERR_OOM);
     }
-    allocs_.push_back(p);
+    allocs_.push_back({p, b});
     bytes += (long long)b;
+    bytes_peak = std::max(bytes_peak, bytes);
     return p;
 }
 
 void EngineBase::free_dev(void* p) {
-    auto it = std::find(allocs_.begin(), allocs_.end(), p);
+    auto it = std::find_if(allocs_.begin(), allocs_.end(), [p](const std::pair<void*, size_t>& a) { return a.first == p; });
     if (it != allocs_.end()) {
         ++graph_gen_;  // captured graphs may reference the freed block
+        bytes -= (long long)it->second;
         allocs_.erase(it);
         cudaFree(p);
     }

@@ -176,7 +176,8 @@ class EngineBase {
     cudaEvent_t ev_take();  // from the engine's pool of events
     void ev_give(cudaEvent_t e) { evpool_.push_back(e); }
 
-    std::vector<void*> allocs_;
+    std::vector<std::pair<void*, size_t>> allocs_;
+    long long bytes_peak = 0;  // most device bytes held at once
 };
 
 template <class Fn>

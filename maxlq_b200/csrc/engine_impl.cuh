@@ -257,6 +257,7 @@ std::string Engine<T>::kernel_config() const {
                     ", \"graph_replays\": " + std::to_string(graph_launches_) +
                     ", \"line_search_trials_polynomial\": " + std::to_string(ls_poly_trials_) +
                     ", \"line_search_trials_transform\": " + std::to_string(ls_fft_trials_) +
+                    ", \"device_bytes_peak\": " + std::to_string(bytes_peak) +
                     ", \"yz_variants\": \"" + (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
     return r;
 }
