@@ -104,6 +104,21 @@ class Dist:
             self.pg.destroy_process_group()
 
 
+def pinned_like(a: np.ndarray) -> np.ndarray:
+    """A page-locked host copy of a (plain copy when no GPU is present)."""
+    import torch
+    if not torch.cuda.is_available():
+        return np.ascontiguousarray(a.copy())
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    out = t.numpy()
+    out[...] = a
+    pinned_like.keep.append(t)  # the numpy view does not own the memory
+    return out
+
+
+pinned_like.keep = []
+
+
 def device_sync():
     try:
         import torch
@@ -525,10 +540,11 @@ def main():
         rel_dR = abs(R_m0[0] - R_d0[0]) / abs(R_d0[0])
         fp64.close()
 
-    # e2e: each step copies u host->device, iterates once, copies u back
+    # e2e: each step copies u host->device from pinned host memory, iterates
+    # once, copies u back (the library DMAs a pinned buffer directly)
     e2e = None
     if not args.no_e2e:
-        uh = np.ascontiguousarray(u0.copy())
+        uh = pinned_like(u0)
         mixed.state_load(uh)
         for _ in range(min(W, 1)):
             mixed.state_step(uh)

@@ -2261,8 +2261,25 @@ static void par_range(long count, Fn&& fn) {
 
 static constexpr long XFER_CHUNK = 1L << 25;  // elements per pipelined chunk
 
+// A host buffer the caller allocated pinned (page-locked): the DMA engine
+// reads and writes it directly, with no staging copy.
+static bool host_pinned(const void* p) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 template <typename T>
 void Engine<T>::load_scalar_phys(const double* host, int dst) {
+    if (sizeof(T) == 8 && host_pinned(host)) {
+        MLQ_CUDA(cudaMemcpyAsync(phys(dst), host, n3 * sizeof(T), cudaMemcpyHostToDevice, stream));
+        MLQ_CUDA(cudaStreamSynchronize(stream));
+        if (slab_) slot(dst).kind = PSlot::FULL;
+        return;
+    }
     const long ch = std::min(n3, XFER_CHUNK);
     T* buf[2];
     buf[0] = (T*)stage(2 * ch * sizeof(T));
@@ -2293,6 +2310,15 @@ template <typename T>
 void Engine<T>::store_scalar_phys(int src, double* host) {
     // chunks of whole slabs in slab mode (each expanded just before its copy)
     const long ch = slab_ ? (long)zs_ * n * n : std::min(n3, XFER_CHUNK);
+    if (sizeof(T) == 8 && host_pinned(host)) {
+        for (long off = 0; off < n3; off += ch) {
+            const long cnt = std::min(ch, n3 - off);
+            const T* d = slab_ ? expand(src, (int)(off / ((long)n * n)), 0) : phys(src) + off;
+            MLQ_CUDA(cudaMemcpyAsync(host + off, d, cnt * sizeof(T), cudaMemcpyDeviceToHost, stream));
+        }
+        MLQ_CUDA(cudaStreamSynchronize(stream));
+        return;
+    }
     T* buf[2];
     buf[0] = (T*)stage(2 * ch * sizeof(T));
     buf[1] = buf[0] + ch;
