@@ -112,8 +112,12 @@ class EngineBase {
         bool ls = false, tr = false, sac = false;
         double tau = 0.0, cs = 0.0;
     } pm_;
+    // the state spectrum whose S = P2(|u|^2) the physical field 18 and a work
+    // spectrum hold (set by the gradient program), for the line-search setup
+    const void* ws_of_ = nullptr;
     void state_written(const void* p) {
         if (p == pu_of_) pu_of_ = nullptr;
+        if (p == ws_of_) ws_of_ = nullptr;
         if (p && (p == pm_.u || p == pm_.d || p == pm_.next)) pm_ = PhysMemo{};
     }
     // u <- cs (u + tau d), keeping the transport's physical fields of
@@ -396,6 +400,9 @@ class Engine : public EngineBase {
     void phys_written(int idx);  // clears the physical-field memo when it covers idx
     bool w_from_memo(const double2* u, const double2* d, double tau);
     bool ls_clamp_free(double tau);  // S(tau) >= 0 at every point (the interval, else one check)
+    int ls_p0_ = -1, ls_w0_ = -1;    // physical field and work spectrum of S_0 in this line search
+    int ls_phys(int a) const;        // physical field of S_a
+    int ls_wspec(int a) const;       // work spectrum of S_a
 
     // register-resident FFT kernels (power-of-two n >= 64); E elements per thread
     int ereg_ = 8;  // elements per thread: 8 up to n = 512, 16 above

@@ -1197,6 +1197,7 @@ enum : int {
     WLG = 40,   // work spectra: P2 coefficients of |grad phi|^2 (3)
     WLS = 43,   // work spectra: S_a (3)
     WLQ = 46,   // work spectra: -Lap^-1 P2(Q_a) (3), read by the next gradient
+    WS = 49,    // work spectrum of S = P2(|u|^2) (gradient program, transport)
 };
 }  // namespace
 
@@ -1205,6 +1206,18 @@ enum : int {
 template <typename T>
 void Engine<T>::phys_written(int idx) {
     if ((idx >= PU && idx < PL) || idx == PS || idx == PA || (idx >= LU && idx < LS)) pm_ = PhysMemo{};
+    if (idx == PS) ws_of_ = nullptr;
+}
+
+// S_0 of the line search is the gradient program's S when it was formed for
+// the same u (field 18 and work spectrum WS), else the setup's own
+template <typename T>
+int Engine<T>::ls_phys(int a) const {
+    return a == 0 ? ls_p0_ : LS + a;
+}
+template <typename T>
+int Engine<T>::ls_wspec(int a) const {
+    return a == 0 ? ls_w0_ : WLS + a;
 }
 
 // PU <- u + tau d from the line search's physical fields of u and d, when the
@@ -1551,6 +1564,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
              [&] { grad_l2_body(u, v, c, lqq != nullptr, rt); });
     pm_ = PhysMemo{};        // a replayed graph runs no host code: clear here
     if (!slab_) pu_of_ = u;  // PU, PD hold u and grad u until the next program
+    ws_of_ = slab_ ? nullptr : (const void*)u;  // and PS, WS its S
     if (lqq) {
         fetch_results();
         *lqq = h_results[grad_lq_slot_];
@@ -1589,9 +1603,11 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
             f.coef = d_coef_;
             pointwise(f, in, out);
             const long nsp = (long)b.nb * b.nb * b.nx;
-            cudaEvent_t ev = prof_mark();
-            spec_scale_pow_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(wspec(WA), wspec(WA), nsp, d_coef_, 2);
-            launched("spec_scale", 2.0 * nsp * sizeof(cpx<T>), ev);
+            for (int w : {WA, WS}) {
+                cudaEvent_t ev = prof_mark();
+                spec_scale_pow_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(wspec(w), wspec(w), nsp, d_coef_, 2);
+                launched("spec_scale", 2.0 * nsp * sizeof(cpx<T>), ev);
+            }
             ev = prof_mark();
             spec_scale_pow_kernel<double2><<<grid_for(3 * nc, 256), 256, 0, stream>>>(c, c_tmp_, 3 * nc, d_coef_, 3);
             launched("spec_scale", 2.0 * 3 * nc * sizeof(double2), ev);
@@ -1623,6 +1639,8 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
     {
         FwdOut oS, oQ;
         oS.phys_out = PS;
+        oS.spec = wspec(WS);
+        oS.spec_f64 = wf64<T>();
         oQ.sym = SYM_INV_KSQ;
         oQ.spec = wspec(WP);
         oQ.spec_f64 = wf64<T>();
@@ -1817,15 +1835,18 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
         // fields, P2 linear) is >= 0 at every point, so A = P2(max(S, 0)) = S
         FPolyS f;
         f.tau = tau;
-        pointwise(f, {LS, LS + 1, LS + 2}, {PS, PA});
+        pointwise(f, {ls_phys(0), ls_phys(1), ls_phys(2)}, {PS, PA});
         const long nsp = (long)b2.nb * b2.nb * b2.nx;
         cudaEvent_t ev = prof_mark();
         spec_poly3_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(
-            wspec(WA), wspec(WLS), wspec(WLS + 1), wspec(WLS + 2), nsp, 1.0, tau, tau * tau, nullptr);
+            wspec(WS), wspec(ls_wspec(0)), wspec(ls_wspec(1)), wspec(ls_wspec(2)), nsp, 1.0, tau, tau * tau, nullptr);
         launched("spec_poly", 4.0 * nsp * sizeof(cpx<T>), ev);
+        MLQ_CUDA(cudaMemcpyAsync(wspec(WA), wspec(WS), nsp * sizeof(cpx<T>), cudaMemcpyDeviceToDevice, stream));
     } else {
         FwdOut oS;
         oS.phys_out = PS;
+        oS.spec = wspec(WS);
+        oS.spec_f64 = wf64<T>();
         fwd(b2, FSq3{}, {PU, PU + 1, PU + 2}, {oS});
         A_and_S(true);
     }
@@ -2030,15 +2051,22 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     std::vector<int> grads;
     for (int i = 0; i < 9; ++i) grads.push_back(idu + i);
     for (int i = 0; i < 9; ++i) grads.push_back(LDD + i);
-    // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333)
+    // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333).  The tau^0 one,
+    // P2(|u|^2), is the gradient program's S when it ran for this u.
     {
+        const bool s0 = !slab_ && ws_of_ == (const void*)u;
+        ls_p0_ = s0 ? PS : LS;
+        ls_w0_ = s0 ? WS : WLS;
         FwdOut o[3];
         for (int a = 0; a < 3; ++a) {
             o[a].phys_out = LS + a;
             o[a].spec = wspec(WLS + a);
             o[a].spec_f64 = wf64<T>();
         }
-        fwd(b2, FLSS{}, ud, {o[0], o[1], o[2]});
+        if (s0)
+            fwd(b2, FLSS12{}, ud, {o[1], o[2]});
+        else
+            fwd(b2, FLSS{}, ud, {o[0], o[1], o[2]});
     }
     // P2 of the coefficients of W_j = sum_i phi_i d_j phi_i (calc_vgraduvgradu /
     // calc_vvgradu, v = phi).  W_j = (1/2) d_j |phi|^2, and when the cut c
@@ -2053,7 +2081,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
             for (int j = 0; j < 3; ++j) {
                 InvOut o;
                 o.nsrc = 1;
-                o.src[0] = ZSrc{wspec(WLS + a), wf64<T>(), SYM_IKX + j, 0, 0.5};
+                o.src[0] = ZSrc{wspec(ls_wspec(a)), wf64<T>(), SYM_IKX + j, 0, 0.5};
                 o.phys_out = LV + 3 * a + j;
                 g.push_back(o);
             }
@@ -2107,9 +2135,10 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     {
         std::vector<std::pair<const cpx<T>*, const cpx<T>*>> p1, p2, p3;
         for (int i = 0; i < 3; ++i)
-            for (int a = 0; a < 3; ++a) (i < 2 ? p1 : p2).push_back({wspec(WLS + i), wspec(WLG + a)});
+            for (int a = 0; a < 3; ++a) (i < 2 ? p1 : p2).push_back({wspec(ls_wspec(i)), wspec(WLG + a)});
         for (int i = 0; i < 3; ++i)
-            for (int j = i; j < 3; ++j) (p2.size() < 6 ? p2 : p3).push_back({wspec(WLS + i), wspec(WLS + j)});
+            for (int j = i; j < 3; ++j)
+                (p2.size() < 6 ? p2 : p3).push_back({wspec(ls_wspec(i)), wspec(ls_wspec(j))});
         sdots(*this, p1, 140);
         sdots(*this, p2, 146);
         sdots(*this, p3, 152);
@@ -2124,10 +2153,10 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
         for (int z0 = 0; z0 < n; z0 += (slab_ ? zs_ : n)) {
             const T* s[3];
             if (slab_) {
-                const std::vector<const T*> p = expand_many({LS, LS + 1, LS + 2}, z0);
+                const std::vector<const T*> p = expand_many({ls_phys(0), ls_phys(1), ls_phys(2)}, z0);
                 for (int a = 0; a < 3; ++a) s[a] = p[a];
             } else {
-                for (int a = 0; a < 3; ++a) s[a] = phys(LS + a);
+                for (int a = 0; a < 3; ++a) s[a] = phys(ls_phys(a));
             }
             ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(s[0], s[1], s[2], npts, d_partials);
             launched();
@@ -2170,10 +2199,10 @@ bool Engine<T>::ls_clamp_free(double tau) {
         for (int z0 = 0; z0 < n; z0 += (slab_ ? zs_ : n)) {
             const T* sp[3];
             if (slab_) {
-                const std::vector<const T*> p = expand_many({LS, LS + 1, LS + 2}, z0);
+                const std::vector<const T*> p = expand_many({ls_phys(0), ls_phys(1), ls_phys(2)}, z0);
                 for (int a = 0; a < 3; ++a) sp[a] = p[a];
             } else {
-                for (int a = 0; a < 3; ++a) sp[a] = phys(LS + a);
+                for (int a = 0; a < 3; ++a) sp[a] = phys(ls_phys(a));
             }
             cudaEvent_t ev = prof_mark();
             ls_min_kernel<T><<<grid, RED_THREADS, 0, stream>>>(sp[0], sp[1], sp[2], npts, tau, d_partials);
@@ -2222,7 +2251,7 @@ void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
     }
     FLSA f;
     f.tau = tau;
-    fwd(b2, f, {LS, LS + 1, LS + 2}, {o}, 130);
+    fwd(b2, f, {ls_phys(0), ls_phys(1), ls_phys(2)}, {o}, 130);
     fetch_results();
     const double* r = h_results + 130;
     const double I1 = r[1] + tau * (r[2] + tau * r[3]);

@@ -367,6 +367,17 @@ struct FLSS {
     }
 };
 
+// The tau^1 and tau^2 coefficients of |phi|^2 alone (the tau^0 one, |u|^2, is
+// the gradient program's S).  inputs u(3), d(3)
+struct FLSS12 {
+    static constexpr int NIN = 6, NOUT = 2, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        out[0] = T(2) * (in[0] * in[3] + in[1] * in[4] + in[2] * in[5]);
+        out[1] = in[3] * in[3] + in[4] * in[4] + in[5] * in[5];
+    }
+};
+
 // Coefficients of W_j = sum_i phi_i d_j phi_i in tau.  A = 0: v_i d_j v_i,
 // inputs v(3), Dv(9) (the tau^0 term with v = u, the tau^2 term with v = d);
 // A = 1: the tau^1 term u_i d_j d_i + d_i d_j u_i, inputs u(3), Du(9), d(3), Dd(9).
