@@ -1603,12 +1603,13 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
             f.coef = d_coef_;
             pointwise(f, in, out);
             const long nsp = (long)b.nb * b.nb * b.nx;
-            for (int w : {WA, WS}) {
-                cudaEvent_t ev = prof_mark();
+            const int ws2[2] = {WA, WS};
+            for (int w : ws2) {
+                cudaEvent_t ew = prof_mark();
                 spec_scale_pow_kernel<cpx<T>><<<grid_for(nsp, 256), 256, 0, stream>>>(wspec(w), wspec(w), nsp, d_coef_, 2);
-                launched("spec_scale", 2.0 * nsp * sizeof(cpx<T>), ev);
+                launched("spec_scale", 2.0 * nsp * sizeof(cpx<T>), ew);
             }
-            ev = prof_mark();
+            cudaEvent_t ev = prof_mark();
             spec_scale_pow_kernel<double2><<<grid_for(3 * nc, 256), 256, 0, stream>>>(c, c_tmp_, 3 * nc, d_coef_, 3);
             launched("spec_scale", 2.0 * 3 * nc * sizeof(double2), ev);
         } else {
