@@ -294,9 +294,12 @@ struct YShape {
     // V: 0 default; 1 the other element count; 2 the other tile width;
     // 3 and 4 as 0 and 1 with the stage twiddles held in registers;
     // 5 and 6 column-per-warp (CW): one warp transforms one column, 32
-    // threads x N/32 elements, tiles of 8 or 16 (FP32) / 4 or 2 (FP64) columns
-    static constexpr bool CW = V >= 5;
-    static constexpr int VB = CW ? 0 : (V >= 3 ? V - 3 : V);
+    // threads x N/32 elements, tiles of 8 or 16 (FP32) / 4 or 2 (FP64) columns;
+    // 7 the shape of 0 compiled for three resident blocks (fewer registers,
+    // more warps to hide latency)
+    static constexpr bool CW = V == 5 || V == 6;
+    static constexpr bool MB3 = V == 7;
+    static constexpr int VB = (CW || MB3) ? 0 : (V >= 3 ? V - 3 : V);
     static constexpr int EY = CW ? N / 32 : (VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8)));
     static constexpr int TX = CW ? (V == 5 ? (F32 ? 8 : 4) : (F32 ? 16 : 2))
                                  : (VB == 0 ? CShape<N, T>::TX : (VB == 1 ? 8 : (F32 ? 16 : 4)));
@@ -320,10 +323,11 @@ struct YShape {
     static constexpr int CW_RGB = 65536 / (YTHREADS * 96);
     static constexpr int CW_MINB = CW_SMB < CW_RGB ? CW_SMB : CW_RGB;
     static constexpr int YMINB = CW ? (CW_MINB < 1 ? 1 : CW_MINB)
-                                    : (TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1)));
+                                    : MB3 ? 3 : (TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1)));
     static constexpr bool valid =
         V == 0 ||
-        (CW ? (N >= 256 && EY >= 2 && EY <= 16 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 227 * 1024)
+        (MB3 ? (N >= 256 && YTHREADS <= 256 && 3 * (ZSMEM + 1024) <= 228 * 1024) :
+         CW ? (N >= 256 && EY >= 2 && EY <= 16 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 227 * 1024)
             : (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
                (V >= 3 || EY != CShape<N, T>::EY || TX != CShape<N, T>::TX) && (V != 4 || F32)));
     static_assert(V != 0 || ZSMEM <= 200 * 1024, "default y/z tile fits the shared-memory limit");

@@ -227,6 +227,9 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
     if constexpr (YShape<NN, T, 6>::valid) {
         if (v == 6) return f(std::integral_constant<int, 6>{});
     }
+    if constexpr (YShape<NN, T, 7>::valid) {
+        if (v == 7) return f(std::integral_constant<int, 7>{});
+    }
     f(std::integral_constant<int, 0>{});
 }
 
@@ -276,7 +279,7 @@ void Engine<T>::tune_yz() {
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid || YShape<NN, T, 3>::valid ||
-              YShape<NN, T, 5>::valid || YShape<NN, T, 6>::valid;
+              YShape<NN, T, 5>::valid || YShape<NN, T, 6>::valid || YShape<NN, T, 7>::valid;
     });
     if (!any) return;
     if (const char* e = std::getenv("MLQ_YZ_VARIANT")) {  // fixed variant (measurement runs)
@@ -286,7 +289,8 @@ void Engine<T>::tune_yz() {
             constexpr int NN = decltype(nc)::value;
             ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid) ||
                  (v == 3 && YShape<NN, T, 3>::valid) || (v == 4 && YShape<NN, T, 4>::valid) ||
-                 (v == 5 && YShape<NN, T, 5>::valid) || (v == 6 && YShape<NN, T, 6>::valid);
+                 (v == 5 && YShape<NN, T, 5>::valid) || (v == 6 && YShape<NN, T, 6>::valid) ||
+                 (v == 7 && YShape<NN, T, 7>::valid);
         });
         if (ok)
             for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
@@ -349,8 +353,8 @@ void Engine<T>::tune_yz() {
         });
         MLQ_CUDA(cudaGetLastError());
     };
-    constexpr int NV = 7;
-    bool valid[NV] = {true, false, false, false, false, false, false};
+    constexpr int NV = 8;
+    bool valid[NV] = {true, false, false, false, false, false, false, false};
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         valid[1] = YShape<NN, T, 1>::valid;
@@ -359,6 +363,7 @@ void Engine<T>::tune_yz() {
         valid[4] = YShape<NN, T, 4>::valid;
         valid[5] = YShape<NN, T, 5>::valid;
         valid[6] = YShape<NN, T, 6>::valid;
+        valid[7] = YShape<NN, T, 7>::valid;
     });
     // every variant of every kind once first (clocks, attributes, page-in)
     for (int kind = 0; kind < YV_KINDS; ++kind)

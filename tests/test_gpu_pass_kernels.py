@@ -113,7 +113,7 @@ def _variant_run(n, precision, variant, monkeypatch):
 _VARIANT0 = {}
 
 
-@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("variant", [1, 2, 3, 4, 5, 6, 7])
 @pytest.mark.parametrize("n,precision,tol", [(256, "fp64", 1e-12), (256, "mixed", 2e-6)])
 def test_yz_tile_variants_match_default(n, precision, tol, variant, monkeypatch):
     """Every y/z tile-shape variant the autotuner may pick (including the
