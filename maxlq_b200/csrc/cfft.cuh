@@ -197,17 +197,6 @@ __device__ __forceinline__ void cp_async_elem(cpx<T>* sdst, const cpx<T>* gsrc, 
                      : "memory");
     }
 }
-// Asynchronous copy of SZ = 8 or 16 bytes, zero-filled when `valid` is false
-// (the source address must still be a mapped one).
-template <int SZ>
-__device__ __forceinline__ void cp_async_bytes(void* sdst, const void* gsrc, bool valid) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
-    if constexpr (SZ == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0) : "memory");
-    else
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 16 : 0)
-                     : "memory");
-}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
@@ -327,9 +316,6 @@ struct YShape {
     static constexpr size_t ZSMEM = YSMEM + 2 * N * sizeof(T);
     static constexpr size_t ZISMEM =
         CW ? ZSMEM : ((size_t)N * TX + N) * sizeof(cpx<T>) + 2 * N * sizeof(T);  // z inverse: one tile
-    // z inverse, single-source launches: the next column tile's spectrum
-    // (FP64 or FP32 elements, 16-byte slots) staged ahead
-    static constexpr size_t ZISTG = (size_t)N * TX * 16;
     // resident blocks the register budget aims at (8 elements per thread in
     // FP32 leave room for two 512-thread blocks: 64 registers); CW: as many
     // blocks as the shared memory holds, keeping at least 96 registers
@@ -941,10 +927,6 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
     cpx<T>* stw = sm + N * TX;
     C* kt = reinterpret_cast<C*>(stw + N);
-    // staged spectrum: slot (p, l) holds this thread's own element (each
-    // thread reads what it copied); the next item's copies are issued after
-    // the transform, whose barriers follow the reads
-    unsigned char* stg = reinterpret_cast<unsigned char*>(kt + 2 * N);
     for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
     fill_k_table<N>(kt);
     __syncthreads();
@@ -958,25 +940,6 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const int plane = nb * nx;
     const int nsrc = op.nsrc;
     cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out);
-    static_assert(CPlan<N, E>::NST >= 2, "the prefetch relies on the transform's barriers");
-    const bool staged = a.staged != 0;  // uniform over the launch (every op has one source)
-    const int sf64 = op.src[0].f64;
-    auto stage = [&](long it2) {
-        const int cy2 = (int)(it2 / ntile);
-        const int kx2 = (int)(it2 - (long)cy2 * ntile) * TX + l;
-        const bool ok2 = kx2 < nx;
-        const ZCol<N, TPL> id2{t, cut, nb, plane, cy2 * nx + (ok2 ? kx2 : nx - 1), ok2};
-#pragma unroll
-        for (int m = 0; m < E; ++m) {
-            unsigned char* d = stg + ((size_t)(t + TPL * m) * TX + l) * 16;
-            if (sf64)
-                cp_async_bytes<16>(d, reinterpret_cast<const double2*>(op.src[0].spec) + id2(m), id2.valid(m));
-            else
-                cp_async_bytes<8>(d, reinterpret_cast<const float2*>(op.src[0].spec) + id2(m), id2.valid(m));
-        }
-        cp_async_commit();
-    };
-    if (staged && (long)blockIdx.x < items) stage(blockIdx.x);
     for (long it = blockIdx.x; it < items; it += gridDim.x) {
         const int cy = (int)(it / ntile);
         const int kx = (int)(it - (long)cy * ntile) * TX + l;
@@ -990,47 +953,22 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         cpx<C> Y[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) Y[m] = mk(C(0), C(0));
-        if (staged) {
-            cp_async_wait_all();
-            cpx<C> Vs[E];
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const unsigned char* sp = stg + ((size_t)(t + TPL * m) * TX + l) * 16;
-                if (sf64) {
-                    const double2 w = *reinterpret_cast<const double2*>(sp);
-                    Vs[m] = mk((C)w.x, (C)w.y);
-                } else {
-                    const float2 w = *reinterpret_cast<const float2*>(sp);
-                    Vs[m] = mk((C)w.x, (C)w.y);
-                }
-            }
-            const SymD<C> d = make_symd<C>(op.src[0].sym, op.src[0].ab, op.src[0].coef);
-#pragma unroll
-            for (int m = 0; m < E; ++m) {
-                const int fz = t + TPL * m;
-                const C kz = kt[fz], oz = kt[N + fz];
-                const C ksq = kxy2 + kz * kz;
-                const C ri = d.inv ? rinv_of(ksq) : C(0);
-                if (idx.valid(m)) Y[m] = sym_apply(d, ox, oy, oz, ksq, ri, Vs[m]);
-            }
-        } else {
 #pragma unroll 1
-            for (int s = 0; s < nsrc; ++s) {
-                const void* spec = op.src[s].spec;
-                const int f64 = op.src[s].f64;
-                const SymD<C> d = make_symd<C>(op.src[s].sym, op.src[s].ab, op.src[s].coef);
+        for (int s = 0; s < nsrc; ++s) {
+            const void* spec = op.src[s].spec;
+            const int f64 = op.src[s].f64;
+            const SymD<C> d = make_symd<C>(op.src[s].sym, op.src[s].ab, op.src[s].coef);
 #pragma unroll
-                for (int m0 = 0; m0 < E; m0 += CH) {
-                    cpx<C> V[CH];
-                    ld_chunk<CH>(spec, f64, idx, m0, V);
+            for (int m0 = 0; m0 < E; m0 += CH) {
+                cpx<C> V[CH];
+                ld_chunk<CH>(spec, f64, idx, m0, V);
 #pragma unroll
-                    for (int j = 0; j < CH; ++j) {
-                        const int fz = t + TPL * (m0 + j);
-                        const C kz = kt[fz], oz = kt[N + fz];
-                        const C ksq = kxy2 + kz * kz;
-                        const C ri = d.inv ? rinv_of(ksq) : C(0);
-                        if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(d, ox, oy, oz, ksq, ri, V[j]);
-                    }
+                for (int j = 0; j < CH; ++j) {
+                    const int fz = t + TPL * (m0 + j);
+                    const C kz = kt[fz], oz = kt[N + fz];
+                    const C ksq = kxy2 + kz * kz;
+                    const C ri = d.inv ? rinv_of(ksq) : C(0);
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(d, ox, oy, oz, ksq, ri, V[j]);
                 }
             }
         }
@@ -1038,9 +976,6 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
 #pragma unroll
         for (int m = 0; m < E; ++m) v[m] = mk((T)Y[m].x, (T)Y[m].y);
         cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
-        // the transform's barriers order this thread's reads of its slots
-        // before the copies that refill them
-        if (staged && it + gridDim.x < items) stage(it + gridDim.x);
         if (ok) {
 #pragma unroll
             for (int m = 0; m < E; ++m) dst[(t + TPL * m) * plane + col] = v[m];

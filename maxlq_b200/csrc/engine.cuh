@@ -412,7 +412,7 @@ class Engine : public EngineBase {
     // kernels specialised at compile time for n in {64, ..., 1024} (cfft.cuh)
     bool cfft_ok_ = false;
     int persistent_blocks(const void* kernel, int threads, size_t smem);
-    std::map<std::pair<const void*, size_t>, int> occ_;  // resident blocks by (kernel, shared bytes)
+    std::map<const void*, int> occ_;
     int num_sms_ = 148;
     template <int NN>
     void xinv_c(XInvArgs<T>& xa, int narr);

@@ -116,13 +116,12 @@ int Engine<T>::reg_lx(int nrows_per_line, size_t pitch) const {
 // resident blocks of a kernel on the whole device (occupancy x SMs), cached
 template <typename T>
 int Engine<T>::persistent_blocks(const void* kernel, int threads, size_t smem) {
-    const auto key = std::make_pair(kernel, smem);
-    auto it = occ_.find(key);
+    auto it = occ_.find(kernel);
     if (it != occ_.end()) return it->second;
     int nb = 0;
     MLQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, threads, smem));
     if (nb < 1) throw CudaError("pass kernel does not fit on an SM", MLQ_ERR_CUDA);
-    occ_[key] = nb * num_sms_;
+    occ_[kernel] = nb * num_sms_;
     return nb * num_sms_;
 }
 
@@ -191,18 +190,10 @@ template <typename T>
 template <int NN, int V>
 void Engine<T>::zinv_cv(ZInvArgs<T>& za, int narr) {
     using S = YShape<NN, T, V>;
+    const size_t smem = S::ZISMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
     auto run = [&](auto kern) {
         allow_smem(kern);
-        // prefetch the next column only where its buffer costs no resident block
-        size_t smem = S::ZISMEM;
-        if (!S::CW && za.staged) {
-            if (persistent_blocks((const void*)kern, S::YTHREADS, S::ZISMEM + S::ZISTG) >=
-                persistent_blocks((const void*)kern, S::YTHREADS, S::ZISMEM))
-                smem += S::ZISTG;
-            else
-                za.staged = 0;
-        }
         const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
         dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
         kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
@@ -329,7 +320,6 @@ void Engine<T>::tune_yz() {
     zi.n = n;
     zi.nx = b.nx;
     zi.band = b;
-    zi.staged = 1;  // one source per array, as most programs' launches
     for (int a = 0; a < NA; ++a) {
         yf.in[a] = A + a * xs_n;
         yf.out[a] = B + a * ys_n;
@@ -582,8 +572,6 @@ void Engine<T>::launch_zfwd(ZFwdArgs<T>& za, int narr, const Band& b, bool any_r
 template <typename T>
 void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zbytes) {
     if (cfft_ok_) {
-        za.staged = 1;
-        for (int i = 0; i < narr; ++i) za.staged &= za.op[i].nsrc == 1 ? 1 : 0;
         cudaEvent_t ev = prof_mark();
         dispatch_n(n, [&](auto nc) { this->template zinv_c<decltype(nc)::value>(za, narr); });
         launched("z_inv", zbytes, ev);

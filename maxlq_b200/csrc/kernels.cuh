@@ -503,7 +503,6 @@ struct ZInvArgs {
     ZInvOp op[MAX_ARR];
     FftPlan plan;
     const cpx<double>* tw;
-    int staged = 0;  // every op has one source: its next column is prefetched (compile-time kernels)
 };
 
 template <typename T>
