@@ -154,6 +154,10 @@ class EngineBase {
     std::map<std::string, ProgGraph> graphs_;
     long graph_gen_ = 0;
     bool graphs_on_ = true;
+    // the exact-arithmetic reuse paths (fields formed pointwise or from the
+    // line search's coefficients, W as half-gradients of |phi|^2); MLQ_REUSE=0
+    // runs every program in its plain transform sequence instead
+    bool reuse_on_ = true;
     long long graph_launches_ = 0;  // graphs launched (replays)
     template <class Fn>
     void as_graph(const std::string& name, const std::vector<const void*>& key, Fn&& body);

@@ -1229,7 +1229,7 @@ int Engine<T>::ls_wspec(int a) const {
 // memo holds them; records the transport fields (tr) for the next gradient
 template <typename T>
 bool Engine<T>::w_from_memo(const double2* u, const double2* d, double tau) {
-    if (slab_ || !d || !pm_.ls || pm_.u != (const void*)u || pm_.d != (const void*)d) {
+    if (slab_ || !reuse_on_ || !d || !pm_.ls || pm_.u != (const void*)u || pm_.d != (const void*)d) {
         pm_ = PhysMemo{};
         return false;
     }
@@ -1556,7 +1556,7 @@ template <typename T>
 void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
     if (!c) throw CudaError("grad_l2 needs a spectrum buffer for |u|^{q-2}u", MLQ_ERR_BADARG);
     // u = cs w from the last line search's transport: u and grad u pointwise
-    const bool rt = !slab_ && pm_.tr && pm_.next == (const void*)u;
+    const bool rt = !slab_ && reuse_on_ && pm_.tr && pm_.next == (const void*)u;
     if (rt) {
         if (!d_coef_) d_coef_ = (double*)dev_alloc(2 * sizeof(double));
         const double h[2] = {pm_.cs, pm_.tau};
@@ -2025,7 +2025,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     const long nc = spec_ncomp();
     // u and grad u are still in PU, PD when the gradient program of this
     // iteration transformed the same spectrum
-    const bool reuse_u = !slab_ && pu_of_ == (const void*)u;
+    const bool reuse_u = !slab_ && reuse_on_ && pu_of_ == (const void*)u;
     if (slab_) release_slots(0, LU);  // the programs' fields are rebuilt by the next program
     const int iu = reuse_u ? PU : LU, idu = reuse_u ? PD : LDU;
     // phi's pieces: u, d and their gradients (function_ops.f90:3147-3195)
@@ -2040,7 +2040,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
                 io.push_back(o);
             }
     inv(b2, io);
-    if (!slab_) {
+    if (!slab_ && reuse_on_) {
         pm_ = PhysMemo{};
         pm_.u = u;
         pm_.d = d;
@@ -2060,7 +2060,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     // P2 of the coefficients of |phi|^2 (calc_uk 2332-2333).  The tau^0 one,
     // P2(|u|^2), is the gradient program's S when it ran for this u.
     {
-        const bool s0 = !slab_ && ws_of_ == (const void*)u;
+        const bool s0 = !slab_ && reuse_on_ && ws_of_ == (const void*)u;
         ls_p0_ = s0 ? PS : LS;
         ls_w0_ = s0 ? WS : WLS;
         FwdOut o[3];
@@ -2081,7 +2081,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     // the cut), so P2(W_j) = (1/2) d_j P2(|phi|^2): the derivatives of the
     // S_a spectra just formed.  For 3c >= N (N divisible by 3) the products
     // are formed and dealiased as the reference does.
-    if (3 * b2.cut < n) {
+    if (reuse_on_ && 3 * b2.cut < n) {
         std::vector<InvOut> g;
         for (int a = 0; a < 3; ++a)
             for (int j = 0; j < 3; ++j) {
