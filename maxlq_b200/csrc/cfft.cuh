@@ -960,15 +960,15 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
             const SymD<C> d = make_symd<C>(op.src[s].sym, op.src[s].ab, op.src[s].coef);
 #pragma unroll
             for (int m0 = 0; m0 < E; m0 += CH) {
-                cpx<C> V[CH];
-                ld_chunk<CH>(spec, f64, idx, m0, V);
+                cpx<C> Vv[CH];
+                ld_chunk<CH>(spec, f64, idx, m0, Vv);
 #pragma unroll
                 for (int j = 0; j < CH; ++j) {
                     const int fz = t + TPL * (m0 + j);
                     const C kz = kt[fz], oz = kt[N + fz];
                     const C ksq = kxy2 + kz * kz;
                     const C ri = d.inv ? rinv_of(ksq) : C(0);
-                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(d, ox, oy, oz, ksq, ri, V[j]);
+                    if (idx.valid(m0 + j)) Y[m0 + j] = Y[m0 + j] + sym_apply(d, ox, oy, oz, ksq, ri, Vv[j]);
                 }
             }
         }

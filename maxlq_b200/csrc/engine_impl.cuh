@@ -2027,7 +2027,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     // iteration transformed the same spectrum
     const bool reuse_u = !slab_ && reuse_on_ && pu_of_ == (const void*)u;
     if (slab_) release_slots(0, LU);  // the programs' fields are rebuilt by the next program
-    const int iu = reuse_u ? PU : LU, idu = reuse_u ? PD : LDU;
+    const int iu = reuse_u ? (int)PU : (int)LU, idu = reuse_u ? (int)PD : (int)LDU;
     // phi's pieces: u, d and their gradients (function_ops.f90:3147-3195)
     std::vector<InvOut> io;
     for (int f = reuse_u ? 1 : 0; f < 2; ++f)
@@ -2061,7 +2061,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
     // P2(|u|^2), is the gradient program's S when it ran for this u.
     {
         const bool s0 = !slab_ && reuse_on_ && ws_of_ == (const void*)u;
-        ls_p0_ = s0 ? PS : LS;
+        ls_p0_ = s0 ? (int)PS : (int)LS;
         ls_w0_ = s0 ? WS : WLS;
         FwdOut o[3];
         for (int a = 0; a < 3; ++a) {
