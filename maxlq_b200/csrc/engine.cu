@@ -307,12 +307,47 @@ void EngineBase::hilbert_leray(double2* f, double order, double scale) {
     launched("spec_hilbert_leray", 96.0 * g.ncomp, ev);
 }
 
-void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
+void EngineBase::hilbert_leray_pair_dots(double2* f1, double2* f2, double order, double s2, double out[2]) {
+    state_written(f1);
+    state_written(f2);
+    SpecGeom g = geom(b2);
+    const double* t = hilbert_table(order);
+    const double* hw = hweight_table(1.5 - 1.0 / P.q);  // (3/2)-(1/q), function_ops.f90:3467
+    const int grid = spec_rows_grid(g);
+    ensure_partials((long)grid * 2);
+    cudaEvent_t ev = prof_mark();
+    spec_hilbert_leray_pair_dot_kernel<<<grid, 128, 0, stream>>>(g, f1, 1.0, f2, s2, t, hw, d_partials);
+    launched("spec_hilbert_leray", 2 * 96.0 * g.ncomp, ev);
+    finalize(grid, 2, 1.0, 200);
+    fetch_results();
+    out[0] = h_results[200];
+    out[1] = h_results[201];
+}
+
+void EngineBase::direction(double2* gv, double sg, double2* d, double beta, const double2* td) {
+    state_written(gv);
+    state_written(d);
+    SpecGeom g = geom(b2);
+    const long nt = 3 * g.ncomp;
+    cudaEvent_t ev = prof_mark();
+    spec_direction_kernel<<<grid_for(nt, 256), 256, 0, stream>>>(nt, gv, sg, d, td ? beta : 0.0, td);
+    launched("spec_lincomb", 16.0 * nt * (3 + (td ? 1 : 0)), ev);
+}
+
+void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, double2* ax_out, const double2* ax_x,
+                      double ax_a, const double2* ax_y) {
     if (np < 1 || np > 8) throw CudaError("dots: 1 to 8 pairs per call", MLQ_ERR_BADARG);
     SpecDotArgs a;
     a.g = geom(b2);
     for (int i = 0; i < np; ++i) a.pr[i] = pairs[i];
     a.npairs = np;
+    if (ax_out) {
+        state_written(ax_out);
+        a.ax_out = ax_out;
+        a.ax_x = ax_x;
+        a.ax_y = ax_y;
+        a.ax_a = ax_a;
+    }
     bool need_h = false;
     for (int i = 0; i < np; ++i) need_h |= pairs[i].kind == 1;
     a.hwtab = need_h ? hweight_table(1.5 - 1.0 / P.q) : nullptr;  // (3/2)-(1/q), function_ops.f90:3467
@@ -336,7 +371,12 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out) {
             uniq.insert(pairs[i].a);
             if (pairs[i].kind != 2) uniq.insert(pairs[i].b);
         }
-        launched("spec_dot", 48.0 * a.g.ncomp * uniq.size(), ev);
+        if (ax_out) {  // x, y read, ax_out written (and read back from cache by the pairs)
+            uniq.erase(ax_out);
+            uniq.insert(ax_x);
+            uniq.insert(ax_y);
+        }
+        launched("spec_dot", 48.0 * a.g.ncomp * (uniq.size() + (ax_out ? 1 : 0)), ev);
     }
     finalize(grid, 8, 1.0, 200);
     fetch_results();

@@ -82,7 +82,14 @@ class EngineBase {
     const double* hilbert_table(double order);
     const double* hweight_table(double order);
     // up to 6 vector inner products; kinds 0 L2, 1 H_l, 2 div energy
-    void dots(const SpecDotPair* pairs, int np, double* out);
+    // pairs' inner products; optionally ax_out <- ax_x + ax_a ax_y first, in
+    // the same pass (the pairs may name ax_out)
+    void dots(const SpecDotPair* pairs, int np, double* out, double2* ax_out = nullptr,
+              const double2* ax_x = nullptr, double ax_a = 0.0, const double2* ax_y = nullptr);
+    // hilbert_leray of f1 (scale 1) and f2 (scale s2), then out = {<f2, f1>_H, <f2, f2>_H}
+    void hilbert_leray_pair_dots(double2* f1, double2* f2, double order, double s2, double out[2]);
+    // g <- sg g, d <- g + beta td (td null: d <- g)
+    void direction(double2* g, double sg, double2* d, double beta, const double2* td);
     void zeroth(const double2* f, double out[3]);
 
     void finalize(int nblocks, int nr, double scale, int dst, bool accumulate = false);

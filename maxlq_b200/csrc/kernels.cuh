@@ -642,6 +642,27 @@ struct SpecRow {
 // the Hilbert gradient symbol s = 1/(1+(lambda1|K|)^(2 order))
 // (function_ops.f90:3611) read from a table indexed by |j|^2, and divAvg_free
 // (2843-2918): u - K(K.u)/|K|^2 (odd factors), k = 0 -> 0.
+// f <- Leray(s f) at one mode (ox, oy, oz: the odd-factor wavenumbers, 0 at a
+// Nyquist index; ksq = |K|^2), the mode k = 0 set to 0
+__device__ __forceinline__ void hilbert_leray_point(double2& u0, double2& u1, double2& u2, double s, bool leray,
+                                                    double ox, double oy, double oz, double ksq) {
+    u0.x *= s; u0.y *= s;
+    u1.x *= s; u1.y *= s;
+    u2.x *= s; u2.y *= s;
+    if (leray) {
+        if (ksq > MACH_EPSILON) {
+            const double dr = ox * u0.x + oy * u1.x + oz * u2.x;
+            const double di = ox * u0.y + oy * u1.y + oz * u2.y;
+            const double is = 1.0 / ksq;
+            u0.x -= ox * dr * is; u0.y -= ox * di * is;
+            u1.x -= oy * dr * is; u1.y -= oy * di * is;
+            u2.x -= oz * dr * is; u2.y -= oz * di * is;
+        } else {
+            u0 = u1 = u2 = make_double2(0.0, 0.0);
+        }
+    }
+}
+
 static __global__ void spec_hilbert_leray_kernel(SpecGeom g, double2* f, const double* __restrict__ htab,
                                                  double scale, int do_leray) {
     const double twopi = 2.0 * 3.14159265358979311600;
@@ -650,35 +671,80 @@ static __global__ void spec_hilbert_leray_kernel(SpecGeom g, double2* f, const d
         const SpecRow row(g, r);
         const long base = (long)r * g.nx;
         const double ky = twopi * (double)row.jy, kz = twopi * (double)row.jz;
+        const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
+        const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
         for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
             const long i = base + fx;
             double2 u0 = f[i], u1 = f[g.ncomp + i], u2 = f[2 * g.ncomp + i];
             double s = scale;
             if (htab) s *= htab[fx * fx + row.jy * row.jy + row.jz * row.jz];
-            u0.x *= s; u0.y *= s;
-            u1.x *= s; u1.y *= s;
-            u2.x *= s; u2.y *= s;
-            if (do_leray) {
-                const double kx = twopi * (double)fx;
-                const double ox = (2 * fx == g.n) ? 0.0 : kx;
-                const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
-                const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
-                const double ksq = kx * kx + ky * ky + kz * kz;
-                if (ksq > MACH_EPSILON) {
-                    const double dr = ox * u0.x + oy * u1.x + oz * u2.x;
-                    const double di = ox * u0.y + oy * u1.y + oz * u2.y;
-                    const double is = 1.0 / ksq;
-                    u0.x -= ox * dr * is; u0.y -= ox * di * is;
-                    u1.x -= oy * dr * is; u1.y -= oy * di * is;
-                    u2.x -= oz * dr * is; u2.y -= oz * di * is;
-                } else {
-                    u0 = u1 = u2 = make_double2(0.0, 0.0);
-                }
-            }
+            const double kx = twopi * (double)fx;
+            const double ox = (2 * fx == g.n) ? 0.0 : kx;
+            hilbert_leray_point(u0, u1, u2, s, do_leray != 0, ox, oy, oz, kx * kx + ky * ky + kz * kz);
             f[i] = u0;
             f[g.ncomp + i] = u1;
             f[2 * g.ncomp + i] = u2;
         }
+    }
+}
+
+// Hilbert gradient + Leray projection of two fields (f1 scaled by s1, f2 by
+// s2) and, on the results, the H inner products <f2, f1> and <f2, f2> (the
+// weights of spec_dot_kernel's kind 1) as per-block partials [block][2]
+static __global__ void __launch_bounds__(128) spec_hilbert_leray_pair_dot_kernel(SpecGeom g, double2* f1, double s1,
+                                                                              double2* f2, double s2,
+                                                                              const double* __restrict__ htab,
+                                                                              const double* __restrict__ hwtab,
+                                                                              double* partials) {
+    const double twopi = 2.0 * 3.14159265358979311600;
+    const int nrows = g.nb * g.nb;
+    double acc[2] = {0.0, 0.0};
+    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+        const SpecRow row(g, r);
+        const long base = (long)r * g.nx;
+        const double ky = twopi * (double)row.jy, kz = twopi * (double)row.jz;
+        const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
+        const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
+        const int jyz = row.jy * row.jy + row.jz * row.jz;
+        for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
+            const long i = base + fx;
+            double2 a0 = f1[i], a1 = f1[g.ncomp + i], a2 = f1[2 * g.ncomp + i];
+            double2 b0 = f2[i], b1 = f2[g.ncomp + i], b2 = f2[2 * g.ncomp + i];
+            const double h = htab[fx * fx + jyz];
+            const double kx = twopi * (double)fx;
+            const double ox = (2 * fx == g.n) ? 0.0 : kx;
+            const double ksq = kx * kx + ky * ky + kz * kz;
+            hilbert_leray_point(a0, a1, a2, s1 * h, true, ox, oy, oz, ksq);
+            hilbert_leray_point(b0, b1, b2, s2 * h, true, ox, oy, oz, ksq);
+            f1[i] = a0;
+            f1[g.ncomp + i] = a1;
+            f1[2 * g.ncomp + i] = a2;
+            f2[i] = b0;
+            f2[g.ncomp + i] = b1;
+            f2[2 * g.ncomp + i] = b2;
+            const double w = kx_weight(g.n, fx) * hwtab[fx * fx + jyz];
+            acc[0] += w * ((b0.x * a0.x + b0.y * a0.y) + (b1.x * a1.x + b1.y * a1.y) + (b2.x * a2.x + b2.y * a2.y));
+            acc[1] += w * ((b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y) + (b2.x * b2.x + b2.y * b2.y));
+        }
+    }
+    block_reduce_store<2>(acc, partials, blockIdx.x);
+}
+
+// The search direction from the projected gradient: g <- sg g, then
+// d <- g + beta td (td may be null: d <- g)
+static __global__ void spec_direction_kernel(long nt, double2* g, double sg, double2* d, double beta,
+                                             const double2* td) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += (long)gridDim.x * blockDim.x) {
+        double2 v = g[i];
+        v.x *= sg;
+        v.y *= sg;
+        g[i] = v;
+        if (td) {
+            const double2 w = td[i];
+            v.x += beta * w.x;
+            v.y += beta * w.y;
+        }
+        d[i] = v;
     }
 }
 
@@ -694,6 +760,12 @@ struct SpecDotArgs {
     SpecGeom g;
     SpecDotPair pr[8];
     int npairs;
+    // optional ax_out <- ax_x + ax_a ax_y before the products (the pairs may
+    // read ax_out: each element is updated by the thread that then reads it)
+    double2* ax_out = nullptr;
+    const double2* ax_x = nullptr;
+    const double2* ax_y = nullptr;
+    double ax_a = 0.0;
     const double* hwtab;  // H_l weight (1+(lambda1|K|)^order)^2 by |j|^2 (function_ops.f90:3472), or null
     double* partials;
 };
@@ -720,6 +792,15 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
             const double wgt[2] = {kx_weight(g.n, fx), two ? kx_weight(g.n, fx1) : 0.0};
             const double hw[2] = {a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0, a.hwtab ? a.hwtab[fx1 * fx1 + jyz] : 1.0};
             const double ox[2] = {(2 * fx == g.n) ? 0.0 : twopi * (double)fx, (2 * fx1 == g.n) ? 0.0 : twopi * (double)fx1};
+            if (a.ax_out) {
+                for (int e = 0; e < (two ? 2 : 1); ++e)  // not twice when fx + 32 repeats fx
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        const long k = c * g.ncomp + i[e];
+                        const double2 x = a.ax_x[k], y = a.ax_y[k];
+                        a.ax_out[k] = make_double2(x.x + a.ax_a * y.x, x.y + a.ax_a * y.y);
+                    }
+            }
             for (int p = 0; p < a.npairs; ++p) {
                 const SpecDotPair& q = a.pr[p];
                 if (q.kind == 2) {

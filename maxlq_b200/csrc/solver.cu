@@ -301,18 +301,14 @@ class Solver : public SolverBase {
         double2* g1 = gu1;
         double lqq_u = 0;
         e.grad_l2(u, g1, c, &lqq_u);  // 146
-        e.hilbert_leray(g1, s);       // 151, 153
-        // normal of the tangent space: ||u||_q^{1-q} P2(|u|^{q-2} u) (162)
+        // Hilbert gradient of g (151, 153) and of the normal of the tangent
+        // space ||u||_q^{1-q} P2(|u|^{q-2} u) (162, 164, 169), with <c, g>
+        // and <c, c> (170-171) in the same pass
         const double unorm = std::pow(lqq_u, 1.0 / qq);
-        e.hilbert_leray(c, s, std::pow(unorm, 1.0 - qq));  // 162, 164, 169
-        double dd[6];
-        {
-            SpecDotPair p[2] = {{c, g1, 1}, {c, c, 1}};
-            e.dots(p, 2, dd);
-        }
+        double dd[2];
+        e.hilbert_leray_pair_dots(g1, c, s, std::pow(unorm, 1.0 - qq), dd);
         const double alpha = dd[0] / dd[1];  // 170-171
         info.alpha = alpha;
-        e.lincomb(g1, 1.0, g1, -alpha, c);  // gradJproj (177), kept in gu1
         if (!e.P.use_tangential_gradient) throw CudaError("useTangentialGradient=.false. is not supported",
                                                           MLQ_ERR_BADARG);
         // Every inner product the rest of the update needs, in one pass.  The
@@ -324,17 +320,15 @@ class Solver : public SolverBase {
         enum { GC, GDIV, GG, UU, GTG, G0G0, GTD, TDTD };
         double ip[8];
         {
+            // gradJproj g <- g - alpha c (177, kept in gu1) in the same pass
             SpecDotPair p[8] = {{g1, c, 1},    {g1, nullptr, 2}, {g1, g1, 1},   {u, u, 1},
                                 {g1, vtg0, 1}, {gu0, gu0, 1},    {g1, vtd0, 1}, {vtd0, vtd0, 1}};
-            e.dots(p, 8, ip);
+            e.dots(p, 8, ip, g1, g1, -alpha, c);
         }
         info.ortho_check = std::fabs(ip[GC] / (ip[GG] + 2.0 * ip[GC] + cc));  // <g,c> / <g+c, g+c>
         info.div_check = ip[GDIV] / ip[GG];
-        double sg = 1.0;  // gradient normalisation (213)
-        if (e.P.normalize_gradient) {
-            sg = std::sqrt(ip[UU] / ip[GG]);
-            e.lincomb(g1, sg, g1);
-        }
+        double sg = 1.0;  // gradient normalisation (213), applied with d1 below
+        if (e.P.normalize_gradient) sg = std::sqrt(ip[UU] / ip[GG]);
         const double gg = sg * sg * ip[GG], gtd = sg * ip[GTD];  // <g', g'>, <g', T d0>
         double beta = 0.0;
         if (e.P.use_conjugate_gradient) {
@@ -345,9 +339,9 @@ class Solver : public SolverBase {
             else
                 beta = beta / g0n;
             if (e.P.reset_momentum_every > 0 && iter % e.P.reset_momentum_every == 0) beta = 0.0;  // 235-238
-            e.lincomb(d1, 1.0, g1, beta, vtd0);                                                      // 240
+            e.direction(g1, sg, d1, beta, vtd0);                                                     // 213, 240
         } else {
-            e.lincomb(d1, 1.0, g1);
+            e.direction(g1, sg, d1, 0.0, nullptr);
         }
         info.beta = beta;
         info.norm_grad = std::sqrt(gg);
