@@ -36,6 +36,7 @@ extern "C" {
 #define MLQ_ERR_BADARG 8          /* invalid argument / unsupported configuration */
 #define MLQ_ERR_CUDA 9            /* other CUDA runtime error */
 #define MLQ_ERR_NOT_BANDLIMITED 10 /* input field has modes outside the 2/3 dealiasing cube */
+#define MLQ_ERR_IO 11             /* a file could not be opened, read or written, or is not netCDF-3 */
 
 /* precision of the transform pipeline; CG state and reductions are FP64 */
 #define MLQ_PREC_FP64 0
@@ -187,6 +188,24 @@ int mlq_seed_field(mlq_ctx* ctx, unsigned long long seed, double slope, double k
  * 0..c, -c..-1.  Returns c via *cut. */
 int mlq_seed_spectrum(int n, unsigned long long seed, double slope, double k0, double* spec, int* cut);
 int mlq_band_cut(int n, double order); /* largest |j| kept by a dealias of that order */
+
+/* ---- netCDF-3 classic field files (host only, no libnetcdf) ---------------- */
+/* save_field_R3toR3_ncdf (data_ops.f90:362-487, the parallel_data layout the
+ * reference uses for N >= 16): a CDF-1 file with dimensions "x" = n1, "y" = n2
+ * and an unlimited "z" holding n3 records, and three NC_DOUBLE record
+ * variables name1..3 of dimensions (z, y, x), no attributes.  u is the
+ * (n1, n2, n3, 3) column-major host field. */
+int mlq_ncdf_write_field(const char* path, int n1, int n2, int n3, const double* u, const char* name1,
+                         const char* name2, const char* name3);
+/* the lengths of the dimensions "x", "y", "z" of a classic or 64-bit-offset
+ * netCDF file (data_ops.f90:1237-1265) */
+int mlq_ncdf_read_dims(const char* path, int dims[3]);
+/* read_field_R3toR3_ncdf (data_ops.f90:1198-1397): the NC_DOUBLE variables
+ * name1..3 of dimensions (z, y, x), z a record or a fixed dimension, into the
+ * (n1, n2, n3, 3) column-major host field u.  MLQ_ERR_BADARG when a variable
+ * is missing, not NC_DOUBLE or of other dimensions. */
+int mlq_ncdf_read_field(const char* path, int n1, int n2, int n3, double* u, const char* name1, const char* name2,
+                        const char* name3);
 
 /* ---- allocation-free variant ----------------------------------------------- */
 /* No counterpart in the reference.  dealias_scalar for callers that cannot

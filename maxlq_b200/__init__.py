@@ -24,7 +24,8 @@ from ._capi import (  # noqa: F401
     load_library,
 )
 
-__all__ = ["MaxLq", "MlqError", "default_params", "band_cut", "seed_spectrum", "load_library"]
+__all__ = ["MaxLq", "MlqError", "default_params", "band_cut", "seed_spectrum", "load_library", "ncdf_write_field",
+           "ncdf_read_field"]
 
 _MODES = {"maxdLqdt": 0, "LineMin": 1, "||u||_q": 2}
 _INNER = {"L2": 0, "H_l^(3/2-1/q)": 1, "H": 1}
@@ -64,6 +65,35 @@ def seed_spectrum(n: int, seed: int, slope: float, k0: float):
     if st != MLQ_OK:
         raise MlqError(st, "mlq_seed_spectrum")
     return out[..., 0] + 1j * out[..., 1], cut.value
+
+
+def ncdf_write_field(path: str, u: np.ndarray, names=("Ux", "Uy", "Uz")) -> None:
+    """save_field_R3toR3_ncdf (data_ops.f90:362-487): u of shape (3, n3, n2, n1)
+    (the Fortran array U(1:n1, 1:n2, 1:n3, 1:3)) into a netCDF-3 classic file
+    with dimensions x, y and an unlimited z, as the reference writes it."""
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    if u.ndim != 4 or u.shape[0] != 3:
+        raise ValueError("ncdf_write_field needs a (3, n3, n2, n1) field")
+    _, n3, n2, n1 = u.shape
+    st = load_library().mlq_ncdf_write_field(str(path).encode(), n1, n2, n3, dptr(u), *(x.encode() for x in names))
+    if st != MLQ_OK:
+        raise MlqError(st, f"ncdf_write_field {path}")
+
+
+def ncdf_read_field(path: str, names=("Ux", "Uy", "Uz")) -> np.ndarray:
+    """read_field_R3toR3_ncdf (data_ops.f90:1198-1397): the three named
+    variables of a netCDF-3 file as a (3, n3, n2, n1) float64 field."""
+    lib = load_library()
+    dims = (C.c_int * 3)()
+    st = lib.mlq_ncdf_read_dims(str(path).encode(), dims)
+    if st != MLQ_OK:
+        raise MlqError(st, f"ncdf_read_dims {path}")
+    n1, n2, n3 = dims[0], dims[1], dims[2]
+    u = np.empty((3, n3, n2, n1))
+    st = lib.mlq_ncdf_read_field(str(path).encode(), n1, n2, n3, dptr(u), *(x.encode() for x in names))
+    if st != MLQ_OK:
+        raise MlqError(st, f"ncdf_read_field {path}")
+    return u
 
 
 class MaxLq:

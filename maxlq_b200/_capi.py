@@ -24,6 +24,7 @@ MLQ_ERR_OOM = 7
 MLQ_ERR_BADARG = 8
 MLQ_ERR_CUDA = 9
 MLQ_ERR_NOT_BANDLIMITED = 10
+MLQ_ERR_IO = 11
 
 MLQ_PREC_FP64 = 0
 MLQ_PREC_MIXED = 1
@@ -31,6 +32,7 @@ MLQ_PREC_MIXED = 1
 STATUS_NAMES = {
     0: "ok", 1: "nan", 2: "mnbrak uphill", 3: "mnbrak itmax", 4: "tau > TAU_MAX", 5: "J decreased",
     6: "device timeout", 7: "out of device memory", 8: "bad argument", 9: "cuda error", 10: "not band-limited",
+    11: "file error",
 }
 
 
@@ -118,6 +120,11 @@ SIGNATURES = {
     "mlq_seed_spectrum": (C.c_int, [C.c_int, C.c_ulonglong, C.c_double, C.c_double, _DP, C.POINTER(C.c_int)]),
     "mlq_band_cut": (C.c_int, [C.c_int, C.c_double]),
     "mlq_dealias_scalar_noalloc": (C.c_int, [_DP, C.c_int, C.c_double]),
+    "mlq_ncdf_write_field": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.c_char_p, C.c_char_p,
+                                       C.c_char_p]),
+    "mlq_ncdf_read_dims": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
+    "mlq_ncdf_read_field": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.c_char_p, C.c_char_p,
+                                      C.c_char_p]),
 }
 
 _lib = None
