@@ -189,6 +189,18 @@ int mlq_seed_field(mlq_ctx* ctx, unsigned long long seed, double slope, double k
 int mlq_seed_spectrum(int n, unsigned long long seed, double slope, double k0, double* spec, int* cut);
 int mlq_band_cut(int n, double order); /* largest |j| kept by a dealias of that order */
 
+/* ---- gradient check (host only) -------------------------------------------- */
+/* kappa_test (optimization.f90:957-1129): eps[i-1] = 10^(-7 - n/2 + i),
+ * i = 1..n (the reference uses n = 16, 1037-1038) */
+int mlq_kappa_epsilons(int n, double* eps);
+/* the kappa table from J0 = J(phi), J1[i-1] = J(phi + eps_i phi_pert) and
+ * inner = <grad J, phi_pert> (1027-1081): table is n x 5, row-major, rows
+ * (eps, inner, J1 - J0, kappa, adjusted kappa) as kappaArray; *adj_factor is
+ * the divisor of the adjusted column, *best_index (1-based) and *best_kappa
+ * the reference's best kappa.  n >= 5. */
+int mlq_kappa_table(double J0, const double* J1, double inner, int n, double* table, double* adj_factor,
+                    int* best_index, double* best_kappa);
+
 /* ---- netCDF-3 classic field files (host only, no libnetcdf) ---------------- */
 /* save_field_R3toR3_ncdf (data_ops.f90:362-487, the parallel_data layout the
  * reference uses for N >= 16): a CDF-1 file with dimensions "x" = n1, "y" = n2

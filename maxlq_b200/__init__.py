@@ -288,6 +288,30 @@ class MaxLq:
         self._check(self._lib.mlq_eval_J(self._ctx, dptr(self._vec(u)), _MODES[mysystem], C.byref(out)), "eval_J")
         return out.value
 
+    def kappa_test(self, phi, gradJ, phi_pert, mysystem: str = "maxdLqdt", inner_product_space: str = "L2",
+                   n: int = 16) -> dict:
+        """kappa_test (optimization.f90:957-1129) with a given perturbation:
+        J at phi and at phi + eps_i phi_pert (eps_i = 10^(-7 - n/2 + i)), the
+        kappa table, the reference's best kappa and the adjusted kappa.  The
+        perturbation must be band-limited like every field this engine takes
+        (the reference's own perturbation files are not part of the path)."""
+        lib = self._lib
+        eps = np.empty(n)
+        self._check(lib.mlq_kappa_epsilons(n, dptr(eps)), "kappa_epsilons")
+        phi = self._vec(phi)
+        pert = self._vec(phi_pert)
+        inner = self.global_summed_field_inner_product(gradJ, pert, inner_product_space)
+        J0 = self.eval_J(phi, mysystem)
+        J1 = np.array([self.eval_J(phi + e * pert, mysystem) for e in eps])
+        table = np.empty((n, 5))
+        frac, best = C.c_double(0.0), C.c_double(0.0)
+        bi = C.c_int(0)
+        self._check(lib.mlq_kappa_table(J0, dptr(J1), inner, n, dptr(table), C.byref(frac), C.byref(bi),
+                                        C.byref(best)), "kappa_table")
+        return {"epsilon": table[:, 0], "inner_product": inner, "deltaJ": table[:, 2], "kappa": table[:, 3],
+                "kappa_adjusted": table[:, 4], "adjust_factor": frac.value, "best_index": bi.value,
+                "best_kappa": best.value, "J0": J0}
+
     def mnbrak(self, phi, grad, tA0: float, tB0: float):
         """Returns (tau_brack, myflag) like the Fortran function and its inout flag."""
         tb = np.zeros(2)

@@ -120,6 +120,8 @@ SIGNATURES = {
     "mlq_seed_spectrum": (C.c_int, [C.c_int, C.c_ulonglong, C.c_double, C.c_double, _DP, C.POINTER(C.c_int)]),
     "mlq_band_cut": (C.c_int, [C.c_int, C.c_double]),
     "mlq_dealias_scalar_noalloc": (C.c_int, [_DP, C.c_int, C.c_double]),
+    "mlq_kappa_epsilons": (C.c_int, [C.c_int, _DP]),
+    "mlq_kappa_table": (C.c_int, [C.c_double, _DP, C.c_double, C.c_int, _DP, _DP, C.POINTER(C.c_int), _DP]),
     "mlq_ncdf_write_field": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, _DP, C.c_char_p, C.c_char_p,
                                        C.c_char_p]),
     "mlq_ncdf_read_dims": (C.c_int, [C.c_char_p, C.POINTER(C.c_int)]),
