@@ -78,3 +78,29 @@ def test_seed_field_is_divfree_meanfree_dealiased():
     assert np.abs(u.mean(axis=(1, 2, 3))).max() < 1e-15
     for c in range(3):
         assert np.abs(r.dealias(u[c], 2.0) - u[c]).max() < 1e-13
+
+
+def test_context_calls_reject_a_null_context():
+    """Every entry point that takes a context returns MLQ_ERR_BADARG for a
+    null one (no device work is attempted)."""
+    lib = maxlq_b200.load_library()
+    skip = {"mlq_init", "mlq_last_error", "mlq_kernel_launches", "mlq_device_bytes"}
+    checked = 0
+    for name, (res, args) in _capi.SIGNATURES.items():
+        if name in skip or not args or args[0] is not _capi._VP or res is not ctypes.c_int:
+            continue
+        vals = [None]
+        for a in args[1:]:
+            if a in (ctypes.c_int, ctypes.c_ulonglong):
+                vals.append(0)
+            elif a is ctypes.c_double:
+                vals.append(0.0)
+            elif a is _capi.ITER_CB:
+                vals.append(ctypes.cast(None, _capi.ITER_CB))  # a null callback
+            else:
+                vals.append(None)  # pointers: NULL
+        # the text reports return the length they need, or minus a status
+        want = -_capi.MLQ_ERR_BADARG if name in ("mlq_profile_report", "mlq_kernel_config") else _capi.MLQ_ERR_BADARG
+        assert getattr(lib, name)(*vals) == want, name
+        checked += 1
+    assert checked >= 30
