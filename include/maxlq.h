@@ -120,6 +120,7 @@ int mlq_fft_fwdr(mlq_ctx* ctx, const double* u, double* fu);
 int mlq_fft_bwdr(mlq_ctx* ctx, const double* fu, double* u);
 
 /* ---- function_ops.f90 operators ------------------------------------------ */
+/* order non-finite or below -1 (no mode kept) -> MLQ_ERR_BADARG */
 int mlq_dealias_scalar(mlq_ctx* ctx, double* g, double order);            /* 3332-3350 */
 int mlq_gradient(mlq_ctx* ctx, const double* f, double* grad);             /* 3147-3195 */
 int mlq_divergence(mlq_ctx* ctx, const double* u, double* div);            /* 3200-3243 */
@@ -227,12 +228,14 @@ int mlq_ncdf_read_field(const char* path, int n1, int n2, int n3, double* u, con
  * field (n,n,n), dealiased in place exactly as mlq_dealias_scalar does.  All
  * device memory it uses is one static array of about 6.4 MiB that every GPU
  * loading this library holds until exit, which limits n to
- * MLQ_NOALLOC_MAX_N; larger n is rejected with MLQ_ERR_BADARG (message on
- * stderr).  The first call on a device looks up the array's device address,
- * so make that call before any stream capture.  Calls run on the legacy
- * default stream and share the array: calls that overlap on the GPU (from
- * several host threads) race.  Every call overwrites all of the array it
- * reads, so nothing carries over from the previous call. */
+ * MLQ_NOALLOC_MAX_N; larger n, a non-finite order and an order below -1 are
+ * rejected with MLQ_ERR_BADARG (message on stderr).  The call works in the
+ * calling thread's current device and context and looks up the array's
+ * address there on every call.  It copies with synchronous cudaMemcpy on the
+ * legacy default stream, so it must not be called during stream capture.
+ * Calls share the array: calls that overlap on the GPU (from several host
+ * threads) race.  Every call overwrites all of the array it reads, so
+ * nothing carries over from the previous call. */
 #define MLQ_NOALLOC_MAX_N 64
 int mlq_dealias_scalar_noalloc(double* g, int n, double order);
 

@@ -2570,7 +2570,9 @@ void Engine<T>::fft_c2r(const double* in, double* out) {
 
 template <typename T>
 void Engine<T>::dealias_scalar(double* g, double order) {
+    if (!std::isfinite(order)) throw CudaError("dealias order must be finite", MLQ_ERR_BADARG);
     const int c = band_cut_for_order(n, order);
+    if (c < 0) throw CudaError("dealias order < -1 keeps no mode; dealias orders are >= 0", MLQ_ERR_BADARG);
     if (c >= n / 2) return;  // the mask removes nothing (order <= 1)
     const Band bk = make_band(c);
     widen_to(bk);

@@ -10,7 +10,6 @@
 // library routine that allocates.
 #include <cmath>
 #include <cstdio>
-#include <mutex>
 
 #include "functors.cuh"
 #include "kernels.cuh"
@@ -43,20 +42,15 @@ static_assert(OFF_XS % 256 == 0 && OFF_YS % 256 == 0 && OFF_PART % 256 == 0 && O
 // cudaGetSymbolAddress; kernels receive the device address obtained that way.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[MAX_DEVICES] = {nullptr};
-
-// Once per device, with that device current: the device address of the scratch.
-cudaError_t scratch_address(int dev, unsigned char** out) {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return e;
-        g_scratch_addr[dev] = p;
-    }
-    *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+// The device address of the scratch in the calling thread's current context.
+// It is looked up on every call (a cheap runtime query): a symbol's address
+// belongs to a CUDA context, and a caller may switch contexts on a device
+// (another runtime's driver-API context, or a cudaDeviceReset) between calls.
+cudaError_t scratch_address(unsigned char** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    *out = static_cast<unsigned char*>(p);
     return cudaSuccess;
 }
 
@@ -91,6 +85,12 @@ int fail(int status, const char* msg) {
     return status;
 }
 
+int launch_failed(const char* kernel, cudaError_t e) {
+    char m[200];
+    snprintf(m, sizeof(m), "launch of the %s kernel failed: %s", kernel, cudaGetErrorString(e));
+    return fail(MLQ_ERR_CUDA, m);
+}
+
 }  // namespace
 
 extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
@@ -103,13 +103,20 @@ extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
                  n, NMAX);
         return fail(MLQ_ERR_BADARG, m);
     }
+    if (!std::isfinite(order)) return fail(MLQ_ERR_BADARG, "order must be finite");
     const int cut = band_cut_for_order(n, order);
+    if (cut < 0) return fail(MLQ_ERR_BADARG, "order < -1 keeps no mode; dealias orders are >= 0");
     if (cut >= n / 2) return MLQ_OK;  // the mask removes nothing (order <= 1), as mlq_dealias_scalar
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES)
-        return fail(MLQ_ERR_CUDA, "no current CUDA device");
+    // an error left pending by earlier work of the caller is reported as such,
+    // not blamed on a launch below
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        char m[200];
+        snprintf(m, sizeof(m), "a CUDA error was pending before this call: %s", cudaGetErrorString(e));
+        return fail(MLQ_ERR_CUDA, m);
+    }
     unsigned char* base = nullptr;
-    cudaError_t e = scratch_address(dev, &base);
+    e = scratch_address(&base);
     if (e != cudaSuccess) return fail(MLQ_ERR_CUDA, cudaGetErrorString(e));
 
     double* phys = reinterpret_cast<double*>(base + OFF_PHYS);
@@ -159,6 +166,7 @@ extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
     xa.tw = tw;
     xa.partials = partials;
     xfwd_kernel<double, FCopy><<<(unsigned)((long)n * n / lx), 256, 2 * lx * h * sizeof(cpx<double>)>>>(xa, FCopy{});
+    if ((e = cudaGetLastError()) != cudaSuccess) return launch_failed("x stage (r2c)", e);
     // y forward (keep |ky| <= cut)
     YArgs<double> ya;
     ya.n = n;
@@ -172,6 +180,7 @@ extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
     const size_t ysm = 2 * (size_t)n * tx * sizeof(cpx<double>);
     dim3 yg((b.nx + tx - 1) / tx, n, 1);
     ypass_kernel<-1, double><<<yg, 256, ysm>>>(ya);
+    if ((e = cudaGetLastError()) != cudaSuccess) return launch_failed("y forward", e);
     // z round trip with the mask and the 1/N^3 of the forward transform
     ZFwdArgs<double> za;
     za.n = n;
@@ -192,11 +201,13 @@ extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
     dim3 zg((b.nx + tx - 1) / tx, b.nb, 1);
     if ((size_t)zg.x * zg.y * MAX_RED > PART_DOUBLES) return fail(MLQ_ERR_BADARG, "partials scratch too small");
     zfwd_kernel<double><<<zg, 256, ysm>>>(za);
+    if ((e = cudaGetLastError()) != cudaSuccess) return launch_failed("z round trip", e);
     // y inverse, x inverse (c2r) back into the field
     YArgs<double> yb = ya;
     yb.in[0] = ys;
     yb.out[0] = xs;
     ypass_kernel<+1, double><<<yg, 256, ysm>>>(yb);
+    if ((e = cudaGetLastError()) != cudaSuccess) return launch_failed("y inverse", e);
     XInvArgs<double> xb;
     xb.n = n;
     xb.nx_in = b.nx;
@@ -208,7 +219,7 @@ extern "C" int mlq_dealias_scalar_noalloc(double* g, int n, double order) {
     xb.tw = tw;
     dim3 xg((unsigned)((long)n * n / lx), 1);
     xinv_kernel<double><<<xg, 256, (size_t)(3 * h + 1) * lx * sizeof(cpx<double>)>>>(xb);
-    if ((e = cudaGetLastError()) != cudaSuccess) return fail(MLQ_ERR_CUDA, cudaGetErrorString(e));
+    if ((e = cudaGetLastError()) != cudaSuccess) return launch_failed("x inverse (c2r)", e);
     if ((e = cudaMemcpy(g, phys, n3 * sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess)
         return fail(MLQ_ERR_CUDA, cudaGetErrorString(e));
     return MLQ_OK;

@@ -104,3 +104,11 @@ def test_context_calls_reject_a_null_context():
         assert getattr(lib, name)(*vals) == want, name
         checked += 1
     assert checked >= 30
+
+
+@pytest.mark.parametrize("order", [float("nan"), float("inf"), -3.0])
+def test_noalloc_rejects_orders_that_keep_no_mode_before_any_cuda_call(order):
+    # argument checks come before the first CUDA call, so they hold without a GPU
+    lib = maxlq_b200.load_library()
+    g = np.zeros((16, 16, 16))
+    assert lib.mlq_dealias_scalar_noalloc(_capi.dptr(g), 16, order) == _capi.MLQ_ERR_BADARG
