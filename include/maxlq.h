@@ -112,9 +112,15 @@ long long mlq_kernel_launches(const mlq_ctx* ctx);
 long long mlq_device_bytes(const mlq_ctx* ctx);
 
 /* ---- fftwfunction.f90 ---------------------------------------------------- */
-/* fftfwd / fftbwd (62-113): 3D c2c of N^3 complex(8), normal order */
+/* fftfwd / fftbwd (62-113): 3D c2c of N^3 complex(8), normal order.
+ * mlq_fft_fwd returns MLQ_ERR_NAN when the real part of an output is NaN
+ * (fftfwd's scan, 78-89). */
 int mlq_fft_fwd(mlq_ctx* ctx, const double* u, double* fu);
 int mlq_fft_bwd(mlq_ctx* ctx, const double* fu, double* u);
+/* fftfwdV / fftbwdV (24-58): the three components of a complex(8)
+ * (N,N,N,3) field, each through fftfwd / fftbwd */
+int mlq_fft_fwdV(mlq_ctx* ctx, const double* u, double* fu);
+int mlq_fft_bwdV(mlq_ctx* ctx, const double* fu, double* u);
 /* fftfwdr / fftbwdr (118-164): real (N,N,N) <-> complex (N/2+1,N,N) */
 int mlq_fft_fwdr(mlq_ctx* ctx, const double* u, double* fu);
 int mlq_fft_bwdr(mlq_ctx* ctx, const double* fu, double* u);

@@ -19,7 +19,8 @@ import ctypes as C
 import numpy as np
 
 from ._capi import (  # noqa: F401
-    ITER_CB, MLQ_ERR_J_DECREASED, MLQ_ERR_MNBRAK_ITMAX, MLQ_ERR_MNBRAK_UPHILL, MLQ_ERR_NOT_BANDLIMITED,
+    ITER_CB, MLQ_ERR_BADARG, MLQ_ERR_IO, MLQ_ERR_J_DECREASED, MLQ_ERR_MNBRAK_ITMAX, MLQ_ERR_MNBRAK_UPHILL,
+    MLQ_ERR_NAN, MLQ_ERR_NOT_BANDLIMITED,
     MLQ_ERR_TAU_MAX, MLQ_OK, MLQ_PREC_FP64, MLQ_PREC_MIXED, STATUS_NAMES, MlqIterInfo, MlqParams, dptr,
     load_library,
 )
@@ -174,10 +175,18 @@ class MaxLq:
         return out
 
     def fftfwdV(self, u):
-        return np.stack([self.fftfwd(c) for c in u])
+        a = np.ascontiguousarray(u, dtype=np.complex128)
+        out = np.empty_like(a)
+        self._check(self._lib.mlq_fft_fwdV(self._ctx, dptr(a.view(np.float64)), dptr(out.view(np.float64))),
+                    "fftfwdV")
+        return out
 
     def fftbwdV(self, fu):
-        return np.stack([self.fftbwd(c) for c in fu])
+        a = np.ascontiguousarray(fu, dtype=np.complex128)
+        out = np.empty_like(a)
+        self._check(self._lib.mlq_fft_bwdV(self._ctx, dptr(a.view(np.float64)), dptr(out.view(np.float64))),
+                    "fftbwdV")
+        return out
 
     def fftfwdr(self, u):
         u = self._sca(u)

@@ -86,6 +86,8 @@ SIGNATURES = {
     "mlq_device_bytes": (C.c_longlong, [_VP]),
     "mlq_fft_fwd": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_bwd": (C.c_int, [_VP, _DP, _DP]),
+    "mlq_fft_fwdV": (C.c_int, [_VP, _DP, _DP]),
+    "mlq_fft_bwdV": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_fwdr": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_bwdr": (C.c_int, [_VP, _DP, _DP]),
     "mlq_dealias_scalar": (C.c_int, [_VP, _DP, C.c_double]),

@@ -206,8 +206,35 @@ long long mlq_device_bytes(const mlq_ctx* c) {
     return b;
 }
 
-int mlq_fft_fwd(mlq_ctx* c, const double* u, double* fu) { return guard(c, [&] { fft64(c).fft_c2c(u, fu, -1); }); }
+// fftfwd's NaN scan (fftwfunction.f90:78-89): a NaN in the real part of an
+// output stops the reference; here the call returns MLQ_ERR_NAN.
+static void nan_scan_real_parts(const double* fu, long n3) {
+    for (long i = 0; i < n3; ++i)
+        if (std::isnan(fu[2 * i])) throw CudaError("NaN in the forward transform's output", MLQ_ERR_NAN);
+}
+
+int mlq_fft_fwd(mlq_ctx* c, const double* u, double* fu) {
+    return guard(c, [&] {
+        fft64(c).fft_c2c(u, fu, -1);
+        nan_scan_real_parts(fu, fft64(c).n3);
+    });
+}
 int mlq_fft_bwd(mlq_ctx* c, const double* fu, double* u) { return guard(c, [&] { fft64(c).fft_c2c(fu, u, +1); }); }
+int mlq_fft_fwdV(mlq_ctx* c, const double* u, double* fu) {
+    return guard(c, [&] {
+        Engine<double>& e = fft64(c);
+        for (int k = 0; k < 3; ++k) {
+            e.fft_c2c(u + 2 * k * e.n3, fu + 2 * k * e.n3, -1);
+            nan_scan_real_parts(fu + 2 * k * e.n3, e.n3);
+        }
+    });
+}
+int mlq_fft_bwdV(mlq_ctx* c, const double* fu, double* u) {
+    return guard(c, [&] {
+        Engine<double>& e = fft64(c);
+        for (int k = 0; k < 3; ++k) e.fft_c2c(fu + 2 * k * e.n3, u + 2 * k * e.n3, +1);
+    });
+}
 int mlq_fft_fwdr(mlq_ctx* c, const double* u, double* fu) { return guard(c, [&] { fft64(c).fft_r2c(u, fu); }); }
 int mlq_fft_bwdr(mlq_ctx* c, const double* fu, double* u) { return guard(c, [&] { fft64(c).fft_c2r(fu, u); }); }
 

@@ -539,6 +539,7 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
                 for (int m = 0; m < E; ++m) v[m] = stg[((o - 1) * LPB + ls) * L + t + TPL * m];
             }
             cfft<L, E, -1, SyncWarp>(v, t, sm, map, tw);
+            if (t == 0 && a.nanflag && !cpx_finite(v[0])) *a.nanflag = 1.0;  // the DC bin of the line
             cpx<T>* __restrict__ dst = a.out[o] + line * nx;
             // X[k] = E[k] + W_N^k O[k], E = (Z_k + conj Z_{L-k})/2, O = -i (Z_k - conj Z_{L-k})/2
             SFor<0, E>::run([&](auto mc) {

@@ -137,6 +137,14 @@ void EngineBase::finalize(int nblocks, int nr, double scale, int dst, bool accum
 void EngineBase::fetch_results() {
     MLQ_CUDA(cudaMemcpyAsync(h_results, d_results, NRES * sizeof(double), cudaMemcpyDeviceToHost, stream));
     MLQ_CUDA(cudaStreamSynchronize(stream));
+    if (h_results[NAN_SLOT] != 0.0) {
+        // the reference stops the program here (fftwfunction.f90:78-89); the
+        // flag is cleared so the context stays usable for a new field
+        MLQ_CUDA(cudaMemsetAsync(d_results + NAN_SLOT, 0, sizeof(double), stream));
+        MLQ_CUDA(cudaStreamSynchronize(stream));
+        h_results[NAN_SLOT] = 0.0;
+        throw CudaError("NaN or Inf in a field entering a forward transform", MLQ_ERR_NAN);
+    }
 }
 
 cudaEvent_t EngineBase::ev_take() {

@@ -51,8 +51,11 @@ class EngineBase {
     long partials_cap = 0;
     double* d_results = nullptr;  // 256 slots
     static constexpr int NRES = 256;
+    // result slot the forward transforms set when they meet a non-finite
+    // value; fetch_results() turns it into MLQ_ERR_NAN
+    static constexpr int NAN_SLOT = NRES - 1;
     double h_results[NRES];
-    void fetch_results();  // sync + copy all slots
+    void fetch_results();  // sync + copy all slots; throws MLQ_ERR_NAN if a NaN was seen
 
     // FP64 state spectra (3 components each) of band b2
     long spec_ncomp() const { return (long)b2.nb * b2.nb * b2.nx; }

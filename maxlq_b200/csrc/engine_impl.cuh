@@ -428,6 +428,7 @@ template <typename T>
 template <class F>
 void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b) {
     const int h = n / 2;
+    xa.nanflag = d_results + NAN_SLOT;
     // compulsory bytes: each distinct input field read once, each output written once
     int nin_distinct = 0;
     for (int i = 0; i < F::NIN; ++i) {
@@ -2403,6 +2404,7 @@ double Engine<T>::load_vec(const double* host, double2* spec) {
         out += h_results[30 + 2 * c];
         tot += h_results[31 + 2 * c];
     }
+    if (std::isnan(out) || std::isnan(tot)) return std::nan("");
     return tot > 0 ? out / tot : 0.0;
 }
 

@@ -78,7 +78,18 @@ struct XFwdArgs {
     const cpx<double>* tw;
     double* partials;
     long nlines = 0;    // lines (rows along x) processed; a slab of planes is nlines = planes * n
+    // Set to 1 when a forward transform meets a non-finite value (null: not
+    // checked).  The DC bin of a packed line is the sum of all its values, so
+    // it is non-finite exactly when some input of the line is (or the sum
+    // overflows), the condition of the reference's NaN scan after fftfwd
+    // (fftwfunction.f90:78-89).
+    double* nanflag = nullptr;
 };
+
+template <typename T>
+__device__ __forceinline__ bool cpx_finite(cpx<T> v) {
+    return isfinite(v.x) && isfinite(v.y);
+}
 
 template <typename T, class F>
 __global__ void __launch_bounds__(256) xfwd_kernel(XFwdArgs<T> a, F f) {
@@ -107,6 +118,7 @@ __global__ void __launch_bounds__(256) xfwd_kernel(XFwdArgs<T> a, F f) {
     }
     __syncthreads();
     cpx<T>* Z = fft_lines<-1, T>(bufA, bufB, a.plan_half, nl, nl, a.tw, threadIdx.x, blockDim.x);
+    if (a.nanflag && (int)threadIdx.x < nl && !cpx_finite(Z[threadIdx.x])) *a.nanflag = 1.0;
     // split into the half spectrum of the real line: X[k] = E[k] + W_n^k O[k]
     const double2* twn = reinterpret_cast<const double2*>(a.tw + a.tw_n_off);
     for (int p = threadIdx.x; p < nl * a.nx; p += blockDim.x) {

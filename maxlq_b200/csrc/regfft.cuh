@@ -299,6 +299,7 @@ __global__ void __launch_bounds__(256, 3) xfwd_reg_kernel(XFwdArgs<T> a, F f, RP
     for (int m = 0; m < E; ++m) v[m] = sm[si(t + nT * m)];
     __syncthreads();
     reg_fft<E, -1>(v, t, nT, pl, sm, si, tw);
+    if (a.nanflag && t == 0 && !cpx_finite(v[0])) *a.nanflag = 1.0;  // the DC bin of the row
 #pragma unroll
     for (int m = 0; m < E; ++m) sm[si(t + nT * m)] = v[m];
     __syncthreads();

@@ -78,7 +78,10 @@ class Solver : public SolverBase {
         const double rel = io().load_vec(host, spec);
         trim_io();
         const double tol = 1e-24;  // relative energy; FP64 FFT round-trip noise is ~1e-32
-        if (rel > tol)
+        if (std::isnan(rel))
+            throw CudaError("input field holds NaN or Inf (the reference stops at fftwfunction.f90:78-89)",
+                            MLQ_ERR_NAN);
+        if (!(rel <= tol))
             throw CudaError("input field is not band-limited to the 2/3 dealiasing cube (relative energy outside: " +
                                 fmt_e(rel) + ")",
                             MLQ_ERR_NOT_BANDLIMITED);
@@ -112,7 +115,13 @@ class Solver : public SolverBase {
         ++eval_count;
         ++evals_this_iter;
         const Trial t = trial(base, dir, tau);
-        return -1.0 * scaled_R(t);
+        const double J = -1.0 * scaled_R(t);
+        // The reference's trial rescales the field and transforms it; a NaN
+        // there stops the program at the FFT's NaN scan (fftwfunction.f90:78-89).
+        // A trial that needs no transform (homogeneity, polynomial path)
+        // reports the same condition from its value.
+        if (std::isnan(J)) throw CudaError("NaN in a line-search trial value", MLQ_ERR_NAN);
+        return J;
     }
     double scaled_R(const Trial& t) const {
         const double nrm = std::pow(t.lqq, 1.0 / q());

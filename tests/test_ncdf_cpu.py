@@ -111,3 +111,16 @@ def test_errors(tmp_path):
     with pytest.raises(mlq.MlqError) as e:
         mlq.ncdf_read_field(bad)
     assert e.value.status == 11
+
+
+def test_truncated_restart_file_is_an_io_error(tmp_path):
+    # a restart file cut short in its data (a run killed while saving)
+    u = _field(8, 8, 8)
+    p = tmp_path / "u_result.nc"
+    mlq.ncdf_write_field(p, u)
+    raw = p.read_bytes()
+    cut = tmp_path / "cut.nc"
+    cut.write_bytes(raw[: len(raw) - 100])
+    with pytest.raises(mlq.MlqError) as e:
+        mlq.ncdf_read_field(cut)
+    assert e.value.status == 11
