@@ -23,15 +23,25 @@ const double MACH_EPSILON = 2.0e-16;  // global_variables.f90:28
 const double TAU_MAX = 1.0e2;         // global_variables.f90:29
 
 // ---------------------------------------------------------------------------
-// 1D mixed-radix Stockham FFT (radices 4, 2, 3, 5, generic).  The oracle's
-// own FFT; FFTW is not vendored by the reference (makefile:20-21), so parity
-// at this boundary is the mathematical DFT.
+// 1D mixed-radix Stockham FFT (radices 4, 2, 3, 5, generic), applied to B
+// interleaved lines at once (element p of line b at x[p*B + b]) so that the
+// strided y and z lines of a 3D array are transformed in cache-friendly tiles
+// of B neighbouring columns.  The oracle's own FFT: FFTW is not vendored by
+// the reference (makefile:20-21), so parity at this boundary is the
+// mathematical DFT (checked against numpy's pocketfft in the tests).
+// Complex products are written out in real arithmetic.
 // ---------------------------------------------------------------------------
 struct Fft1D {
     int n = 0;
-    std::vector<int> radix;
-    std::vector<cplx> w;  // w[k] = exp(-2 pi i k / n)
+    std::vector<int> radix, ns;          // radix and span of every stage
+    std::vector<std::vector<cplx>> stw;  // stage twiddles [k*(R-1) + r-1] = exp(-2 pi i r k / (ns R))
+    std::vector<std::vector<cplx>> roots;  // roots[R][m] = exp(-2 pi i m / R) for the generic radices
 
+    static cplx expi(long num, long den) {  // exp(-2 pi i num / den), angle reduced in integers
+        long k = ((num % den) + den) % den;
+        const double a = 2.0 * M_PI * (double)k / (double)den;
+        return cplx(std::cos(a), -std::sin(a));
+    }
     void init(int nn) {
         n = nn;
         radix.clear();
@@ -41,42 +51,123 @@ struct Fft1D {
         for (int p = 3; m > 1; p += 2) {
             while (m % p == 0) { radix.push_back(p); m /= p; }
         }
-        w.resize(n);
-        for (int k = 0; k < n; ++k) {
-            // angle reduced to [0, 2pi) exactly in integers first
-            double a = 2.0 * M_PI * (double)k / (double)n;
-            w[k] = cplx(std::cos(a), -std::sin(a));
+        ns.clear();
+        stw.clear();
+        roots.assign(64, {});
+        int span = 1;
+        for (int R : radix) {
+            ns.push_back(span);
+            std::vector<cplx> t((size_t)span * (R - 1));
+            for (int k = 0; k < span; ++k)
+                for (int r = 1; r < R; ++r) t[(size_t)k * (R - 1) + r - 1] = expi((long)r * k, (long)span * R);
+            stw.push_back(t);
+            if (R != 2 && R != 4 && R < 64 && roots[R].empty()) {
+                roots[R].resize(R);
+                for (int q = 0; q < R; ++q) roots[R][q] = expi(q, R);
+            }
+            span *= R;
         }
-    }
-    inline cplx tw(long e, int sign) const {
-        long k = ((e % n) + n) % n;
-        cplx v = w[k];
-        return sign < 0 ? v : std::conj(v);
     }
     // sign -1: forward exp(-i...), +1: backward exp(+i...).  Unnormalised.
-    void exec(cplx* x, cplx* work, int sign) const {
-        cplx* src = x;
-        cplx* dst = work;
-        int ns = 1;
-        for (int R : radix) {
-            int nr = n / R;
-            cplx v[16], o[16];
+    // work holds n*B elements.
+    void exec_batch(cplx* x, cplx* work, int B, int sign) const {
+        double* src = reinterpret_cast<double*>(x);
+        double* dst = reinterpret_cast<double*>(work);
+        const double sg = (double)sign;  // conj of the forward twiddles when +1
+        for (size_t s = 0; s < radix.size(); ++s) {
+            const int R = radix[s], NS = ns[s], nr = n / R;
+            const double* tw = reinterpret_cast<const double*>(stw[s].data());
             for (int j = 0; j < nr; ++j) {
-                int k = j % ns;
-                long step = (long)n / ((long)ns * R);
-                for (int r = 0; r < R; ++r) v[r] = src[j + r * nr] * tw((long)r * k * step, sign);
-                for (int m = 0; m < R; ++m) {
-                    cplx acc = 0.0;
-                    for (int r = 0; r < R; ++r) acc += v[r] * tw((long)r * m * (n / R), sign);
-                    o[m] = acc;
+                const int k = j % NS;
+                const long od = ((long)(j / NS) * NS * R + k) * B;
+                const double* twk = tw + 2 * (long)k * (R - 1);
+                if (R == 4) {
+                    double wr[3], wi[3];
+                    for (int r = 0; r < 3; ++r) {
+                        wr[r] = twk[2 * r];
+                        wi[r] = sign < 0 ? twk[2 * r + 1] : -twk[2 * r + 1];
+                    }
+                    for (int b = 0; b < B; ++b) {
+                        double vr[4], vi[4];
+                        for (int r = 0; r < 4; ++r) {
+                            const long is = 2 * ((long)(j + r * nr) * B + b);
+                            vr[r] = src[is];
+                            vi[r] = src[is + 1];
+                        }
+                        if (NS > 1) {
+                            for (int r = 1; r < 4; ++r) {
+                                const double ar = vr[r], ai = vi[r];
+                                vr[r] = ar * wr[r - 1] - ai * wi[r - 1];
+                                vi[r] = ar * wi[r - 1] + ai * wr[r - 1];
+                            }
+                        }
+                        const double s0r = vr[0] + vr[2], s0i = vi[0] + vi[2];
+                        const double d0r = vr[0] - vr[2], d0i = vi[0] - vi[2];
+                        const double s1r = vr[1] + vr[3], s1i = vi[1] + vi[3];
+                        const double d1r = vr[1] - vr[3], d1i = vi[1] - vi[3];
+                        // o1 = d0 + sign * i * d1, o3 = d0 - sign * i * d1
+                        const long o = 2 * (od + b);
+                        const long st = 2 * (long)NS * B;
+                        dst[o] = s0r + s1r;
+                        dst[o + 1] = s0i + s1i;
+                        dst[o + st] = d0r - sg * d1i;
+                        dst[o + st + 1] = d0i + sg * d1r;
+                        dst[o + 2 * st] = s0r - s1r;
+                        dst[o + 2 * st + 1] = s0i - s1i;
+                        dst[o + 3 * st] = d0r + sg * d1i;
+                        dst[o + 3 * st + 1] = d0i - sg * d1r;
+                    }
+                } else if (R == 2) {
+                    const double wr = twk[0], wi = sign < 0 ? twk[1] : -twk[1];
+                    for (int b = 0; b < B; ++b) {
+                        const long i0 = 2 * ((long)j * B + b), i1 = 2 * ((long)(j + nr) * B + b);
+                        double ar = src[i1], ai = src[i1 + 1];
+                        if (NS > 1) {
+                            const double tr = ar * wr - ai * wi;
+                            ai = ar * wi + ai * wr;
+                            ar = tr;
+                        }
+                        const long o = 2 * (od + b), st = 2 * (long)NS * B;
+                        dst[o] = src[i0] + ar;
+                        dst[o + 1] = src[i0 + 1] + ai;
+                        dst[o + st] = src[i0] - ar;
+                        dst[o + st + 1] = src[i0 + 1] - ai;
+                    }
+                } else {
+                    const std::vector<cplx>& rt = roots[R];
+                    cplx v[64];
+                    for (int b = 0; b < B; ++b) {
+                        for (int r = 0; r < R; ++r) {
+                            const long is = 2 * ((long)(j + r * nr) * B + b);
+                            double ar = src[is], ai = src[is + 1];
+                            if (r > 0 && NS > 1) {
+                                const double wr = twk[2 * (r - 1)];
+                                const double wi = sign < 0 ? twk[2 * (r - 1) + 1] : -twk[2 * (r - 1) + 1];
+                                const double tr = ar * wr - ai * wi;
+                                ai = ar * wi + ai * wr;
+                                ar = tr;
+                            }
+                            v[r] = cplx(ar, ai);
+                        }
+                        for (int m = 0; m < R; ++m) {
+                            double accr = 0.0, acci = 0.0;
+                            for (int r = 0; r < R; ++r) {
+                                const cplx w = rt[(long)r * m % R];
+                                const double wr = w.real(), wi = sign < 0 ? w.imag() : -w.imag();
+                                accr += v[r].real() * wr - v[r].imag() * wi;
+                                acci += v[r].real() * wi + v[r].imag() * wr;
+                            }
+                            const long o = 2 * (od + (long)m * NS * B + b);
+                            dst[o] = accr;
+                            dst[o + 1] = acci;
+                        }
+                    }
                 }
-                int idxD = (j / ns) * ns * R + k;
-                for (int r = 0; r < R; ++r) dst[idxD + r * ns] = o[r];
             }
             std::swap(src, dst);
-            ns *= R;
         }
-        if (src != x) std::memcpy(x, src, sizeof(cplx) * n);
+        double* xd = reinterpret_cast<double*>(x);
+        if (src != xd) std::memcpy(xd, src, sizeof(double) * 2 * (size_t)n * B);
     }
 };
 
@@ -98,31 +189,41 @@ inline long IDX(const orc_ctx* c, int x, int y, int z) {
     return ((long)z * c->n + y) * c->n + x;
 }
 
-// 3D c2c over [z][y][x], all three axes; sign as Fft1D.
+// 3D c2c over [z][y][x], all three axes; sign as Fft1D.  y and z lines are
+// transformed in tiles of TB neighbouring x columns.
 void fft3(orc_ctx* c, cplx* a, int sign) {
     const int n = c->n;
+    int TB = 16;
+    while (n % TB) TB /= 2;
+    const int ntile = n / TB;
 #pragma omp parallel
     {
-        std::vector<cplx> line(n), work(n);
+        std::vector<cplx> buf((size_t)n * TB), work((size_t)n * TB);
         // x lines (contiguous)
-#pragma omp for collapse(2)
+#pragma omp for collapse(2) schedule(static)
         for (int z = 0; z < n; ++z)
-            for (int y = 0; y < n; ++y) c->fft.exec(a + IDX(c, 0, y, z), work.data(), sign);
-        // y lines
-#pragma omp for collapse(2)
+            for (int y = 0; y < n; ++y) c->fft.exec_batch(a + IDX(c, 0, y, z), work.data(), 1, sign);
+        // y lines, TB columns at a time
+#pragma omp for collapse(2) schedule(static)
         for (int z = 0; z < n; ++z)
-            for (int x = 0; x < n; ++x) {
-                for (int y = 0; y < n; ++y) line[y] = a[IDX(c, x, y, z)];
-                c->fft.exec(line.data(), work.data(), sign);
-                for (int y = 0; y < n; ++y) a[IDX(c, x, y, z)] = line[y];
+            for (int t = 0; t < ntile; ++t) {
+                const int x0 = t * TB;
+                for (int y = 0; y < n; ++y)
+                    std::memcpy(&buf[(size_t)y * TB], a + IDX(c, x0, y, z), sizeof(cplx) * TB);
+                c->fft.exec_batch(buf.data(), work.data(), TB, sign);
+                for (int y = 0; y < n; ++y)
+                    std::memcpy(a + IDX(c, x0, y, z), &buf[(size_t)y * TB], sizeof(cplx) * TB);
             }
         // z lines
-#pragma omp for collapse(2)
+#pragma omp for collapse(2) schedule(static)
         for (int y = 0; y < n; ++y)
-            for (int x = 0; x < n; ++x) {
-                for (int z = 0; z < n; ++z) line[z] = a[IDX(c, x, y, z)];
-                c->fft.exec(line.data(), work.data(), sign);
-                for (int z = 0; z < n; ++z) a[IDX(c, x, y, z)] = line[z];
+            for (int t = 0; t < ntile; ++t) {
+                const int x0 = t * TB;
+                for (int z = 0; z < n; ++z)
+                    std::memcpy(&buf[(size_t)z * TB], a + IDX(c, x0, y, z), sizeof(cplx) * TB);
+                c->fft.exec_batch(buf.data(), work.data(), TB, sign);
+                for (int z = 0; z < n; ++z)
+                    std::memcpy(a + IDX(c, x0, y, z), &buf[(size_t)z * TB], sizeof(cplx) * TB);
             }
     }
 }
