@@ -563,6 +563,7 @@ void R_parts(orc_ctx* c, const double* u, double out[3]) {
         R2 = -vc * (q - 2.0) * nu * inner_l2(c, a_q4.data(), aux.data());
     }
     nabla_u_nabla_ut(c, u, aux.data());
+    #pragma omp parallel for
     for (long i = 0; i < n3; ++i) tmp[i] = -aux[i];
     solve_poisson(c, tmp.data(), 1.0, p.data());
     double R3;
@@ -589,6 +590,7 @@ double lq_norm(orc_ctx* c, const double* u) {
 void rescale(orc_ctx* c, double* u, double B) {
     double nrm = lq_norm(c, u);
     const long m = 3 * c->n3;
+    #pragma omp parallel for
     for (long i = 0; i < m; ++i) u[i] = B / nrm * u[i];
 }
 
@@ -626,6 +628,7 @@ void divavg_free(orc_ctx* c, double* f) {
         real_part(c, gp[d], g.data());
         fftbwd(c, uh[d].data());
         real_part(c, uh[d], f + d * n3);
+        #pragma omp parallel for
         for (long i = 0; i < n3; ++i) f[d * n3 + i] -= g[i];
     }
 }
@@ -665,10 +668,12 @@ void normal_l2(orc_ctx* c, const double* u, double* out) {
     RV a(n3);
     calc_uk(c, u, q - 2.0, a.data());
     for (int d = 0; d < 3; ++d) {
+        #pragma omp parallel for
         for (long i = 0; i < n3; ++i) out[d * n3 + i] = a[i] * u[d * n3 + i];
         if (c->p.to_dealias && (q - 2.0 > MACH_EPSILON)) dealias_scalar(c, out + d * n3, 2.0);
     }
     const double f = std::pow(nrm, 1.0 - q);
+    #pragma omp parallel for
     for (long i = 0; i < 3 * n3; ++i) out[i] = f * out[i];
 }
 
@@ -677,81 +682,119 @@ void vector_transport(orc_ctx* c, const double* u, double q, double B, const dou
                       const double* xi, double* out) {
     const long n3 = c->n3, m = 3 * n3;
     RV w(m), a(n3), aux(m);
+    #pragma omp parallel for
     for (long i = 0; i < m; ++i) w[i] = u[i] + eta[i];
     calc_uk(c, w.data(), q - 2.0, a.data());
     for (int d = 0; d < 3; ++d) {
+        #pragma omp parallel for
         for (long i = 0; i < n3; ++i) aux[d * n3 + i] = a[i] * w[d * n3 + i];
         if (c->p.to_dealias && (q - 2.0 > MACH_EPSILON)) dealias_scalar(c, aux.data() + d * n3, 2.0);
     }
     double ir = field_inner(c, aux.data(), xi, 0);
     double ln = lq_norm(c, w.data());
+    #pragma omp parallel for
     for (long i = 0; i < m; ++i) out[i] = xi[i] - std::pow(ln, -q) * ir * w[i];
+    #pragma omp parallel for
     for (long i = 0; i < m; ++i) out[i] = B / ln * out[i];
 }
 
-// GradL2ForLq (1066-1211)
+// GradL2ForLq (1066-1211).  Temporaries are scoped so that each is freed
+// once its last use is done (the reference holds all of them: 1076-1077);
+// the arithmetic of every value is unchanged, which keeps 512^3 within a few
+// tens of GB of host memory.
 void grad_l2(orc_ctx* c, const double* u, double* v) {
     const long n3 = c->n3, m = 3 * n3;
     const double q = c->p.q, nu = c->p.visc, vc = c->p.visc_coef, pc = c->p.press_coef;
-    RV a_q2(n3), aux(n3), aux2(n3), aux3(n3), aux4(n3), p(n3), a_q4(n3), tmp(n3);
-    RV gradP(m), dU(m), uq2u(m), a3v(m), a4v(m), a5v(m), a6v(m), a7v(m), e(m);
+    RV a_q2(n3);
     calc_uk(c, u, q - 2.0, a_q2.data());
-    nabla_u_nabla_ut(c, u, aux.data());
-    for (long i = 0; i < n3; ++i) tmp[i] = -aux[i];
-    solve_poisson(c, tmp.data(), 1.0, p.data());
-    gradient(c, p.data(), gradP.data());
+    RV gradP(m), dU(m), a3v(m);
+    {
+        RV aux(n3), tmp(n3), p(n3);
+        nabla_u_nabla_ut(c, u, aux.data());
+        #pragma omp parallel for
+        for (long i = 0; i < n3; ++i) tmp[i] = -aux[i];
+        solve_poisson(c, tmp.data(), 1.0, p.data());
+        gradient(c, p.data(), gradP.data());
+    }
     std::memcpy(dU.data(), u, sizeof(double) * m);
     laplacian(c, dU.data());
-    std::fill(aux2.begin(), aux2.end(), 0.0);
-    if (c->p.use_e_u) {
-        unit_vector(c, u, e.data());
-        for (int d = 0; d < 3; ++d)
-            for (long i = 0; i < n3; ++i)
-                aux2[i] = aux2[i] + e[d * n3 + i] * (vc * nu * dU[d * n3 + i] - pc * gradP[d * n3 + i]);
-        if (c->p.to_dealias && c->p.dealias_e_u) dealias_scalar(c, aux2.data(), 2.0);
-        for (long i = 0; i < n3; ++i) aux2[i] = a_q2[i] * aux2[i];
-        maybe_dealias(c, aux2.data(), 2.0);
-        for (int d = 0; d < 3; ++d) {
-            for (long i = 0; i < n3; ++i) a3v[d * n3 + i] = aux2[i] * e[d * n3 + i];
-            if (c->p.to_dealias && c->p.dealias_e_u) dealias_scalar(c, a3v.data() + d * n3, 2.0);
-        }
-    } else {
-        for (int d = 0; d < 3; ++d)
-            for (long i = 0; i < n3; ++i)
-                aux2[i] = aux2[i] + u[d * n3 + i] * (vc * nu * dU[d * n3 + i] - pc * gradP[d * n3 + i]);
-        maybe_dealias(c, aux2.data(), 2.0);
-        calc_uk(c, u, q - 4.0, a_q4.data());
-        for (long i = 0; i < n3; ++i) aux2[i] = a_q4[i] * aux2[i];
-        maybe_dealias(c, aux2.data(), 2.0);
-        for (int d = 0; d < 3; ++d) {
-            for (long i = 0; i < n3; ++i) a3v[d * n3 + i] = aux2[i] * u[d * n3 + i];
-            maybe_dealias(c, a3v.data() + d * n3, 2.0);
+    {
+        RV aux2(n3, 0.0);
+        if (c->p.use_e_u) {
+            RV e(m);
+            unit_vector(c, u, e.data());
+            for (int d = 0; d < 3; ++d)
+                #pragma omp parallel for
+                for (long i = 0; i < n3; ++i)
+                    aux2[i] = aux2[i] + e[d * n3 + i] * (vc * nu * dU[d * n3 + i] - pc * gradP[d * n3 + i]);
+            if (c->p.to_dealias && c->p.dealias_e_u) dealias_scalar(c, aux2.data(), 2.0);
+            #pragma omp parallel for
+            for (long i = 0; i < n3; ++i) aux2[i] = a_q2[i] * aux2[i];
+            maybe_dealias(c, aux2.data(), 2.0);
+            for (int d = 0; d < 3; ++d) {
+                #pragma omp parallel for
+                for (long i = 0; i < n3; ++i) a3v[d * n3 + i] = aux2[i] * e[d * n3 + i];
+                if (c->p.to_dealias && c->p.dealias_e_u) dealias_scalar(c, a3v.data() + d * n3, 2.0);
+            }
+        } else {
+            for (int d = 0; d < 3; ++d)
+                #pragma omp parallel for
+                for (long i = 0; i < n3; ++i)
+                    aux2[i] = aux2[i] + u[d * n3 + i] * (vc * nu * dU[d * n3 + i] - pc * gradP[d * n3 + i]);
+            maybe_dealias(c, aux2.data(), 2.0);
+            {
+                RV a_q4(n3);
+                calc_uk(c, u, q - 4.0, a_q4.data());
+                #pragma omp parallel for
+                for (long i = 0; i < n3; ++i) aux2[i] = a_q4[i] * aux2[i];
+            }
+            maybe_dealias(c, aux2.data(), 2.0);
+            for (int d = 0; d < 3; ++d) {
+                #pragma omp parallel for
+                for (long i = 0; i < n3; ++i) a3v[d * n3 + i] = aux2[i] * u[d * n3 + i];
+                maybe_dealias(c, a3v.data() + d * n3, 2.0);
+            }
         }
     }
+    RV uq2u(m);
     for (int d = 0; d < 3; ++d) {
+        #pragma omp parallel for
         for (long i = 0; i < n3; ++i) uq2u[d * n3 + i] = a_q2[i] * u[d * n3 + i];
         maybe_dealias(c, uq2u.data() + d * n3, 2.0);
     }
-    divergence(c, uq2u.data(), aux3.data());
-    solve_poisson(c, aux3.data(), 1.0, aux4.data());
-    gradient(c, aux4.data(), a4v.data());
-    RV gU = grad_tensor(c, u);  // gU[k][i] = d_i u_k  (gradUk(:,:,:,ii))
-    for (int ii = 0; ii < 3; ++ii) {
-        for (long i = 0; i < n3; ++i)
-            a5v[ii * n3 + i] = GU(gU, c, 0, ii)[i] * a4v[0 * n3 + i] + GU(gU, c, 1, ii)[i] * a4v[1 * n3 + i] +
-                               GU(gU, c, 2, ii)[i] * a4v[2 * n3 + i];
-        maybe_dealias(c, a5v.data() + ii * n3, 2.0);
+    RV a4v(m);
+    {
+        RV aux3(n3), aux4(n3);
+        divergence(c, uq2u.data(), aux3.data());
+        solve_poisson(c, aux3.data(), 1.0, aux4.data());
+        gradient(c, aux4.data(), a4v.data());
     }
-    std::memcpy(a7v.data(), uq2u.data(), sizeof(double) * m);
-    laplacian(c, a7v.data());
+    RV a5v(m);
+    {
+        RV gU = grad_tensor(c, u);  // gU[k][i] = d_i u_k  (gradUk(:,:,:,ii))
+        for (int ii = 0; ii < 3; ++ii) {
+            #pragma omp parallel for
+            for (long i = 0; i < n3; ++i)
+                a5v[ii * n3 + i] = GU(gU, c, 0, ii)[i] * a4v[0 * n3 + i] + GU(gU, c, 1, ii)[i] * a4v[1 * n3 + i] +
+                                   GU(gU, c, 2, ii)[i] * a4v[2 * n3 + i];
+            maybe_dealias(c, a5v.data() + ii * n3, 2.0);
+        }
+    }
+    laplacian(c, uq2u.data());  // the a7v term: uq2u is not read again
+    const double* a7v = uq2u.data();
+    RV a6(n3);
     for (int d = 0; d < 3; ++d) {
-        for (long i = 0; i < n3; ++i) a4v[d * n3 + i] = a_q2[i] * gradP[d * n3 + i];
-        maybe_dealias(c, a4v.data() + d * n3, 2.0);
-        for (long i = 0; i < n3; ++i) a6v[d * n3 + i] = a_q2[i] * dU[d * n3 + i];
-        maybe_dealias(c, a6v.data() + d * n3, 2.0);
+        double* a4 = a4v.data() + d * n3;
+        #pragma omp parallel for
+        for (long i = 0; i < n3; ++i) a4[i] = a_q2[i] * gradP[d * n3 + i];
+        maybe_dealias(c, a4, 2.0);
+        #pragma omp parallel for
+        for (long i = 0; i < n3; ++i) a6[i] = a_q2[i] * dU[d * n3 + i];
+        maybe_dealias(c, a6.data(), 2.0);
+        #pragma omp parallel for
         for (long i = 0; i < n3; ++i)
-            v[d * n3 + i] = (q - 2.0) * a3v[d * n3 + i] - pc * a4v[d * n3 + i] + pc * 2.0 * a5v[d * n3 + i] +
-                            vc * nu * a6v[d * n3 + i] + vc * nu * a7v[d * n3 + i];
+            v[d * n3 + i] = (q - 2.0) * a3v[d * n3 + i] - pc * a4[i] + pc * 2.0 * a5v[d * n3 + i] +
+                            vc * nu * a6[i] + vc * nu * a7v[d * n3 + i];
     }
 }
 
@@ -777,6 +820,7 @@ double eval_J(orc_ctx* c, const double* field, int mode) {
 
 double lm_eval(orc_ctx* c, const double* phi, const double* d, double t, RV& buf) {
     const long m = 3 * c->n3;
+    #pragma omp parallel for
     for (long i = 0; i < m; ++i) buf[i] = phi[i] + t * d[i];
     return eval_J(c, buf.data(), 1);
 }
@@ -1014,17 +1058,21 @@ int orc_maxdlqdt(orc_ctx* c, double* uvec, int max_iter, double optim_tol, int s
         divavg_free(c, normalHs.data());                       // 169
         double alpha = field_inner(c, normalHs.data(), gradJ1.data(), 1);
         alpha = alpha / field_inner(c, normalHs.data(), normalHs.data(), 1);  // 170-171
+        #pragma omp parallel for
         for (long i = 0; i < m; ++i) gradJproj[i] = gradJ1[i] - alpha * normalHs[i];  // 177
         gu1 = gradJproj;                                                             // 202
         {
             double r = std::sqrt(field_inner(c, uvec, uvec, 1) / field_inner(c, gu1.data(), gu1.data(), 1));
+            #pragma omp parallel for
             for (long i = 0; i < m; ++i) gu1[i] = r * gu1[i];  // 213
         }
+        #pragma omp parallel for
         for (long i = 0; i < m; ++i) tmp[i] = gu1[i] - vtg0[i];
         double beta = field_inner(c, gu1.data(), tmp.data(), 1);       // 226
         double g0n = field_inner(c, gu0.data(), gu0.data(), 1);        // 227
         if (g0n < MACH_EPSILON || beta < MACH_EPSILON) beta = 0.0; else beta = beta / g0n;
         if (iter % resetEvery == 0) beta = 0.0;                        // 235-238
+        #pragma omp parallel for
         for (long i = 0; i < m; ++i) d1[i] = gu1[i] + beta * vtd0[i];  // 240
         double nG = std::sqrt(field_inner(c, gu1.data(), gu1.data(), 1));
         double nT = std::sqrt(field_inner(c, vtd0.data(), vtd0.data(), 1));
@@ -1048,9 +1096,11 @@ int orc_maxdlqdt(orc_ctx* c, double* uvec, int max_iter, double optim_tol, int s
             *flag = 4;
             tau1 = 0.0;
         }
+        #pragma omp parallel for
         for (long i = 0; i < m; ++i) tmp2[i] = tau1 * d1[i];
         vector_transport(c, uvec, q, Bc, tmp2.data(), gu1.data(), vtg0.data());  // 326
         vector_transport(c, uvec, q, Bc, tmp2.data(), d1.data(), vtd0.data());   // 327
+        #pragma omp parallel for
         for (long i = 0; i < m; ++i) uvec[i] = uvec[i] + tau1 * d1[i];           // 345
         rescale(c, uvec, Bc);                                                   // 346
         J1 = eval_J(c, uvec, 0);                                                // 349

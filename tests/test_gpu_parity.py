@@ -166,6 +166,28 @@ def test_maxdlqdt_trajectory(q):
     assert rel(uc, uo) < 1e-6
 
 
+def test_maxdlqdt_momentum_reset_and_rolling_stop_match_the_oracle():
+    """32 iterations at 16^3: beta is reset at iteration 25
+    (optimization.f90:235-238) and the rolling stop (439-445: the sum of the
+    last 10 relative improvements over the iteration count) ends the loop
+    after iteration 32 with OPTIM_TOL = 3e-5 (its value falls from 3.9e-5 to
+    2.6e-5 there, far from the threshold)."""
+    n, q = 16, 4.0
+    o = Oracle(n, q, 1.0)
+    u0 = seed_field(n, 0, 2.0, 2.0)
+    uo, it_o, fl_o, rec_o = o.maxdlqdt(u0, max_iter=40, optim_tol=3e-5)
+    c = mlq.MaxLq(n, q, 1.0, max_iter=40, optim_tol=3e-5)
+    uc, it_c, st_c, rec_c = c.maxdLqdt(u0)
+    c.close()
+    assert it_o == it_c == 32 and st_c == 0 and fl_o == 0
+    assert rec_o[24]["beta"] == 0.0 and rec_c[24]["beta"] == 0.0
+    assert all(r["beta"] > 0.0 for r in rec_c[1:24] + rec_c[25:])
+    for a, b in zip(rec_c, rec_o):
+        assert a["J1"] == pytest.approx(b["J1"], rel=1e-8)
+        assert a["tau"] == pytest.approx(b["tau"], rel=1e-5)
+    assert rel(uc, uo) < 1e-5
+
+
 def test_taylor_gpu_matches_oracle_kappa():
     n, q = 16, 4.0
     o = Oracle(n, q, 1.0)
