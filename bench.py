@@ -33,11 +33,26 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "CG iters/s at 512³ q=4: mixed vs FP64 GPU (rel ΔR≤1e-6); FFT HBM GB/s"
-# c2c N^3 transforms per CG iteration in the reference at q >= 4 (outside the
-# line search) and per eval_J("LineMin") trial, counted from its operator
-# sequence (optimization.f90:136-446 and the routines they call).
-REF_T_PER_ITER = 548
-REF_T_PER_TRIAL = 94
+# The calls one CG iteration of the reference makes at q >= 4
+# (optimization.f90:136-446), each timed as a whole reference-order call of
+# the CPU port; the line search adds n_evals calls of eval_J("LineMin")
+# (mnbrak 613-778 and brent 784-951).
+REF_CALLS = (
+    ("GradL2ForLq", 1),                  # 146
+    ("HilbertGradient", 2),              # 151, 164
+    ("divAvg_free", 2),                  # 153, 165
+    ("calcConstraintDerivativeL2", 1),   # 162
+    ("H inner product", 12),             # 170-171, 180 (2), 189, 213 (2), 226-227, 245-247
+    ("divergence", 1),                   # 188
+    ("calc0thFourierModes", 2),          # 251, 257
+    ("vectorTransport", 2),              # 324-325
+    ("rescaleLqNorm", 1),                # 346
+    ("eval_J maxdLqdt", 1),              # 349
+    ("calc_global_Lq_norm", 1),          # 421
+    ("calc_global_dLqdt_inclParts", 1),  # 423
+    ("CG algebra", 1),                   # the array updates 177, 213, 240, 329, 344, 432-436
+)
+TRIAL_CALL = "eval_J LineMin"
 
 
 def parse():
@@ -233,17 +248,121 @@ def run_path(ctx, u0, K, W, dist, profile=False):
             "iters": len(timed)}
 
 
-def cpu_reference_sample(n, q, n_evals, workers):
-    """One reference-order dealias round trip (2 c2c transforms) of an N^3 field
-    with the CPU transcription; returns (seconds per c2c transform, sample text)."""
-    from oracle.ref_numpy import RefNumpy
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
 
-    r = RefNumpy(n, q, workers=workers)
-    g = np.random.default_rng(0).standard_normal((n, n, n))
+
+class RefCallTimer:
+    """Whole reference-order calls of the CPU port (oracle/mlq_oracle.cpp,
+    OpenMP on every host core) at one grid size, on the seeded workload
+    field u (rescaled to B) and a seeded divergence-free direction d."""
+
+    def __init__(self, n, q, threads):
+        from oracle.oracle import Oracle
+        from oracle.seedfield import seed_field
+
+        self.n, self.q = n, q
+        self.o = Oracle(n, q, 1.0, threads=threads)
+        self.u = self.o.rescale(self.o.divavg_free(seed_field(n, 0, 2.0, n / 32.0)))
+        d = self.o.divavg_free(seed_field(n, 1, 2.0, n / 32.0))
+        self.d = d * np.sqrt(self.o.field_inner(self.u, self.u, "H") / self.o.field_inner(d, d, "H"))
+        self.tau = 0.05
+
+    def run(self, name):
+        o, u, d, q, tau = self.o, self.u, self.d, self.q, self.tau
+        t0 = time.perf_counter()
+        if name == "GradL2ForLq":
+            o.grad_l2(u)
+        elif name == "HilbertGradient":
+            o.hilbert_gradient(d, 1.5 - 1.0 / q)
+        elif name == "divAvg_free":
+            o.divavg_free(d)
+        elif name == "calcConstraintDerivativeL2":
+            o.normal_l2(u)
+        elif name == "H inner product":
+            o.field_inner(u, d, "H")
+        elif name == "divergence":
+            o.divergence(d)
+        elif name == "calc0thFourierModes":
+            o.zeroth_modes(d)
+        elif name == "vectorTransport":
+            o.vector_transport(u, tau * d, d)
+        elif name == "rescaleLqNorm":
+            o.rescale(u)
+        elif name == "eval_J maxdLqdt":
+            o.eval_J(u, "maxdLqdt")
+        elif name == "calc_global_Lq_norm":
+            o.lq_norm(u)
+        elif name == "calc_global_dLqdt_inclParts":
+            o.R_parts(u)
+        elif name == TRIAL_CALL:
+            o.eval_J(u + tau * d, "LineMin")
+        elif name == "CG algebra":
+            # gradJproj, the normalisation, d1, uvec0, Uvec + tau d1 and the
+            # shift of the CG memory: about ten passes over a vector field
+            a = u.copy()
+            for _ in range(3):
+                a = u - tau * d
+                a = tau * a
+                a = a + tau * d
+        elif name == "dealias_scalar":
+            o.dealias_scalar(u[0], 2.0)
+        else:
+            raise KeyError(name)
+        return time.perf_counter() - t0
+
+
+def compose_iteration(t, n_evals):
+    """Seconds of one reference CG iteration from whole-call times t[name]."""
+    return sum(c * t[name] for name, c in REF_CALLS) + n_evals * t[TRIAL_CALL]
+
+
+ALL_CALLS = [name for name, _ in REF_CALLS] + [TRIAL_CALL]
+
+
+def cpu_reference_baseline(n, q, n_evals, threads, sample_n=256, check_n=64):
+    """The reference's CG iteration on the host cores, from timed whole calls.
+
+    Every call of one iteration (REF_CALLS and the n_evals line-search trials)
+    is timed once as a whole reference-order call at sample_n^3; the sum is
+    scaled to n^3 by the measured ratio of a whole dealias_scalar call at n^3
+    and at sample_n^3.  The same composition is checked against one fully
+    timed reference-order CG iteration (the oracle's maxdLqdt) at check_n^3."""
+    out = {}
+    small = RefCallTimer(check_n, q, threads)
     t0 = time.perf_counter()
-    r.dealias(g, 2.0)
-    dt = time.perf_counter() - t0
-    return dt / 2.0
+    _, it, _, rec = small.o.maxdlqdt(small.u, max_iter=1, optim_tol=1e-14)
+    t_full = time.perf_counter() - t0
+    ne_small = rec[0]["n_evals"] if rec else n_evals
+    t_small = {k: min(small.run(k) for _ in range(3)) for k in ALL_CALLS}
+    out["c1_full_iteration_iters_per_s"] = 1.0 / t_full
+    out["c1_composed_over_measured"] = compose_iteration(t_small, ne_small) / t_full
+    del small
+    mid = RefCallTimer(sample_n, q, threads)
+    t_mid = {k: mid.run(k) for k in ALL_CALLS}
+    t_dm = min(mid.run("dealias_scalar") for _ in range(2))
+    del mid
+    if n != sample_n:
+        big = RefCallTimer(n, q, threads)
+        t_db = min(big.run("dealias_scalar") for _ in range(2))
+        del big
+    else:
+        t_db = t_dm
+    ratio = t_db / t_dm
+    it_s = compose_iteration(t_mid, n_evals) * ratio
+    out["value"] = 1.0 / it_s
+    out["size_ratio"] = ratio
+    out["calls_s"] = {k: round(v, 4) for k, v in t_mid.items()}
+    out["sample"] = (f"the oracle port (reference order, {threads} host threads): every call of one reference CG "
+                     f"iteration timed whole at {sample_n}^3 ({', '.join(f'{c} x {k}' for k, c in REF_CALLS)}, "
+                     f"{n_evals:.1f} x eval_J LineMin), scaled to {n}^3 by the measured {n}^3/{sample_n}^3 time "
+                     f"ratio {ratio:.2f} of a whole dealias_scalar call; composition checked against one fully timed "
+                     f"CG iteration at {check_n}^3 (composed/measured "
+                     f"{out['c1_composed_over_measured']:.2f})")
+    return out
 
 
 def workload_name(n, q):
@@ -252,37 +371,61 @@ def workload_name(n, q):
 
 
 def bench_reference(args, dist):
-    """--impl reference: the reference algorithm (reference-order CPU
-    transcription, scipy pocketfft on all host threads) on the host cores."""
+    """--impl reference: the reference's CG iteration on the host cores (the
+    reference-order CPU port, every host thread).  Each step times one whole
+    reference-order call of the iteration at 256^3 (cycling through every call
+    the iteration makes), or a whole dealias_scalar at the workload size and
+    at 256^3 for the size ratio; the iteration is composed from the per-call
+    means as in cpu_reference_baseline."""
     if dist.rank != 0:
         dist.close()
         return
     n, q = args.n, args.q
-    workers = os.cpu_count() or 1
+    threads = host_cores()
+    sample_n = min(256, n)
+    mid = RefCallTimer(sample_n, q, threads)
+    big = RefCallTimer(n, q, threads) if n != sample_n else mid
+    kinds = ALL_CALLS + ["dealias_scalar@big", "dealias_scalar@mid"]
+    times = {k: [] for k in kinds}
+    step_s = []
+    total = args.warmup + args.steps
+    # every kind is timed at least once even when there are fewer steps
+    order = [kinds[i % len(kinds)] for i in range(max(total, len(kinds)))]
+    for i, k in enumerate(order):
+        if k == "dealias_scalar@big":
+            dt = big.run("dealias_scalar")
+        elif k == "dealias_scalar@mid":
+            dt = mid.run("dealias_scalar")
+        else:
+            dt = mid.run(k)
+        times[k].append(dt)
+        if i >= args.warmup and len(step_s) < args.steps:
+            step_s.append(dt)
+    mean = {k: statistics.fmean(v) for k, v in times.items()}
+    ratio = mean["dealias_scalar@big"] / mean["dealias_scalar@mid"]
     n_evals = REF_TRIALS_PER_ITER
-    per_iter = []
-    for i in range(args.warmup + args.steps):
-        t_T = cpu_reference_sample(n, q, n_evals, workers)
-        if i >= args.warmup:
-            per_iter.append(t_T * (REF_T_PER_ITER + REF_T_PER_TRIAL * n_evals))
-    tot = sum(per_iter)
-    value = len(per_iter) / tot
-    sample = (f"one reference-order dealias_scalar round trip (2 c2c {n}^3 FFTs, scipy pocketfft, "
-              f"{workers} threads) per step, scaled by the reference's {REF_T_PER_ITER} + {REF_T_PER_TRIAL} x "
-              f"{n_evals} transforms per CG iteration")
+    it_s = compose_iteration(mean, n_evals) * ratio
+    value = 1.0 / it_s
+    sample = (f"the oracle port (reference order, {threads} host threads): each step one whole call of the "
+              f"reference CG iteration at {sample_n}^3, cycling through all of its calls "
+              f"({', '.join(f'{c} x {k}' for k, c in REF_CALLS)}, {n_evals} x eval_J LineMin) and a whole "
+              f"dealias_scalar at {n}^3 and {sample_n}^3; iteration = sum of the per-call means x counts, scaled "
+              f"to {n}^3 by the measured dealias time ratio {ratio:.2f}")
     line = {"metric": METRIC, "value": value, "unit": "iters/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * tot / len(per_iter), "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * statistics.fmean(step_s), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": workload_name(n, q), "n": n, "q": q},
-            "cpu_baseline": {"value": value, "unit": "iters/s", "cores": workers, "kind": "port", "sample": sample},
+            "config": {"workload": workload_name(n, q), "n": n, "q": q,
+                       "step": "one whole reference-order call (see cpu_baseline.sample); ms_per_step is its mean",
+                       "iteration_s": it_s, "calls_s": {k: round(v, 4) for k, v in mean.items()}},
+            "cpu_baseline": {"value": value, "unit": "iters/s", "cores": threads, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     dist.close()
 
 
-# trials per CG iteration used to scale the CPU sample: the mean count the GPU
-# run measures on this workload is reported beside it in our arm's line
+# trials per CG iteration of the reference arm's composition: the mean count
+# the GPU run measures on this workload (12.3-12.8) is used in our arm's line
 REF_TRIALS_PER_ITER = 12
 
 
@@ -530,15 +673,31 @@ def main():
 
     # the all-FP64 path, and the accuracy of the mixed path against it on the
     # same field: relative |R_mixed - R_fp64| / |R_fp64|
-    res_d, rel_dR = None, None
+    res_d, rel_dR, acc = None, None, {}
     if not args.no_fp64:
         fp64 = mlq.MaxLq(n, q, 1.0, precision="fp64", device=dev, optim_tol=0.0)
         res_d = run_path(fp64, u0, K, W, dist)
+        # after the timed iterations: R of the mixed path's own state, by the
+        # mixed and by the FP64 pipeline
+        u_end = mixed.state_store()
+        R_mK, _ = mixed.state_R()
+        fp64.state_load(u_end)
+        fp64.state_iterate(0)  # the pre-loop steps only (rescale, projection)
+        R_dK, _ = fp64.state_R()
+        acc["rel_dR_mixed_vs_fp64_after_timed"] = abs(R_mK[0] - R_dK[0]) / abs(R_dK[0])
+        # at the start (u0 after the pre-loop steps), and against the oracle
         fp64.state_load(u0)
+        fp64.state_iterate(0)
         R_d0, _ = fp64.state_R()
         mixed.state_load(u0)
+        mixed.state_iterate(0)
         R_m0, _ = mixed.state_R()
         rel_dR = abs(R_m0[0] - R_d0[0]) / abs(R_d0[0])
+        fx = os.path.join(ROOT, "tests", "golden", f"headline_n{n}_q{q:g}.npz")
+        if seed == 0 and os.path.exists(fx):
+            R_or = float(np.load(fx)["R_parts"][0])
+            acc["rel_dR_mixed_vs_oracle_iter0"] = abs(R_m0[0] - R_or) / abs(R_or)
+            acc["rel_dR_fp64_vs_oracle_iter0"] = abs(R_d0[0] - R_or) / abs(R_or)
         fp64.close()
 
     # e2e: each step copies u host->device from pinned host memory, iterates
@@ -587,14 +746,12 @@ def main():
     n_evals = [r["n_evals"] for r in res_m["records"]]
     cpu = None
     if dist.rank == 0 and not args.no_cpu:
-        workers = os.cpu_count() or 1
+        threads = host_cores()
         ne = float(np.mean(n_evals)) if n_evals else REF_TRIALS_PER_ITER
-        t_T = cpu_reference_sample(n, q, ne, workers)
-        it_s = t_T * (REF_T_PER_ITER + REF_T_PER_TRIAL * ne)
-        cpu = {"value": 1.0 / it_s, "unit": "iters/s", "cores": workers, "kind": "port",
-               "sample": (f"one reference-order dealias_scalar round trip (2 c2c {n}^3 FFTs, scipy pocketfft, "
-                          f"{workers} threads), scaled by the reference's {REF_T_PER_ITER} + {REF_T_PER_TRIAL} x "
-                          f"{ne:.1f} transforms per CG iteration")}
+        cb = cpu_reference_baseline(n, q, ne, threads, sample_n=min(256, n))
+        cpu = {"value": cb["value"], "unit": "iters/s", "cores": threads, "kind": "port", "sample": cb["sample"],
+               "c1_full_iteration_iters_per_s": cb["c1_full_iteration_iters_per_s"],
+               "c1_composed_over_measured": cb["c1_composed_over_measured"], "calls_s": cb["calls_s"]}
 
     kcfg = mixed.kernel_config()
     per_kernel = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
@@ -608,7 +765,7 @@ def main():
                        "n": n, "q": q, "precision": "mixed: FP32 fields and FFTs, FP64 state/reductions/control",
                        "fp64_iters_per_s": fp64_value,
                        "mixed_over_fp64": (value / fp64_value) if fp64_value else None,
-                       "rel_dR_mixed_vs_fp64": rel_dR,
+                       "rel_dR_mixed_vs_fp64": rel_dR, **acc,
                        "line_search_trials_per_iter": float(np.mean(n_evals)) if n_evals else None,
                        "l2": "working set (GBs) far above the 126 MB L2; no flush needed",
                        "parallelism": f"replicas x{dist.world}",
