@@ -184,7 +184,8 @@ def test_maxdlqdt_momentum_reset_and_rolling_stop_match_the_oracle():
     assert all(r["beta"] > 0.0 for r in rec_c[1:24] + rec_c[25:])
     for a, b in zip(rec_c, rec_o):
         assert a["J1"] == pytest.approx(b["J1"], rel=1e-8)
-        assert a["tau"] == pytest.approx(b["tau"], rel=1e-5)
+        # Brent stops at TOL = 1e-6 relative to its bracket (optimization.f90:804)
+        assert a["tau"] == pytest.approx(b["tau"], rel=1e-4)
     assert rel(uc, uo) < 1e-5
 
 
