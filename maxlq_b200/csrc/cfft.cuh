@@ -299,6 +299,8 @@ struct YShape {
     // more warps to hide latency)
     static constexpr bool CW = V == 5 || V == 6;
     static constexpr bool MB3 = V == 7;
+    // 8: the y pass on column pairs (FP32 only; ypass_pair_kernel, PairShape)
+    static constexpr bool PAIR = V == 8;
     static constexpr int VB = (CW || MB3) ? 0 : (V >= 3 ? V - 3 : V);
     static constexpr int EY = CW ? N / 32 : (VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8)));
     static constexpr int TX = CW ? (V == 5 ? (F32 ? 8 : 4) : (F32 ? 16 : 2))
@@ -325,11 +327,11 @@ struct YShape {
     static constexpr int YMINB = CW ? (CW_MINB < 1 ? 1 : CW_MINB)
                                     : MB3 ? 3 : (TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1)));
     static constexpr bool valid =
-        V == 0 ||
+        V == 0 || (PAIR ? (F32 && N >= 64 && N <= 1024) :
         (MB3 ? (N >= 256 && YTHREADS <= 256 && 3 * (ZSMEM + 1024) <= 228 * 1024) :
          CW ? (N >= 256 && EY >= 2 && EY <= 16 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 227 * 1024)
             : (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
-               (V >= 3 || EY != CShape<N, T>::EY || TX != CShape<N, T>::TX) && (V != 4 || F32)));
+               (V >= 3 || EY != CShape<N, T>::EY || TX != CShape<N, T>::TX) && (V != 4 || F32))));
     static_assert(V != 0 || ZSMEM <= 200 * 1024, "default y/z tile fits the shared-memory limit");
 };
 
@@ -405,12 +407,13 @@ __global__ void __launch_bounds__(256, 2)
     }
     const cpx<T> wt = twN[t];  // W_N^t
     const int nx_in = a.nx_in;
+    const int px = a.px ? a.px : nx_in;  // row pitch of xs
     const cpx<T>* __restrict__ src0 = a.in[blockIdx.y];
     T* __restrict__ dst0 = a.out[blockIdx.y];
     const int src_lane = (TPL - t) & (TPL - 1);
     for (long g = blockIdx.x; g < NG; g += gridDim.x) {
         const long line = g * LPB + ls;
-        const cpx<T>* __restrict__ src = src0 + line * nx_in;
+        const cpx<T>* __restrict__ src = src0 + line * px;
         cpx<T> v[E];
 #pragma unroll
         for (int m = 0; m < E; ++m) {
@@ -496,6 +499,7 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
     }
     const cpx<T> wt = twN[t];  // W_N^t
     const int nx = a.nx;
+    const int px = a.px ? a.px : nx;  // row pitch of xs
     const int src_lane = (TPL - t) & (TPL - 1);
     double acc[NR > 0 ? NR : 1];
 #pragma unroll
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
             }
             cfft<L, E, -1, SyncWarp>(v, t, sm, map, tw);
             if (t == 0 && a.nanflag && !cpx_finite(v[0])) *a.nanflag = 1.0;  // the DC bin of the line
-            cpx<T>* __restrict__ dst = a.out[o] + line * nx;
+            cpx<T>* __restrict__ dst = a.out[o] + line * px;
             // X[k] = E[k] + W_N^k O[k], E = (Z_k + conj Z_{L-k})/2, O = -i (Z_k - conj Z_{L-k})/2
             SFor<0, E>::run([&](auto mc) {
                 constexpr int m = decltype(mc)::value;
@@ -558,6 +562,7 @@ __global__ void __launch_bounds__(256, xfwd_minb<F>())
             });
             // Nyquist column (full band only): X[N/2] = Re Z0 - Im Z0
             if (t == 0 && L < nx) dst[L] = mk(v[0].x - v[0].y, T(0));
+            if (t == 0 && nx < px) dst[nx] = czero<T>();  // the pitch's pad column stays zero
             __syncwarp();
         }
     }
@@ -582,6 +587,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const YTw<N, E, T, S::TWREG> tw(stw, twN, t);
     const ColMap<TX> map{l};
     const int nx = a.nx, nb = a.band.nb;
+    const int px = a.px ? a.px : nx;  // row pitch of xs and ys
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)a.nz * ntile;
     const cpx<T>* __restrict__ src = a.in[blockIdx.y];
@@ -596,10 +602,10 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         for (int m = 0; m < E; ++m) {
             const int p = t + TPL * m;
             if constexpr (SIGN < 0) {
-                cp_async_elem(b + p * TX + l, src + ((long)z * N + p) * nx + kxc, ok);
+                cp_async_elem(b + p * TX + l, src + ((long)z * N + p) * px + kxc, ok);
             } else {
                 const int ci = band_compact_index(a.band, p);
-                cp_async_elem(b + p * TX + l, src + ((long)z * nb + (ci >= 0 ? ci : 0)) * nx + kxc, ok && ci >= 0);
+                cp_async_elem(b + p * TX + l, src + ((long)z * nb + (ci >= 0 ? ci : 0)) * px + kxc, ok && ci >= 0);
             }
         }
         cp_async_commit();
@@ -626,9 +632,9 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
                 const int p = t + TPL * m;
                 if constexpr (SIGN < 0) {
                     const int ci = band_compact_index(a.band, p);
-                    if (ci >= 0) dst[((long)z * nb + ci) * nx + kx] = v[m];
+                    if (ci >= 0) dst[((long)z * nb + ci) * px + kx] = v[m];
                 } else {
-                    dst[((long)z * N + p) * nx + kx] = v[m];
+                    dst[((long)z * N + p) * px + kx] = v[m];
                 }
             }
         }
@@ -862,7 +868,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)nb * ntile;
     const ZFwdOp& op = a.op[blockIdx.y];
-    const int plane = nb * nx;
+    const int plane = nb * nx;                      // spectra
+    const int px = a.px ? a.px : nx, yplane = nb * px;  // y-stage arrays
     const cpx<T>* __restrict__ src = reinterpret_cast<const cpx<T>*>(op.in);
     cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
     const SymD<C> dmain = make_symd<C>(op.sym, op.sym_ab, a.norm);  // the 1/N^3 folded in
@@ -873,9 +880,9 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         const int cy = (int)(it / ntile);
         const int kx = (int)(it - (long)cy * ntile) * TX + l;
         const bool ok = kx < nx;
-        const int col = cy * nx + (ok ? kx : nx - 1);
+        const int ycol = cy * px + (ok ? kx : nx - 1);
 #pragma unroll
-        for (int m = 0; m < E; ++m) cp_async_elem(b + (t + TPL * m) * TX + l, src + (t + TPL * m) * plane + col, ok);
+        for (int m = 0; m < E; ++m) cp_async_elem(b + (t + TPL * m) * TX + l, src + (t + TPL * m) * yplane + ycol, ok);
         cp_async_commit();
     };
     long it0 = blockIdx.x;
@@ -908,7 +915,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
             cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
             if (ok) {
 #pragma unroll
-                for (int m = 0; m < E; ++m) yout[(t + TPL * m) * plane + col] = v[m];
+                for (int m = 0; m < E; ++m) yout[(t + TPL * m) * yplane + cy * px + kx] = v[m];
             }
         }
     }
@@ -938,7 +945,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)nb * ntile;
     const ZInvOp& op = a.op[blockIdx.y];
-    const int plane = nb * nx;
+    const int plane = nb * nx;                      // spectra
+    const int px = a.px ? a.px : nx, yplane = nb * px;  // y-stage arrays
     const int nsrc = op.nsrc;
     cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out);
     for (long it = blockIdx.x; it < items; it += gridDim.x) {
@@ -979,7 +987,162 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
         if (ok) {
 #pragma unroll
-            for (int m = 0; m < E; ++m) dst[(t + TPL * m) * plane + col] = v[m];
+            for (int m = 0; m < E; ++m) dst[(t + TPL * m) * yplane + cy * px + kx] = v[m];
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
+// y pass on column pairs (FP32, variant V = 8 of YShape).  Each thread
+// transforms the two neighbouring kx columns 2j and 2j+1 of a tile at once:
+// they share every twiddle, index and address computation, and move through
+// global and shared memory as one 16-byte float4 (a row pitch that is even
+// keeps every pair 16-byte aligned; the pad column of an odd nx rides along
+// as the second column of the last pair).  E = 8 elements per column and
+// thread, radix-8 Stockham stages.  Tile: NP = 4 pairs (8 columns) x N rows
+// of float4, swizzled so that the stage exchanges are free of bank conflicts.
+// ----------------------------------------------------------------------------
+template <int N>
+struct PairShape {
+    static constexpr int E = 8, NP = 4;
+    static constexpr int TPL = N / E;         // threads per column pair
+    static constexpr int THREADS = NP * TPL;
+    static constexpr int TILE = N * NP;       // float4 slots of one tile
+    static constexpr size_t SMEM = (size_t)2 * TILE * sizeof(float4) + (size_t)N * sizeof(cpx<float>);
+    static_assert(THREADS % 32 == 0 && THREADS <= 512, "pair block");
+};
+
+// slot of row p, pair l: row-major, with rows 8..15 (mod 16) swapped with
+// their neighbour row so that rows p and p + 8 fall in different halves of
+// the 8 16-byte bank groups (16-byte accesses are served 8 threads at a time)
+__device__ __forceinline__ int pair_slot(int p, int l) { return (4 * p + l) ^ (((p >> 3) & 1) << 2); }
+
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+
+template <int L, int E, int S, int SIGN, class Tw>
+__device__ __forceinline__ void pstage(cpx<float> (&va)[E], cpx<float> (&vb)[E], int t, int l, float4* sm,
+                                       const Tw& tw) {
+    using P = CPlan<L, E>;
+    constexpr int R = P::radix(S), NS = P::ns(S), Q = E / R, TPL = P::TPL;
+    constexpr bool LAST = S == P::NST - 1;
+    SFor<0, Q>::run([&](auto ic) {
+        constexpr int I = decltype(ic)::value;
+        const int b = t + TPL * I;
+        const int k = b & (NS - 1);
+        cpx<float> a[R], c[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            a[r] = va[I + Q * r];
+            c[r] = vb[I + Q * r];
+        }
+        if constexpr (S > 0) {
+            SFor<1, R>::run([&](auto rc) {
+                constexpr int RI = decltype(rc)::value;
+                const cpx<float> w = tw.template get<S, I, RI>(k);
+                a[RI] = cmul_s<SIGN>(a[RI], w);
+                c[RI] = cmul_s<SIGN>(c[RI], w);
+            });
+        }
+        dftR<R, SIGN>(a);
+        dftR<R, SIGN>(c);
+        if constexpr (LAST) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                va[I + Q * r] = a[r];
+                vb[I + Q * r] = c[r];
+            }
+        } else {
+            const int base = (b - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) sm[pair_slot(base + r * NS, l)] = make_float4(a[r].x, a[r].y, c[r].x, c[r].y);
+        }
+    });
+    if constexpr (!LAST) {
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const float4 q = sm[pair_slot(t + TPL * m, l)];
+            va[m] = mk(q.x, q.y);
+            vb[m] = mk(q.z, q.w);
+        }
+        __syncthreads();
+    }
+}
+
+template <int N, int SIGN>
+__global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
+    ypass_pair_kernel(YArgs<float> a, const cpx<float>* __restrict__ twN) {
+    using S = PairShape<N>;
+    constexpr int E = S::E, TPL = S::TPL, NP = S::NP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* buf0 = reinterpret_cast<float4*>(smem_raw);
+    float4* buf1 = buf0 + S::TILE;
+    cpx<float>* stw = reinterpret_cast<cpx<float>*>(buf1 + S::TILE);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    __syncthreads();
+    const int l = threadIdx.x % NP, t = threadIdx.x / NP;
+    const TwTab<N, E, float> tw{stw};
+    const int nx = a.nx, nb = a.band.nb;
+    const int pp = (a.px ? a.px : nx) / 2;  // row pitch in pairs (the pitch is even)
+    const int npair = (nx + 1) / 2;
+    const int ntile = (npair + NP - 1) / NP;
+    const long items = (long)a.nz * ntile;
+    const float4* __restrict__ src = reinterpret_cast<const float4*>(a.in[blockIdx.y]);
+    float4* __restrict__ dst = reinterpret_cast<float4*>(a.out[blockIdx.y]);
+    auto stage = [&](long it, float4* b) {
+        const int z = (int)(it / ntile);
+        const int pr = (int)(it - (long)z * ntile) * NP + l;
+        const bool ok = pr < npair;
+        const int prc = ok ? pr : npair - 1;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int p = t + TPL * m;
+            if constexpr (SIGN < 0) {
+                cp_async16(b + pair_slot(p, l), src + ((long)z * N + p) * pp + prc, ok);
+            } else {
+                const int ci = band_compact_index(a.band, p);
+                cp_async16(b + pair_slot(p, l), src + ((long)z * nb + (ci >= 0 ? ci : 0)) * pp + prc, ok && ci >= 0);
+            }
+        }
+        cp_async_commit();
+    };
+    long it = blockIdx.x;
+    if (it < items) stage(it, buf0);
+    for (int k = 0; it < items; it += gridDim.x, k ^= 1) {
+        float4* cur = k ? buf1 : buf0;
+        float4* nxt = k ? buf0 : buf1;
+        cp_async_wait_all();
+        cpx<float> va[E], vb[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const float4 q = cur[pair_slot(t + TPL * m, l)];
+            va[m] = mk(q.x, q.y);
+            vb[m] = mk(q.z, q.w);
+        }
+        // every thread has its pair in registers and the previous transform is
+        // done: cur becomes this transform's exchange buffer, nxt the next stage
+        __syncthreads();
+        if (it + gridDim.x < items) stage(it + gridDim.x, nxt);
+        SFor<0, CPlan<N, E>::NST>::run(
+            [&](auto sc) { pstage<N, E, decltype(sc)::value, SIGN>(va, vb, t, l, cur, tw); });
+        const int z = (int)(it / ntile);
+        const int pr = (int)(it - (long)z * ntile) * NP + l;
+        if (pr < npair) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int p = t + TPL * m;
+                const float4 q = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+                if constexpr (SIGN < 0) {
+                    const int ci = band_compact_index(a.band, p);
+                    if (ci >= 0) dst[((long)z * nb + ci) * pp + pr] = q;
+                } else {
+                    dst[((long)z * N + p) * pp + pr] = q;
+                }
+            }
         }
     }
 }
@@ -1032,6 +1195,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const TwTab<N, E, T> tw{stw};
     const RowMap<E> xmap{g.w * S::WPITCH};
     const int nx = a.nx, nb = a.band.nb;
+    const int px = a.px ? a.px : nx;  // row pitch of xs and ys
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)a.nz * ntile;
     const cpx<T>* __restrict__ src = a.in[blockIdx.y];
@@ -1045,10 +1209,10 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         for (int m = 0; m < E; ++m) {
             const int p = g.ts + SR * m;
             if constexpr (SIGN < 0) {
-                cp_async_elem(b + g.slot(m), src + ((long)z * N + p) * nx + kxc, ok);
+                cp_async_elem(b + g.slot(m), src + ((long)z * N + p) * px + kxc, ok);
             } else {
                 const int ci = band_compact_index(a.band, p);
-                cp_async_elem(b + g.slot(m), src + ((long)z * nb + (ci >= 0 ? ci : 0)) * nx + kxc, ok && ci >= 0);
+                cp_async_elem(b + g.slot(m), src + ((long)z * nb + (ci >= 0 ? ci : 0)) * px + kxc, ok && ci >= 0);
             }
         }
         cp_async_commit();
@@ -1076,9 +1240,9 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
                 const int p = g.ts + SR * m;
                 if constexpr (SIGN < 0) {
                     const int ci = band_compact_index(a.band, p);
-                    if (ci >= 0) dst[((long)z * nb + ci) * nx + kx] = cur[g.slot(m)];
+                    if (ci >= 0) dst[((long)z * nb + ci) * px + kx] = cur[g.slot(m)];
                 } else {
-                    dst[((long)z * N + p) * nx + kx] = cur[g.slot(m)];
+                    dst[((long)z * N + p) * px + kx] = cur[g.slot(m)];
                 }
             }
         }
@@ -1108,7 +1272,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)nb * ntile;
     const ZFwdOp& op = a.op[blockIdx.y];
-    const int plane = nb * nx;
+    const int plane = nb * nx;                      // spectra
+    const int px = a.px ? a.px : nx, yplane = nb * px;  // y-stage arrays
     const cpx<T>* __restrict__ src = reinterpret_cast<const cpx<T>*>(op.in);
     cpx<T>* __restrict__ yout = reinterpret_cast<cpx<T>*>(op.ys_out);
     const SymD<C> dmain = make_symd<C>(op.sym, op.sym_ab, a.norm);  // the 1/N^3 folded in
@@ -1118,9 +1283,9 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         const int cy = (int)(it / ntile);
         const int kx = (int)(it - (long)cy * ntile) * TX + g.ls;
         const bool ok = kx < nx;
-        const int col = cy * nx + (ok ? kx : nx - 1);
+        const int ycol = cy * px + (ok ? kx : nx - 1);
 #pragma unroll
-        for (int m = 0; m < E; ++m) cp_async_elem(b + g.slot(m), src + (g.ts + SR * m) * plane + col, ok);
+        for (int m = 0; m < E; ++m) cp_async_elem(b + g.slot(m), src + (g.ts + SR * m) * yplane + ycol, ok);
         cp_async_commit();
     };
     long it0 = blockIdx.x;
@@ -1161,7 +1326,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
             __syncthreads();
             if (ok) {
 #pragma unroll
-                for (int m = 0; m < E; ++m) yout[(g.ts + SR * m) * plane + col] = cur[g.slot(m)];
+                for (int m = 0; m < E; ++m) yout[(g.ts + SR * m) * yplane + cy * px + kx] = cur[g.slot(m)];
             }
         }
     }
@@ -1191,7 +1356,8 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
     const int ntile = (nx + TX - 1) / TX;
     const long items = (long)nb * ntile;
     const ZInvOp& op = a.op[blockIdx.y];
-    const int plane = nb * nx;
+    const int plane = nb * nx;                      // spectra
+    const int px = a.px ? a.px : nx, yplane = nb * px;  // y-stage arrays
     const int nsrc = op.nsrc;
     cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out);
     int kbuf = 0;
@@ -1240,7 +1406,7 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
         __syncthreads();
         if (ok) {
 #pragma unroll
-            for (int m = 0; m < E; ++m) dst[(g.ts + SR * m) * plane + col] = cur[g.slot(m)];
+            for (int m = 0; m < E; ++m) dst[(g.ts + SR * m) * yplane + cy * px + kx] = cur[g.slot(m)];
         }
     }
 }

@@ -318,6 +318,14 @@ class Engine : public EngineBase {
     cpx<T>* ysbuf(int i);                 // [n][nbcap][nxcap]
     cpx<T>* wspec(int i);                 // work spectrum in band b2, nb*nb*nx
     int nxcap, nbcap;
+    // Row pitch (elements) of the x- and y-stage arrays of band b: rounded up
+    // to even in FP32 with the compile-time kernels, so that every row starts
+    // on a 16-byte boundary and two neighbouring kx columns move as one
+    // 16-byte vector; the pad column is kept zero.  Spectra keep pitch nx.
+    bool pitch_even_ = false;
+    int px_of(int nx) const { return pitch_even_ ? ((nx + 1) & ~1) : nx; }
+    int px_of(const Band& b) const { return px_of(b.nx); }
+    int pxcap() const { return px_of(nxcap); }
     std::vector<T*> phys_;
     std::vector<cpx<T>*> xs_, ys_, ws_;
 

@@ -27,6 +27,7 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
     reg_ok_ = n >= 64 && (n & (n - 1)) == 0;
     cfft_ok_ = reg_ok_ && n <= 1024;
     if (const char* kv = std::getenv("MLQ_PASS_KERNELS")) cfft_ok_ = cfft_ok_ && std::string(kv) != "reg";
+    pitch_even_ = cfft_ok_ && sizeof(T) == 4;
     {
         int dev = 0;
         MLQ_CUDA(cudaGetDevice(&dev));
@@ -144,6 +145,24 @@ template <typename T>
 template <int NN, int V>
 void Engine<T>::y_cv(YArgs<T>& ya, int sign, int narr) {
     using S = YShape<NN, T, V>;
+    if constexpr (S::PAIR) {
+        if constexpr (std::is_same<T, float>::value) {
+            using PS = PairShape<NN>;
+            const size_t smem = PS::SMEM;
+            const long items = (long)ya.nz * (((ya.nx + 1) / 2 + PS::NP - 1) / PS::NP);
+            auto run = [&](auto kern) {
+                allow_smem(kern);
+                const int G = persistent_blocks((const void*)kern, PS::THREADS, smem);
+                dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
+                kern<<<grid, PS::THREADS, smem, stream>>>(ya, d_twT_ + tw_off.at(NN));
+            };
+            if (sign < 0)
+                run(ypass_pair_kernel<NN, -1>);
+            else
+                run(ypass_pair_kernel<NN, +1>);
+        }
+        return;
+    }
     const size_t smem = S::YSMEM;
     const long items = (long)ya.nz * ((ya.nx + S::TX - 1) / S::TX);
     auto run = [&](auto kern) {
@@ -168,6 +187,10 @@ void Engine<T>::y_cv(YArgs<T>& ya, int sign, int narr) {
 template <typename T>
 template <int NN, int V>
 void Engine<T>::zfwd_cv(ZFwdArgs<T>& za, int narr) {
+    if constexpr (YShape<NN, T, V>::PAIR) {
+        zfwd_cv<NN, 0>(za, narr);
+        return;
+    }
     using S = YShape<NN, T, V>;
     const size_t smem = S::ZSMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
@@ -189,6 +212,10 @@ void Engine<T>::zfwd_cv(ZFwdArgs<T>& za, int narr) {
 template <typename T>
 template <int NN, int V>
 void Engine<T>::zinv_cv(ZInvArgs<T>& za, int narr) {
+    if constexpr (YShape<NN, T, V>::PAIR) {
+        zinv_cv<NN, 0>(za, narr);
+        return;
+    }
     using S = YShape<NN, T, V>;
     const size_t smem = S::ZISMEM;
     const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
@@ -229,6 +256,9 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
     }
     if constexpr (YShape<NN, T, 7>::valid) {
         if (v == 7) return f(std::integral_constant<int, 7>{});
+    }
+    if constexpr (YShape<NN, T, 8>::valid) {
+        if (v == 8 && (kind == YV_YFWD || kind == YV_YINV)) return f(std::integral_constant<int, 8>{});
     }
     f(std::integral_constant<int, 0>{});
 }
@@ -278,7 +308,7 @@ void Engine<T>::tune_yz() {
     bool any = false;
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
-        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid || YShape<NN, T, 3>::valid ||
+        any = YShape<NN, T, 1>::valid || YShape<NN, T, 2>::valid || YShape<NN, T, 3>::valid || YShape<NN, T, 8>::valid ||
               YShape<NN, T, 5>::valid || YShape<NN, T, 6>::valid || YShape<NN, T, 7>::valid;
     });
     if (!any) return;
@@ -290,16 +320,17 @@ void Engine<T>::tune_yz() {
             ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid) ||
                  (v == 3 && YShape<NN, T, 3>::valid) || (v == 4 && YShape<NN, T, 4>::valid) ||
                  (v == 5 && YShape<NN, T, 5>::valid) || (v == 6 && YShape<NN, T, 6>::valid) ||
-                 (v == 7 && YShape<NN, T, 7>::valid);
+                 (v == 7 && YShape<NN, T, 7>::valid) || (v == 8 && YShape<NN, T, 8>::valid);
         });
         if (ok)
-            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
+            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = (v == 8 && k >= YV_ZFWD) ? 0 : v;
         tune_report_ = std::string("fixed by MLQ_YZ_VARIANT=") + e;
         return;
     }
     const Band b = b2;
     constexpr int NA = 3;
-    const long xs_n = (long)n * n * b.nx, ys_n = (long)n * b.nb * b.nx, sp_n = (long)b.nb * b.nb * b.nx;
+    const int pxb = px_of(b);
+    const long xs_n = (long)n * n * pxb, ys_n = (long)n * b.nb * pxb, sp_n = (long)b.nb * b.nb * b.nx;
     cpx<T>* A = (cpx<T>*)dev_alloc(NA * xs_n * sizeof(cpx<T>));
     cpx<T>* B = (cpx<T>*)dev_alloc(NA * ys_n * sizeof(cpx<T>));
     double2* C = (double2*)dev_alloc(NA * sp_n * sizeof(double2));
@@ -310,15 +341,18 @@ void Engine<T>::tune_yz() {
     yf.n = yi.n = n;
     yf.nz = yi.nz = n;
     yf.nx = yi.nx = b.nx;
+    yf.px = yi.px = pxb;
     yf.band = yi.band = b;
     ZFwdArgs<T> zf{};
     zf.n = n;
     zf.nx = b.nx;
+    zf.px = pxb;
     zf.band = b;
     zf.norm = 1.0 / (double)n3;
     ZInvArgs<T> zi{};
     zi.n = n;
     zi.nx = b.nx;
+    zi.px = pxb;
     zi.band = b;
     for (int a = 0; a < NA; ++a) {
         yf.in[a] = A + a * xs_n;
@@ -353,8 +387,8 @@ void Engine<T>::tune_yz() {
         });
         MLQ_CUDA(cudaGetLastError());
     };
-    constexpr int NV = 8;
-    bool valid[NV] = {true, false, false, false, false, false, false, false};
+    constexpr int NV = 9;
+    bool valid[NV] = {true, false, false, false, false, false, false, false, false};
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         valid[1] = YShape<NN, T, 1>::valid;
@@ -364,11 +398,14 @@ void Engine<T>::tune_yz() {
         valid[5] = YShape<NN, T, 5>::valid;
         valid[6] = YShape<NN, T, 6>::valid;
         valid[7] = YShape<NN, T, 7>::valid;
+        valid[8] = YShape<NN, T, 8>::valid;
     });
+    // variant 8 (column pairs) exists for the y passes only
+    auto valid_for = [&](int kind, int v) { return valid[v] && (v != 8 || kind == YV_YFWD || kind == YV_YINV); };
     // every variant of every kind once first (clocks, attributes, page-in)
     for (int kind = 0; kind < YV_KINDS; ++kind)
         for (int v = 0; v < NV; ++v)
-            if (valid[v]) {
+            if (valid_for(kind, v)) {
                 yvar_[kind] = v;
                 launch(kind);
             }
@@ -380,7 +417,7 @@ void Engine<T>::tune_yz() {
         std::fill(best_ms, best_ms + NV, 1e30f);
         for (int r = 0; r < 5; ++r)
             for (int v = 0; v < NV; ++v) {
-                if (!valid[v]) continue;
+                if (!valid_for(kind, v)) continue;
                 yvar_[kind] = v;
                 MLQ_CUDA(cudaEventRecord(e0, stream));
                 launch(kind);
@@ -393,7 +430,7 @@ void Engine<T>::tune_yz() {
         int bestv = 0;
         std::string times;
         for (int v = 0; v < NV; ++v) {
-            if (!valid[v]) continue;
+            if (!valid_for(kind, v)) continue;
             times += (times.empty() ? "" : " ") + std::to_string(v) + ":" + std::to_string(best_ms[v]);
             if (best_ms[v] < 0.97f * best_ms[bestv]) bestv = v;
         }
@@ -428,6 +465,7 @@ template <typename T>
 template <class F>
 void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b) {
     const int h = n / 2;
+    xa.px = px_of(b);
     xa.nanflag = d_results + NAN_SLOT;
     // compulsory bytes: each distinct input field read once, each output written once
     int nin_distinct = 0;
@@ -479,6 +517,7 @@ void Engine<T>::launch_xfwd(XFwdArgs<T>& xa, const F& f, int nout, const Band& b
 
 template <typename T>
 void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
+    ya.px = px_of(b);
     if (ya.nz <= 0) ya.nz = n;
     const double bytes = (double)narr * ya.nz * ((double)n * b.nx + (double)b.nb * b.nx) * sizeof(cpx<T>);
     const char* nm = sign < 0 ? "y_fwd" : "y_inv";
@@ -534,6 +573,7 @@ void Engine<T>::launch_y(YArgs<T>& ya, int sign, int narr, const Band& b) {
 
 template <typename T>
 void Engine<T>::launch_zfwd(ZFwdArgs<T>& za, int narr, const Band& b, bool any_rt, double zbytes) {
+    za.px = px_of(b);
     if (cfft_ok_) {
         cudaEvent_t ev = prof_mark();
         dispatch_n(n, [&](auto nc) { this->template zfwd_c<decltype(nc)::value>(za, narr); });
@@ -572,6 +612,7 @@ void Engine<T>::launch_zfwd(ZFwdArgs<T>& za, int narr, const Band& b, bool any_r
 
 template <typename T>
 void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zbytes) {
+    za.px = px_of(b);
     if (cfft_ok_) {
         cudaEvent_t ev = prof_mark();
         dispatch_n(n, [&](auto nc) { this->template zinv_c<decltype(nc)::value>(za, narr); });
@@ -606,6 +647,7 @@ void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zby
 
 template <typename T>
 void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
+    xa.px = px_of(b);
     const int h = n / 2;
     if (xa.nlines <= 0) xa.nlines = (long)n * n;
     const double bytes = (double)narr * xa.nlines * ((double)b.nx * sizeof(cpx<T>) + (double)n * sizeof(T));
@@ -659,13 +701,19 @@ T* Engine<T>::phys(int i) {
 template <typename T>
 cpx<T>* Engine<T>::xsbuf(int i) {
     if ((int)xs_.size() <= i) xs_.resize(i + 1, nullptr);
-    if (!xs_[i]) xs_[i] = (cpx<T>*)dev_alloc((size_t)n * n * nxcap * sizeof(cpx<T>));
+    if (!xs_[i]) {
+        xs_[i] = (cpx<T>*)dev_alloc((size_t)n * n * pxcap() * sizeof(cpx<T>));
+        if (pitch_even_) MLQ_CUDA(cudaMemsetAsync(xs_[i], 0, (size_t)n * n * pxcap() * sizeof(cpx<T>), stream));
+    }
     return xs_[i];
 }
 template <typename T>
 cpx<T>* Engine<T>::ysbuf(int i) {
     if ((int)ys_.size() <= i) ys_.resize(i + 1, nullptr);
-    if (!ys_[i]) ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * nxcap * sizeof(cpx<T>));
+    if (!ys_[i]) {
+        ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * pxcap() * sizeof(cpx<T>));
+        if (pitch_even_) MLQ_CUDA(cudaMemsetAsync(ys_[i], 0, (size_t)n * nbcap * pxcap() * sizeof(cpx<T>), stream));
+    }
     return ys_[i];
 }
 template <typename T>
@@ -961,7 +1009,9 @@ cpx<T>* Engine<T>::slot_ys(int i) {
             slot_ys_[i] = slot_pool_.back();
             slot_pool_.pop_back();
         } else {
-            slot_ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * nxcap * sizeof(cpx<T>));
+            slot_ys_[i] = (cpx<T>*)dev_alloc((size_t)n * nbcap * pxcap() * sizeof(cpx<T>));
+            if (pitch_even_)
+                MLQ_CUDA(cudaMemsetAsync(slot_ys_[i], 0, (size_t)n * nbcap * pxcap() * sizeof(cpx<T>), stream));
         }
     }
     return slot_ys_[i];
@@ -997,7 +1047,7 @@ std::vector<const T*> Engine<T>::expand_many(const std::vector<int>& in, int z0)
         xa.plan_half = plan(n / 2);
         xa.tw = d_tw;
         for (size_t j = 0; j < batch.size(); ++j) {
-            ya.in[j] = slot_ys_[in[batch[j]]] + (long)z0 * bb.nb * bb.nx;
+            ya.in[j] = slot_ys_[in[batch[j]]] + (long)z0 * bb.nb * px_of(bb);
             ya.out[j] = xslab(MAX_ARR + (int)j);
             xa.in[j] = xslab(MAX_ARR + (int)j);
             xa.out[j] = slab_buf(batch[j]);
@@ -1030,7 +1080,7 @@ bool Engine<T>::ls_fits() {
     long held = (long)slot_pool_.size();
     for (int i = 0; i < 60 && i < (int)slot_ys_.size(); ++i) held += slot_ys_[i] ? 1 : 0;
     for (int i = 60; i < (int)slot_ys_.size(); ++i) held += slot_ys_[i] ? 1 : 0;
-    const double blk = (double)n * nbcap * nxcap * sizeof(cpx<T>);
+    const double blk = (double)n * nbcap * pxcap() * sizeof(cpx<T>);
     return (39.0 - (double)held) * blk < 0.9 * (double)fr;
 }
 
@@ -1044,7 +1094,10 @@ T* Engine<T>::slab_buf(int k) {
 template <typename T>
 cpx<T>* Engine<T>::xslab(int k) {
     if ((int)xslab_.size() <= k) xslab_.resize(k + 1, nullptr);
-    if (!xslab_[k]) xslab_[k] = (cpx<T>*)dev_alloc((size_t)zs_ * n * nxcap * sizeof(cpx<T>));
+    if (!xslab_[k]) {
+        xslab_[k] = (cpx<T>*)dev_alloc((size_t)zs_ * n * pxcap() * sizeof(cpx<T>));
+        if (pitch_even_) MLQ_CUDA(cudaMemsetAsync(xslab_[k], 0, (size_t)zs_ * n * pxcap() * sizeof(cpx<T>), stream));
+    }
     return xslab_[k];
 }
 
@@ -1067,7 +1120,7 @@ const T* Engine<T>::expand(int i, int z0, int k) {
             ya.nx = s.band.nx;
             ya.band = s.band;
             ya.nz = zs_;
-            ya.in[0] = slot_ys_[i] + (long)z0 * s.band.nb * s.band.nx;
+            ya.in[0] = slot_ys_[i] + (long)z0 * s.band.nb * px_of(s.band);
             ya.out[0] = xslab(MAX_ARR);
             launch_y(ya, +1, 1, s.band);
             XInvArgs<T> xa{};
@@ -1134,7 +1187,7 @@ void Engine<T>::fwd_slab(const Band& b, const F& f, const std::vector<int>& in, 
         if constexpr (NOUT > 0) {
             for (int o = 0; o < NOUT; ++o) {
                 ya.in[o] = xslab(o);
-                ya.out[o] = ysbuf(o) + (long)z0 * b.nb * b.nx;
+                ya.out[o] = ysbuf(o) + (long)z0 * b.nb * px_of(b);
             }
             launch_y(ya, -1, NOUT, b);
         }
@@ -1924,7 +1977,7 @@ void Engine<T>::calc_uk(const double2* u, double k, int dst) {
         const PSlot src = slot(f.phys);
         slot(dst) = src;
         if (src.kind == PSlot::YS)
-            MLQ_CUDA(cudaMemcpyAsync(slot_ys(dst), slot_ys_[f.phys], (size_t)n * src.band.nb * src.band.nx * sizeof(cpx<T>),
+            MLQ_CUDA(cudaMemcpyAsync(slot_ys(dst), slot_ys_[f.phys], (size_t)n * src.band.nb * px_of(src.band) * sizeof(cpx<T>),
                                      cudaMemcpyDeviceToDevice, stream));
         return;
     }

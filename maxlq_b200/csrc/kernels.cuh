@@ -78,6 +78,7 @@ struct XFwdArgs {
     const cpx<double>* tw;
     double* partials;
     long nlines = 0;    // lines (rows along x) processed; a slab of planes is nlines = planes * n
+    int px = 0;         // row pitch of the outputs in elements (0: nx); compile-time kernels only
     // Set to 1 when a forward transform meets a non-finite value (null: not
     // checked).  The DC bin of a packed line is the sum of all its values, so
     // it is non-finite exactly when some input of the line is (or the sum
@@ -198,6 +199,7 @@ struct XInvArgs {
     int tw_n_off;
     const cpx<double>* tw;
     long nlines = 0;  // lines processed (planes * n for a slab)
+    int px = 0;       // row pitch of the inputs in elements (0: nx_in); compile-time kernels only
 };
 
 template <typename T>
@@ -285,6 +287,7 @@ struct YArgs {
     FftPlan plan;
     const cpx<double>* tw;
     int nz = 0;          // z planes processed (a slab), n for a whole array
+    int px = 0;          // row pitch of both sides in elements (0: nx); compile-time kernels only
 };
 
 template <int SIGN, typename T>
@@ -432,6 +435,7 @@ struct ZFwdArgs {
     const cpx<double>* tw;
     double* partials;  // [blocks][MAX_RED]
     double norm;       // 1/N^3
+    int px = 0;        // row pitch of the y-stage arrays (0: nx); spectra keep pitch nx
 };
 
 template <typename T>
@@ -515,6 +519,7 @@ struct ZInvArgs {
     ZInvOp op[MAX_ARR];
     FftPlan plan;
     const cpx<double>* tw;
+    int px = 0;  // row pitch of the y-stage arrays (0: nx); spectra keep pitch nx
 };
 
 template <typename T>

@@ -140,3 +140,17 @@ def test_column_per_warp_variants_512_mixed(variant, monkeypatch):
     assert rel(b[0], a[0]) < 2e-6
     assert b[1] == pytest.approx(a[1], rel=2e-6)
     assert b[3]["J1"] == pytest.approx(a[3]["J1"], rel=2e-6)
+
+
+@pytest.mark.parametrize("n", [128, 256, 512])
+def test_column_pair_y_pass_matches_default(n, monkeypatch):
+    """Variant 8, the y pass on column pairs (FP32 only), computes what
+    variant 0 does, with an odd nx (128: 43, 512: 171, the pad column of the
+    even row pitch rides in the last pair) and an even one (256: 86)."""
+    a = _variant_run(n, "mixed", 0, monkeypatch)
+    b = _variant_run(n, "mixed", 8, monkeypatch)
+    for k in ("uk", "dealias", "R"):
+        assert rel(b[k], a[k]) < 2e-6, k
+    for k in ("g", "vt"):
+        assert rel(b[k], a[k]) < 1e-3, k
+    assert b["J1"] == pytest.approx(a["J1"], rel=1e-5)
