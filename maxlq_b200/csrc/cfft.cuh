@@ -327,7 +327,7 @@ struct YShape {
     static constexpr int YMINB = CW ? (CW_MINB < 1 ? 1 : CW_MINB)
                                     : MB3 ? 3 : (TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1)));
     static constexpr bool valid =
-        V == 0 || (PAIR ? (F32 && N >= 64 && N <= 1024) :
+        V == 0 || (PAIR ? (F32 && N >= 256 && N <= 1024) :
         (MB3 ? (N >= 256 && YTHREADS <= 256 && 3 * (ZSMEM + 1024) <= 228 * 1024) :
          CW ? (N >= 256 && EY >= 2 && EY <= 16 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 227 * 1024)
             : (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&

@@ -951,6 +951,150 @@ double brent(orc_ctx* c, const double* phi, const double* grad, const double tau
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Diagnostics the reference computes around the CG loop (maxdLpdt.f90:263-299,
+// optimization.f90:119-123, 377-384)
+// ---------------------------------------------------------------------------
+
+// calculate_spectral_data (function_ops.f90:2614-2677): shell sums of
+// |fftfwd(u_c)|^2 over kk_min < |K| <= kk_max, kk = 2 pi i, i = 0..n-1, then
+// (normalizeSpectrumByL2Norm, global_variables.f90:76) scaled by
+// <u,u>_L2 / (2 pi sum).  out[0..n) = kk_max, out[n..2n) = the spectrum.
+void spectral_data(orc_ctx* c, const double* u, double* out, int normalize) {
+    const int n = c->n;
+    const long n3 = c->n3;
+    std::vector<CV> fu(3);
+    for (int d = 0; d < 3; ++d) {
+        fu[d] = to_complex(c, u + d * n3);
+        fftfwd(c, fu[d].data());
+    }
+    for (int i = 0; i < n; ++i) {
+        const double kk_min = 2.0 * c->PI * (double)i;
+        const double kk_max = 2.0 * c->PI * (double)(i + 1);
+        out[i] = kk_max;
+        double s = 0.0;
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) {
+                    const double nk = std::sqrt(Kx(c, x) * Kx(c, x) + Kx(c, y) * Kx(c, y) + Kx(c, z) * Kx(c, z));
+                    if (kk_min < nk && nk <= kk_max) {
+                        const long j = IDX(c, x, y, z);
+                        s += std::norm(fu[0][j]) + std::norm(fu[1][j]) + std::norm(fu[2][j]);
+                    }
+                }
+        out[n + i] = s;
+    }
+    if (normalize) {
+        double l2 = 0.0;
+        for (int d = 0; d < 3; ++d) l2 += inner_l2(c, u + d * n3, u + d * n3);
+        double tot = 0.0;
+        for (int i = 0; i < n; ++i) tot += out[n + i];
+        const double spectral_Ener = 2.0 * c->PI * tot;
+        for (int i = 0; i < n; ++i) out[n + i] = l2 / spectral_Ener * out[n + i];
+    }
+}
+
+// vel2vort + Enstrophy + calc_global_summed_enstrophy (function_ops.f90:
+// 2422-2467): 1/2 ||curl u||^2 summed over the components
+double summed_enstrophy(orc_ctx* c, const double* u) {
+    const int n = c->n;
+    const long n3 = c->n3;
+    CV uh[3];
+    for (int d = 0; d < 3; ++d) {
+        uh[d] = to_complex(c, u + d * n3);
+        fftfwd(c, uh[d].data());
+    }
+    double ens[3] = {0.0, 0.0, 0.0};
+    CV w(n3);
+    RV wr(n3);
+    for (int d = 0; d < 3; ++d) {
+#pragma omp parallel for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) {
+                    const long i = IDX(c, x, y, z);
+                    const cplx ik1(0.0, Kx(c, x)), ik2(0.0, Kx(c, y)), ik3(0.0, Kx(c, z));
+                    if (d == 0) w[i] = ik2 * uh[2][i] - ik3 * uh[1][i];
+                    if (d == 1) w[i] = ik3 * uh[0][i] - ik1 * uh[2][i];
+                    if (d == 2) w[i] = ik1 * uh[1][i] - ik2 * uh[0][i];
+                }
+        CV a = w;
+        fftbwd(c, a.data());
+        real_part(c, a, wr.data());
+        for (long i = 0; i < n3; ++i) ens[d] = ens[d] + 0.5 * wr[i] * wr[i] * c->dV;
+    }
+    return ens[0] + ens[1] + ens[2];
+}
+
+// calc_global_dEnstrophydt (function_ops.f90:1417-1481): out = {R1 + R2, R1, R2},
+// R1 = -viscCoefficient visc ||Lap u||^2, R2 = <P2((u.grad) u), Lap u>
+void dEnstrophydt(orc_ctx* c, const double* u, double out[3]) {
+    const long n3 = c->n3, m = 3 * n3;
+    RV lap(u, u + m);
+    laplacian(c, lap.data());
+    const double R1 = -c->p.visc_coef * c->p.visc * field_inner(c, lap.data(), lap.data(), 0);
+    RV gU = grad_tensor(c, u);  // gU[i][j] = d_j u_i
+    RV ug(m, 0.0);
+    for (int ii = 0; ii < 3; ++ii)
+        for (int jj = 0; jj < 3; ++jj)
+#pragma omp parallel for
+            for (long i = 0; i < n3; ++i) ug[ii * n3 + i] = ug[ii * n3 + i] + u[jj * n3 + i] * GU(gU, c, ii, jj)[i];
+    for (int ii = 0; ii < 3; ++ii) maybe_dealias(c, ug.data() + ii * n3, 2.0);
+    const double R2 = field_inner(c, ug.data(), lap.data(), 0);
+    out[0] = R1 + R2;
+    out[1] = R1;
+    out[2] = R2;
+}
+
+// calc_uv_scalar (function_ops.f90:2069-2081)
+void uv_scalar(orc_ctx* c, const double* a, const double* b, double* res) {
+#pragma omp parallel for
+    for (long i = 0; i < c->n3; ++i) res[i] = a[i] * b[i];
+    maybe_dealias(c, res, 2.0);
+}
+
+// calc_local_pointwise_dLqdt_inclParts (function_ops.f90:1224-1291): the
+// fields R1 + R2 + R3, R1 + R2 and R3 (res is 3 n^3)
+void pointwise_R(orc_ctx* c, const double* u, double* res) {
+    const long n3 = c->n3;
+    const double q = c->p.q, nu = c->p.visc, vc = c->p.visc_coef, pc = c->p.press_coef;
+    RV a_q2(n3), aux(n3), e(3 * n3), a_q4(n3), p(n3), tmp(n3), pt(n3), R1(n3), R2(n3), R3(n3);
+    calc_uk(c, u, q - 2.0, a_q2.data());
+    nabla_mod_squared(c, u, aux.data());
+    uv_scalar(c, a_q2.data(), aux.data(), pt.data());
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) R1[i] = -vc * nu * pt[i];
+    unit_vector(c, u, e.data());
+    if (c->p.use_e_u) {
+        vgraduvgradu(c, u, e.data(), aux.data());
+        uv_scalar(c, a_q2.data(), aux.data(), pt.data());
+    } else {
+        calc_uk(c, u, q - 4.0, a_q4.data());
+        vgraduvgradu(c, u, u, aux.data());
+        uv_scalar(c, a_q4.data(), aux.data(), pt.data());
+    }
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) R2[i] = -vc * (q - 2.0) * nu * pt[i];
+    nabla_u_nabla_ut(c, u, aux.data());
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) tmp[i] = -aux[i];
+    solve_poisson(c, tmp.data(), 1.0, p.data());
+    const double* mult = c->p.use_e_u ? a_q2.data() : a_q4.data();
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) aux[i] = p[i] * mult[i];
+    maybe_dealias(c, aux.data(), 2.0);
+    vvgradu(c, u, c->p.use_e_u ? e.data() : u, tmp.data());
+    uv_scalar(c, aux.data(), tmp.data(), pt.data());
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) R3[i] = pc * (q - 2.0) * pt[i];
+#pragma omp parallel for
+    for (long i = 0; i < n3; ++i) {
+        res[i] = R1[i] + R2[i] + R3[i];
+        res[n3 + i] = R1[i] + R2[i];
+        res[2 * n3 + i] = R3[i];
+    }
+}
+
 extern "C" {
 
 void orc_default_params(orc_params* p, int n, double q, double B) {
@@ -1015,6 +1159,12 @@ void orc_vector_transport(orc_ctx* c, const double* u, double q, double B, const
 void orc_R_parts(orc_ctx* c, const double* u, double out[3]) { R_parts(c, u, out); }
 void orc_grad_l2(orc_ctx* c, const double* u, double* v) { grad_l2(c, u, v); }
 double orc_eval_J(orc_ctx* c, const double* u, int mode) { return eval_J(c, u, mode); }
+void orc_spectral_data(orc_ctx* c, const double* u, double* out, int normalize) {
+    spectral_data(c, u, out, normalize);
+}
+double orc_summed_enstrophy(orc_ctx* c, const double* u) { return summed_enstrophy(c, u); }
+void orc_dEnstrophydt(orc_ctx* c, const double* u, double out[3]) { dEnstrophydt(c, u, out); }
+void orc_pointwise_R(orc_ctx* c, const double* u, double* res) { pointwise_R(c, u, res); }
 int orc_mnbrak(orc_ctx* c, const double* phi, const double* d, double tA0, double tB0, double tau_brack[2],
                int* flag) {
     *flag = 0;

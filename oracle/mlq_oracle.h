@@ -94,6 +94,16 @@ int orc_mnbrak(orc_ctx* c, const double* phi, const double* d, double tA0,
                double tB0, double tau_brack[2], int* flag);
 double orc_brent(orc_ctx* c, const double* phi, const double* d,
                  const double tau_brack[2]);
+/* diagnostics: calculate_spectral_data (function_ops.f90:2614-2677; out is
+ * 2n: kk_max then the spectrum, normalize = normalizeSpectrumByL2Norm),
+ * calc_global_summed_enstrophy (2449-2467), calc_global_dEnstrophydt
+ * (1417-1481; out = {R1 + R2, R1, R2}) and
+ * calc_local_pointwise_dLqdt_inclParts (1224-1291; res = 3 n^3 fields
+ * R1 + R2 + R3, R1 + R2, R3) */
+void orc_spectral_data(orc_ctx* c, const double* u, double* out, int normalize);
+double orc_summed_enstrophy(orc_ctx* c, const double* u);
+void orc_dEnstrophydt(orc_ctx* c, const double* u, double out[3]);
+void orc_pointwise_R(orc_ctx* c, const double* u, double* res);
 /* optimization.f90:7-514 without the file I/O and kappa tests.  u in/out.
  * Returns the number of iterations; status in *flag (0 converged/limit,
  * 1 mnbrak uphill, 2 mnbrak ITMAX, 4 tau > TAU_MAX, 5 J decreased). */

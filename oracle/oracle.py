@@ -71,6 +71,10 @@ def _load():
         "orc_eval_count": (C.c_int, [vp]),
         "orc_fft_c2c": (None, [vp, _DP, C.c_int]),
         "orc_dealias_scalar": (None, [vp, _DP, C.c_double]),
+        "orc_spectral_data": (None, [vp, _DP, _DP, C.c_int]),
+        "orc_summed_enstrophy": (C.c_double, [vp, _DP]),
+        "orc_dEnstrophydt": (None, [vp, _DP, _DP]),
+        "orc_pointwise_R": (None, [vp, _DP, _DP]),
         "orc_gradient": (None, [vp, _DP, _DP]),
         "orc_divergence": (None, [vp, _DP, _DP]),
         "orc_laplacian": (None, [vp, _DP]),
@@ -263,6 +267,26 @@ class Oracle:
     def brent(self, phi, d, tau_brack):
         tb = np.ascontiguousarray(tau_brack, dtype=np.float64)
         return self._lib.orc_brent(self._ctx, _p(self._vec(phi)), _p(self._vec(d)), _p(tb))
+
+    # -- diagnostics (maxdLpdt.f90:263-299, optimization.f90:119-123, 377-384) --
+    def spectral_data(self, u, normalize=True):
+        """calculate_spectral_data: (kk_max, spectrum), each of length n."""
+        out = np.zeros(2 * self.n)
+        self._lib.orc_spectral_data(self._ctx, _p(self._vec(u)), _p(out), 1 if normalize else 0)
+        return out[: self.n].copy(), out[self.n:].copy()
+
+    def summed_enstrophy(self, u):
+        return self._lib.orc_summed_enstrophy(self._ctx, _p(self._vec(u)))
+
+    def dEnstrophydt(self, u):
+        out = np.zeros(3)
+        self._lib.orc_dEnstrophydt(self._ctx, _p(self._vec(u)), _p(out))
+        return out
+
+    def pointwise_R(self, u):
+        out = np.zeros((3, self.n, self.n, self.n))
+        self._lib.orc_pointwise_R(self._ctx, _p(self._vec(u)), _p(out))
+        return out
 
     def maxdlqdt(self, u, max_iter=99999, optim_tol=1e-5, start_iter=0, callback=None):
         """Run the CG loop on a copy of u; returns (u, iterations, flag, records)."""
