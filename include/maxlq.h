@@ -145,6 +145,25 @@ int mlq_vector_transport(mlq_ctx* ctx, const double* u, double q, double B,
 int mlq_R_parts(mlq_ctx* ctx, const double* u, double out[3]);             /* 1392-1405 */
 int mlq_grad_l2(mlq_ctx* ctx, const double* u, double* v);                 /* GradL2ForLq 1066-1211 */
 
+/* ---- diagnostics (maxdLpdt.f90:263-299, optimization.f90:119-123, 377-384) -- */
+/* calculate_spectral_data (function_ops.f90:2614-2677): out is the Fortran
+ * array spectral_data(1:n, 1:2), out[0..n) = kk_max = 2 pi i (i = 1..n) and
+ * out[n..2n) the energy of fftfwd(u) in the shell kk_max - 2 pi < |K| <=
+ * kk_max; normalize = normalizeSpectrumByL2Norm (global_variables.f90:76)
+ * scales it by <u,u>_L2 / (2 pi sum).  u must be band-limited like every field
+ * of the path (MLQ_ERR_NOT_BANDLIMITED otherwise). */
+int mlq_spectral_data(mlq_ctx* ctx, const double* u, int normalize, double* out);
+/* the same for the resident state (calculateSaveSpectrum(uvec) inside the loop) */
+int mlq_state_spectral_data(mlq_ctx* ctx, int normalize, double* out);
+/* calc_global_summed_enstrophy (2449-2467): 1/2 ||curl u||_2^2 */
+int mlq_summed_enstrophy(mlq_ctx* ctx, const double* u, double* out);
+/* calc_global_dEnstrophydt (1417-1481): out = {R1 + R2, R1, R2} with
+ * R1 = -viscCoefficient visc ||Lap u||^2, R2 = <P2((u.grad) u), Lap u> */
+int mlq_dEnstrophydt(mlq_ctx* ctx, const double* u, double out[3]);
+/* calc_local_pointwise_dLqdt_inclParts (1224-1291): out is the (n,n,n,3)
+ * field (R1 + R2 + R3, R1 + R2, R3) saved as "Ru" (maxdLpdt.f90:299) */
+int mlq_pointwise_R(mlq_ctx* ctx, const double* u, double* out);
+
 /* ---- optimization.f90 ---------------------------------------------------- */
 int mlq_eval_J(mlq_ctx* ctx, const double* u, int mode, double* J);        /* 520-547 */
 int mlq_mnbrak(mlq_ctx* ctx, const double* phi, const double* d, double tA0, double tB0,

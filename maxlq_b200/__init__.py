@@ -321,6 +321,33 @@ class MaxLq:
                 "kappa_adjusted": table[:, 4], "adjust_factor": frac.value, "best_index": bi.value,
                 "best_kappa": best.value, "J0": J0}
 
+    # -- diagnostics (maxdLpdt.f90:263-299, optimization.f90:119-123, 377-384) --
+    def calculate_spectral_data(self, u=None, normalize: bool = True):
+        """(kk_max, spectrum) of u, or of the resident state when u is None."""
+        out = np.zeros(2 * self.n)
+        if u is None:
+            self._check(self._lib.mlq_state_spectral_data(self._ctx, 1 if normalize else 0, dptr(out)),
+                        "state_spectral_data")
+        else:
+            self._check(self._lib.mlq_spectral_data(self._ctx, dptr(self._vec(u)), 1 if normalize else 0, dptr(out)),
+                        "spectral_data")
+        return out[: self.n].copy(), out[self.n:].copy()
+
+    def calc_global_summed_enstrophy(self, u) -> float:
+        out = C.c_double(0.0)
+        self._check(self._lib.mlq_summed_enstrophy(self._ctx, dptr(self._vec(u)), C.byref(out)), "summed_enstrophy")
+        return out.value
+
+    def calc_global_dEnstrophydt(self, u) -> np.ndarray:
+        out = np.zeros(3)
+        self._check(self._lib.mlq_dEnstrophydt(self._ctx, dptr(self._vec(u)), dptr(out)), "dEnstrophydt")
+        return out
+
+    def calc_local_pointwise_dLqdt_inclParts(self, u) -> np.ndarray:
+        out = np.zeros((3, self.n, self.n, self.n))
+        self._check(self._lib.mlq_pointwise_R(self._ctx, dptr(self._vec(u)), dptr(out)), "pointwise_R")
+        return out
+
     def mnbrak(self, phi, grad, tA0: float, tB0: float):
         """Returns (tau_brack, myflag) like the Fortran function and its inout flag."""
         tb = np.zeros(2)

@@ -87,6 +87,11 @@ SIGNATURES = {
     "mlq_fft_fwd": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_bwd": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_fwdV": (C.c_int, [_VP, _DP, _DP]),
+    "mlq_spectral_data": (C.c_int, [_VP, _DP, C.c_int, _DP]),
+    "mlq_state_spectral_data": (C.c_int, [_VP, C.c_int, _DP]),
+    "mlq_summed_enstrophy": (C.c_int, [_VP, _DP, _DP]),
+    "mlq_dEnstrophydt": (C.c_int, [_VP, _DP, _DP]),
+    "mlq_pointwise_R": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_bwdV": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_fwdr": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_bwdr": (C.c_int, [_VP, _DP, _DP]),

@@ -18,7 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmaxlq_b200.so")
-SOURCES = ["engine.cu", "engine_f32.cu", "engine_f64.cu", "solver.cu", "capi.cu", "noalloc.cu", "ncdf.cpp", "kappa.cpp"]
+SOURCES = ["engine.cu", "engine_f32.cu", "engine_f64.cu", "solver.cu", "capi.cu", "noalloc.cu", "diag.cu", "ncdf.cpp",
+           "kappa.cpp"]
 HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "regfft.cuh", "cfft.cuh", "engine.cuh",
            "engine_common.cuh", "engine_impl.cuh", "solver.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

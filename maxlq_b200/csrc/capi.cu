@@ -220,6 +220,22 @@ int mlq_fft_fwd(mlq_ctx* c, const double* u, double* fu) {
     });
 }
 int mlq_fft_bwd(mlq_ctx* c, const double* fu, double* u) { return guard(c, [&] { fft64(c).fft_c2c(fu, u, +1); }); }
+int mlq_spectral_data(mlq_ctx* c, const double* u, int normalize, double* out) {
+    return guard(c, [&] { c->solver->spectral_data_host(u, normalize, out); });
+}
+int mlq_state_spectral_data(mlq_ctx* c, int normalize, double* out) {
+    return guard(c, [&] { c->solver->state_spectral_data(normalize, out); });
+}
+int mlq_summed_enstrophy(mlq_ctx* c, const double* u, double* out) {
+    return guard(c, [&] { *out = c->solver->enstrophy_host(u); });
+}
+int mlq_dEnstrophydt(mlq_ctx* c, const double* u, double out[3]) {
+    return guard(c, [&] { c->solver->dEnstrophydt_host(u, out); });
+}
+int mlq_pointwise_R(mlq_ctx* c, const double* u, double* out) {
+    return guard(c, [&] { c->solver->pointwise_R_host(u, out); });
+}
+
 int mlq_fft_fwdV(mlq_ctx* c, const double* u, double* fu) {
     return guard(c, [&] {
         Engine<double>& e = fft64(c);

@@ -377,7 +377,7 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, double2* ax
         std::set<const void*> uniq;
         for (int i = 0; i < np; ++i) {
             uniq.insert(pairs[i].a);
-            if (pairs[i].kind != 2) uniq.insert(pairs[i].b);
+            if (pairs[i].kind < 2) uniq.insert(pairs[i].b);
         }
         if (ax_out) {  // x, y read, ax_out written (and read back from cache by the pairs)
             uniq.erase(ax_out);

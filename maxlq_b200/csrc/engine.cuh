@@ -84,7 +84,9 @@ class EngineBase {
     std::map<double, double*> htab_, hwtab_;
     const double* hilbert_table(double order);
     const double* hweight_table(double order);
-    // up to 6 vector inner products; kinds 0 L2, 1 H_l, 2 div energy
+    // up to 8 vector inner products; kinds 0 L2, 1 H_l, 2 div energy,
+    // 3 curl energy sum |K x a|^2, 4 Laplacian energy sum |K|^4 |a|^2
+    // (kinds 2-4 read only a)
     // pairs' inner products; optionally ax_out <- ax_x + ax_a ax_y first, in
     // the same pass (the pairs may name ax_out)
     void dots(const SpecDotPair* pairs, int np, double* out, double2* ax_out = nullptr,
@@ -94,6 +96,18 @@ class EngineBase {
     // g <- sg g, d <- g + beta td (td null: d <- g)
     void direction(double2* g, double sg, double2* d, double beta, const double2* td);
     void zeroth(const double2* f, double out[3]);
+
+    // ---- diagnostics (maxdLpdt.f90:263-299, optimization.f90:119-123, 377-384) ----
+    // calculate_spectral_data (function_ops.f90:2614-2677) of the state
+    // spectra u: out[0..n) = kk_max = 2 pi (i+1), out[n..2n) = the shell
+    // energies of fftfwd(u), scaled by <u,u>/(2 pi sum) when normalize
+    void spectrum(const double2* u, bool normalize, double* out);
+    // calc_global_summed_enstrophy (2449-2467): 1/2 ||curl u||^2
+    double enstrophy(const double2* u);
+    // per-shell lists of the band's modes (|K| in (2 pi i, 2 pi (i+1)]),
+    // built once; the shell sums then run in a fixed order
+    int* d_shell_modes_ = nullptr;
+    int* d_shell_off_ = nullptr;
 
     void finalize(int nblocks, int nr, double scale, int dst, bool accumulate = false);
     // The state spectrum whose u and grad u the physical fields 0..11 hold
@@ -366,6 +380,11 @@ class Engine : public EngineBase {
     // ---- programs ----
     // R parts at phi = u + tau*d (d may be null) -> results; also ||phi||_q^q.
     void R_eval(const double2* u, const double2* d, double tau, double out[3], double* lqq);
+    // calc_global_dEnstrophydt (function_ops.f90:1417-1481): out = {R1 + R2, R1, R2}
+    void dEnstrophydt(const double2* u, double out[3]);
+    // calc_local_pointwise_dLqdt_inclParts (1224-1291): the fields R1 + R2 +
+    // R3, R1 + R2, R3 into the host (n,n,n,3) array
+    void pointwise_R(const double2* u, double* host);
     // L2 gradient of R at u (GradL2ForLq) into v (FP64 spectra); also the
     // dealiased |u|^{q-2} u spectra (for calcConstraintDerivativeL2) into
     // c (FP64, may be null) and ||u||_q^q.

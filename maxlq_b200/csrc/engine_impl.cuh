@@ -1603,6 +1603,132 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
     if (lqq) *lqq = nrm;
 }
 
+// ----------------------------------------------------------------------------
+// diagnostics
+// ----------------------------------------------------------------------------
+namespace {
+enum : int { PDG2 = 100, PDR1 = 101, PDR2 = 102, PDR3 = 103, PDT1 = 104, PDT2 = 105, PDO = 106 /*106..108*/ };
+}
+
+// calc_global_dEnstrophydt: R1 = -viscCoefficient visc ||Lap u||^2 by Parseval,
+// R2 = <P2((u.grad) u), Lap u> as one forward pipeline whose z stage applies
+// -|K|^2 and reduces against the spectra of u (Lap is self-adjoint)
+template <typename T>
+void Engine<T>::dEnstrophydt(const double2* u, double out[3]) {
+    pu_of_ = nullptr;
+    const long nc = spec_ncomp();
+    std::vector<InvOut> io;
+    for (int i = 0; i < 3; ++i)
+        for (int j = -1; j < 3; ++j) {
+            InvOut o;
+            o.nsrc = 1;
+            o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+            o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
+            io.push_back(o);
+        }
+    inv(b2, io);
+    std::vector<int> uin;
+    for (int i = 0; i < 3; ++i) uin.push_back(PU + i);
+    for (int i = 0; i < 9; ++i) uin.push_back(PD + i);
+    FwdOut o[3];
+    for (int i = 0; i < 3; ++i) {
+        o[i].sym = SYM_NEG_KSQ;
+        o[i].red_with[0] = u + i * nc;
+        o[i].red_with_f64[0] = 1;
+        o[i].red_with_slot[0] = 0;
+    }
+    fwd(b2, FUGradU{}, uin, {o[0], o[1], o[2]}, 48);
+    fetch_results();
+    const double R2 = h_results[48];
+    const SpecDotPair p = {u, nullptr, 4};
+    double lap2 = 0.0;
+    dots(&p, 1, &lap2);
+    const double R1 = -P.visc_coef * P.visc * lap2;
+    out[0] = R1 + R2;
+    out[1] = R1;
+    out[2] = R2;
+}
+
+// calc_local_pointwise_dLqdt_inclParts: the products R_eval integrates, kept
+// as dealiased fields: R1 = -cv P2(a2 P2|grad u|^2), R2 = -cv (q-2) P2(a4
+// P2(sum_j V_j^2)) (a2 and E_j on the e_u branch), R3 = cp (q-2) P2(P2(p a4)
+// P2(u . V)) (a2, e_u . E on the e_u branch); the coefficients are applied
+// after the dealias, as the reference does
+template <typename T>
+void Engine<T>::pointwise_R(const double2* u, double* host) {
+    if (slab_) throw CudaError("pointwise R fields need the resident (not z-slab) mode", MLQ_ERR_BADARG);
+    pu_of_ = nullptr;
+    const long nc = spec_ncomp();
+    const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
+    chain_reset();
+    std::vector<InvOut> io;
+    for (int i = 0; i < 3; ++i)
+        for (int j = -1; j < 3; ++j) {
+            InvOut o;
+            o.nsrc = 1;
+            o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+            o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
+            io.push_back(o);
+        }
+    inv(b2, io);
+    std::vector<int> uin;
+    for (int i = 0; i < 3; ++i) uin.push_back(PU + i);
+    for (int i = 0; i < 9; ++i) uin.push_back(PD + i);
+    FwdOut oS, oQ, oG2;
+    oS.phys_out = PS;
+    oQ.sym = SYM_INV_KSQ;  // p = -Lap^-1 P2(grad u : grad u^T) (1281-1282)
+    oQ.phys_out = PP;
+    oG2.phys_out = PDG2;   // P2(|grad u|^2) (calc_nablaModSquared)
+    if (!use_e_u) {
+        FwdOut oW[3];
+        for (int j = 0; j < 3; ++j) oW[j].phys_out = PV + j;
+        fwd(b2, FRProd{}, uin, {oS, oW[0], oW[1], oW[2], oQ, oG2});
+    } else {
+        fwd(b2, FRProdE{}, uin, {oS, oQ, oG2});
+        std::vector<int> ein = uin;
+        ein.push_back(PS);
+        FwdOut oE[3];
+        for (int j = 0; j < 3; ++j) oE[j].phys_out = PV + j;
+        fwd(b2, FRE{}, ein, {oE[0], oE[1], oE[2]});
+    }
+    A_and_S(true);
+    PowField a2 = chain(q - 2.0);
+    ensure_phys(a2);
+    PowField mult = a2;
+    if (!use_e_u) {
+        mult = chain(q - 4.0);
+        ensure_phys(mult);
+    }
+    auto product = [&](int a, int b, int dst) {  // dst = P2(a b) (calc_uv_scalar 2069-2081)
+        FwdOut o;
+        o.phys_out = dst;
+        fwd(b2, FMul{}, {a, b}, {o});
+    };
+    product(a2.phys, PDG2, PDR1);
+    {
+        FwdOut o;  // P2(sum_j V_j^2): calc_vgraduvgradu
+        o.phys_out = PDT1;
+        fwd(b2, FSq3{}, {PV, PV + 1, PV + 2}, {o});
+    }
+    product(mult.phys, PDT1, PDR2);
+    product(PP, mult.phys, PDT2);  // P2(p |u|^{q-4}) or P2(p |u|^{q-2})
+    {
+        FwdOut o;  // calc_vvgradu: P2(u . V) or P2(e_u . E)
+        o.phys_out = PDT1;
+        if (!use_e_u)
+            fwd(b2, FDot3{}, {PU, PU + 1, PU + 2, PV, PV + 1, PV + 2}, {o});
+        else
+            fwd(b2, FEDot{}, {PU, PU + 1, PU + 2, PS, PV, PV + 1, PV + 2}, {o});
+    }
+    product(PDT2, PDT1, PDR3);
+    FRSum fs;
+    fs.c1 = -cv;
+    fs.c2 = -cv * (q - 2.0);
+    fs.c3 = cp * (q - 2.0);
+    pointwise(fs, {PDR1, PDR2, PDR3}, {PDO, PDO + 1, PDO + 2});
+    for (int k = 0; k < 3; ++k) store_scalar_phys(PDO + k, host + k * n3);
+}
+
 // GradL2ForLq (function_ops.f90:1066-1211).  Each of the reference's five
 // terms is a dealiased product; their sum is dealiased once (the projection
 // is linear), the fifth term nu Lap P2(|u|^{q-2}u) is added in the spectrum.

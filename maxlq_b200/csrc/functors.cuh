@@ -144,6 +144,53 @@ struct FRE {
     }
 };
 
+// ---- diagnostics -------------------------------------------------------------
+// (u . grad) u: out_i = sum_j u_j d_j u_i (calc_global_dEnstrophydt 1452-1458).
+// inputs u(3), D(9)
+struct FUGradU {
+    static constexpr int NIN = 12, NOUT = 3, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+#pragma unroll
+        for (int i = 0; i < 3; ++i) out[i] = U(0) * D(i, 0) + U(1) * D(i, 1) + U(2) * D(i, 2);
+    }
+};
+
+// a . b of two stored vector fields (calc_vvgradu 2052-2058).  inputs a(3), b(3)
+struct FDot3 {
+    static constexpr int NIN = 6, NOUT = 1, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        out[0] = in[0] * in[3] + in[1] * in[4] + in[2] * in[5];
+    }
+};
+
+// e_u . E with e_u = u / sqrt(|S|) (calc_vvgradu with v = e_u).  inputs u(3), S, E(3)
+struct FEDot {
+    static constexpr int NIN = 7, NOUT = 1, NRED = 0;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        T e[3];
+        unit_vec(in, in[3], e);
+        out[0] = e[0] * in[4] + e[1] * in[5] + e[2] * in[6];
+    }
+};
+
+// the pointwise R fields from the dealiased products x1, x2, x3: R_i = c_i x_i
+// -> (R1 + R2 + R3, R1 + R2, R3) (calc_local_pointwise_dLqdt_inclParts 1240,
+// 1255, 1280, 1286-1288)
+struct FRSum {
+    static constexpr int NIN = 3, NOUT = 3, NRED = 0;
+    double c1, c2, c3;
+    template <typename T>
+    __device__ void operator()(const T* in, T* out, double*) const {
+        const T r1 = (T)c1 * in[0], r2 = (T)c2 * in[1], r3 = (T)c3 * in[2];
+        out[0] = r1 + r2 + r3;
+        out[1] = r1 + r2;
+        out[2] = r3;
+    }
+};
+
 // q >= 4 with |u|^{q-4} == 1: R2 and R3 integrands from V (dealiased W), p, u.
 // inputs V0,V1,V2, p, u0,u1,u2 -> acc0 += sum V^2 ; acc1 += p * u.V
 struct FRRed1 {

@@ -820,7 +820,33 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
             }
             for (int p = 0; p < a.npairs; ++p) {
                 const SpecDotPair& q = a.pr[p];
-                if (q.kind == 2) {
+                if (q.kind == 3 || q.kind == 4) {
+                    // 3: |K x a|^2 (vel2vort, function_ops.f90:2485-2495);
+                    // 4: |K|^4 |a|^2 (||Lap a||^2).  In-band modes have no
+                    // Nyquist index, so K = 2 pi j on every axis.
+                    double2 v[2][3];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e)
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) v[e][c] = q.a[c * g.ncomp + i[e]];
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        double s;
+                        if (q.kind == 3) {
+                            const double w0r = oy * v[e][2].x - oz * v[e][1].x, w0i = oy * v[e][2].y - oz * v[e][1].y;
+                            const double w1r = oz * v[e][0].x - ox[e] * v[e][2].x, w1i = oz * v[e][0].y - ox[e] * v[e][2].y;
+                            const double w2r = ox[e] * v[e][1].x - oy * v[e][0].x, w2i = ox[e] * v[e][1].y - oy * v[e][0].y;
+                            s = w0r * w0r + w0i * w0i + w1r * w1r + w1i * w1i + w2r * w2r + w2i * w2i;
+                        } else {
+                            const double k2 = ox[e] * ox[e] + oy * oy + oz * oz;
+                            double m2 = 0.0;
+#pragma unroll
+                            for (int c = 0; c < 3; ++c) m2 += v[e][c].x * v[e][c].x + v[e][c].y * v[e][c].y;
+                            s = k2 * k2 * m2;
+                        }
+                        acc[p] += wgt[e] * s;
+                    }
+                } else if (q.kind == 2) {
                     double2 v[2][3];
 #pragma unroll
                     for (int e = 0; e < 2; ++e)

@@ -542,6 +542,23 @@ class Solver : public SolverBase {
         e.calc_uk(tmp, k, 40);
         e.store_scalar_phys(40, out);
     }
+    void spectral_data_host(const double* uh, int normalize, double* out) override {
+        load(uh, tmp);
+        e.spectrum(tmp, normalize != 0, out);
+    }
+    void state_spectral_data(int normalize, double* out) override { e.spectrum(u, normalize != 0, out); }
+    double enstrophy_host(const double* uh) override {
+        load(uh, tmp);
+        return e.enstrophy(tmp);
+    }
+    void dEnstrophydt_host(const double* uh, double out[3]) override {
+        load(uh, tmp);
+        e.dEnstrophydt(tmp, out);
+    }
+    void pointwise_R_host(const double* uh, double* out) override {
+        load(uh, tmp);
+        e.pointwise_R(tmp, out);
+    }
     int mnbrak_host(const double* phi, const double* d, double tA0, double tB0, double br[2], int* flag) override {
         load(phi, tmp);
         load(d, c);

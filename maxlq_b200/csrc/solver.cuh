@@ -40,6 +40,12 @@ class SolverBase {
     virtual double inner_host(const double* f, const double* g, int type) = 0;
     virtual void zeroth_host(const double* u, double out[3]) = 0;
     virtual void calc_uk_host(const double* u, double k, double* out) = 0;
+    // diagnostics of a host field, and the spectrum of the resident state
+    virtual void spectral_data_host(const double* u, int normalize, double* out) = 0;
+    virtual void state_spectral_data(int normalize, double* out) = 0;
+    virtual double enstrophy_host(const double* u) = 0;
+    virtual void dEnstrophydt_host(const double* u, double out[3]) = 0;
+    virtual void pointwise_R_host(const double* u, double* out) = 0;
     virtual int mnbrak_host(const double* phi, const double* d, double tA0, double tB0, double br[2], int* flag) = 0;
     virtual double brent_host(const double* phi, const double* d, const double br[2]) = 0;
     // resident state

@@ -13,7 +13,7 @@ from oracle.seedfield import seed_field
 
 pytestmark = pytest.mark.gpu
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "golden_*.npz")))
 TOL64 = 1e-10
 TOL32 = 2e-5
 

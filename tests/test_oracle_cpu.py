@@ -10,7 +10,7 @@ from oracle.oracle import Oracle
 from oracle.ref_numpy import RefNumpy
 from oracle.seedfield import seed_field
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "golden_*.npz")))
 
 
 def abc_field(n):
