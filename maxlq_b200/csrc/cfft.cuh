@@ -993,6 +993,74 @@ __global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YM
 }
 
 // ----------------------------------------------------------------------------
+// z stage, inverse, one source and up to ZMULTI outputs per op: the column of
+// the source spectrum is loaded once, then each output applies its symbol,
+// transforms and stores.  grid = (G, nops); the tile shape of variant V.
+// ----------------------------------------------------------------------------
+template <int N, int V, typename T>
+__global__ void __launch_bounds__(YShape<N, T, V>::YTHREADS, YShape<N, T, V>::YMINB)
+    zinv_multi_c_kernel(ZInvMultiArgs<T> a, const cpx<T>* __restrict__ twN) {
+    using S = YShape<N, T, V>;
+    using C = T;
+    constexpr int E = S::EY, TPL = S::TPLY, TX = S::TX, CH = E < 8 ? E : 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cpx<T>* sm = reinterpret_cast<cpx<T>*>(smem_raw);
+    cpx<T>* stw = sm + N * TX;
+    C* kt = reinterpret_cast<C*>(stw + N);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    fill_k_table<N>(kt);
+    __syncthreads();
+    const int l = threadIdx.x % TX, t = threadIdx.x / TX;
+    const YTw<N, E, T, S::TWREG> tw(stw, twN, t);
+    const ColMap<TX> map{l};
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
+    const int ntile = (nx + TX - 1) / TX;
+    const long items = (long)nb * ntile;
+    const ZInvMultiOp& op = a.op[blockIdx.y];
+    const int plane = nb * nx;                          // spectra
+    const int px = a.px ? a.px : nx, yplane = nb * px;  // y-stage arrays
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int cy = (int)(it / ntile);
+        const int kx = (int)(it - (long)cy * ntile) * TX + l;
+        const bool ok = kx < nx;
+        const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
+        const int fy = band_fft_index(a.band, cy);
+        const int kxc = col - cy * nx;
+        const C ox = kt[N + kxc], oy = kt[N + fy];
+        const C kxy2 = kt[kxc] * kt[kxc] + kt[fy] * kt[fy];
+        const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
+        cpx<C> Vv[E];
+#pragma unroll
+        for (int m0 = 0; m0 < E; m0 += CH) {
+            cpx<C> ch[CH];
+            ld_chunk<CH>(op.spec, op.f64, idx, m0, ch);
+#pragma unroll
+            for (int j = 0; j < CH; ++j) Vv[m0 + j] = ch[j];
+        }
+#pragma unroll 1
+        for (int o = 0; o < op.nout; ++o) {
+            const SymD<C> d = make_symd<C>(op.sym[o], op.ab[o], op.coef[o]);
+            cpx<T> v[E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int fz = t + TPL * m;
+                const C kz = kt[fz], oz = kt[N + fz];
+                const C ksq = kxy2 + kz * kz;
+                const C ri = d.inv ? rinv_of(ksq) : C(0);
+                const cpx<C> y = idx.valid(m) ? sym_apply(d, ox, oy, oz, ksq, ri, Vv[m]) : mk(C(0), C(0));
+                v[m] = mk((T)y.x, (T)y.y);
+            }
+            cfft<N, E, +1, SyncBlock>(v, t, sm, map, tw);
+            if (ok) {
+                cpx<T>* __restrict__ dst = reinterpret_cast<cpx<T>*>(op.ys_out[o]);
+#pragma unroll
+                for (int m = 0; m < E; ++m) dst[(t + TPL * m) * yplane + cy * px + kx] = v[m];
+            }
+        }
+    }
+}
+
+// ----------------------------------------------------------------------------
 // y pass on column pairs (FP32, variant V = 8 of YShape).  Each thread
 // transforms the two neighbouring kx columns 2j and 2j+1 of a tile at once:
 // they share every twiddle, index and address computation, and move through

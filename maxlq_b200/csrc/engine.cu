@@ -58,6 +58,7 @@ EngineBase::EngineBase(const mlq_params& p) : P(p) {
     ensure_partials(1 << 20);
     if (const char* e = std::getenv("MLQ_GRAPHS")) graphs_on_ = std::string(e) != "0";
     if (const char* e = std::getenv("MLQ_REUSE")) reuse_on_ = std::string(e) != "0";
+    if (const char* e = std::getenv("MLQ_ZMULTI")) multi_zinv_ = std::string(e) != "0";
 }
 
 EngineBase::~EngineBase() {

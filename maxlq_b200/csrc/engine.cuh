@@ -182,6 +182,9 @@ class EngineBase {
     // line search's coefficients, W as half-gradients of |phi|^2); MLQ_REUSE=0
     // runs every program in its plain transform sequence instead
     bool reuse_on_ = true;
+    // single-source z inverse launches grouped by source (one load per
+    // column for a field and its derivatives); MLQ_ZMULTI=0 turns it off
+    bool multi_zinv_ = true;
     long long graph_launches_ = 0;  // graphs launched (replays)
     template <class Fn>
     void as_graph(const std::string& name, const std::vector<const void*>& key, Fn&& body);
@@ -468,6 +471,10 @@ class Engine : public EngineBase {
     void zfwd_cv(ZFwdArgs<T>& za, int narr);
     template <int NN, int V>
     void zinv_cv(ZInvArgs<T>& za, int narr);
+    template <int NN, int V>
+    void zinv_multi_cv(ZInvMultiArgs<T>& za, int nops);
+    // z inverse of ops that each share one source among up to ZMULTI outputs
+    void launch_zinv_multi(ZInvMultiArgs<T>& za, int nops, const Band& b, double zbytes);
     template <int NN, class Fn>
     void with_variant(int kind, Fn&& f);
     // y/z tile-shape variant per pass kind, chosen by tune_yz()

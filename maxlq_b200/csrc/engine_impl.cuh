@@ -646,6 +646,35 @@ void Engine<T>::launch_zinv(ZInvArgs<T>& za, int narr, const Band& b, double zby
 }
 
 template <typename T>
+template <int NN, int V>
+void Engine<T>::zinv_multi_cv(ZInvMultiArgs<T>& za, int nops) {
+    using S = YShape<NN, T, V>;
+    if constexpr (S::CW || S::PAIR) {  // the multi-output kernel has the plain tile shapes only
+        zinv_multi_cv<NN, 0>(za, nops);
+    } else {
+        const size_t smem = S::ZISMEM;
+        const long items = (long)za.band.nb * ((za.nx + S::TX - 1) / S::TX);
+        auto kern = zinv_multi_c_kernel<NN, V, T>;
+        allow_smem(kern);
+        const int G = persistent_blocks((const void*)kern, S::YTHREADS, smem);
+        dim3 grid((unsigned)std::min<long>(items, std::max(1, G / nops)), nops);
+        kern<<<grid, S::YTHREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+    }
+}
+
+template <typename T>
+void Engine<T>::launch_zinv_multi(ZInvMultiArgs<T>& za, int nops, const Band& b, double zbytes) {
+    za.px = px_of(b);
+    cudaEvent_t ev = prof_mark();
+    dispatch_n(n, [&](auto nc) {
+        constexpr int NN = decltype(nc)::value;
+        this->template with_variant<NN>(
+            YV_ZINV, [&](auto vc) { this->template zinv_multi_cv<NN, decltype(vc)::value>(za, nops); });
+    });
+    launched("z_inv", zbytes, ev);
+}
+
+template <typename T>
 void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
     xa.px = px_of(b);
     const int h = n / 2;
@@ -895,8 +924,52 @@ template <typename T>
 void Engine<T>::inv(const Band& b, const std::vector<InvOut>& outs) {
     if (b.nx > nxcap || b.nb > nbcap) throw CudaError("inv: band exceeds buffers", MLQ_ERR_BADARG);
     const int G = 6;
-    for (size_t g0 = 0; g0 < outs.size(); g0 += G) {
-        const int k = (int)std::min<size_t>(G, outs.size() - g0);
+    bool multi = cfft_ok_ && multi_zinv_;
+    for (const InvOut& io : outs) multi = multi && io.nsrc == 1;
+    const size_t GM = multi ? MAX_ARR : G;
+    for (size_t g0 = 0; g0 < outs.size(); g0 += GM) {
+        const int k = (int)std::min<size_t>(GM, outs.size() - g0);
+        if (multi) {
+            // consecutive outputs of one source spectrum share a load
+            ZInvMultiArgs<T> zm;
+            zm.n = n;
+            zm.nx = b.nx;
+            zm.band = b;
+            std::vector<cpx<T>*> ys(k);
+            std::vector<int> po(k);
+            int nops = 0;
+            double zb = 0;
+            for (int i = 0; i < k; ++i) {
+                const InvOut& io = outs[g0 + i];
+                ZInvMultiOp* op = nops ? &zm.op[nops - 1] : nullptr;
+                if (!op || op->nout == ZMULTI || op->spec != io.src[0].spec || op->f64 != io.src[0].f64) {
+                    op = &zm.op[nops++];
+                    op->spec = io.src[0].spec;
+                    op->f64 = io.src[0].f64;
+                    op->nout = 0;
+                    zb += (double)b.nb * b.nb * b.nx * (io.src[0].f64 ? 16 : 8);
+                }
+                const int o = op->nout++;
+                op->sym[o] = io.src[0].sym;
+                op->ab[o] = io.src[0].ab;
+                op->coef[o] = io.src[0].coef;
+                ys[i] = slab_ ? slot_ys(io.phys_out) : ysbuf(i);
+                op->ys_out[o] = ys[i];
+                po[i] = io.phys_out;
+                zb += (double)n * b.nb * b.nx * sizeof(cpx<T>);
+            }
+            launch_zinv_multi(zm, nops, b, zb);
+            if (slab_) {
+                for (int i = 0; i < k; ++i) {
+                    PSlot& sl = slot(po[i]);
+                    sl.kind = PSlot::YS;
+                    sl.band = b;
+                }
+                continue;
+            }
+            yx_inverse(b, ys, po);
+            continue;
+        }
         ZInvArgs<T> za;
         za.n = n;
         za.nx = b.nx;

@@ -522,6 +522,24 @@ struct ZInvArgs {
     int px = 0;  // row pitch of the y-stage arrays (0: nx); spectra keep pitch nx
 };
 
+// One spectrum, up to four symbols: the z inverse of a field and of its
+// derivatives (u and grad u, p and grad p, ...) from one load of the source
+constexpr int ZMULTI = 4;
+struct ZInvMultiOp {
+    const void* spec;
+    int f64, nout;
+    int sym[ZMULTI], ab[ZMULTI];
+    double coef[ZMULTI];
+    void* ys_out[ZMULTI];
+};
+template <typename T>
+struct ZInvMultiArgs {
+    int n, nx;
+    Band band;
+    ZInvMultiOp op[MAX_ARR];
+    int px = 0;  // row pitch of the y-stage arrays (0: nx); spectra keep pitch nx
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256) zinv_kernel(ZInvArgs<T> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -154,3 +154,26 @@ def test_column_pair_y_pass_matches_default(n, monkeypatch):
     for k in ("g", "vt"):
         assert rel(b[k], a[k]) < 1e-3, k
     assert b["J1"] == pytest.approx(a["J1"], rel=1e-5)
+
+
+@pytest.mark.parametrize("n,precision", [(256, "fp64"), (512, "mixed")])
+def test_multi_output_z_inverse_matches_one_output_per_launch_row(n, precision, monkeypatch):
+    """z inverse launches that share one source spectrum among a field and
+    its derivatives (MLQ_ZMULTI, the default) give what one op per output
+    gives, bit for bit: the same symbol arithmetic on the same loaded values."""
+    runs = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("MLQ_ZMULTI", flag)
+        monkeypatch.setenv("MLQ_AUTOTUNE", "0")
+        with mlq.MaxLq(n, 4.0, 1.0, precision=precision, optim_tol=1e-14) as c:
+            u = c.seed_field(1, 2.0, n / 16)
+            R = c.calc_global_dLqdt_inclParts(u)
+            g = c.GradL2ForLq(u) if n <= 256 else None
+            c.state_load(u)
+            _, _, rec = c.state_iterate(2)
+            runs[flag] = (R, g, [r["J1"] for r in rec], [r["tau"] for r in rec])
+    a, b = runs["0"], runs["1"]
+    assert np.array_equal(a[0], b[0])
+    if a[1] is not None:
+        assert np.array_equal(a[1], b[1])
+    assert a[2] == b[2] and a[3] == b[3]
