@@ -112,3 +112,11 @@ def test_noalloc_rejects_orders_that_keep_no_mode_before_any_cuda_call(order):
     lib = maxlq_b200.load_library()
     g = np.zeros((16, 16, 16))
     assert lib.mlq_dealias_scalar_noalloc(_capi.dptr(g), 16, order) == _capi.MLQ_ERR_BADARG
+
+
+def test_fortran_module_binds_every_declared_symbol():
+    # the ISO_C_BINDING module the reference's Fortran driver uses
+    text = open(os.path.join(ROOT, "maxlq_b200", "fortran", "maxlq_gpu.f90")).read()
+    bound = set(re.findall(r"(?:function|subroutine)\s+(mlq_\w+)\s*\(", text))
+    missing = [n for n in declared_symbols() if n not in bound]
+    assert not missing, missing
