@@ -299,7 +299,7 @@ struct YShape {
     // more warps to hide latency)
     static constexpr bool CW = V == 5 || V == 6;
     static constexpr bool MB3 = V == 7;
-    // 8: the y pass on column pairs (FP32 only; ypass_pair_kernel, PairShape)
+    // 8: column pairs (FP32 only; ypass_pair_kernel, zfwd_pair_kernel, PairShape)
     static constexpr bool PAIR = V == 8;
     static constexpr int VB = (CW || MB3) ? 0 : (V >= 3 ? V - 3 : V);
     static constexpr int EY = CW ? N / 32 : (VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8)));
@@ -1213,6 +1213,98 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
             }
         }
     }
+}
+
+// ----------------------------------------------------------------------------
+// z stage, forward (+ optional round trip), on column pairs (FP32, variant
+// V = 8).  The pair's y-stage columns are staged and transformed together as
+// in ypass_pair_kernel; the spectral side (symbols, added term, reductions,
+// spectrum stores; zfwd_spectral) runs once per column of the pair.
+// ----------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
+    zfwd_pair_kernel(ZFwdArgs<float> a, const cpx<float>* __restrict__ twN) {
+    using S = PairShape<N>;
+    using C = float;
+    constexpr int E = S::E, TPL = S::TPL, NP = S::NP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* buf0 = reinterpret_cast<float4*>(smem_raw);
+    float4* buf1 = buf0 + S::TILE;
+    cpx<float>* stw = reinterpret_cast<cpx<float>*>(buf1 + S::TILE);
+    C* kt = reinterpret_cast<C*>(stw + N);
+    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    fill_k_table<N>(kt);
+    __syncthreads();
+    const int l = threadIdx.x % NP, t = threadIdx.x / NP;
+    const TwTab<N, E, float> tw{stw};
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
+    const int pp = (a.px ? a.px : nx) / 2;  // row pitch of the y-stage arrays in pairs
+    const int npair = (nx + 1) / 2;
+    const int ntile = (npair + NP - 1) / NP;
+    const long items = (long)nb * ntile;
+    const ZFwdOp& op = a.op[blockIdx.y];
+    const int plane = nb * nx;  // spectra
+    const long yplane = (long)nb * pp;
+    const float4* __restrict__ src = reinterpret_cast<const float4*>(op.in);
+    float4* __restrict__ yout = reinterpret_cast<float4*>(op.ys_out);
+    const SymD<C> dmain = make_symd<C>(op.sym, op.sym_ab, a.norm);  // the 1/N^3 folded in
+    const SymD<C> dadd = make_symd<C>(op.add_sym, op.add_ab, op.add_coef);
+    ZAcc acc;
+    auto stage = [&](long it, float4* b) {
+        const int cy = (int)(it / ntile);
+        const int pr = (int)(it - (long)cy * ntile) * NP + l;
+        const bool ok = pr < npair;
+        const long ycol = (long)cy * pp + (ok ? pr : npair - 1);
+#pragma unroll
+        for (int m = 0; m < E; ++m) cp_async16(b + pair_slot(t + TPL * m, l), src + (t + TPL * m) * yplane + ycol, ok);
+        cp_async_commit();
+    };
+    long it0 = blockIdx.x;
+    if (it0 < items) stage(it0, buf0);
+    int kbuf = 0;
+    for (long it = it0; it < items; it += gridDim.x, kbuf ^= 1) {
+        float4* cur = kbuf ? buf1 : buf0;
+        float4* nxt = kbuf ? buf0 : buf1;
+        cp_async_wait_all();
+        cpx<float> va[E], vb[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const float4 q = cur[pair_slot(t + TPL * m, l)];
+            va[m] = mk(q.x, q.y);
+            vb[m] = mk(q.z, q.w);
+        }
+        __syncthreads();
+        if (it + gridDim.x < items) stage(it + gridDim.x, nxt);
+        SFor<0, CPlan<N, E>::NST>::run(
+            [&](auto sc) { pstage<N, E, decltype(sc)::value, -1>(va, vb, t, l, cur, tw); });
+        const int cy = (int)(it / ntile);
+        const int pr = (int)(it - (long)cy * ntile) * NP + l;
+        const int fy = band_fft_index(a.band, cy);
+        {
+            const int kx = 2 * pr;
+            const bool ok = kx < nx;
+            const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
+            const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
+            zfwd_spectral<N, E, TPL>(op, dmain, dadd, kt, idx, fy, col - cy * nx, kx_weight(N, kx), va, acc);
+        }
+        {
+            const int kx = 2 * pr + 1;
+            const bool ok = kx < nx;
+            const int col = cy * nx + (ok ? kx : nx - 1);
+            const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
+            zfwd_spectral<N, E, TPL>(op, dmain, dadd, kt, idx, fy, col - cy * nx, kx_weight(N, kx), vb, acc);
+        }
+        if (yout) {  // uniform over the block
+            SFor<0, CPlan<N, E>::NST>::run(
+                [&](auto sc) { pstage<N, E, decltype(sc)::value, +1>(va, vb, t, l, cur, tw); });
+            if (pr < npair) {
+#pragma unroll
+                for (int m = 0; m < E; ++m)
+                    yout[(t + TPL * m) * yplane + (long)cy * pp + pr] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+            }
+        }
+    }
+    zfwd_partials(op, acc, a.partials + (long)(blockIdx.y * gridDim.x + blockIdx.x) * MAX_RED);
 }
 
 // ----------------------------------------------------------------------------

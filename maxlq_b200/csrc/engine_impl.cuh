@@ -188,7 +188,19 @@ template <typename T>
 template <int NN, int V>
 void Engine<T>::zfwd_cv(ZFwdArgs<T>& za, int narr) {
     if constexpr (YShape<NN, T, V>::PAIR) {
-        zfwd_cv<NN, 0>(za, narr);
+        if constexpr (std::is_same<T, float>::value) {
+            using PS = PairShape<NN>;
+            const size_t smem = PS::SMEM + 2 * NN * sizeof(float);  // + the K table
+            const long items = (long)za.band.nb * (((za.nx + 1) / 2 + PS::NP - 1) / PS::NP);
+            auto kern = zfwd_pair_kernel<NN>;
+            allow_smem(kern);
+            const int G = persistent_blocks((const void*)kern, PS::THREADS, smem);
+            dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
+            last_zblocks_ = (long)grid.x * narr;
+            ensure_partials(last_zblocks_ * MAX_RED);
+            za.partials = d_partials;
+            kern<<<grid, PS::THREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+        }
         return;
     }
     using S = YShape<NN, T, V>;
@@ -258,7 +270,7 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
         if (v == 7) return f(std::integral_constant<int, 7>{});
     }
     if constexpr (YShape<NN, T, 8>::valid) {
-        if (v == 8 && (kind == YV_YFWD || kind == YV_YINV)) return f(std::integral_constant<int, 8>{});
+        if (v == 8 && kind != YV_ZINV) return f(std::integral_constant<int, 8>{});
     }
     f(std::integral_constant<int, 0>{});
 }
@@ -323,7 +335,7 @@ void Engine<T>::tune_yz() {
                  (v == 7 && YShape<NN, T, 7>::valid) || (v == 8 && YShape<NN, T, 8>::valid);
         });
         if (ok)
-            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = (v == 8 && k >= YV_ZFWD) ? 0 : v;
+            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = (v == 8 && k == YV_ZINV) ? 0 : v;
         tune_report_ = std::string("fixed by MLQ_YZ_VARIANT=") + e;
         return;
     }
@@ -400,8 +412,8 @@ void Engine<T>::tune_yz() {
         valid[7] = YShape<NN, T, 7>::valid;
         valid[8] = YShape<NN, T, 8>::valid;
     });
-    // variant 8 (column pairs) exists for the y passes only
-    auto valid_for = [&](int kind, int v) { return valid[v] && (v != 8 || kind == YV_YFWD || kind == YV_YINV); };
+    // variant 8 (column pairs) exists for the y passes and the z forward
+    auto valid_for = [&](int kind, int v) { return valid[v] && (v != 8 || kind != YV_ZINV); };
     // every variant of every kind once first (clocks, attributes, page-in)
     for (int kind = 0; kind < YV_KINDS; ++kind)
         for (int v = 0; v < NV; ++v)

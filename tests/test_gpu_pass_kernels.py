@@ -144,7 +144,8 @@ def test_column_per_warp_variants_512_mixed(variant, monkeypatch):
 
 @pytest.mark.parametrize("n", [256, 512])
 def test_column_pair_y_pass_matches_default(n, monkeypatch):
-    """Variant 8, the y pass on column pairs (FP32 only), computes what
+    """Variant 8, the y passes and the z forward (with its round trips,
+    symbols and reductions) on column pairs (FP32 only), computes what
     variant 0 does, with an even nx (256: 86) and an odd one (512: 171, the
     pad column of the even row pitch rides in the last pair)."""
     a = _variant_run(n, "mixed", 0, monkeypatch)
