@@ -174,6 +174,38 @@ struct TwTab {
     }
 };
 
+// Stage-major twiddles in shared memory: stage S holds W_L^(r k STEP) at
+// off(S) + (r - 1) NS + k, so threads with consecutive k (the threads of one
+// exchange row) read consecutive words, free of bank conflicts (a table
+// indexed r k STEP strides by STEP words).  At most L entries.
+template <int L, int E, typename T>
+struct TwStage {
+    using P = CPlan<L, E>;
+    __host__ __device__ static constexpr int off(int s) {
+        int o = 0;
+        for (int i = 1; i < s; ++i) o += (P::radix(i) - 1) * P::ns(i);
+        return o;
+    }
+    static constexpr int SIZE = off(P::NST);
+    static_assert(SIZE <= L, "stage tables fit in L entries");
+    const cpx<T>* tab;
+    // fill from the table W_L^j (global memory); every thread of the block calls it
+    __device__ __forceinline__ static void fill(cpx<T>* dst, const cpx<T>* __restrict__ twL) {
+        SFor<1, P::NST>::run([&](auto sc) {
+            constexpr int S = decltype(sc)::value;
+            constexpr int R = P::radix(S), NS = P::ns(S), STEP = L / (NS * R);
+            for (int j = threadIdx.x; j < (R - 1) * NS; j += blockDim.x) {
+                const int r = j / NS + 1, k = j - (r - 1) * NS;
+                dst[off(S) + j] = twL[r * k * STEP];
+            }
+        });
+    }
+    template <int S, int I, int RI>
+    __device__ __forceinline__ cpx<T> get(int k) const {
+        return tab[off(S) + (RI - 1) * P::ns(S) + k];
+    }
+};
+
 struct SyncWarp {
     __device__ __forceinline__ static void sync() { __syncwarp(); }
 };
@@ -1150,10 +1182,10 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
     float4* buf0 = reinterpret_cast<float4*>(smem_raw);
     float4* buf1 = buf0 + S::TILE;
     cpx<float>* stw = reinterpret_cast<cpx<float>*>(buf1 + S::TILE);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    TwStage<N, E, float>::fill(stw, twN);
     __syncthreads();
     const int l = threadIdx.x % NP, t = threadIdx.x / NP;
-    const TwTab<N, E, float> tw{stw};
+    const TwStage<N, E, float> tw{stw};
     const int nx = a.nx, nb = a.band.nb;
     const int pp = (a.px ? a.px : nx) / 2;  // row pitch in pairs (the pitch is even)
     const int npair = (nx + 1) / 2;
@@ -1232,11 +1264,11 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
     float4* buf1 = buf0 + S::TILE;
     cpx<float>* stw = reinterpret_cast<cpx<float>*>(buf1 + S::TILE);
     C* kt = reinterpret_cast<C*>(stw + N);
-    for (int i = threadIdx.x; i < N; i += blockDim.x) stw[i] = twN[i];
+    TwStage<N, E, float>::fill(stw, twN);
     fill_k_table<N>(kt);
     __syncthreads();
     const int l = threadIdx.x % NP, t = threadIdx.x / NP;
-    const TwTab<N, E, float> tw{stw};
+    const TwStage<N, E, float> tw{stw};
     const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
     const int pp = (a.px ? a.px : nx) / 2;  // row pitch of the y-stage arrays in pairs
     const int npair = (nx + 1) / 2;
@@ -1305,6 +1337,75 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
         }
     }
     zfwd_partials(op, acc, a.partials + (long)(blockIdx.y * gridDim.x + blockIdx.x) * MAX_RED);
+}
+
+// ----------------------------------------------------------------------------
+// z stage, inverse, on column pairs (FP32, variant V = 8), one source and up
+// to ZMULTI outputs per op as zinv_multi_c_kernel: the pair's two source
+// columns are loaded once, each output applies its symbol to both, and the
+// pair is transformed and stored as 16-byte vectors.
+// ----------------------------------------------------------------------------
+template <int N>
+__global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
+    zinv_multi_pair_kernel(ZInvMultiArgs<float> a, const cpx<float>* __restrict__ twN) {
+    using S = PairShape<N>;
+    using C = float;
+    constexpr int E = S::E, TPL = S::TPL, NP = S::NP, CH = E;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* xch = reinterpret_cast<float4*>(smem_raw);
+    cpx<float>* stw = reinterpret_cast<cpx<float>*>(xch + S::TILE);
+    C* kt = reinterpret_cast<C*>(stw + N);
+    TwStage<N, E, float>::fill(stw, twN);
+    fill_k_table<N>(kt);
+    __syncthreads();
+    const int l = threadIdx.x % NP, t = threadIdx.x / NP;
+    const TwStage<N, E, float> tw{stw};
+    const int nx = a.nx, nb = a.band.nb, cut = a.band.cut;
+    const int pp = (a.px ? a.px : nx) / 2;  // row pitch of the y-stage arrays in pairs
+    const int npair = (nx + 1) / 2;
+    const int ntile = (npair + NP - 1) / NP;
+    const long items = (long)nb * ntile;
+    const ZInvMultiOp& op = a.op[blockIdx.y];
+    const int plane = nb * nx;  // spectra
+    const long yplane = (long)nb * pp;
+    for (long it = blockIdx.x; it < items; it += gridDim.x) {
+        const int cy = (int)(it / ntile);
+        const int pr = (int)(it - (long)cy * ntile) * NP + l;
+        const int fy = band_fft_index(a.band, cy);
+        const C oy = kt[N + fy], ky2 = kt[fy] * kt[fy];
+        const int kx0 = 2 * pr, kx1 = 2 * pr + 1;
+        const bool ok0 = kx0 < nx, ok1 = kx1 < nx;
+        const int col0 = cy * nx + (ok0 ? kx0 : nx - 1), col1 = cy * nx + (ok1 ? kx1 : nx - 1);
+        const int kc0 = col0 - cy * nx, kc1 = col1 - cy * nx;
+        const C ox0 = kt[N + kc0], ox1 = kt[N + kc1];
+        const C kxy0 = kt[kc0] * kt[kc0] + ky2, kxy1 = kt[kc1] * kt[kc1] + ky2;
+        const ZCol<N, TPL> idx0{t, cut, nb, plane, col0, ok0}, idx1{t, cut, nb, plane, col1, ok1};
+        cpx<C> V0[E], V1[E];
+        ld_chunk<CH>(op.spec, op.f64, idx0, 0, V0);
+        ld_chunk<CH>(op.spec, op.f64, idx1, 0, V1);
+#pragma unroll 1
+        for (int o = 0; o < op.nout; ++o) {
+            const SymD<C> d = make_symd<C>(op.sym[o], op.ab[o], op.coef[o]);
+            cpx<float> va[E], vb[E];
+#pragma unroll
+            for (int m = 0; m < E; ++m) {
+                const int fz = t + TPL * m;
+                const C kz = kt[fz], oz = kt[N + fz];
+                const C ksq0 = kxy0 + kz * kz, ksq1 = kxy1 + kz * kz;
+                const C ri0 = d.inv ? rinv_of(ksq0) : C(0), ri1 = d.inv ? rinv_of(ksq1) : C(0);
+                va[m] = idx0.valid(m) ? sym_apply(d, ox0, oy, oz, ksq0, ri0, V0[m]) : mk(C(0), C(0));
+                vb[m] = idx1.valid(m) ? sym_apply(d, ox1, oy, oz, ksq1, ri1, V1[m]) : mk(C(0), C(0));
+            }
+            SFor<0, CPlan<N, E>::NST>::run(
+                [&](auto sc) { pstage<N, E, decltype(sc)::value, +1>(va, vb, t, l, xch, tw); });
+            if (pr < npair) {
+                float4* __restrict__ dst = reinterpret_cast<float4*>(op.ys_out[o]);
+#pragma unroll
+                for (int m = 0; m < E; ++m)
+                    dst[(t + TPL * m) * yplane + (long)cy * pp + pr] = make_float4(va[m].x, va[m].y, vb[m].x, vb[m].y);
+            }
+        }
+    }
 }
 
 // ----------------------------------------------------------------------------

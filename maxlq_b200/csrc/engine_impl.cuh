@@ -225,7 +225,30 @@ template <typename T>
 template <int NN, int V>
 void Engine<T>::zinv_cv(ZInvArgs<T>& za, int narr) {
     if constexpr (YShape<NN, T, V>::PAIR) {
-        zinv_cv<NN, 0>(za, narr);
+        // single-source ops run as one-output ops of the pair kernel; ops
+        // that add several sources take the default tile shape
+        bool single = true;
+        for (int i = 0; i < narr; ++i) single = single && za.op[i].nsrc == 1;
+        if (!single) {
+            zinv_cv<NN, 0>(za, narr);
+            return;
+        }
+        ZInvMultiArgs<T> zm;
+        zm.n = za.n;
+        zm.nx = za.nx;
+        zm.band = za.band;
+        zm.px = za.px;
+        for (int i = 0; i < narr; ++i) {
+            ZInvMultiOp& o = zm.op[i];
+            o.spec = za.op[i].src[0].spec;
+            o.f64 = za.op[i].src[0].f64;
+            o.nout = 1;
+            o.sym[0] = za.op[i].src[0].sym;
+            o.ab[0] = za.op[i].src[0].ab;
+            o.coef[0] = za.op[i].src[0].coef;
+            o.ys_out[0] = za.op[i].ys_out;
+        }
+        zinv_multi_cv<NN, V>(zm, narr);
         return;
     }
     using S = YShape<NN, T, V>;
@@ -270,7 +293,7 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
         if (v == 7) return f(std::integral_constant<int, 7>{});
     }
     if constexpr (YShape<NN, T, 8>::valid) {
-        if (v == 8 && kind != YV_ZINV) return f(std::integral_constant<int, 8>{});
+        if (v == 8) return f(std::integral_constant<int, 8>{});
     }
     f(std::integral_constant<int, 0>{});
 }
@@ -335,7 +358,7 @@ void Engine<T>::tune_yz() {
                  (v == 7 && YShape<NN, T, 7>::valid) || (v == 8 && YShape<NN, T, 8>::valid);
         });
         if (ok)
-            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = (v == 8 && k == YV_ZINV) ? 0 : v;
+            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
         tune_report_ = std::string("fixed by MLQ_YZ_VARIANT=") + e;
         return;
     }
@@ -412,8 +435,7 @@ void Engine<T>::tune_yz() {
         valid[7] = YShape<NN, T, 7>::valid;
         valid[8] = YShape<NN, T, 8>::valid;
     });
-    // variant 8 (column pairs) exists for the y passes and the z forward
-    auto valid_for = [&](int kind, int v) { return valid[v] && (v != 8 || kind != YV_ZINV); };
+    auto valid_for = [&](int kind, int v) { return valid[v] && kind >= 0; };
     // every variant of every kind once first (clocks, attributes, page-in)
     for (int kind = 0; kind < YV_KINDS; ++kind)
         for (int v = 0; v < NV; ++v)
@@ -661,7 +683,18 @@ template <typename T>
 template <int NN, int V>
 void Engine<T>::zinv_multi_cv(ZInvMultiArgs<T>& za, int nops) {
     using S = YShape<NN, T, V>;
-    if constexpr (S::CW || S::PAIR) {  // the multi-output kernel has the plain tile shapes only
+    if constexpr (S::PAIR) {
+        if constexpr (std::is_same<T, float>::value) {
+            using PS = PairShape<NN>;
+            const size_t smem = (size_t)PS::TILE * sizeof(float4) + NN * sizeof(cpx<float>) + 2 * NN * sizeof(float);
+            const long items = (long)za.band.nb * (((za.nx + 1) / 2 + PS::NP - 1) / PS::NP);
+            auto kern = zinv_multi_pair_kernel<NN>;
+            allow_smem(kern);
+            const int G = persistent_blocks((const void*)kern, PS::THREADS, smem);
+            dim3 grid((unsigned)std::min<long>(items, std::max(1, G / nops)), nops);
+            kern<<<grid, PS::THREADS, smem, stream>>>(za, d_twT_ + tw_off.at(NN));
+        }
+    } else if constexpr (S::CW) {  // the multi-output kernels have the plain and pair tile shapes only
         zinv_multi_cv<NN, 0>(za, nops);
     } else {
         const size_t smem = S::ZISMEM;

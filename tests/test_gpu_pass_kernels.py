@@ -157,15 +157,18 @@ def test_column_pair_y_pass_matches_default(n, monkeypatch):
     assert b["J1"] == pytest.approx(a["J1"], rel=1e-5)
 
 
-@pytest.mark.parametrize("n,precision", [(256, "fp64"), (512, "mixed")])
-def test_multi_output_z_inverse_matches_one_output_per_launch_row(n, precision, monkeypatch):
+@pytest.mark.parametrize("n,precision,variant", [(256, "fp64", None), (512, "mixed", None), (512, "mixed", "8")])
+def test_multi_output_z_inverse_matches_one_output_per_launch_row(n, precision, variant, monkeypatch):
     """z inverse launches that share one source spectrum among a field and
     its derivatives (MLQ_ZMULTI, the default) give what one op per output
     gives, bit for bit: the same symbol arithmetic on the same loaded values."""
     runs = {}
     for flag in ("0", "1"):
         monkeypatch.setenv("MLQ_ZMULTI", flag)
-        monkeypatch.setenv("MLQ_AUTOTUNE", "0")
+        if variant is None:
+            monkeypatch.setenv("MLQ_AUTOTUNE", "0")
+        else:  # the column-pair kernels (one-output ops of the pair kernel without grouping)
+            monkeypatch.setenv("MLQ_YZ_VARIANT", variant)
         with mlq.MaxLq(n, 4.0, 1.0, precision=precision, optim_tol=1e-14) as c:
             u = c.seed_field(1, 2.0, n / 16)
             R = c.calc_global_dLqdt_inclParts(u)
