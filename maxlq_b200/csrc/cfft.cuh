@@ -331,8 +331,11 @@ struct YShape {
     // more warps to hide latency)
     static constexpr bool CW = V == 5 || V == 6;
     static constexpr bool MB3 = V == 7;
-    // 8: column pairs (FP32 only; ypass_pair_kernel, zfwd_pair_kernel, PairShape)
-    static constexpr bool PAIR = V == 8;
+    // 8: column pairs (FP32 only; ypass_pair_kernel, zfwd_pair_kernel,
+    // zinv_multi_pair_kernel, PairShape), two resident blocks per SM;
+    // 9: the same compiled for three (fewer registers, more warps in flight)
+    static constexpr bool PAIR = V == 8 || V == 9;
+    static constexpr int PAIR_MINB = V == 9 ? 3 : 2;
     static constexpr int VB = (CW || MB3) ? 0 : (V >= 3 ? V - 3 : V);
     static constexpr int EY = CW ? N / 32 : (VB == 0 ? CShape<N, T>::EY : (VB == 1 ? (F32 ? 8 : 16) : (F32 ? 16 : 8)));
     static constexpr int TX = CW ? (V == 5 ? (F32 ? 8 : 4) : (F32 ? 16 : 2))
@@ -359,7 +362,7 @@ struct YShape {
     static constexpr int YMINB = CW ? (CW_MINB < 1 ? 1 : CW_MINB)
                                     : MB3 ? 3 : (TWREG ? 1 : (YTHREADS <= 256 ? 2 : (F32 && EY <= 8 ? 2 : 1)));
     static constexpr bool valid =
-        V == 0 || (PAIR ? (F32 && N >= 256 && N <= 1024) :
+        V == 0 || (PAIR ? (F32 && N >= 256 && N <= (V == 9 ? 512 : 1024)) :
         (MB3 ? (N >= 256 && YTHREADS <= 256 && 3 * (ZSMEM + 1024) <= 228 * 1024) :
          CW ? (N >= 256 && EY >= 2 && EY <= 16 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 227 * 1024)
             : (N >= 256 && TPLY >= 2 && YTHREADS % 32 == 0 && YTHREADS <= 512 && ZSMEM <= 200 * 1024 &&
@@ -1173,8 +1176,8 @@ __device__ __forceinline__ void pstage(cpx<float> (&va)[E], cpx<float> (&vb)[E],
     }
 }
 
-template <int N, int SIGN>
-__global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
+template <int N, int SIGN, int MINB>
+__global__ void __launch_bounds__(PairShape<N>::THREADS, MINB)
     ypass_pair_kernel(YArgs<float> a, const cpx<float>* __restrict__ twN) {
     using S = PairShape<N>;
     constexpr int E = S::E, TPL = S::TPL, NP = S::NP;
@@ -1253,8 +1256,8 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
 // in ypass_pair_kernel; the spectral side (symbols, added term, reductions,
 // spectrum stores; zfwd_spectral) runs once per column of the pair.
 // ----------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
+template <int N, int MINB>
+__global__ void __launch_bounds__(PairShape<N>::THREADS, MINB)
     zfwd_pair_kernel(ZFwdArgs<float> a, const cpx<float>* __restrict__ twN) {
     using S = PairShape<N>;
     using C = float;
@@ -1345,8 +1348,8 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
 // columns are loaded once, each output applies its symbol to both, and the
 // pair is transformed and stored as 16-byte vectors.
 // ----------------------------------------------------------------------------
-template <int N>
-__global__ void __launch_bounds__(PairShape<N>::THREADS, 2)
+template <int N, int MINB>
+__global__ void __launch_bounds__(PairShape<N>::THREADS, MINB)
     zinv_multi_pair_kernel(ZInvMultiArgs<float> a, const cpx<float>* __restrict__ twN) {
     using S = PairShape<N>;
     using C = float;

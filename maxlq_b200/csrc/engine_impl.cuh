@@ -157,9 +157,9 @@ void Engine<T>::y_cv(YArgs<T>& ya, int sign, int narr) {
                 kern<<<grid, PS::THREADS, smem, stream>>>(ya, d_twT_ + tw_off.at(NN));
             };
             if (sign < 0)
-                run(ypass_pair_kernel<NN, -1>);
+                run(ypass_pair_kernel<NN, -1, S::PAIR_MINB>);
             else
-                run(ypass_pair_kernel<NN, +1>);
+                run(ypass_pair_kernel<NN, +1, S::PAIR_MINB>);
         }
         return;
     }
@@ -192,7 +192,7 @@ void Engine<T>::zfwd_cv(ZFwdArgs<T>& za, int narr) {
             using PS = PairShape<NN>;
             const size_t smem = PS::SMEM + 2 * NN * sizeof(float);  // + the K table
             const long items = (long)za.band.nb * (((za.nx + 1) / 2 + PS::NP - 1) / PS::NP);
-            auto kern = zfwd_pair_kernel<NN>;
+            auto kern = zfwd_pair_kernel<NN, YShape<NN, T, V>::PAIR_MINB>;
             allow_smem(kern);
             const int G = persistent_blocks((const void*)kern, PS::THREADS, smem);
             dim3 grid((unsigned)std::min<long>(items, std::max(1, G / narr)), narr);
@@ -295,6 +295,9 @@ void Engine<T>::with_variant(int kind, Fn&& f) {
     if constexpr (YShape<NN, T, 8>::valid) {
         if (v == 8) return f(std::integral_constant<int, 8>{});
     }
+    if constexpr (YShape<NN, T, 9>::valid) {
+        if (v == 9) return f(std::integral_constant<int, 9>{});
+    }
     f(std::integral_constant<int, 0>{});
 }
 
@@ -355,7 +358,8 @@ void Engine<T>::tune_yz() {
             ok = ok || (v == 1 && YShape<NN, T, 1>::valid) || (v == 2 && YShape<NN, T, 2>::valid) ||
                  (v == 3 && YShape<NN, T, 3>::valid) || (v == 4 && YShape<NN, T, 4>::valid) ||
                  (v == 5 && YShape<NN, T, 5>::valid) || (v == 6 && YShape<NN, T, 6>::valid) ||
-                 (v == 7 && YShape<NN, T, 7>::valid) || (v == 8 && YShape<NN, T, 8>::valid);
+                 (v == 7 && YShape<NN, T, 7>::valid) || (v == 8 && YShape<NN, T, 8>::valid) ||
+                 (v == 9 && YShape<NN, T, 9>::valid);
         });
         if (ok)
             for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v;
@@ -422,8 +426,8 @@ void Engine<T>::tune_yz() {
         });
         MLQ_CUDA(cudaGetLastError());
     };
-    constexpr int NV = 9;
-    bool valid[NV] = {true, false, false, false, false, false, false, false, false};
+    constexpr int NV = 10;
+    bool valid[NV] = {true, false, false, false, false, false, false, false, false, false};
     dispatch_n(n, [&](auto nc) {
         constexpr int NN = decltype(nc)::value;
         valid[1] = YShape<NN, T, 1>::valid;
@@ -434,6 +438,7 @@ void Engine<T>::tune_yz() {
         valid[6] = YShape<NN, T, 6>::valid;
         valid[7] = YShape<NN, T, 7>::valid;
         valid[8] = YShape<NN, T, 8>::valid;
+        valid[9] = YShape<NN, T, 9>::valid;
     });
     auto valid_for = [&](int kind, int v) { return valid[v] && kind >= 0; };
     // every variant of every kind once first (clocks, attributes, page-in)
@@ -688,7 +693,7 @@ void Engine<T>::zinv_multi_cv(ZInvMultiArgs<T>& za, int nops) {
             using PS = PairShape<NN>;
             const size_t smem = (size_t)PS::TILE * sizeof(float4) + NN * sizeof(cpx<float>) + 2 * NN * sizeof(float);
             const long items = (long)za.band.nb * (((za.nx + 1) / 2 + PS::NP - 1) / PS::NP);
-            auto kern = zinv_multi_pair_kernel<NN>;
+            auto kern = zinv_multi_pair_kernel<NN, S::PAIR_MINB>;
             allow_smem(kern);
             const int G = persistent_blocks((const void*)kern, PS::THREADS, smem);
             dim3 grid((unsigned)std::min<long>(items, std::max(1, G / nops)), nops);
