@@ -478,8 +478,9 @@ class Engine : public EngineBase {
     template <int NN, class Fn>
     void with_variant(int kind, Fn&& f);
     // y/z tile-shape variant per pass kind, chosen by tune_yz()
-    enum { YV_YFWD = 0, YV_YINV = 1, YV_ZFWD = 2, YV_ZINV = 3, YV_KINDS = 4 };
-    int yvar_[YV_KINDS] = {0, 0, 0, 0};
+    // (YV_ZRT: z forward launches with a round trip back into the y stage)
+    enum { YV_YFWD = 0, YV_YINV = 1, YV_ZFWD = 2, YV_ZINV = 3, YV_ZRT = 4, YV_KINDS = 5 };
+    int yvar_[YV_KINDS] = {0, 0, 0, 0, 0};
     void tune_yz();
     std::string tune_report_;
     std::string kernel_config() const override;

@@ -311,7 +311,10 @@ void Engine<T>::y_c(YArgs<T>& ya, int sign, int narr) {
 template <typename T>
 template <int NN>
 void Engine<T>::zfwd_c(ZFwdArgs<T>& za, int narr) {
-    with_variant<NN>(YV_ZFWD, [&](auto vc) { this->template zfwd_cv<NN, decltype(vc)::value>(za, narr); });
+    bool rt = false;
+    for (int i = 0; i < narr; ++i) rt = rt || za.op[i].ys_out != nullptr;
+    with_variant<NN>(rt ? YV_ZRT : YV_ZFWD,
+                     [&](auto vc) { this->template zfwd_cv<NN, decltype(vc)::value>(za, narr); });
 }
 
 template <typename T>
@@ -415,7 +418,14 @@ void Engine<T>::tune_yz() {
     cudaEvent_t e0, e1;
     MLQ_CUDA(cudaEventCreate(&e0));
     MLQ_CUDA(cudaEventCreate(&e1));
-    const char* names[YV_KINDS] = {"y_fwd", "y_inv", "z_fwd", "z_inv"};
+    const char* names[YV_KINDS] = {"y_fwd", "y_inv", "z_fwd", "z_inv", "z_roundtrip"};
+    // the round-trip kind: dealias round trips in place, no spectrum, no reduction
+    ZFwdArgs<T> zr = zf;
+    for (int a = 0; a < NA; ++a) {
+        zr.op[a].spec_out = nullptr;
+        zr.op[a].red_self = -1;
+        zr.op[a].ys_out = B + a * ys_n;
+    }
     auto launch = [&](int kind) {
         dispatch_n(n, [&](auto nc) {
             constexpr int NN = decltype(nc)::value;
@@ -423,6 +433,7 @@ void Engine<T>::tune_yz() {
             if (kind == YV_YINV) y_c<NN>(yi, +1, NA);
             if (kind == YV_ZFWD) zfwd_c<NN>(zf, NA);
             if (kind == YV_ZINV) zinv_c<NN>(zi, NA);
+            if (kind == YV_ZRT) zfwd_c<NN>(zr, NA);
         });
         MLQ_CUDA(cudaGetLastError());
     };
