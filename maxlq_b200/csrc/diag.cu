@@ -15,10 +15,11 @@ static const double PI_DIAG = 4.0 * std::atan2(1.0, 1.0);  // initialize.f90:164
 
 // One block per shell: the energies sum_c |u_c|^2 of the shell's modes, in
 // the fixed order of its mode list, times scale.
-static __global__ void __launch_bounds__(256) shell_energy_kernel(SpecGeom g, const double2* __restrict__ u,
-                                                                  const int* __restrict__ modes,
-                                                                  const int* __restrict__ off, double scale,
-                                                                  double* __restrict__ out) {
+template <typename V>
+__global__ void __launch_bounds__(256) shell_energy_kernel(SpecGeom g, const V* __restrict__ u,
+                                                           const int* __restrict__ modes,
+                                                           const int* __restrict__ off, double scale,
+                                                           double* __restrict__ out) {
     const int sh = blockIdx.x;
     double s = 0.0;
     for (int k = off[sh] + threadIdx.x; k < off[sh + 1]; k += blockDim.x) {
@@ -27,7 +28,7 @@ static __global__ void __launch_bounds__(256) shell_energy_kernel(SpecGeom g, co
         double e = 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const double2 v = u[(long)c * g.ncomp + m];
+            const double2 v = ldv(u, (long)c * g.ncomp + m);
             e += v.x * v.x + v.y * v.y;
         }
         s += kx_weight(g.n, fx) * e;
@@ -45,7 +46,7 @@ static __global__ void __launch_bounds__(256) shell_energy_kernel(SpecGeom g, co
     }
 }
 
-void EngineBase::spectrum(const double2* u, bool normalize, double* out) {
+void EngineBase::spectrum(const SVec* u, bool normalize, double* out) {
     const SpecGeom g = geom(b2);
     if (!d_shell_modes_) {
         // shell i of each mode: 2 pi i < |K| <= 2 pi (i + 1) with |K| and the
@@ -84,8 +85,13 @@ void EngineBase::spectrum(const double2* u, bool normalize, double* out) {
     // fftfwd is unnormalised: |N^3 u_hat|^2
     const double scale = (double)n3 * (double)n3;
     cudaEvent_t ev = prof_mark();
-    shell_energy_kernel<<<n, 256, 0, stream>>>(g, u, d_shell_modes_, d_shell_off_, scale, d_partials);
-    launched("spec_shells", 48.0 * g.ncomp, ev);
+    if (state32_)
+        shell_energy_kernel<float2><<<n, 256, 0, stream>>>(g, (const float2*)u, d_shell_modes_, d_shell_off_, scale,
+                                                          d_partials);
+    else
+        shell_energy_kernel<double2><<<n, 256, 0, stream>>>(g, (const double2*)u, d_shell_modes_, d_shell_off_, scale,
+                                                           d_partials);
+    launched("spec_shells", 3.0 * sv_elem() * g.ncomp, ev);
     std::vector<double> sh(n);
     MLQ_CUDA(cudaMemcpyAsync(sh.data(), d_partials, n * sizeof(double), cudaMemcpyDeviceToHost, stream));
     MLQ_CUDA(cudaStreamSynchronize(stream));
@@ -104,7 +110,7 @@ void EngineBase::spectrum(const double2* u, bool normalize, double* out) {
     }
 }
 
-double EngineBase::enstrophy(const double2* u) {
+double EngineBase::enstrophy(const SVec* u) {
     const SpecDotPair p = {u, nullptr, 3};
     double w2 = 0.0;
     dots(&p, 1, &w2);

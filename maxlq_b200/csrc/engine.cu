@@ -119,7 +119,8 @@ void EngineBase::free_dev(void* p) {
     }
 }
 
-double2* EngineBase::alloc_state() { return (double2*)dev_alloc(3 * spec_ncomp() * sizeof(double2)); }
+SVec* EngineBase::alloc_state() { return dev_alloc(3 * spec_ncomp() * sv_elem()); }
+
 
 void EngineBase::ensure_partials(long cnt) {
     if (cnt <= partials_cap) return;
@@ -210,13 +211,17 @@ std::string EngineBase::prof_report(bool reset) {
     return s;
 }
 
-void EngineBase::lincomb(double2* out, double a, const double2* x, double b, const double2* y, double c,
-                         const double2* z) {
+void EngineBase::lincomb(SVec* out, double a, const SVec* x, double b, const SVec* y, double c, const SVec* z) {
     state_written(out);
     SpecGeom g = geom(b2);
     cudaEvent_t ev = prof_mark();
-    spec_lincomb_kernel<<<grid_for(3 * g.ncomp, 256), 256, 0, stream>>>(g, out, a, x, b, y, c, z);
-    launched("spec_lincomb", 48.0 * g.ncomp * (2 + (y ? 1 : 0) + (z ? 1 : 0)), ev);
+    if (state32_)
+        spec_lincomb_kernel<float2><<<grid_for(3 * g.ncomp, 256), 256, 0, stream>>>(
+            g, (float2*)out, a, (const float2*)x, b, (const float2*)y, c, (const float2*)z);
+    else
+        spec_lincomb_kernel<double2><<<grid_for(3 * g.ncomp, 256), 256, 0, stream>>>(
+            g, (double2*)out, a, (const double2*)x, b, (const double2*)y, c, (const double2*)z);
+    launched("spec_lincomb", 3.0 * sv_elem() * g.ncomp * (2 + (y ? 1 : 0) + (z ? 1 : 0)), ev);
 }
 
 // K = 2 pi j: |K|^2 of a mode with |j|^2 = jsq
@@ -256,7 +261,7 @@ const double* EngineBase::hweight_table(double order) {
 
 static int spec_rows_grid(const SpecGeom& g) { return std::max(1, std::min(g.nb * g.nb, 148 * 16)); }
 
-void EngineBase::retract(double2* u, double cs, double tau, const double2* d) {
+void EngineBase::retract(SVec* u, double cs, double tau, const SVec* d) {
     const PhysMemo keep = pm_;
     lincomb(u, cs, u, cs * tau, d);
     if (keep.tr && keep.u == (const void*)u && keep.d == (const void*)d && keep.tau == tau) {
@@ -268,9 +273,8 @@ void EngineBase::retract(double2* u, double cs, double tau, const double2* d) {
     }
 }
 
-void EngineBase::transport_retract(double2* tg, double2* td, const double2* g, const double2* d, double2* u,
-                                   double ag, double bg, double cg, double ad, double bd, double cd, double cs,
-                                   double tau) {
+void EngineBase::transport_retract(SVec* tg, SVec* td, const SVec* g, const SVec* d, SVec* u, double ag,
+                                   double bg, double cg, double ad, double bd, double cd, double cs, double tau) {
     const PhysMemo keep = pm_;
     state_written(tg);
     state_written(td);
@@ -278,9 +282,15 @@ void EngineBase::transport_retract(double2* tg, double2* td, const double2* g, c
     SpecGeom geo = geom(b2);
     const long nt = 3 * geo.ncomp;
     cudaEvent_t ev = prof_mark();
-    spec_transport_kernel<<<grid_for(nt, 256), 256, 0, stream>>>(nt, g, d, u, tg, td, ag, bg, cg, ad, bd, cd, cs,
-                                                                cs * tau);
-    launched("spec_lincomb", 16.0 * nt * 6, ev);
+    if (state32_)
+        spec_transport_kernel<float2><<<grid_for(nt, 256), 256, 0, stream>>>(
+            nt, (const float2*)g, (const float2*)d, (float2*)u, (float2*)tg, (float2*)td, ag, bg, cg, ad, bd, cd, cs,
+            cs * tau);
+    else
+        spec_transport_kernel<double2><<<grid_for(nt, 256), 256, 0, stream>>>(
+            nt, (const double2*)g, (const double2*)d, (double2*)u, (double2*)tg, (double2*)td, ag, bg, cg, ad, bd, cd,
+            cs, cs * tau);
+    launched("spec_lincomb", (double)sv_elem() * nt * 6, ev);
     if (keep.tr && keep.u == (const void*)u && keep.d == (const void*)d && keep.tau == tau) {
         pm_ = keep;
         pm_.u = nullptr;  // the fields describe the old u, no longer stored
@@ -290,33 +300,42 @@ void EngineBase::transport_retract(double2* tg, double2* td, const double2* g, c
     }
 }
 
-void EngineBase::hilbert(double2* f, double order) {
+void EngineBase::hilbert(SVec* f, double order) {
     state_written(f);
     SpecGeom g = geom(b2);
     const double* t = hilbert_table(order);
     cudaEvent_t ev = prof_mark();
-    spec_hilbert_leray_kernel<<<spec_rows_grid(g), 128, 0, stream>>>(g, f, t, 1.0, 0);
-    launched("spec_hilbert", 96.0 * g.ncomp, ev);
+    if (state32_)
+        spec_hilbert_leray_kernel<float2><<<spec_rows_grid(g), 128, 0, stream>>>(g, (float2*)f, t, 1.0, 0);
+    else
+        spec_hilbert_leray_kernel<double2><<<spec_rows_grid(g), 128, 0, stream>>>(g, (double2*)f, t, 1.0, 0);
+    launched("spec_hilbert", 6.0 * sv_elem() * g.ncomp, ev);
 }
 
-void EngineBase::leray(double2* f) {
+void EngineBase::leray(SVec* f) {
     state_written(f);
     SpecGeom g = geom(b2);
     cudaEvent_t ev = prof_mark();
-    spec_hilbert_leray_kernel<<<spec_rows_grid(g), 128, 0, stream>>>(g, f, nullptr, 1.0, 1);
-    launched("spec_leray", 96.0 * g.ncomp, ev);
+    if (state32_)
+        spec_hilbert_leray_kernel<float2><<<spec_rows_grid(g), 128, 0, stream>>>(g, (float2*)f, nullptr, 1.0, 1);
+    else
+        spec_hilbert_leray_kernel<double2><<<spec_rows_grid(g), 128, 0, stream>>>(g, (double2*)f, nullptr, 1.0, 1);
+    launched("spec_leray", 6.0 * sv_elem() * g.ncomp, ev);
 }
 
-void EngineBase::hilbert_leray(double2* f, double order, double scale) {
+void EngineBase::hilbert_leray(SVec* f, double order, double scale) {
     state_written(f);
     SpecGeom g = geom(b2);
     const double* t = hilbert_table(order);
     cudaEvent_t ev = prof_mark();
-    spec_hilbert_leray_kernel<<<spec_rows_grid(g), 128, 0, stream>>>(g, f, t, scale, 1);
-    launched("spec_hilbert_leray", 96.0 * g.ncomp, ev);
+    if (state32_)
+        spec_hilbert_leray_kernel<float2><<<spec_rows_grid(g), 128, 0, stream>>>(g, (float2*)f, t, scale, 1);
+    else
+        spec_hilbert_leray_kernel<double2><<<spec_rows_grid(g), 128, 0, stream>>>(g, (double2*)f, t, scale, 1);
+    launched("spec_hilbert_leray", 6.0 * sv_elem() * g.ncomp, ev);
 }
 
-void EngineBase::hilbert_leray_pair_dots(double2* f1, double2* f2, double order, double s2, double out[2]) {
+void EngineBase::hilbert_leray_pair_dots(SVec* f1, SVec* f2, double order, double s2, double out[2]) {
     state_written(f1);
     state_written(f2);
     SpecGeom g = geom(b2);
@@ -325,26 +344,36 @@ void EngineBase::hilbert_leray_pair_dots(double2* f1, double2* f2, double order,
     const int grid = spec_rows_grid(g);
     ensure_partials((long)grid * 2);
     cudaEvent_t ev = prof_mark();
-    spec_hilbert_leray_pair_dot_kernel<<<grid, 128, 0, stream>>>(g, f1, 1.0, f2, s2, t, hw, d_partials);
-    launched("spec_hilbert_leray", 2 * 96.0 * g.ncomp, ev);
+    if (state32_)
+        spec_hilbert_leray_pair_dot_kernel<float2><<<grid, 128, 0, stream>>>(g, (float2*)f1, 1.0, (float2*)f2, s2, t,
+                                                                              hw, d_partials);
+    else
+        spec_hilbert_leray_pair_dot_kernel<double2><<<grid, 128, 0, stream>>>(g, (double2*)f1, 1.0, (double2*)f2,
+                                                                               s2, t, hw, d_partials);
+    launched("spec_hilbert_leray", 2 * 6.0 * sv_elem() * g.ncomp, ev);
     finalize(grid, 2, 1.0, 200);
     fetch_results();
     out[0] = h_results[200];
     out[1] = h_results[201];
 }
 
-void EngineBase::direction(double2* gv, double sg, double2* d, double beta, const double2* td) {
+void EngineBase::direction(SVec* gv, double sg, SVec* d, double beta, const SVec* td) {
     state_written(gv);
     state_written(d);
     SpecGeom g = geom(b2);
     const long nt = 3 * g.ncomp;
     cudaEvent_t ev = prof_mark();
-    spec_direction_kernel<<<grid_for(nt, 256), 256, 0, stream>>>(nt, gv, sg, d, td ? beta : 0.0, td);
-    launched("spec_lincomb", 16.0 * nt * (3 + (td ? 1 : 0)), ev);
+    if (state32_)
+        spec_direction_kernel<float2><<<grid_for(nt, 256), 256, 0, stream>>>(nt, (float2*)gv, sg, (float2*)d,
+                                                                            td ? beta : 0.0, (const float2*)td);
+    else
+        spec_direction_kernel<double2><<<grid_for(nt, 256), 256, 0, stream>>>(nt, (double2*)gv, sg, (double2*)d,
+                                                                             td ? beta : 0.0, (const double2*)td);
+    launched("spec_lincomb", (double)sv_elem() * nt * (3 + (td ? 1 : 0)), ev);
 }
 
-void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, double2* ax_out, const double2* ax_x,
-                      double ax_a, const double2* ax_y) {
+void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, SVec* ax_out, const SVec* ax_x, double ax_a,
+                      const SVec* ax_y) {
     if (np < 1 || np > 8) throw CudaError("dots: 1 to 8 pairs per call", MLQ_ERR_BADARG);
     SpecDotArgs a;
     a.g = geom(b2);
@@ -364,7 +393,7 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, double2* ax
     // (thread-safe one-time initialisation; every device here is a B200)
     static const int resident = [] {
         int per_sm = 0, dev = 0, sms = 0;
-        MLQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spec_dot_kernel, RED_THREADS, 0));
+        MLQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spec_dot_kernel<double2>, RED_THREADS, 0));
         MLQ_CUDA(cudaGetDevice(&dev));
         MLQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         return std::max(1, per_sm) * sms;
@@ -373,7 +402,10 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, double2* ax
     ensure_partials((long)grid * 8);
     a.partials = d_partials;
     cudaEvent_t ev = prof_mark();
-    spec_dot_kernel<<<grid, RED_THREADS, 0, stream>>>(a);
+    if (state32_)
+        spec_dot_kernel<float2><<<grid, RED_THREADS, 0, stream>>>(a);
+    else
+        spec_dot_kernel<double2><<<grid, RED_THREADS, 0, stream>>>(a);
     {
         std::set<const void*> uniq;
         for (int i = 0; i < np; ++i) {
@@ -385,21 +417,25 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, double2* ax
             uniq.insert(ax_x);
             uniq.insert(ax_y);
         }
-        launched("spec_dot", 48.0 * a.g.ncomp * (uniq.size() + (ax_out ? 1 : 0)), ev);
+        launched("spec_dot", 3.0 * sv_elem() * a.g.ncomp * (uniq.size() + (ax_out ? 1 : 0)), ev);
     }
     finalize(grid, 8, 1.0, 200);
     fetch_results();
     for (int i = 0; i < np; ++i) out[i] = h_results[200 + i];
 }
 
-void EngineBase::zeroth(const double2* f, double out[3]) {
+void EngineBase::zeroth(const SVec* f, double out[3]) {
     double2 h[3];
-    const long nc = spec_ncomp();
-    for (int c = 0; c < 3; ++c)
-        MLQ_CUDA(cudaMemcpyAsync(&h[c], f + c * nc, sizeof(double2), cudaMemcpyDeviceToHost, stream));
+    float2 hf[3];
+    for (int c = 0; c < 3; ++c) {
+        if (state32_)
+            MLQ_CUDA(cudaMemcpyAsync(&hf[c], scomp(f, c), sizeof(float2), cudaMemcpyDeviceToHost, stream));
+        else
+            MLQ_CUDA(cudaMemcpyAsync(&h[c], scomp(f, c), sizeof(double2), cudaMemcpyDeviceToHost, stream));
+    }
     MLQ_CUDA(cudaStreamSynchronize(stream));
     const double s = (double)n3;  // unnormalised k=0 coefficient (function_ops.f90:3084-3086)
-    for (int c = 0; c < 3; ++c) out[c] = h[c].x * s;
+    for (int c = 0; c < 3; ++c) out[c] = (state32_ ? (double)hf[c].x : h[c].x) * s;
 }
 
 }  // namespace mlq

@@ -21,6 +21,12 @@
 
 namespace mlq {
 
+// A state vector: three components of nb*nb*nx Fourier coefficients of band
+// b2, stored as double2 (FP64 path) or float2 (the mixed path's FP32 state);
+// every operation on it computes in FP64.  Components are addressed with
+// EngineBase::scomp, never by pointer arithmetic.
+using SVec = void;
+
 int band_cut_for_order(int n, double order);
 
 struct PhysField;  // fwd
@@ -59,7 +65,13 @@ class EngineBase {
 
     // FP64 state spectra (3 components each) of band b2
     long spec_ncomp() const { return (long)b2.nb * b2.nb * b2.nx; }
-    double2* alloc_state();
+    // state storage: FP32 in the mixed path (MLQ_STATE_F64=1 keeps FP64)
+    bool state32_ = false;
+    size_t sv_elem() const { return state32_ ? sizeof(float2) : sizeof(double2); }
+    int sf64() const { return state32_ ? 0 : 1; }  // the f64 flag of z-stage sources/outputs
+    SVec* scomp(SVec* v, int c) const { return (char*)v + (size_t)c * spec_ncomp() * sv_elem(); }
+    const SVec* scomp(const SVec* v, int c) const { return (const char*)v + (size_t)c * spec_ncomp() * sv_elem(); }
+    SVec* alloc_state();
     void free_dev(void* p);
     void* dev_alloc(size_t bytes);
     SpecGeom geom(const Band& b) const {
@@ -74,12 +86,12 @@ class EngineBase {
     Band make_band(int cut) const;
 
     // spectral state ops (FP64)
-    void lincomb(double2* out, double a, const double2* x, double b = 0, const double2* y = nullptr, double c = 0,
-                 const double2* z = nullptr);
-    void hilbert(double2* f, double order);
-    void leray(double2* f);
+    void lincomb(SVec* out, double a, const SVec* x, double b = 0, const SVec* y = nullptr, double c = 0,
+                 const SVec* z = nullptr);
+    void hilbert(SVec* f, double order);
+    void leray(SVec* f);
     // f <- leray(hilbert(scale * f, order)) in one pass
-    void hilbert_leray(double2* f, double order, double scale = 1.0);
+    void hilbert_leray(SVec* f, double order, double scale = 1.0);
     // tables over |j|^2 of the band b2: Hilbert symbol and H_l inner-product weight
     std::map<double, double*> htab_, hwtab_;
     const double* hilbert_table(double order);
@@ -89,21 +101,21 @@ class EngineBase {
     // (kinds 2-4 read only a)
     // pairs' inner products; optionally ax_out <- ax_x + ax_a ax_y first, in
     // the same pass (the pairs may name ax_out)
-    void dots(const SpecDotPair* pairs, int np, double* out, double2* ax_out = nullptr,
-              const double2* ax_x = nullptr, double ax_a = 0.0, const double2* ax_y = nullptr);
+    void dots(const SpecDotPair* pairs, int np, double* out, SVec* ax_out = nullptr,
+              const SVec* ax_x = nullptr, double ax_a = 0.0, const SVec* ax_y = nullptr);
     // hilbert_leray of f1 (scale 1) and f2 (scale s2), then out = {<f2, f1>_H, <f2, f2>_H}
-    void hilbert_leray_pair_dots(double2* f1, double2* f2, double order, double s2, double out[2]);
+    void hilbert_leray_pair_dots(SVec* f1, SVec* f2, double order, double s2, double out[2]);
     // g <- sg g, d <- g + beta td (td null: d <- g)
-    void direction(double2* g, double sg, double2* d, double beta, const double2* td);
-    void zeroth(const double2* f, double out[3]);
+    void direction(SVec* g, double sg, SVec* d, double beta, const SVec* td);
+    void zeroth(const SVec* f, double out[3]);
 
     // ---- diagnostics (maxdLpdt.f90:263-299, optimization.f90:119-123, 377-384) ----
     // calculate_spectral_data (function_ops.f90:2614-2677) of the state
     // spectra u: out[0..n) = kk_max = 2 pi (i+1), out[n..2n) = the shell
     // energies of fftfwd(u), scaled by <u,u>/(2 pi sum) when normalize
-    void spectrum(const double2* u, bool normalize, double* out);
+    void spectrum(const SVec* u, bool normalize, double* out);
     // calc_global_summed_enstrophy (2449-2467): 1/2 ||curl u||^2
-    double enstrophy(const double2* u);
+    double enstrophy(const SVec* u);
     // per-shell lists of the band's modes (|K| in (2 pi i, 2 pi (i+1)]),
     // built once; the shell sums then run in a fixed order
     int* d_shell_modes_ = nullptr;
@@ -146,10 +158,10 @@ class EngineBase {
     }
     // u <- cs (u + tau d), keeping the transport's physical fields of
     // u + tau d for the next gradient program
-    void retract(double2* u, double cs, double tau, const double2* d);
+    void retract(SVec* u, double cs, double tau, const SVec* d);
     // the vector transport's outputs tg = ag g + bg u + cg d, td = ad d + bd u
     // + cd d and then the retraction u <- cs (u + tau d), in one pass
-    void transport_retract(double2* tg, double2* td, const double2* g, const double2* d, double2* u, double ag,
+    void transport_retract(SVec* tg, SVec* td, const SVec* g, const SVec* d, SVec* u, double ag,
                            double bg, double cg, double ad, double bd, double cd, double cs, double tau);
     void ensure_partials(long n);
     // Count a launch and surface launch-configuration errors immediately.
@@ -382,31 +394,31 @@ class Engine : public EngineBase {
 
     // ---- programs ----
     // R parts at phi = u + tau*d (d may be null) -> results; also ||phi||_q^q.
-    void R_eval(const double2* u, const double2* d, double tau, double out[3], double* lqq);
+    void R_eval(const SVec* u, const SVec* d, double tau, double out[3], double* lqq);
     // calc_global_dEnstrophydt (function_ops.f90:1417-1481): out = {R1 + R2, R1, R2}
-    void dEnstrophydt(const double2* u, double out[3]);
+    void dEnstrophydt(const SVec* u, double out[3]);
     // calc_local_pointwise_dLqdt_inclParts (1224-1291): the fields R1 + R2 +
     // R3, R1 + R2, R3 into the host (n,n,n,3) array
-    void pointwise_R(const double2* u, double* host);
+    void pointwise_R(const SVec* u, double* host);
     // L2 gradient of R at u (GradL2ForLq) into v (FP64 spectra); also the
     // dealiased |u|^{q-2} u spectra (for calcConstraintDerivativeL2) into
     // c (FP64, may be null) and ||u||_q^q.
-    void grad_l2(const double2* u, double2* v, double2* c, double* lqq);
-    void grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq, bool from_retraction);
+    void grad_l2(const SVec* u, SVec* v, SVec* c, double* lqq);
+    void grad_l2_body(const SVec* u, SVec* v, SVec* c, bool want_lq, bool from_retraction);
     int grad_lq_slot_ = 0;
     // vectorTransport pieces at w = u + tau*d: ir[i] = <P2(|w|^{q-2} w), xi_i>,
     // returns ||w||_q^q.
-    double transport_pieces(const double2* u, const double2* d, double tau, const double2* const* xi, int nxi,
+    double transport_pieces(const SVec* u, const SVec* d, double tau, const SVec* const* xi, int nxi,
                             double* ir);
-    double lq_pow(const double2* u, const double2* d, double tau);  // ||u + tau d||_q^q
+    double lq_pow(const SVec* u, const SVec* d, double tau);  // ||u + tau d||_q^q
     // |u|^k physical (calc_uk) of the state u, into phys index dst
-    void calc_uk(const double2* u, double k, int dst);
+    void calc_uk(const SVec* u, double k, int dst);
 
     // Line search along phi = u + tau d when q = 4 (|u|^{q-4} = 1): the
     // setup forms the tau-coefficient fields once; a trial is then one
     // forward transform of g(tau)^2 plus polynomial evaluations.
     bool ls_ok() const { return !use_e_u && P.q == 4.0; }
-    void ls_setup(const double2* u, const double2* d);
+    void ls_setup(const SVec* u, const SVec* d);
     void ls_trial(double tau, double out[3], double* lqq);
     double ls_r2_[5] = {0}, ls_r3_[6] = {0};
     // Where S(tau) = S0 + tau S1 + tau^2 S2 (the dealiased |phi|^2) is >= 0 at
@@ -420,8 +432,9 @@ class Engine : public EngineBase {
     // ---- state <-> host ----
     // Forward transform of a host FP64 vector field into state spectra.
     // Returns the relative energy outside the band.
-    double load_vec(const double* host, double2* spec);
-    void store_vec(const double2* spec, double* host);
+    // spec_f64: storage of spec (-1: this engine's state storage)
+    double load_vec(const double* host, SVec* spec, int spec_f64 = -1);
+    void store_vec(const SVec* spec, double* host, int spec_f64 = -1);
     void load_scalar_phys(const double* host, int dst);
     void store_scalar_phys(int src, double* host);
 
@@ -439,10 +452,10 @@ class Engine : public EngineBase {
     void poisson_full(const double* f, double l, double* phi);
     void widen_to(const Band& b);
 
-    double2* c_tmp_ = nullptr;  // FP64 spectra of P2(|w|^{q-2} w) for the transport
+    SVec* c_tmp_ = nullptr;  // FP64 spectra of P2(|w|^{q-2} w) for the transport
     double* d_coef_ = nullptr;  // cs, tau of the retraction (read by a captured launch)
     void phys_written(int idx);  // clears the physical-field memo when it covers idx
-    bool w_from_memo(const double2* u, const double2* d, double tau);
+    bool w_from_memo(const SVec* u, const SVec* d, double tau);
     bool ls_clamp_free(double tau);  // S(tau) >= 0 at every point (the interval, else one check)
     int ls_p0_ = -1, ls_w0_ = -1;    // physical field and work spectrum of S_0 in this line search
     int ls_phys(int a) const;        // physical field of S_a

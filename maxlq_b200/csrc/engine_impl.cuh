@@ -28,6 +28,10 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
     cfft_ok_ = reg_ok_ && n <= 1024;
     if (const char* kv = std::getenv("MLQ_PASS_KERNELS")) cfft_ok_ = cfft_ok_ && std::string(kv) != "reg";
     pitch_even_ = cfft_ok_ && sizeof(T) == 4;
+    // the mixed path keeps its CG state (every state vector's Fourier
+    // coefficients) in FP32; the operations on it compute in FP64
+    state32_ = sizeof(T) == 4;
+    if (const char* e = std::getenv("MLQ_STATE_F64")) state32_ = state32_ && std::string(e) != "1";
     {
         int dev = 0;
         MLQ_CUDA(cudaGetDevice(&dev));
@@ -375,10 +379,11 @@ void Engine<T>::tune_yz() {
     const long xs_n = (long)n * n * pxb, ys_n = (long)n * b.nb * pxb, sp_n = (long)b.nb * b.nb * b.nx;
     cpx<T>* A = (cpx<T>*)dev_alloc(NA * xs_n * sizeof(cpx<T>));
     cpx<T>* B = (cpx<T>*)dev_alloc(NA * ys_n * sizeof(cpx<T>));
-    double2* C = (double2*)dev_alloc(NA * sp_n * sizeof(double2));
+    // spectra in the state storage, as the programs read and write them
+    char* C = (char*)dev_alloc(NA * sp_n * sv_elem());
     MLQ_CUDA(cudaMemsetAsync(A, 0, NA * xs_n * sizeof(cpx<T>), stream));
     MLQ_CUDA(cudaMemsetAsync(B, 0, NA * ys_n * sizeof(cpx<T>), stream));
-    MLQ_CUDA(cudaMemsetAsync(C, 0, NA * sp_n * sizeof(double2), stream));
+    MLQ_CUDA(cudaMemsetAsync(C, 0, NA * sp_n * sv_elem(), stream));
     YArgs<T> yf{}, yi{};
     yf.n = yi.n = n;
     yf.nz = yi.nz = n;
@@ -403,14 +408,14 @@ void Engine<T>::tune_yz() {
         yi.out[a] = A + a * xs_n;
         ZFwdOp op = {};
         op.in = B + a * ys_n;
-        op.spec_out = C + a * sp_n;
-        op.spec_f64 = 1;
+        op.spec_out = C + a * sp_n * sv_elem();
+        op.spec_f64 = sf64();
         op.sym = SYM_ONE;
         op.red_self = 0;
         for (int r = 0; r < 3; ++r) op.red_with_slot[r] = -1;
         zf.op[a] = op;
         ZInvOp oi = {};
-        oi.src[0] = ZSrc{C + a * sp_n, 1, SYM_IKX, 0, 1.0};
+        oi.src[0] = ZSrc{C + a * sp_n * sv_elem(), sf64(), SYM_IKX, 0, 1.0};
         oi.nsrc = 1;
         oi.ys_out = B + a * ys_n;
         zi.op[a] = oi;
@@ -1416,7 +1421,7 @@ int Engine<T>::ls_wspec(int a) const {
 // PU <- u + tau d from the line search's physical fields of u and d, when the
 // memo holds them; records the transport fields (tr) for the next gradient
 template <typename T>
-bool Engine<T>::w_from_memo(const double2* u, const double2* d, double tau) {
+bool Engine<T>::w_from_memo(const SVec* u, const SVec* d, double tau) {
     if (slab_ || !reuse_on_ || !d || !pm_.ls || pm_.u != (const void*)u || pm_.d != (const void*)d) {
         pm_ = PhysMemo{};
         return false;
@@ -1615,7 +1620,7 @@ static void sdots(Engine<T>& e, const std::vector<std::pair<const cpx<T>*, const
 // an L2 inner product with a band-limited field is applied through Parseval
 // on the band instead of by a round trip (the projection is self-adjoint).
 template <typename T>
-void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double out[3], double* lqq) {
+void Engine<T>::R_eval(const SVec* u, const SVec* d, double tau, double out[3], double* lqq) {
     pu_of_ = nullptr;
     const Band& b = b2;
     const long nc = spec_ncomp();
@@ -1628,8 +1633,8 @@ void Engine<T>::R_eval(const double2* u, const double2* d, double tau, double ou
             InvOut o;
             o.nsrc = d ? 2 : 1;
             const int sym = j < 0 ? SYM_ONE : SYM_IKX + j;
-            o.src[0] = ZSrc{u + i * nc, 1, sym, 0, 1.0};
-            if (d) o.src[1] = ZSrc{d + i * nc, 1, sym, 0, tau};
+            o.src[0] = ZSrc{scomp(u, i), sf64(), sym, 0, 1.0};
+            if (d) o.src[1] = ZSrc{scomp(d, i), sf64(), sym, 0, tau};
             o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
             io.push_back(o);
         }
@@ -1748,7 +1753,7 @@ enum : int { PDG2 = 100, PDR1 = 101, PDR2 = 102, PDR3 = 103, PDT1 = 104, PDT2 = 
 // R2 = <P2((u.grad) u), Lap u> as one forward pipeline whose z stage applies
 // -|K|^2 and reduces against the spectra of u (Lap is self-adjoint)
 template <typename T>
-void Engine<T>::dEnstrophydt(const double2* u, double out[3]) {
+void Engine<T>::dEnstrophydt(const SVec* u, double out[3]) {
     pu_of_ = nullptr;
     const long nc = spec_ncomp();
     std::vector<InvOut> io;
@@ -1756,7 +1761,7 @@ void Engine<T>::dEnstrophydt(const double2* u, double out[3]) {
         for (int j = -1; j < 3; ++j) {
             InvOut o;
             o.nsrc = 1;
-            o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+            o.src[0] = ZSrc{scomp(u, i), sf64(), j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
             o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
             io.push_back(o);
         }
@@ -1767,8 +1772,8 @@ void Engine<T>::dEnstrophydt(const double2* u, double out[3]) {
     FwdOut o[3];
     for (int i = 0; i < 3; ++i) {
         o[i].sym = SYM_NEG_KSQ;
-        o[i].red_with[0] = u + i * nc;
-        o[i].red_with_f64[0] = 1;
+        o[i].red_with[0] = scomp(u, i);
+        o[i].red_with_f64[0] = sf64();
         o[i].red_with_slot[0] = 0;
     }
     fwd(b2, FUGradU{}, uin, {o[0], o[1], o[2]}, 48);
@@ -1789,7 +1794,7 @@ void Engine<T>::dEnstrophydt(const double2* u, double out[3]) {
 // P2(u . V)) (a2, e_u . E on the e_u branch); the coefficients are applied
 // after the dealias, as the reference does
 template <typename T>
-void Engine<T>::pointwise_R(const double2* u, double* host) {
+void Engine<T>::pointwise_R(const SVec* u, double* host) {
     if (slab_) throw CudaError("pointwise R fields need the resident (not z-slab) mode", MLQ_ERR_BADARG);
     pu_of_ = nullptr;
     const long nc = spec_ncomp();
@@ -1800,7 +1805,7 @@ void Engine<T>::pointwise_R(const double2* u, double* host) {
         for (int j = -1; j < 3; ++j) {
             InvOut o;
             o.nsrc = 1;
-            o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+            o.src[0] = ZSrc{scomp(u, i), sf64(), j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
             o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
             io.push_back(o);
         }
@@ -1867,7 +1872,7 @@ void Engine<T>::pointwise_R(const double2* u, double* host) {
 // terms is a dealiased product; their sum is dealiased once (the projection
 // is linear), the fifth term nu Lap P2(|u|^{q-2}u) is added in the spectrum.
 template <typename T>
-void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
+void Engine<T>::grad_l2(const SVec* u, SVec* v, SVec* c, double* lqq) {
     if (!c) throw CudaError("grad_l2 needs a spectrum buffer for |u|^{q-2}u", MLQ_ERR_BADARG);
     // u = cs w from the last line search's transport: u and grad u pointwise
     const bool rt = !slab_ && reuse_on_ && pm_.tr && pm_.next == (const void*)u;
@@ -1891,7 +1896,7 @@ void Engine<T>::grad_l2(const double2* u, double2* v, double2* c, double* lqq) {
 }
 
 template <typename T>
-void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want_lq, bool from_retraction) {
+void Engine<T>::grad_l2_body(const SVec* u, SVec* v, SVec* c, bool want_lq, bool from_retraction) {
     pu_of_ = nullptr;
     const bool sac = from_retraction && pm_.sac;
     const Band& b = b2;
@@ -1929,8 +1934,13 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
                 launched("spec_scale", 2.0 * nsp * sizeof(cpx<T>), ew);
             }
             cudaEvent_t ev = prof_mark();
-            spec_scale_pow_kernel<double2><<<grid_for(3 * nc, 256), 256, 0, stream>>>(c, c_tmp_, 3 * nc, d_coef_, 3);
-            launched("spec_scale", 2.0 * 3 * nc * sizeof(double2), ev);
+            if (state32_)
+                spec_scale_pow_kernel<float2><<<grid_for(3 * nc, 256), 256, 0, stream>>>(
+                    (float2*)c, (const float2*)c_tmp_, 3 * nc, d_coef_, 3);
+            else
+                spec_scale_pow_kernel<double2><<<grid_for(3 * nc, 256), 256, 0, stream>>>(
+                    (double2*)c, (const double2*)c_tmp_, 3 * nc, d_coef_, 3);
+            launched("spec_scale", 2.0 * 3 * nc * sv_elem(), ev);
         } else {
             FRetract<false> f;
             f.coef = d_coef_;
@@ -1941,13 +1951,13 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         for (int j = -1; j < 3 && !from_retraction; ++j) {
             InvOut o;
             o.nsrc = 1;
-            o.src[0] = ZSrc{u + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+            o.src[0] = ZSrc{scomp(u, i), sf64(), j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
             o.phys_out = j < 0 ? PU + i : PD + 3 * i + j;
             io.push_back(o);
         }
         InvOut o;
         o.nsrc = 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_NEG_KSQ, 0, 1.0};  // laplacian (3248-3282)
+        o.src[0] = ZSrc{scomp(u, i), sf64(), SYM_NEG_KSQ, 0, 1.0};  // laplacian (3248-3282)
         o.phys_out = PL + i;
         io.push_back(o);
     }
@@ -2001,8 +2011,8 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         FwdOut oT, oc[3];
         oT.phys_out = PT;
         for (int i = 0; i < 3; ++i) {
-            oc[i].spec = c + i * nc;
-            oc[i].spec_f64 = 1;
+            oc[i].spec = scomp(c, i);
+            oc[i].spec_f64 = sf64();
         }
         std::vector<int> in2;
         for (int i = 0; i < 3; ++i) in2.push_back(PU + i);
@@ -2042,7 +2052,7 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         for (int k = 0; k < 3; ++k) {
             InvOut o;
             o.nsrc = 3;
-            for (int j = 0; j < 3; ++j) o.src[j] = ZSrc{c + j * nc, 1, SYM_KK_KSQ, 3 * k + j, 1.0};
+            for (int j = 0; j < 3; ++j) o.src[j] = ZSrc{scomp(c, j), sf64(), SYM_KK_KSQ, 3 * k + j, 1.0};
             o.phys_out = PGA + k;
             g.push_back(o);
         }
@@ -2060,10 +2070,10 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
         for (int i = 0; i < 3; ++i) in3.push_back(PL + i);
         FwdOut o[3];
         for (int i = 0; i < 3; ++i) {
-            o[i].spec = v + i * nc;
-            o[i].spec_f64 = 1;
-            o[i].add = c + i * nc;
-            o[i].add_f64 = 1;
+            o[i].spec = scomp(v, i);
+            o[i].spec_f64 = sf64();
+            o[i].add = scomp(c, i);
+            o[i].add_f64 = sf64();
             o[i].add_sym = SYM_NEG_KSQ;
             o[i].add_coef = cv;
         }
@@ -2096,7 +2106,7 @@ void Engine<T>::grad_l2_body(const double2* u, double2* v, double2* c, bool want
 
 // ||u + tau d||_q^q (calc_global_Lq_norm)
 template <typename T>
-double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
+double Engine<T>::lq_pow(const SVec* u, const SVec* d, double tau) {
     pu_of_ = nullptr;
     const long nc = spec_ncomp();
     chain_reset();
@@ -2105,8 +2115,8 @@ double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
         for (int i = 0; i < 3; ++i) {
             InvOut o;
             o.nsrc = d ? 2 : 1;
-            o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-            if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
+            o.src[0] = ZSrc{scomp(u, i), sf64(), SYM_ONE, 0, 1.0};
+            if (d) o.src[1] = ZSrc{scomp(d, i), sf64(), SYM_ONE, 0, tau};
             o.phys_out = PU + i;
             io.push_back(o);
         }
@@ -2130,7 +2140,7 @@ double Engine<T>::lq_pow(const double2* u, const double2* d, double tau) {
 
 // vectorTransport (function_ops.f90:1716-1768) pieces at w = u + tau d.
 template <typename T>
-double Engine<T>::transport_pieces(const double2* u, const double2* d, double tau, const double2* const* xi,
+double Engine<T>::transport_pieces(const SVec* u, const SVec* d, double tau, const SVec* const* xi,
                                    int nxi, double* ir) {
     pu_of_ = nullptr;
     const long nc = spec_ncomp();
@@ -2142,8 +2152,8 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
         for (int i = 0; i < 3; ++i) {
             InvOut o;
             o.nsrc = d ? 2 : 1;
-            o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
-            if (d) o.src[1] = ZSrc{d + i * nc, 1, SYM_ONE, 0, tau};
+            o.src[0] = ZSrc{scomp(u, i), sf64(), SYM_ONE, 0, 1.0};
+            if (d) o.src[1] = ZSrc{scomp(d, i), sf64(), SYM_ONE, 0, tau};
             o.phys_out = PU + i;
             io.push_back(o);
         }
@@ -2173,14 +2183,14 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
     PowField a2 = chain(q - 2.0);
     PowField ah = chain(q / 2.0);
     if (!c_tmp_) c_tmp_ = alloc_state();
-    double2* cbuf = c_tmp_;
+    SVec* cbuf = c_tmp_;
     if (q - 2.0 > MACH_EPSILON) {
         // aux = P2(|w|^{q-2} w) (1737-1740)
         ensure_phys(a2);
         FwdOut o[3];
         for (int i = 0; i < 3; ++i) {
-            o[i].spec = cbuf + i * nc;
-            o[i].spec_f64 = 1;
+            o[i].spec = scomp(cbuf, i);
+            o[i].spec_f64 = sf64();
         }
         fwd(b2, FC3{}, {a2.phys, PU, PU + 1, PU + 2}, {o[0], o[1], o[2]});
         if (memo) {
@@ -2214,7 +2224,7 @@ double Engine<T>::transport_pieces(const double2* u, const double2* d, double ta
 
 // calc_uk (function_ops.f90:2324-2343) of the state u into phys(dst)
 template <typename T>
-void Engine<T>::calc_uk(const double2* u, double k, int dst) {
+void Engine<T>::calc_uk(const SVec* u, double k, int dst) {
     pu_of_ = nullptr;
     const long nc = spec_ncomp();
     chain_reset();
@@ -2222,7 +2232,7 @@ void Engine<T>::calc_uk(const double2* u, double k, int dst) {
     for (int i = 0; i < 3; ++i) {
         InvOut o;
         o.nsrc = 1;
-        o.src[0] = ZSrc{u + i * nc, 1, SYM_ONE, 0, 1.0};
+        o.src[0] = ZSrc{scomp(u, i), sf64(), SYM_ONE, 0, 1.0};
         o.phys_out = PU + i;
         io.push_back(o);
     }
@@ -2335,7 +2345,7 @@ __global__ void __launch_bounds__(RED_THREADS)
 }
 
 template <typename T>
-void Engine<T>::ls_setup(const double2* u, const double2* d) {
+void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
     const long nc = spec_ncomp();
     // u and grad u are still in PU, PD when the gradient program of this
     // iteration transformed the same spectrum
@@ -2349,7 +2359,7 @@ void Engine<T>::ls_setup(const double2* u, const double2* d) {
             for (int j = -1; j < 3; ++j) {
                 InvOut o;
                 o.nsrc = 1;
-                o.src[0] = ZSrc{(f == 0 ? u : d) + i * nc, 1, j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
+                o.src[0] = ZSrc{scomp(f == 0 ? u : d, i), sf64(), j < 0 ? SYM_ONE : SYM_IKX + j, 0, 1.0};
                 o.phys_out = j < 0 ? (f == 0 ? LU : LD) + i : (f == 0 ? LDU : LDD) + 3 * i + j;
                 io.push_back(o);
             }
@@ -2700,13 +2710,14 @@ void Engine<T>::store_scalar_phys(int src, double* host) {
 // Forward transform of a host vector field into band-b2 state spectra.  The
 // energy the band drops is measured directly, as ||u - F^-1 P2 F u||^2.
 template <typename T>
-double Engine<T>::load_vec(const double* host, double2* spec) {
+double Engine<T>::load_vec(const double* host, SVec* spec, int spec_f64) {
     const long nc = spec_ncomp();
+    if (spec_f64 < 0) spec_f64 = sf64();
     for (int c = 0; c < 3; ++c) {
         load_scalar_phys(host + c * n3, PIO);
         FwdOut o;
-        o.spec = spec + c * nc;
-        o.spec_f64 = 1;
+        o.spec = (char*)spec + (size_t)c * nc * (spec_f64 ? sizeof(double2) : sizeof(float2));
+        o.spec_f64 = spec_f64;
         o.phys_out = PIO2;
         fwd(b2, FCopy{}, {PIO}, {o});
         pointwise(FDiffSq{}, {PIO, PIO2}, {}, 30 + 2 * c);
@@ -2722,12 +2733,14 @@ double Engine<T>::load_vec(const double* host, double2* spec) {
 }
 
 template <typename T>
-void Engine<T>::store_vec(const double2* spec, double* host) {
+void Engine<T>::store_vec(const SVec* spec, double* host, int spec_f64) {
     const long nc = spec_ncomp();
+    if (spec_f64 < 0) spec_f64 = sf64();
     for (int c = 0; c < 3; ++c) {
         InvOut o;
         o.nsrc = 1;
-        o.src[0] = ZSrc{spec + c * nc, 1, SYM_ONE, 0, 1.0};
+        o.src[0] = ZSrc{(const char*)spec + (size_t)c * nc * (spec_f64 ? sizeof(double2) : sizeof(float2)), spec_f64,
+                        SYM_ONE, 0, 1.0};
         o.phys_out = PIO;
         inv(b2, {o});
         store_scalar_phys(PIO, host + c * n3);

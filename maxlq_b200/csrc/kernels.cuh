@@ -406,6 +406,19 @@ __device__ __forceinline__ void st_spec(void* p, int f64, long idx, cpx<double> 
 // Parseval weight of a half-spectrum column (real fields)
 __device__ __forceinline__ double kx_weight(int n, int fx) { return (fx == 0 || 2 * fx == n) ? 1.0 : 2.0; }
 
+// State-vector storage: double2 (FP64 path) or float2 (mixed path); the
+// spectral state kernels load into double, compute in double and round on
+// the store.
+template <typename V>
+__device__ __forceinline__ double2 ldv(const V* p, long i) {
+    const V v = p[i];
+    return make_double2((double)v.x, (double)v.y);
+}
+template <typename V>
+__device__ __forceinline__ void stv(V* p, long i, double2 v) {
+    p[i] = V{(decltype(p[i].x))v.x, (decltype(p[i].y))v.y};
+}
+
 // ----------------------------------------------------------------------------
 // z stage, forward (optionally round trip).  grid = (ceil(nx/tx), nb, narr).
 // For each array: z FFT, keep |kz| <= cut, scale 1/N^3, multiply by `sym`,
@@ -595,23 +608,24 @@ __device__ __forceinline__ void spec_coords(const SpecGeom& g, long i, int& fx, 
 }
 
 // out = a*x + b*y + c*z  (any pointer may alias out; y/z may be null)
-static __global__ void spec_lincomb_kernel(SpecGeom g, double2* out, double a, const double2* x, double b,
-                                    const double2* y, double c, const double2* z) {
+template <typename V>
+__global__ void spec_lincomb_kernel(SpecGeom g, V* out, double a, const V* x, double b, const V* y, double c,
+                                    const V* z) {
     const long nt = 3 * g.ncomp;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += (long)gridDim.x * blockDim.x) {
-        double2 v = x[i];
+        double2 v = ldv(x, i);
         double2 r = make_double2(a * v.x, a * v.y);
         if (y) {
-            const double2 w = y[i];
+            const double2 w = ldv(y, i);
             r.x += b * w.x;
             r.y += b * w.y;
         }
         if (z) {
-            const double2 w = z[i];
+            const double2 w = ldv(z, i);
             r.x += c * w.x;
             r.y += c * w.y;
         }
-        out[i] = r;
+        stv(out, i, r);
     }
 }
 
@@ -648,14 +662,14 @@ __global__ void spec_poly3_kernel(C* out, const C* a, const C* b, const C* c, lo
 // The vector transport's two outputs and the retraction in one pass over the
 // state (function_ops.f90:1716-1768 with optimization.f90:324-338):
 //   tg = ag g + bg u + cg d,  td = ad d + bd u + cd d,  u <- cs u + ct d
-static __global__ void spec_transport_kernel(long nt, const double2* g, const double2* d, double2* u, double2* tg,
-                                             double2* td, double ag, double bg, double cg, double ad, double bd,
-                                             double cd, double cs, double ct) {
+template <typename V>
+__global__ void spec_transport_kernel(long nt, const V* g, const V* d, V* u, V* tg, V* td, double ag, double bg,
+                                      double cg, double ad, double bd, double cd, double cs, double ct) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += (long)gridDim.x * blockDim.x) {
-        const double2 gv = g[i], dv = d[i], uv = u[i];
-        tg[i] = make_double2(ag * gv.x + bg * uv.x + cg * dv.x, ag * gv.y + bg * uv.y + cg * dv.y);
-        td[i] = make_double2(ad * dv.x + bd * uv.x + cd * dv.x, ad * dv.y + bd * uv.y + cd * dv.y);
-        u[i] = make_double2(cs * uv.x + ct * dv.x, cs * uv.y + ct * dv.y);
+        const double2 gv = ldv(g, i), dv = ldv(d, i), uv = ldv(u, i);
+        stv(tg, i, make_double2(ag * gv.x + bg * uv.x + cg * dv.x, ag * gv.y + bg * uv.y + cg * dv.y));
+        stv(td, i, make_double2(ad * dv.x + bd * uv.x + cd * dv.x, ad * dv.y + bd * uv.y + cd * dv.y));
+        stv(u, i, make_double2(cs * uv.x + ct * dv.x, cs * uv.y + ct * dv.y));
     }
 }
 
@@ -698,8 +712,9 @@ __device__ __forceinline__ void hilbert_leray_point(double2& u0, double2& u1, do
     }
 }
 
-static __global__ void spec_hilbert_leray_kernel(SpecGeom g, double2* f, const double* __restrict__ htab,
-                                                 double scale, int do_leray) {
+template <typename V>
+__global__ void spec_hilbert_leray_kernel(SpecGeom g, V* f, const double* __restrict__ htab, double scale,
+                                          int do_leray) {
     const double twopi = 2.0 * 3.14159265358979311600;
     const int nrows = g.nb * g.nb;
     for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
@@ -710,15 +725,15 @@ static __global__ void spec_hilbert_leray_kernel(SpecGeom g, double2* f, const d
         const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
         for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
             const long i = base + fx;
-            double2 u0 = f[i], u1 = f[g.ncomp + i], u2 = f[2 * g.ncomp + i];
+            double2 u0 = ldv(f, i), u1 = ldv(f, g.ncomp + i), u2 = ldv(f, 2 * g.ncomp + i);
             double s = scale;
             if (htab) s *= htab[fx * fx + row.jy * row.jy + row.jz * row.jz];
             const double kx = twopi * (double)fx;
             const double ox = (2 * fx == g.n) ? 0.0 : kx;
             hilbert_leray_point(u0, u1, u2, s, do_leray != 0, ox, oy, oz, kx * kx + ky * ky + kz * kz);
-            f[i] = u0;
-            f[g.ncomp + i] = u1;
-            f[2 * g.ncomp + i] = u2;
+            stv(f, i, u0);
+            stv(f, g.ncomp + i, u1);
+            stv(f, 2 * g.ncomp + i, u2);
         }
     }
 }
@@ -726,11 +741,11 @@ static __global__ void spec_hilbert_leray_kernel(SpecGeom g, double2* f, const d
 // Hilbert gradient + Leray projection of two fields (f1 scaled by s1, f2 by
 // s2) and, on the results, the H inner products <f2, f1> and <f2, f2> (the
 // weights of spec_dot_kernel's kind 1) as per-block partials [block][2]
-static __global__ void __launch_bounds__(128) spec_hilbert_leray_pair_dot_kernel(SpecGeom g, double2* f1, double s1,
-                                                                              double2* f2, double s2,
-                                                                              const double* __restrict__ htab,
-                                                                              const double* __restrict__ hwtab,
-                                                                              double* partials) {
+template <typename V>
+__global__ void __launch_bounds__(128) spec_hilbert_leray_pair_dot_kernel(SpecGeom g, V* f1, double s1, V* f2,
+                                                                       double s2, const double* __restrict__ htab,
+                                                                       const double* __restrict__ hwtab,
+                                                                       double* partials) {
     const double twopi = 2.0 * 3.14159265358979311600;
     const int nrows = g.nb * g.nb;
     double acc[2] = {0.0, 0.0};
@@ -743,20 +758,20 @@ static __global__ void __launch_bounds__(128) spec_hilbert_leray_pair_dot_kernel
         const int jyz = row.jy * row.jy + row.jz * row.jz;
         for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
             const long i = base + fx;
-            double2 a0 = f1[i], a1 = f1[g.ncomp + i], a2 = f1[2 * g.ncomp + i];
-            double2 b0 = f2[i], b1 = f2[g.ncomp + i], b2 = f2[2 * g.ncomp + i];
+            double2 a0 = ldv(f1, i), a1 = ldv(f1, g.ncomp + i), a2 = ldv(f1, 2 * g.ncomp + i);
+            double2 b0 = ldv(f2, i), b1 = ldv(f2, g.ncomp + i), b2 = ldv(f2, 2 * g.ncomp + i);
             const double h = htab[fx * fx + jyz];
             const double kx = twopi * (double)fx;
             const double ox = (2 * fx == g.n) ? 0.0 : kx;
             const double ksq = kx * kx + ky * ky + kz * kz;
             hilbert_leray_point(a0, a1, a2, s1 * h, true, ox, oy, oz, ksq);
             hilbert_leray_point(b0, b1, b2, s2 * h, true, ox, oy, oz, ksq);
-            f1[i] = a0;
-            f1[g.ncomp + i] = a1;
-            f1[2 * g.ncomp + i] = a2;
-            f2[i] = b0;
-            f2[g.ncomp + i] = b1;
-            f2[2 * g.ncomp + i] = b2;
+            stv(f1, i, a0);
+            stv(f1, g.ncomp + i, a1);
+            stv(f1, 2 * g.ncomp + i, a2);
+            stv(f2, i, b0);
+            stv(f2, g.ncomp + i, b1);
+            stv(f2, 2 * g.ncomp + i, b2);
             const double w = kx_weight(g.n, fx) * hwtab[fx * fx + jyz];
             acc[0] += w * ((b0.x * a0.x + b0.y * a0.y) + (b1.x * a1.x + b1.y * a1.y) + (b2.x * a2.x + b2.y * a2.y));
             acc[1] += w * ((b0.x * b0.x + b0.y * b0.y) + (b1.x * b1.x + b1.y * b1.y) + (b2.x * b2.x + b2.y * b2.y));
@@ -767,19 +782,19 @@ static __global__ void __launch_bounds__(128) spec_hilbert_leray_pair_dot_kernel
 
 // The search direction from the projected gradient: g <- sg g, then
 // d <- g + beta td (td may be null: d <- g)
-static __global__ void spec_direction_kernel(long nt, double2* g, double sg, double2* d, double beta,
-                                             const double2* td) {
+template <typename V>
+__global__ void spec_direction_kernel(long nt, V* g, double sg, V* d, double beta, const V* td) {
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nt; i += (long)gridDim.x * blockDim.x) {
-        double2 v = g[i];
+        double2 v = ldv(g, i);
         v.x *= sg;
         v.y *= sg;
-        g[i] = v;
+        stv(g, i, v);
         if (td) {
-            const double2 w = td[i];
+            const double2 w = ldv(td, i);
             v.x += beta * w.x;
             v.y += beta * w.y;
         }
-        d[i] = v;
+        stv(d, i, v);
     }
 }
 
@@ -787,8 +802,8 @@ static __global__ void spec_direction_kernel(long nt, double2* g, double sg, dou
 // (1+(lambda1|K|)^order)^2 (function_ops.f90:3472), 2 divergence energy
 // |K_odd . f|^2 of pair.a (pair.b ignored).
 struct SpecDotPair {
-    const double2* a;
-    const double2* b;
+    const void* a;  // state vectors (double2 or float2 storage, the kernel's V)
+    const void* b;
     int kind;
 };
 struct SpecDotArgs {
@@ -797,15 +812,16 @@ struct SpecDotArgs {
     int npairs;
     // optional ax_out <- ax_x + ax_a ax_y before the products (the pairs may
     // read ax_out: each element is updated by the thread that then reads it)
-    double2* ax_out = nullptr;
-    const double2* ax_x = nullptr;
-    const double2* ax_y = nullptr;
+    void* ax_out = nullptr;
+    const void* ax_x = nullptr;
+    const void* ax_y = nullptr;
     double ax_a = 0.0;
     const double* hwtab;  // H_l weight (1+(lambda1|K|)^order)^2 by |j|^2 (function_ops.f90:3472), or null
     double* partials;
 };
 
-static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
+template <typename V>
+__global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const SpecGeom& g = a.g;
     const double twopi = 2.0 * 3.14159265358979311600;
@@ -832,8 +848,8 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
 #pragma unroll
                     for (int c = 0; c < 3; ++c) {
                         const long k = c * g.ncomp + i[e];
-                        const double2 x = a.ax_x[k], y = a.ax_y[k];
-                        a.ax_out[k] = make_double2(x.x + a.ax_a * y.x, x.y + a.ax_a * y.y);
+                        const double2 x = ldv((const V*)a.ax_x, k), y = ldv((const V*)a.ax_y, k);
+                        stv((V*)a.ax_out, k, make_double2(x.x + a.ax_a * y.x, x.y + a.ax_a * y.y));
                     }
             }
             for (int p = 0; p < a.npairs; ++p) {
@@ -846,7 +862,7 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
 #pragma unroll
                     for (int e = 0; e < 2; ++e)
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) v[e][c] = q.a[c * g.ncomp + i[e]];
+                        for (int c = 0; c < 3; ++c) v[e][c] = ldv((const V*)q.a, c * g.ncomp + i[e]);
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         double s;
@@ -869,7 +885,7 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
 #pragma unroll
                     for (int e = 0; e < 2; ++e)
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) v[e][c] = q.a[c * g.ncomp + i[e]];
+                        for (int c = 0; c < 3; ++c) v[e][c] = ldv((const V*)q.a, c * g.ncomp + i[e]);
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {
                         const double dr = ox[e] * v[e][0].x + oy * v[e][1].x + oz * v[e][2].x;
@@ -882,8 +898,8 @@ static __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArg
                     for (int e = 0; e < 2; ++e)
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
-                            u[e][c] = q.a[c * g.ncomp + i[e]];
-                            v[e][c] = q.b[c * g.ncomp + i[e]];
+                            u[e][c] = ldv((const V*)q.a, c * g.ncomp + i[e]);
+                            v[e][c] = ldv((const V*)q.b, c * g.ncomp + i[e]);
                         }
 #pragma unroll
                     for (int e = 0; e < 2; ++e) {

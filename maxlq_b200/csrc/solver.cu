@@ -25,7 +25,7 @@ template <typename T>
 class Solver : public SolverBase {
    public:
     Engine<T> e;
-    double2 *u, *d1, *gu0, *gu1, *vtg0, *vtd0, *c, *tmp, *tmp2;
+    SVec *u, *d1, *gu0, *gu1, *vtg0, *vtd0, *c, *tmp, *tmp2;
     // CG memory of the resident loop
     bool started = false;
     int iter = 0, start_iter = 0;
@@ -69,13 +69,13 @@ class Solver : public SolverBase {
     double q() const { return e.P.q; }
     double B() const { return e.P.B; }
 
-    void zero(double2* f) { MLQ_CUDA(cudaMemsetAsync(f, 0, 3 * nc() * sizeof(double2), e.stream)); }
+    void zero(SVec* f) { MLQ_CUDA(cudaMemsetAsync(f, 0, 3 * nc() * e.sv_elem(), e.stream)); }
 
     // load a host vector field, refusing fields with modes outside the band
-    void load(const double* host, double2* spec) {
+    void load(const double* host, SVec* spec) {
         MLQ_CUDA(cudaStreamSynchronize(e.stream));
         e.state_written(spec);
-        const double rel = io().load_vec(host, spec);
+        const double rel = io().load_vec(host, spec, e.sf64());
         trim_io();
         const double tol = 1e-24;  // relative energy; FP64 FFT round-trip noise is ~1e-32
         if (std::isnan(rel))
@@ -91,7 +91,7 @@ class Solver : public SolverBase {
     // Line-search trials go through the polynomial path when q = 4: setup
     // once per (base, dir), then one transform per trial.
     bool ls_ready = false;
-    void ls_begin(const double2* base, const double2* dir) {
+    void ls_begin(const SVec* base, const SVec* dir) {
         trials.clear();
         ls_ready = false;
         if (e.ls_ok() && dir && e.ls_fits()) {
@@ -99,7 +99,7 @@ class Solver : public SolverBase {
             ls_ready = true;
         }
     }
-    Trial trial(const double2* base, const double2* dir, double tau) {
+    Trial trial(const SVec* base, const SVec* dir, double tau) {
         auto it = trials.find(tau);
         if (it != trials.end()) return it->second;
         Trial t;
@@ -111,7 +111,7 @@ class Solver : public SolverBase {
         return t;
     }
     // eval_J(phi + tau d, "LineMin") (optimization.f90:537-539)
-    double lm_eval(const double2* base, const double2* dir, double tau) {
+    double lm_eval(const SVec* base, const SVec* dir, double tau) {
         ++eval_count;
         ++evals_this_iter;
         const Trial t = trial(base, dir, tau);
@@ -131,7 +131,7 @@ class Solver : public SolverBase {
     int evals_this_iter = 0;
 
     // mnbrak (optimization.f90:613-778)
-    int mnbrak(const double2* phi, const double2* grad, double tA0, double tB0, double tau_brack[2], int* myflag) {
+    int mnbrak(const SVec* phi, const SVec* grad, double tA0, double tB0, double tau_brack[2], int* myflag) {
         const double GOLD = (1.0 + std::sqrt(5.0)) / 2.0;
         const double CGOLD = 1.0 / GOLD;
         const double GLIMIT = 10.0;
@@ -197,7 +197,7 @@ class Solver : public SolverBase {
     // brent (optimization.f90:784-951); the constants are the Fortran
     // default-real literals TOL = 1E-6, ZEPS = 1E-8, CGOLD = .381966 widened
     // to double (804-806)
-    double brent(const double2* phi, const double2* grad, const double tau_brack[2], double* fx_out) {
+    double brent(const SVec* phi, const SVec* grad, const double tau_brack[2], double* fx_out) {
         const int ITMAX = 300;
         const double TOL = (double)1E-6f;
         const double ZEPS = (double)1E-8f;
@@ -254,7 +254,7 @@ class Solver : public SolverBase {
     }
 
     // ---- CG loop -------------------------------------------------------------
-    double H(const double2* a, const double2* b) {
+    double H(const SVec* a, const SVec* b) {
         SpecDotPair p{a, b, 1};
         double r;
         e.dots(&p, 1, &r);
@@ -307,7 +307,7 @@ class Solver : public SolverBase {
         trials.clear();
         const double qq = q(), Bc = B();
         const double s = (3.0 / 2.0) - (1.0 / qq);  // 150
-        double2* g1 = gu1;
+        SVec* g1 = gu1;
         double lqq_u = 0;
         e.grad_l2(u, g1, c, &lqq_u);  // 146
         // Hilbert gradient of g (151, 153) and of the normal of the tangent
@@ -385,7 +385,7 @@ class Solver : public SolverBase {
         info.tau = tau1;
         // vector transport of gu1 and d1 to the new point (324-328)
         double ir[2];
-        const double2* xi[2] = {g1, d1};
+        const SVec* xi[2] = {g1, d1};
         ls_ready = false;
         double lqw;
         if (e.P.use_riemannian_geometry)
@@ -506,7 +506,7 @@ class Solver : public SolverBase {
         load(eta, d1);
         load(xi, gu1);
         double ir;
-        const double2* xs[1] = {gu1};
+        const SVec* xs[1] = {gu1};
         const double lqq = e.transport_pieces(tmp, d1, 1.0, xs, 1, &ir);
         const double ln = std::pow(lqq, 1.0 / qv);
         const double f = std::pow(ln, -qv) * ir;
@@ -582,9 +582,9 @@ class Solver : public SolverBase {
         load(uh, u);
         started = false;
     }
-    void store(const double2* spec, double* host) {
+    void store(const SVec* spec, double* host) {
         MLQ_CUDA(cudaStreamSynchronize(e.stream));
-        io().store_vec(spec, host);
+        io().store_vec(spec, host, e.sf64());
         trim_io();
     }
     void state_store(double* uh) override { store(u, uh); }
@@ -603,8 +603,14 @@ class Solver : public SolverBase {
     void seed_field(unsigned long long seed, double slope, double k0, double* out) override {
         std::vector<double> h(3 * nc() * 2);
         seed_spectrum_host(e.n, seed, slope, k0, e.b2, h.data());
-        MLQ_CUDA(cudaMemcpyAsync(tmp, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, e.stream));
-        store(tmp, out);
+        // through an FP64 buffer of the FP64 transfer engine: the seeded field
+        // exactly, whatever the state storage of this context
+        Engine<double>& io64 = io();
+        SVec* t = io64.dev_alloc(3 * nc() * sizeof(double2));
+        MLQ_CUDA(cudaMemcpyAsync(t, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, io64.stream));
+        io64.store_vec(t, out, 1);
+        io64.free_dev(t);
+        trim_io();
     }
     void set_B(double Bv) override {
         e.P.B = Bv;

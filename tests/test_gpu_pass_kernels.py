@@ -185,3 +185,25 @@ def test_multi_output_z_inverse_matches_one_output_per_launch_row(n, precision, 
     if a[1] is not None:
         assert np.array_equal(a[1], b[1])
     assert a[2] == b[2] and a[3] == b[3]
+
+
+def test_fp32_state_of_the_mixed_path_tracks_its_fp64_state(monkeypatch):
+    """The mixed path stores its CG state vectors in FP32 (every operation on
+    them, the reductions, beta and the retraction compute in FP64); with
+    MLQ_STATE_F64=1 it keeps them in FP64.  Five iterations at 256^3 agree to
+    the FP32 rounding of the state: J to 1e-6, the same trial counts within
+    one evaluation."""
+    runs = {}
+    for flag in ("1", "0"):
+        monkeypatch.setenv("MLQ_STATE_F64", flag)
+        with mlq.MaxLq(256, 4.0, 1.0, precision="mixed", optim_tol=1e-14) as c:
+            c.state_load(c.seed_field(0, 2.0, 8.0))
+            _, st, rec = c.state_iterate(5)
+            R, lq = c.state_R()
+            runs[flag] = (rec, R, lq, st)
+    a, b = runs["1"], runs["0"]
+    assert a[3] == b[3] == 0
+    for ra, rb in zip(a[0], b[0]):
+        assert rb["J1"] == pytest.approx(ra["J1"], rel=1e-6)
+        assert abs(rb["n_evals"] - ra["n_evals"]) <= 1
+    assert rel(b[1], a[1]) < 1e-6 and b[2] == pytest.approx(a[2], rel=1e-6)
