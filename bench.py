@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true", help="skip the all-FP64 comparison path")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the summaries of the 64^3 (c1) and 32-instance (c4) configurations in the line")
     ap.add_argument("--profile-detail", action="store_true", help="key x-stage kernel times by fused functor")
     ap.add_argument("--config", default=None, choices=["c1", "c2", "c3", "c4", "c5"],
                     help="run one of the other workload configurations instead of the headline one")
@@ -753,6 +755,17 @@ def main():
                "c1_full_iteration_iters_per_s": cb["c1_full_iteration_iters_per_s"],
                "c1_composed_over_measured": cb["c1_composed_over_measured"], "calls_s": cb["calls_s"]}
 
+    # the small configurations, summarised in the same line (rank 0)
+    configs = None
+    if dist.rank == 0 and not args.no_configs:
+        configs = {}
+        c1 = config_c1(args)
+        configs["c1"] = {k: c1[k] for k in ("workload", "iterations", "status", "iters_per_s", "R_final",
+                                              "lq_norm_final", "max_abs_div_final")}
+        c4 = config_c4(args)
+        configs["c4"] = {k: c4[k] for k in ("workload", "iters_per_s_one_at_a_time", "iters_per_s_concurrent",
+                                              "speedup", "iterations", "identical_trajectories", "timing")}
+
     kcfg = mixed.kernel_config()
     per_kernel = {k: {"launches": v["launches"], "ms": round(v["ms"], 3),
                       "GB/s": round(v["bytes"] / max(v["ms"], 1e-9) / 1e6, 1)} for k, v in prof.items()}
@@ -771,7 +784,7 @@ def main():
                        "parallelism": f"replicas x{dist.world}",
                        "kernels": kcfg},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": res_m["launches"],
-            "clocks": clk, "wall_s_timed": res_m["wall_s"], "per_kernel": per_kernel,
+            "clocks": clk, "wall_s_timed": res_m["wall_s"], "per_kernel": per_kernel, "configs": configs,
         }
         print(json.dumps(line), flush=True)
     mixed.close()
