@@ -717,13 +717,15 @@ __global__ void spec_hilbert_leray_kernel(SpecGeom g, V* f, const double* __rest
                                           int do_leray) {
     const double twopi = 2.0 * 3.14159265358979311600;
     const int nrows = g.nb * g.nb;
-    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    // one warp per row (kx across the lanes), blockDim / 32 rows per block pass
+    const int lane = threadIdx.x & 31, rows_per = blockDim.x >> 5;
+    for (int r = blockIdx.x * rows_per + (threadIdx.x >> 5); r < nrows; r += gridDim.x * rows_per) {
         const SpecRow row(g, r);
         const long base = (long)r * g.nx;
         const double ky = twopi * (double)row.jy, kz = twopi * (double)row.jz;
         const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
         const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
-        for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
+        for (int fx = lane; fx < g.nx; fx += 32) {
             const long i = base + fx;
             double2 u0 = ldv(f, i), u1 = ldv(f, g.ncomp + i), u2 = ldv(f, 2 * g.ncomp + i);
             double s = scale;
@@ -749,14 +751,16 @@ __global__ void __launch_bounds__(128) spec_hilbert_leray_pair_dot_kernel(SpecGe
     const double twopi = 2.0 * 3.14159265358979311600;
     const int nrows = g.nb * g.nb;
     double acc[2] = {0.0, 0.0};
-    for (int r = blockIdx.x; r < nrows; r += gridDim.x) {
+    // one warp per row (kx across the lanes), blockDim / 32 rows per block pass
+    const int lane = threadIdx.x & 31, rows_per = blockDim.x >> 5;
+    for (int r = blockIdx.x * rows_per + (threadIdx.x >> 5); r < nrows; r += gridDim.x * rows_per) {
         const SpecRow row(g, r);
         const long base = (long)r * g.nx;
         const double ky = twopi * (double)row.jy, kz = twopi * (double)row.jz;
         const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
         const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
         const int jyz = row.jy * row.jy + row.jz * row.jz;
-        for (int fx = threadIdx.x; fx < g.nx; fx += blockDim.x) {
+        for (int fx = lane; fx < g.nx; fx += 32) {
             const long i = base + fx;
             double2 a0 = ldv(f1, i), a1 = ldv(f1, g.ncomp + i), a2 = ldv(f1, 2 * g.ncomp + i);
             double2 b0 = ldv(f2, i), b1 = ldv(f2, g.ncomp + i), b2 = ldv(f2, 2 * g.ncomp + i);
@@ -852,7 +856,10 @@ __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
                         stv((V*)a.ax_out, k, make_double2(x.x + a.ax_a * y.x, x.y + a.ax_a * y.y));
                     }
             }
-            for (int p = 0; p < a.npairs; ++p) {
+            // unrolled to the bound of 8 so that acc stays in registers
+#pragma unroll
+            for (int p = 0; p < 8; ++p) {
+                if (p >= a.npairs) break;
                 const SpecDotPair& q = a.pr[p];
                 if (q.kind == 3 || q.kind == 4) {
                     // 3: |K x a|^2 (vel2vort, function_ops.f90:2485-2495);
