@@ -357,6 +357,30 @@ void Engine<T>::tune_yz() {
               YShape<NN, T, 5>::valid || YShape<NN, T, 6>::valid || YShape<NN, T, 7>::valid;
     });
     if (!any) return;
+    if (const char* e = std::getenv("MLQ_YZ_VARIANTS")) {  // one fixed variant per pass kind (measurement runs)
+        std::vector<int> v;
+        for (const char* c = e; *c;) {
+            v.push_back(std::atoi(c));
+            while (*c && *c != ',') ++c;
+            if (*c == ',') ++c;
+        }
+        bool ok = (int)v.size() == YV_KINDS;
+        for (int k = 0; ok && k < YV_KINDS; ++k)
+            dispatch_n(n, [&](auto nc) {
+                constexpr int NN = decltype(nc)::value;
+                const int x = v[k];
+                ok = ok && (x == 0 || (x == 1 && YShape<NN, T, 1>::valid) || (x == 2 && YShape<NN, T, 2>::valid) ||
+                            (x == 3 && YShape<NN, T, 3>::valid) || (x == 4 && YShape<NN, T, 4>::valid) ||
+                            (x == 5 && YShape<NN, T, 5>::valid) || (x == 6 && YShape<NN, T, 6>::valid) ||
+                            (x == 7 && YShape<NN, T, 7>::valid) || (x == 8 && YShape<NN, T, 8>::valid) ||
+                            (x == 9 && YShape<NN, T, 9>::valid));
+            });
+        if (ok) {
+            for (int k = 0; k < YV_KINDS; ++k) yvar_[k] = v[k];
+            tune_report_ = std::string("fixed by MLQ_YZ_VARIANTS=") + e;
+            return;
+        }
+    }
     if (const char* e = std::getenv("MLQ_YZ_VARIANT")) {  // fixed variant (measurement runs)
         const int v = std::atoi(e);
         bool ok = v == 0;
