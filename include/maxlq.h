@@ -163,6 +163,19 @@ int mlq_dEnstrophydt(mlq_ctx* ctx, const double* u, double out[3]);
 /* calc_local_pointwise_dLqdt_inclParts (1224-1291): out is the (n,n,n,3)
  * field (R1 + R2 + R3, R1 + R2, R3) saved as "Ru" (maxdLpdt.f90:299) */
 int mlq_pointwise_R(mlq_ctx* ctx, const double* u, double* out);
+/* kappa_test_pert (function_ops.f90:615-977): the gradient check's
+ * perturbation phi_pert (n,n,n,3) of the reference's type name ("sine",
+ * "divfree-sine", "load-te0080", "load-random-a|b", "load-random-smooth-a|b",
+ * "load-k-random-a|b", "load-random-poly-a|b", "load-random-exp-a|b",
+ * "create-random-poly-b", "save-random"), full band, FP64 on the device.
+ * loaded: the field a load-* type reads from its netCDF file
+ * (mlq_ncdf_read_field), NULL when the file is missing: the field is then
+ * formed from zeros and MLQ_ERR_IO returned (the reference's
+ * successful = .false.).  The random fields come from a seeded generator
+ * (splitmix64 of seed and the element index) where the reference calls an
+ * unseeded random_number.  Unknown type: MLQ_ERR_BADARG. */
+int mlq_kappa_perturbation(mlq_ctx* ctx, const char* type, double m1, double m2, double m3, const double* loaded,
+                           unsigned long long seed, double* phi);
 
 /* ---- optimization.f90 ---------------------------------------------------- */
 int mlq_eval_J(mlq_ctx* ctx, const double* u, int mode, double* J);        /* 520-547 */

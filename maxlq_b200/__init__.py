@@ -348,6 +348,19 @@ class MaxLq:
         self._check(self._lib.mlq_pointwise_R(self._ctx, dptr(self._vec(u)), dptr(out)), "pointwise_R")
         return out
 
+    def kappa_test_pert(self, mytype: str, m1: float = 0.0, m2: float = 0.0, m3: float = 0.0, loaded=None,
+                        seed: int = 0):
+        """kappa_test_pert (function_ops.f90:615-977): (phi_pert, successful).
+        loaded: the field a load-* type reads from its file (None: no file,
+        phi formed from zeros and successful False)."""
+        out = np.zeros((3, self.n, self.n, self.n))
+        src = None if loaded is None else dptr(self._vec(loaded))
+        st = self._lib.mlq_kappa_perturbation(self._ctx, mytype.encode(), m1, m2, m3, src, seed, dptr(out))
+        if st == MLQ_ERR_IO:
+            return out, False
+        self._check(st, "kappa_test_pert")
+        return out, True
+
     def mnbrak(self, phi, grad, tA0: float, tB0: float):
         """Returns (tau_brack, myflag) like the Fortran function and its inout flag."""
         tb = np.zeros(2)

@@ -92,6 +92,8 @@ SIGNATURES = {
     "mlq_summed_enstrophy": (C.c_int, [_VP, _DP, _DP]),
     "mlq_dEnstrophydt": (C.c_int, [_VP, _DP, _DP]),
     "mlq_pointwise_R": (C.c_int, [_VP, _DP, _DP]),
+    "mlq_kappa_perturbation": (C.c_int, [_VP, C.c_char_p, C.c_double, C.c_double, C.c_double, _DP, C.c_ulonglong,
+                                         _DP]),
     "mlq_fft_bwdV": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_fwdr": (C.c_int, [_VP, _DP, _DP]),
     "mlq_fft_bwdr": (C.c_int, [_VP, _DP, _DP]),

@@ -18,10 +18,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libmaxlq_b200.so")
-SOURCES = ["engine.cu", "engine_f32.cu", "engine_f64.cu", "solver.cu", "capi.cu", "noalloc.cu", "diag.cu", "ncdf.cpp",
-           "kappa.cpp"]
+SOURCES = ["engine.cu", "engine_f32.cu", "engine_f64.cu", "solver.cu", "capi.cu", "noalloc.cu", "diag.cu", "lsdev.cu",
+           "ncdf.cpp", "kappa.cpp"]
 HEADERS = ["common.cuh", "fft.cuh", "kernels.cuh", "functors.cuh", "regfft.cuh", "cfft.cuh", "engine.cuh",
-           "engine_common.cuh", "engine_impl.cuh", "solver.cuh"]
+           "engine_common.cuh", "engine_impl.cuh", "solver.cuh", "linesearch.cuh"]
+# the device line search rounds every step as the host search does
+EXTRA_FLAGS = {"lsdev.cu": ["-fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -60,7 +62,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
-        cmds.append(common + ["-c", os.path.join(CSRC, src), "-o", obj])
+        cmds.append(common + EXTRA_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
     # translation units compile in parallel; output of each kept together
     with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:

@@ -235,6 +235,12 @@ int mlq_dEnstrophydt(mlq_ctx* c, const double* u, double out[3]) {
 int mlq_pointwise_R(mlq_ctx* c, const double* u, double* out) {
     return guard(c, [&] { c->solver->pointwise_R_host(u, out); });
 }
+int mlq_kappa_perturbation(mlq_ctx* c, const char* type, double m1, double m2, double m3, const double* loaded,
+                           unsigned long long seed, double* phi) {
+    int st = 0;
+    const int r = guard(c, [&] { st = fft64(c).kappa_pert(type, m1, m2, m3, loaded, seed, phi); });
+    return r != MLQ_OK ? r : (st ? MLQ_ERR_IO : MLQ_OK);
+}
 
 int mlq_fft_fwdV(mlq_ctx* c, const double* u, double* fu) {
     return guard(c, [&] {

@@ -372,6 +372,56 @@ void EngineBase::direction(SVec* gv, double sg, SVec* d, double beta, const SVec
     launched("spec_lincomb", (double)sv_elem() * nt * (3 + (td ? 1 : 0)), ev);
 }
 
+// ---- spectral inner products ----
+using DotLaunch = void (*)(int, cudaStream_t, const SpecDotArgs&);
+template <class K>
+static int dot_resident(K kernel) {
+    int per_sm = 0, dev = 0, sms = 0;
+    MLQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, RED_THREADS, 0));
+    MLQ_CUDA(cudaGetDevice(&dev));
+    MLQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    return std::max(1, per_sm) * sms;
+}
+template <typename V>
+static void launch_dot_generic(int grid, cudaStream_t s, const SpecDotArgs& a) {
+    spec_dot_kernel<V><<<grid, RED_THREADS, 0, s>>>(a);
+}
+template <typename V, int NV, int NP, unsigned long long PAT>
+static void launch_dot_fixed(int grid, cudaStream_t s, const SpecDotArgs& a) {
+    spec_dot_fixed_kernel<V, NV, NP, PAT><<<grid, RED_THREADS, 0, s>>>(a);
+}
+// operand pattern of pair p: vector indices ia, ib
+constexpr unsigned long long dot_pp(int p, int ia, int ib) {
+    return (unsigned long long)(ia | (ib << 3)) << (6 * p);
+}
+constexpr unsigned long long dot_ax(int xi, int yi) {
+    return ((unsigned long long)xi << 48) | ((unsigned long long)yi << 51);
+}
+struct DotVariant {
+    int nv, np;
+    unsigned long long pat;
+    DotLaunch fn[2];  // FP32, FP64 state
+    int resident[2];
+};
+template <int NV, int NP, unsigned long long PAT>
+static DotVariant dot_variant() {
+    return {NV,
+            NP,
+            PAT,
+            {launch_dot_fixed<float2, NV, NP, PAT>, launch_dot_fixed<double2, NV, NP, PAT>},
+            {dot_resident(spec_dot_fixed_kernel<float2, NV, NP, PAT>),
+             dot_resident(spec_dot_fixed_kernel<double2, NV, NP, PAT>)}};
+}
+// The operand patterns the programs use, each with its own kernel:
+//   the CG update (g <- g - alpha c, then <g,c>_H, |div g|^2, <g,g>_H, <u,u>_H,
+//     <g,Tg0>_H, <g0,g0>_H, <g,Td0>_H, <Td0,Td0>_H over c, u, Tg0, g0, Td0, g);
+//   the transport's two products <c, g>, <c, d>; one pair of a vector with
+//   itself or with another.
+constexpr unsigned long long DOT_CG = dot_pp(0, 5, 0) | dot_pp(1, 5, 5) | dot_pp(2, 5, 5) | dot_pp(3, 1, 1) |
+                                      dot_pp(4, 5, 2) | dot_pp(5, 3, 3) | dot_pp(6, 5, 4) | dot_pp(7, 4, 4) |
+                                      dot_ax(5, 0);
+constexpr unsigned long long DOT_TRANSPORT = dot_pp(0, 0, 1) | dot_pp(1, 0, 2);
+
 void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, SVec* ax_out, const SVec* ax_x, double ax_a,
                       const SVec* ax_y) {
     if (np < 1 || np > 8) throw CudaError("dots: 1 to 8 pairs per call", MLQ_ERR_BADARG);
@@ -389,36 +439,67 @@ void EngineBase::dots(const SpecDotPair* pairs, int np, double* out, SVec* ax_ou
     bool need_h = false;
     for (int i = 0; i < np; ++i) need_h |= pairs[i].kind == 1;
     a.hwtab = need_h ? hweight_table(1.5 - 1.0 / P.q) : nullptr;  // (3/2)-(1/q), function_ops.f90:3467
+    // the distinct vectors (update operands first, ax_out moved last) and
+    // the operand pattern over them
+    std::vector<const void*> order;
+    auto add = [&](const void* p) {
+        if (std::find(order.begin(), order.end(), p) == order.end()) order.push_back(p);
+    };
+    if (ax_out) {
+        add(ax_x);
+        add(ax_y);
+    }
+    for (int i = 0; i < np; ++i) {
+        add(pairs[i].a);
+        if (pairs[i].kind < 2) add(pairs[i].b);
+    }
+    if (ax_out) {
+        const auto it = std::find(order.begin(), order.end(), (const void*)ax_out);
+        if (it != order.end()) {
+            order.erase(it);
+            order.push_back(ax_out);
+            a.ax_last = 1;
+        }
+    }
+    auto slot = [&](const void* p) { return (int)(std::find(order.begin(), order.end(), p) - order.begin()); };
+    const int nv = (int)order.size();
+    unsigned long long pat = 0;
+    for (int i = 0; i < np; ++i) {
+        const int ia = slot(pairs[i].a);
+        pat |= dot_pp(i, ia, pairs[i].kind < 2 ? slot(pairs[i].b) : ia);
+    }
+    if (ax_out) pat |= dot_ax(slot(ax_x), slot(ax_y));
+    for (int v = 0; v < nv && v < 8; ++v) a.vec[v] = order[v];
     // as many blocks as are resident at once: the reduction is latency-bound
     // (thread-safe one-time initialisation; every device here is a B200)
-    static const int resident = [] {
-        int per_sm = 0, dev = 0, sms = 0;
-        MLQ_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spec_dot_kernel<double2>, RED_THREADS, 0));
-        MLQ_CUDA(cudaGetDevice(&dev));
-        MLQ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        return std::max(1, per_sm) * sms;
+    struct Table {
+        std::vector<DotVariant> fixed;
+        DotLaunch generic[2];
+        int generic_resident[2];
+    };
+    static const Table tab = [] {
+        Table t;
+        t.fixed = {dot_variant<6, 8, DOT_CG>(), dot_variant<3, 2, DOT_TRANSPORT>(), dot_variant<1, 1, 0>(),
+                   dot_variant<2, 1, dot_pp(0, 0, 1)>()};
+        t.generic[0] = launch_dot_generic<float2>;
+        t.generic[1] = launch_dot_generic<double2>;
+        t.generic_resident[0] = dot_resident(spec_dot_kernel<float2>);
+        t.generic_resident[1] = dot_resident(spec_dot_kernel<double2>);
+        return t;
     }();
-    const int grid = grid_for(a.g.ncomp, RED_THREADS, resident);
+    const int w = state32_ ? 0 : 1;
+    const DotVariant* fv = nullptr;
+    for (const DotVariant& d : tab.fixed)
+        if (d.nv == nv && d.np == np && d.pat == pat) fv = &d;
+    const int grid = grid_for(a.g.ncomp, RED_THREADS, fv ? fv->resident[w] : tab.generic_resident[w]);
     ensure_partials((long)grid * 8);
     a.partials = d_partials;
     cudaEvent_t ev = prof_mark();
-    if (state32_)
-        spec_dot_kernel<float2><<<grid, RED_THREADS, 0, stream>>>(a);
-    else
-        spec_dot_kernel<double2><<<grid, RED_THREADS, 0, stream>>>(a);
-    {
-        std::set<const void*> uniq;
-        for (int i = 0; i < np; ++i) {
-            uniq.insert(pairs[i].a);
-            if (pairs[i].kind < 2) uniq.insert(pairs[i].b);
-        }
-        if (ax_out) {  // x, y read, ax_out written (and read back from cache by the pairs)
-            uniq.erase(ax_out);
-            uniq.insert(ax_x);
-            uniq.insert(ax_y);
-        }
-        launched("spec_dot", 3.0 * sv_elem() * a.g.ncomp * (uniq.size() + (ax_out ? 1 : 0)), ev);
-    }
+    (fv ? fv->fn[w] : tab.generic[w])(grid, stream, a);
+    // vectors read (ax_out only when it is an update operand) and written
+    const bool out_read = ax_out && (ax_out == ax_x || ax_out == ax_y);
+    const int nread = nv - ((a.ax_last && !out_read) ? 1 : 0);
+    launched("spec_dot", 3.0 * sv_elem() * a.g.ncomp * (nread + (ax_out ? 1 : 0)), ev);
     finalize(grid, 8, 1.0, 200);
     fetch_results();
     for (int i = 0; i < np; ++i) out[i] = h_results[200 + i];

@@ -18,8 +18,17 @@
 #include "kernels.cuh"
 #include "regfft.cuh"
 #include "cfft.cuh"
+#include "linesearch.cuh"
 
 namespace mlq {
+
+// launchers of the device line search's kernels (lsdev.cu)
+void ls_launch_coef(LsDevState* s, const double* results, const double* partials, int nblocks, cudaStream_t st);
+void ls_launch_ctrl(LsDevState* s, cudaGraphConditionalHandle h_loop, cudaGraphConditionalHandle h_chk,
+                    cudaStream_t st);
+void ls_launch_check(LsDevState* s, const double* partials, int nblocks, cudaGraphConditionalHandle h_fft,
+                     cudaStream_t st);
+void ls_launch_fft(LsDevState* s, const double* r, cudaStream_t st);
 
 // A state vector: three components of nb*nb*nx Fourier coefficients of band
 // b2, stored as double2 (FP64 path) or float2 (the mixed path's FP32 state);
@@ -420,14 +429,46 @@ class Engine : public EngineBase {
     bool ls_ok() const { return !use_e_u && P.q == 4.0; }
     void ls_setup(const SVec* u, const SVec* d);
     void ls_trial(double tau, double out[3], double* lqq);
-    double ls_r2_[5] = {0}, ls_r3_[6] = {0};
     // Where S(tau) = S0 + tau S1 + tau^2 S2 (the dealiased |phi|^2) is >= 0 at
     // every point, the clamp of calc_uk is inactive and P2(g^2) = S(tau): a
-    // trial in [ls_tlo_, ls_thi_] is then a polynomial in tau of the Parseval
-    // products <S_i, X_a> (X_a: coefficients of P2|grad phi|^2) and <S_i, S_j>.
-    double ls_tlo_ = 0.0, ls_thi_ = 0.0;
-    double ls_sx_[3][3] = {{0}}, ls_ss_[3][3] = {{0}};
+    // trial in [ls_c_.tlo, ls_c_.thi] is then a polynomial in tau of the
+    // Parseval products <S_i, X_a> (X_a: coefficients of P2|grad phi|^2) and
+    // <S_i, S_j>.
+    LsPoly ls_c_{};
+    bool ls_host_poly_ = true;  // ls_c_ holds this line search's coefficients
+    void ls_poly_to_host();     // copies them from the device search's state
     long long ls_poly_trials_ = 0, ls_fft_trials_ = 0;
+
+    // ---- the line search on the device ----
+    // The setup leaves the coefficients in d_ls_ only (ls_dev_), and the
+    // search runs as one CUDA graph: a conditional loop around the controller
+    // kernel, which replays mnbrak and Brent over the trial values found so
+    // far and stops at the first tau it has none for; inside the loop a
+    // conditional check of S(tau) >= 0 at that tau and, where it fails, a
+    // conditional transform trial.  The host reads the outcome once.
+    // MLQ_DEVICE_LS=0 keeps the search on the host.
+    bool ls_dev_on_ = true;
+    // MLQ_LS_TRANSFORM_TRIALS=1: every trial by a transform, on host and
+    // device alike (the polynomial shortcut off; for tests of that branch)
+    bool ls_transform_trials_ = false;
+    bool ls_dev_ = false;
+    LsDevState* d_ls_ = nullptr;
+    void* h_ls_ = nullptr;  // pinned: LsParams, LsOut, LsPoly
+    struct LsGraph {
+        cudaGraphExec_t exec = nullptr;
+        long gen = -1;
+        int key = -1;
+        long long nfwd = 0;  // launches of one transform trial
+    };
+    LsGraph lsg_[2];
+    bool lsg_failed_ = false;
+    long long ls_dev_searches_ = 0, ls_dev_loops_ = 0;
+    double ls_free_tau_ = 0.0;  // the last device search's tau1 and whether
+    int ls_free_val_ = -1;      // S(tau1) >= 0 everywhere (-1: none)
+    bool ls_device_ready() const { return ls_dev_on_ && graphs_on_ && !slab_ && !lsg_failed_; }
+    // 0: the search ran (out filled); 1: not available, search on the host
+    int ls_device_search(double B, double tA0, double tB0, LsOut* out);
+    bool ls_graph_build(LsGraph& g, int key);
 
     // ---- state <-> host ----
     // Forward transform of a host FP64 vector field into state spectra.
@@ -450,6 +491,11 @@ class Engine : public EngineBase {
     void divergence_full(const double* u, double* div);
     void laplacian_full(double* u);
     void poisson_full(const double* f, double l, double* phi);
+    // kappa_test_pert (function_ops.f90:615-977): the gradient-check
+    // perturbations, full band; returns 0, or 1 for a load-* type without
+    // its field (formed from zeros: the reference's successful = .false.)
+    int kappa_pert(const char* type, double m1, double m2, double m3, const double* loaded, unsigned long long seed,
+                   double* out);
     void widen_to(const Band& b);
 
     SVec* c_tmp_ = nullptr;  // FP64 spectra of P2(|w|^{q-2} w) for the transport

@@ -32,6 +32,8 @@ Engine<T>::Engine(const mlq_params& p) : EngineBase(p) {
     // coefficients) in FP32; the operations on it compute in FP64
     state32_ = sizeof(T) == 4;
     if (const char* e = std::getenv("MLQ_STATE_F64")) state32_ = state32_ && std::string(e) != "1";
+    if (const char* e = std::getenv("MLQ_DEVICE_LS")) ls_dev_on_ = std::string(e) != "0";
+    if (const char* e = std::getenv("MLQ_LS_TRANSFORM_TRIALS")) ls_transform_trials_ = std::string(e) == "1";
     {
         int dev = 0;
         MLQ_CUDA(cudaGetDevice(&dev));
@@ -335,6 +337,8 @@ std::string Engine<T>::kernel_config() const {
                     ", \"graph_replays\": " + std::to_string(graph_launches_) +
                     ", \"line_search_trials_polynomial\": " + std::to_string(ls_poly_trials_) +
                     ", \"line_search_trials_transform\": " + std::to_string(ls_fft_trials_) +
+                    ", \"line_searches_on_device\": " + std::to_string(ls_dev_searches_) +
+                    ", \"line_search_device_passes\": " + std::to_string(ls_dev_loops_) +
                     ", \"device_bytes_peak\": " + std::to_string(bytes_peak) +
                     ", \"yz_variants\": \"" + (tune_report_.empty() ? std::string("default") : tune_report_) + "\"}";
     return r;
@@ -809,6 +813,9 @@ void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
 template <typename T>
 Engine<T>::~Engine() {
     if (h_stage_) cudaFreeHost(h_stage_);
+    for (LsGraph& g : lsg_)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (h_ls_) cudaFreeHost(h_ls_);
 }
 
 template <typename T>
@@ -2352,8 +2359,8 @@ __global__ void __launch_bounds__(RED_THREADS)
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS)
     ls_min_kernel(const T* __restrict__ s0, const T* __restrict__ s1, const T* __restrict__ s2, long npts, double tau,
-                  double* __restrict__ out) {
-    const T t = (T)tau;
+                  const double* __restrict__ taup, double* __restrict__ out) {
+    const T t = (T)(taup ? *taup : tau);
     T m = T(1e30);
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long)gridDim.x * blockDim.x)
         m = fmin(m, s0[i] + t * (s1[i] + t * s2[i]));
@@ -2371,6 +2378,12 @@ __global__ void __launch_bounds__(RED_THREADS)
 template <typename T>
 void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
     const long nc = spec_ncomp();
+    ls_free_val_ = -1;
+    ls_dev_ = ls_device_ready();
+    if (ls_dev_ && !d_ls_) {
+        d_ls_ = (LsDevState*)dev_alloc(sizeof(LsDevState));
+        MLQ_CUDA(cudaMallocHost(&h_ls_, 1024));
+    }
     // u and grad u are still in PU, PD when the gradient program of this
     // iteration transformed the same spectrum
     const bool reuse_u = !slab_ && reuse_on_ && pu_of_ == (const void*)u;
@@ -2471,20 +2484,11 @@ void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
     for (int a = 0; a < 3; ++a) rin.push_back(LP + a);
     for (int i = 0; i < 6; ++i) rin.push_back(ud[i]);
     pointwise(FLSRed{}, rin, {}, 100);
-    fetch_results();
+    if (!ls_dev_) fetch_results();
     if (slab_) {  // the trials read only S_a
         release_slots(LU, LS);
         release_slots(LV, LP + 3);
     }
-    const double* r = h_results + 100;
-    const double M[3][3] = {{r[0], r[1], r[2]}, {r[1], r[3], r[4]}, {r[2], r[4], r[5]}};
-    for (int k = 0; k < 5; ++k) ls_r2_[k] = 0.0;
-    for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b) ls_r2_[a + b] += M[a][b];
-    for (int k = 0; k < 6; ++k) ls_r3_[k] = 0.0;
-    for (int a = 0; a < 3; ++a)
-        for (int cc = 0; cc < 2; ++cc)
-            for (int b = 0; b < 3; ++b) ls_r3_[a + cc + b] += r[6 + 3 * (2 * a + cc) + b];
     // Parseval products for the transform-free trials
     {
         std::vector<std::pair<const cpx<T>*, const cpx<T>*>> p1, p2, p3;
@@ -2498,12 +2502,24 @@ void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
         sdots(*this, p3, 152);
     }
     // the interval of tau around 0 on which S(tau) >= 0 everywhere
+    if (ls_dev_) {
+        // on the device, with the coefficients: no host round trip
+        const int grid = grid_for(n3, RED_THREADS, 148 * 4);
+        ensure_partials((long)grid * 2);
+        ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(phys(ls_phys(0)), phys(ls_phys(1)),
+                                                                phys(ls_phys(2)), n3, d_partials);
+        launched();
+        ls_launch_coef(d_ls_, d_results, d_partials, grid, stream);
+        launched();
+        ls_host_poly_ = false;
+        return;
+    }
+    double lo = -1e300, hi = 1e300;
     {
         const long npts = slab_ ? (long)zs_ * n * n : n3;
         const int grid = grid_for(npts, RED_THREADS, 148 * 4);
         ensure_partials((long)grid * 2);
         std::vector<double> h((size_t)grid * 2);
-        double lo = -1e300, hi = 1e300;
         for (int z0 = 0; z0 < n; z0 += (slab_ ? zs_ : n)) {
             const T* s[3];
             if (slab_) {
@@ -2521,28 +2537,198 @@ void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
                 hi = std::min(hi, h[2 * g + 1]);
             }
         }
-        // stay clear of the ends, where the T-precision trial may round either way
-        ls_tlo_ = lo <= 0.0 ? lo * (1.0 - 1e-6) : 1.0;
-        ls_thi_ = hi >= 0.0 ? hi * (1.0 - 1e-6) : -1.0;
     }
     fetch_results();
-    {
-        const double* q1 = h_results + 140;
-        int k = 0;
-        for (int i = 0; i < 3; ++i)
-            for (int a = 0; a < 3; ++a) ls_sx_[i][a] = q1[k++];  // slots 140..148 (146.. holds i = 2)
-        const double* q2 = h_results + 149;
-        k = 0;
-        for (int i = 0; i < 3; ++i)
-            for (int j = i; j < 3; ++j) {
-                ls_ss_[i][j] = ls_ss_[j][i] = q2[k++];
-            }
+    // <S_i, G_a> in slots 140..148 (146.. holds i = 2), <S_i, S_j> in 149..154
+    ls_assemble(h_results + 100, h_results + 140, h_results + 149, lo, hi, ls_c_);
+    ls_host_poly_ = true;
+}
+
+template <typename T>
+void Engine<T>::ls_poly_to_host() {
+    if (ls_host_poly_) return;
+    LsPoly* hp = (LsPoly*)((char*)h_ls_ + 512);
+    MLQ_CUDA(cudaMemcpyAsync(hp, &d_ls_->poly, sizeof(LsPoly), cudaMemcpyDeviceToHost, stream));
+    MLQ_CUDA(cudaStreamSynchronize(stream));
+    ls_c_ = *hp;
+    ls_host_poly_ = true;
+}
+
+// the only node of a captured sequence without successors
+static cudaGraphNode_t graph_leaf(cudaGraph_t g) {
+    size_t nn = 0;
+    MLQ_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+    std::vector<cudaGraphNode_t> nodes(nn);
+    MLQ_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+    cudaGraphNode_t leaf = nullptr;
+    int nleaf = 0;
+    for (cudaGraphNode_t x : nodes) {
+        size_t nd = 0;
+        MLQ_CUDA(cudaGraphNodeGetDependentNodes(x, nullptr, &nd));
+        if (nd == 0) {
+            leaf = x;
+            ++nleaf;
+        }
     }
+    if (nleaf != 1) throw CudaError("line-search graph: captured sequence is not a chain", MLQ_ERR_CUDA);
+    return leaf;
+}
+
+// an If (or While) node after dep (or at the root) of g; returns its body
+static cudaGraph_t add_conditional(cudaGraph_t g, cudaGraphNode_t dep, cudaGraphConditionalHandle h,
+                                   cudaGraphConditionalNodeType type) {
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = type;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    MLQ_CUDA(cudaGraphAddNode(&node, g, dep ? &dep : nullptr, dep ? 1 : 0, &np));
+    return np.conditional.phGraph_out[0];
+}
+
+// The device search as one graph:
+//   while (h_loop) { ctrl; if (h_chk) { ls_min; check; if (h_fft) { transform trial; fft } } }
+// Each conditional handle is set by a kernel of the graph that holds its node
+// (the loop's by the controller in its body).  The controller ends the loop
+// after LS_MAX_LOOPS passes, so the loop is bounded whatever the kernels see.
+template <typename T>
+bool Engine<T>::ls_graph_build(LsGraph& g, int key) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+    const int grid = grid_for(n3, RED_THREADS, 148 * 4);
+    ensure_partials((long)grid * 2);
+    FwdOut o;
+    o.red_self = 0;
+    for (int a = 0; a < 3; ++a) {
+        o.red_with[a] = wspec(WLG + a);
+        o.red_with_f64[a] = wf64<T>();
+        o.red_with_slot[a] = 1 + a;
+    }
+    const std::vector<int> in = {ls_phys(0), ls_phys(1), ls_phys(2)};
+    const bool prof_was = prof_on;
+    prof_on = false;
+    // one transform trial run directly, so that the buffers it allocates on
+    // first use exist before the capture (its sums land in unused slots)
+    FLSA f0;
+    f0.tau = 0.0;
+    const long long l0 = launches;
+    bool ok = true;
+    try {
+        fwd(b2, f0, in, {o}, 130);
+    } catch (...) {
+        ok = false;
+    }
+    const long long nfwd = launches - l0;
+    cudaGraph_t G = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    auto capture_into = [&](cudaGraph_t body, auto&& fn) {
+        MLQ_CUDA(cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        bool fine = true;
+        try {
+            fn();
+        } catch (...) {
+            fine = false;
+        }
+        cudaGraph_t got = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(stream, &got);
+        if (!fine || e != cudaSuccess || got != body)
+            throw CudaError("line-search graph: capture failed", MLQ_ERR_CUDA);
+    };
+    if (ok) try {
+            MLQ_CUDA(cudaGraphCreate(&G, 0));
+            cudaGraphConditionalHandle h_loop, h_chk, h_fft;
+            MLQ_CUDA(cudaGraphConditionalHandleCreate(&h_loop, G, 1, cudaGraphCondAssignDefault));
+            cudaGraph_t body_loop = add_conditional(G, nullptr, h_loop, cudaGraphCondTypeWhile);
+            MLQ_CUDA(cudaGraphConditionalHandleCreate(&h_chk, body_loop, 0, cudaGraphCondAssignDefault));
+            capture_into(body_loop, [&] { ls_launch_ctrl(d_ls_, h_loop, h_chk, stream); });
+            cudaGraph_t body_chk = add_conditional(body_loop, graph_leaf(body_loop), h_chk, cudaGraphCondTypeIf);
+            MLQ_CUDA(cudaGraphConditionalHandleCreate(&h_fft, body_chk, 0, cudaGraphCondAssignDefault));
+            capture_into(body_chk, [&] {
+                ls_min_kernel<T><<<grid, RED_THREADS, 0, stream>>>(phys(in[0]), phys(in[1]), phys(in[2]), n3, 0.0,
+                                                                   &d_ls_->ptau, d_partials);
+                ls_launch_check(d_ls_, d_partials, grid, h_fft, stream);
+            });
+            cudaGraph_t body_fft = add_conditional(body_chk, graph_leaf(body_chk), h_fft, cudaGraphCondTypeIf);
+            capture_into(body_fft, [&] {
+                FLSA f;
+                f.tau = 0.0;
+                f.taup = &d_ls_->ptau;
+                fwd(b2, f, in, {o}, 130);
+                ls_launch_fft(d_ls_, d_results + 130, stream);
+            });
+            MLQ_CUDA(cudaGraphInstantiate(&exec, G, 0));
+        } catch (...) {
+            ok = false;
+        }
+    if (G) cudaGraphDestroy(G);
+    cudaGetLastError();
+    launches = l0 + nfwd;  // captured launches did not run
+    prof_on = prof_was;
+    if (!ok) {
+        if (exec) cudaGraphExecDestroy(exec);
+        return false;
+    }
+    g.exec = exec;
+    g.gen = graph_gen_;
+    g.key = key;
+    g.nfwd = nfwd;
+    return true;
+}
+
+template <typename T>
+int Engine<T>::ls_device_search(double B, double tA0, double tB0, LsOut* out) {
+    if (!ls_dev_) return 1;
+    const int key = ls_phys(0);
+    LsGraph* g = nullptr;
+    for (LsGraph& x : lsg_)
+        if (x.exec && x.key == key && x.gen == graph_gen_) g = &x;
+    if (!g) {
+        g = &lsg_[0];
+        for (LsGraph& x : lsg_)
+            if (!x.exec || x.gen != graph_gen_) {
+                g = &x;
+                break;
+            }
+        if (!ls_graph_build(*g, key)) {
+            lsg_failed_ = true;
+            return 1;
+        }
+    }
+    char* h = (char*)h_ls_;
+    LsParams* hp = (LsParams*)h;
+    *hp = LsParams{P.q, P.visc_coef * P.visc, P.press_coef, B, tA0, tB0, ls_transform_trials_ ? 1 : 0};
+    MLQ_CUDA(cudaMemcpyAsync(&d_ls_->par, hp, sizeof(LsParams), cudaMemcpyHostToDevice, stream));
+    cudaEvent_t ev = prof_mark();
+    MLQ_CUDA(cudaGraphLaunch(g->exec, stream));
+    launched("line_search", 0.0, ev);
+    LsOut* ho = (LsOut*)(h + 256);
+    LsPoly* hpoly = (LsPoly*)(h + 512);
+    MLQ_CUDA(cudaMemcpyAsync(ho, &d_ls_->out, sizeof(LsOut), cudaMemcpyDeviceToHost, stream));
+    MLQ_CUDA(cudaMemcpyAsync(hpoly, &d_ls_->poly, sizeof(LsPoly), cudaMemcpyDeviceToHost, stream));
+    fetch_results();  // the transform trials' NaN flag
+    ls_c_ = *hpoly;
+    ls_host_poly_ = true;
+    *out = *ho;
+    // the graph's kernels (one launch counted above)
+    launches += out->loops + 2LL * out->checks + out->nfft * (g->nfwd + 1) - 1;
+    ++ls_dev_searches_;
+    ls_dev_loops_ += out->loops;
+    ls_poly_trials_ += out->npoly;
+    ls_fft_trials_ += out->nfft;
+    if (out->status == 0 && out->mflag == 0) {
+        ls_free_tau_ = out->tau1;
+        ls_free_val_ = out->fft1 ? 0 : 1;
+    }
+    return 0;
 }
 
 template <typename T>
 bool Engine<T>::ls_clamp_free(double tau) {
-    bool clamp_off = tau >= ls_tlo_ && tau <= ls_thi_;
+    if (ls_free_val_ >= 0 && tau == ls_free_tau_) return ls_free_val_ != 0;  // decided by the device search
+    if (ls_transform_trials_) return false;
+    ls_poly_to_host();
+    bool clamp_off = tau >= ls_c_.tlo && tau <= ls_c_.thi;
     if (!clamp_off) {
         // outside the interval: one read of S_0..2 decides for this tau
         const long npts = slab_ ? (long)zs_ * n * n : n3;
@@ -2559,7 +2745,7 @@ bool Engine<T>::ls_clamp_free(double tau) {
                 for (int a = 0; a < 3; ++a) sp[a] = phys(ls_phys(a));
             }
             cudaEvent_t ev = prof_mark();
-            ls_min_kernel<T><<<grid, RED_THREADS, 0, stream>>>(sp[0], sp[1], sp[2], npts, tau, d_partials);
+            ls_min_kernel<T><<<grid, RED_THREADS, 0, stream>>>(sp[0], sp[1], sp[2], npts, tau, nullptr, d_partials);
             launched("ls_min", 3.0 * npts * sizeof(T), ev);
             MLQ_CUDA(cudaMemcpyAsync(h.data(), d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
             MLQ_CUDA(cudaStreamSynchronize(stream));
@@ -2573,24 +2759,12 @@ bool Engine<T>::ls_clamp_free(double tau) {
 template <typename T>
 void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
     const double q = P.q, cv = P.visc_coef * P.visc, cp = P.press_coef;
+    double l = 0.0;
     if (ls_clamp_free(tau)) {
         // S(tau) >= 0 everywhere: P2(g^2) = S(tau), every product is a polynomial
         ++ls_poly_trials_;
-        const double tp[5] = {1.0, tau, tau * tau, tau * tau * tau, tau * tau * tau * tau};
-        double ra[3] = {0, 0, 0}, r0 = 0.0;
-        for (int i = 0; i < 3; ++i)
-            for (int a = 0; a < 3; ++a) ra[a] += tp[i] * ls_sx_[i][a];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) r0 += tp[i + j] * ls_ss_[i][j];
-        const double I1 = ra[0] + tau * (ra[1] + tau * ra[2]);
-        double I2 = 0.0, I3 = 0.0;
-        for (int k = 4; k >= 0; --k) I2 = I2 * tau + ls_r2_[k];
-        for (int k = 5; k >= 0; --k) I3 = I3 * tau + ls_r3_[k];
-        const double R1 = -cv * I1, R2 = -cv * (q - 2.0) * I2, R3 = cp * (q - 2.0) * I3;
-        out[0] = R1 + R2 + R3;
-        out[1] = R1 + R2;
-        out[2] = R3;
-        if (lqq) *lqq = r0;
+        ls_poly_R(ls_c_, q, cv, cp, tau, out, &l);
+        if (lqq) *lqq = l;
         return;
     }
     ++ls_fft_trials_;
@@ -2607,18 +2781,8 @@ void Engine<T>::ls_trial(double tau, double out[3], double* lqq) {
     f.tau = tau;
     fwd(b2, f, {ls_phys(0), ls_phys(1), ls_phys(2)}, {o}, 130);
     fetch_results();
-    const double* r = h_results + 130;
-    const double I1 = r[1] + tau * (r[2] + tau * r[3]);
-    double I2 = 0.0, I3 = 0.0;
-    for (int k = 4; k >= 0; --k) I2 = I2 * tau + ls_r2_[k];
-    for (int k = 5; k >= 0; --k) I3 = I3 * tau + ls_r3_[k];
-    const double R1 = -cv * I1;                 // -nu <|u|^2, P2 |grad u|^2>  (1318)
-    const double R2 = -cv * (q - 2.0) * I2;     // -(q-2) nu <1, P2 sum_j V_j^2> (1333)
-    const double R3 = cp * (q - 2.0) * I3;      // (q-2) <p, u.V>  (1352)
-    out[0] = R1 + R2 + R3;
-    out[1] = R1 + R2;
-    out[2] = R3;
-    if (lqq) *lqq = r[0];
+    ls_fft_R(ls_c_, q, cv, cp, h_results + 130, tau, out, &l);
+    if (lqq) *lqq = l;
 }
 
 // ----------------------------------------------------------------------------
@@ -3037,6 +3201,217 @@ void Engine<T>::poisson_full(const double* f, double l, double* phi) {
     inv(full, {o});
     store_scalar_phys(PIO2, phi);
     free_dev(sp);
+}
+
+// ---- kappa_test_pert (function_ops.f90:615-977) ---------------------------
+// The random fields of create-random-poly-b and save-random come from a
+// seeded counter generator (the reference draws them from an unseeded
+// random_number, 784-785): element i of phi_pert(x,y,z,c) is
+// 2 U(seed, i) - 1, U the top 53 bits of the splitmix64 finaliser of
+// seed + (i + 1) * 0x9E3779B97F4A7C15.
+__device__ __forceinline__ double pert_uniform(unsigned long long seed, long i) {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+template <typename T>
+__global__ void pert_random_kernel(long n3, unsigned long long seed, T* u0, T* u1, T* u2) {
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < 3 * n3; i += (long)gridDim.x * blockDim.x) {
+        const int c = (int)(i / n3);
+        T* u = c == 0 ? u0 : (c == 1 ? u1 : u2);
+        u[i - (long)c * n3] = (T)(2.0 * pert_uniform(seed, i) - 1.0);
+    }
+}
+
+// "sine" / "divfree-sine" (658-688): m2 is m1 + m3 for the latter
+template <typename T>
+__global__ void pert_sine_kernel(int n, double m1, double m2, double m3, T* u0, T* u1, T* u2) {
+    const long n3 = (long)n * n * n;
+    const double PI = 3.14159265358979311600;  // 4 atan2(1, 1)
+    const double dx = 1.0 / (double)n;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long)gridDim.x * blockDim.x) {
+        const int x = (int)(i % n), y = (int)((i / n) % n), z = (int)(i / ((long)n * n));
+        const double X = (double)x * dx, Y = (double)y * dx, Z = (double)z * dx;
+        const double a = 2.0 * PI * m1 * X, b = 2.0 * PI * m2 * Y, c = 2.0 * PI * m3 * Z;
+        u0[i] = (T)(sin(a) * cos(b) * cos(c));
+        u1[i] = (T)(-cos(a) * sin(b) * cos(c));
+        u2[i] = (T)(cos(a) * cos(b) * sin(c));
+    }
+}
+
+// One spectral pass over the three full-band spectra of a perturbation:
+// times scale * f(|K|) (0 at |K| < MACH_EPSILON) when filter > 0 -- 1: m1
+// (load-k-random), 2: 10^m2 (|K| / (N/4))^m1 (poly), 3: 10^(-|K|/5) (exp),
+// 4: 1 (the k = 0 mode removed) -- then, when leray, divAvg_free
+// (2843-2918): u - K_odd (K_odd . u) / |K|^2 with the mean removed (the
+// divergence and the gradient each pass through REAL(c2c), which cancels a
+// Nyquist index's odd factor; |K|^2 keeps it).
+static __global__ void pert_spec_kernel(int n, int nb, int nx, cpx<double>* s0, cpx<double>* s1, cpx<double>* s2, int filter,
+                                 double m1, double m2, double scale, int leray) {
+    const long ns = (long)nb * nb * nx;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < ns; i += (long)gridDim.x * blockDim.x) {
+        const int fx = (int)(i % nx), fy = (int)((i / nx) % nb), fz = (int)(i / ((long)nx * nb));
+        const Kvec k = make_k(n, fx, fy, fz);
+        cpx<double> v[3] = {s0[i], s1[i], s2[i]};
+        if (filter > 0) {
+            const double norm_K = sqrt(k.kx * k.kx + k.ky * k.ky + k.kz * k.kz);
+            double f = 0.0;
+            if (!(norm_K < MACH_EPSILON)) {
+                if (filter == 1)
+                    f = m1;
+                else if (filter == 2)
+                    f = pow(10.0, m2) * pow(norm_K / ((double)n / 4.0), m1);
+                else if (filter == 3)
+                    f = pow(10.0, -norm_K / 5.0);
+                else
+                    f = 1.0;
+            }
+            f *= scale;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] = v[c] * f;
+        }
+        if (leray) {
+            if (k.ksq > MACH_EPSILON) {
+                const cpx<double> d = v[0] * k.ox + v[1] * k.oy + v[2] * k.oz;
+                v[0] = v[0] - d * (k.ox / k.ksq);
+                v[1] = v[1] - d * (k.oy / k.ksq);
+                v[2] = v[2] - d * (k.oz / k.ksq);
+            } else {
+                v[0] = v[1] = v[2] = mk(0.0, 0.0);
+            }
+        }
+        s0[i] = v[0];
+        s1[i] = v[1];
+        s2[i] = v[2];
+    }
+}
+
+template <typename T>
+int Engine<T>::kappa_pert(const char* type, double m1, double m2, double m3, const double* loaded,
+                          unsigned long long seed, double* out) {
+    if (sizeof(T) != 8) throw CudaError("full-band operators run in FP64", MLQ_ERR_BADARG);
+    if (!type) throw CudaError("kappa_test_pert: no type", MLQ_ERR_BADARG);
+    const std::string t(type);
+    enum { SINE, DFSINE, RAW, DIV, SMOOTH_DIV, SMOOTH, KRAND, POLY, EXPF, CREATE, SAVE };
+    static const std::map<std::string, int> kinds = {
+        {"sine", SINE},
+        {"divfree-sine", DFSINE},
+        {"load-te0080", RAW},
+        {"load-random-a", DIV},
+        {"load-random-b", DIV},
+        {"load-random-smooth-a", SMOOTH_DIV},
+        {"load-random-smooth-b", SMOOTH},
+        {"load-k-random-a", KRAND},
+        {"load-k-random-b", KRAND},
+        {"load-random-poly-a", POLY},
+        {"load-random-poly-b", POLY},
+        {"load-random-exp-a", EXPF},
+        {"load-random-exp-b", EXPF},
+        {"create-random-poly-b", CREATE},
+        {"save-random", SAVE},
+    };
+    const auto it = kinds.find(t);
+    if (it == kinds.end()) throw CudaError("kappa_test_pert: unknown type " + t, MLQ_ERR_BADARG);
+    const int kind = it->second;
+    const Band full = make_band(n / 2);
+    widen_to(full);
+    T* u[3] = {phys(PU), phys(PU + 1), phys(PU + 2)};
+    int status = 0;
+    // the field
+    if (kind == SINE || kind == DFSINE) {
+        pert_sine_kernel<T><<<grid_for(n3, 256), 256, 0, stream>>>(n, m1, kind == DFSINE ? m1 + m3 : m2, m3, u[0],
+                                                                     u[1], u[2]);
+        launched();
+    } else if (kind == CREATE || kind == SAVE) {
+        pert_random_kernel<T><<<grid_for(3 * n3, 256), 256, 0, stream>>>(n3, seed, u[0], u[1], u[2]);
+        launched();
+    } else if (loaded) {
+        for (int c = 0; c < 3; ++c) load_scalar_phys(loaded + c * n3, PU + c);
+    } else {
+        for (int c = 0; c < 3; ++c) MLQ_CUDA(cudaMemsetAsync(u[c], 0, n3 * sizeof(T), stream));
+        status = 1;
+    }
+    for (int c = 0; c < 3; ++c) phys_written(PU + c);
+    // spectral passes: forward (normalised), the per-mode multiplier and/or
+    // divAvg_free, inverse
+    const size_t nspec = (size_t)full.nb * full.nb * full.nx;
+    cpx<double>* sp[3] = {nullptr, nullptr, nullptr};
+    auto spec_pass = [&](int filter, double scale, int leray) {
+        for (int c = 0; c < 3; ++c) {
+            if (!sp[c]) sp[c] = (cpx<double>*)dev_alloc(nspec * sizeof(cpx<double>));
+            FwdOut o;
+            o.spec = sp[c];
+            o.spec_f64 = 1;
+            fwd(full, FCopy{}, {PU + c}, {o});
+        }
+        pert_spec_kernel<<<grid_for((long)nspec, 256), 256, 0, stream>>>(n, full.nb, full.nx, sp[0], sp[1], sp[2],
+                                                                         filter, m1, m2, scale, leray);
+        launched();
+        for (int c = 0; c < 3; ++c) {
+            InvOut o;
+            o.nsrc = 1;
+            o.src[0] = ZSrc{sp[c], 1, SYM_ONE, 0, 1.0};
+            o.phys_out = PU + c;
+            inv(full, {o});
+        }
+    };
+    // 100 <phi, phi>_L2 (global_summed_field_inner_product, 3557-3577)
+    auto norm_const = [&] {
+        for (int c = 0; c < 3; ++c) pointwise(FSqRed{}, {PU + c}, {}, 20 + c);
+        fetch_results();
+        const double dV = 1.0 / ((double)n * (double)n * (double)n);
+        double s = 0.0;
+        for (int c = 0; c < 3; ++c) s = s + h_results[20 + c] * dV;
+        return 100.0 * s;
+    };
+    try {
+        switch (kind) {
+            case SINE:
+            case DIV: spec_pass(0, 1.0, 1); break;
+            case SMOOTH:
+            case SMOOTH_DIV: {
+                // dealias_scalar(phi(:,:,:,c), 20.0) (708-710): a round trip through
+                // the band of order 20
+                const int cut = band_cut_for_order(n, 20.0);
+                if (cut < n / 2) {
+                    const Band bk = make_band(cut);
+                    for (int c = 0; c < 3; ++c) {
+                        FwdOut o;
+                        o.phys_out = PV + c;
+                        fwd(bk, FCopy{}, {PU + c}, {o});
+                        MLQ_CUDA(cudaMemcpyAsync(u[c], phys(PV + c), n3 * sizeof(T), cudaMemcpyDeviceToDevice, stream));
+                    }
+                }
+                if (kind == SMOOTH_DIV) spec_pass(0, 1.0, 1);
+                break;
+            }
+            case KRAND: spec_pass(1, 1.0, 1); break;
+            case POLY: spec_pass(2, 1.0, 1); break;
+            case EXPF: spec_pass(3, 1.0, 1); break;
+            case CREATE:
+            case SAVE: {
+                spec_pass(4, 1.0, 1);
+                const double nc = norm_const();
+                if (kind == CREATE)
+                    spec_pass(2, 1.0 / nc, 1);
+                else
+                    spec_pass(4, 1.0 / nc, 0);  // phi / nc (the field has no k = 0 mode left)
+                break;
+            }
+            default: break;
+        }
+        for (int c = 0; c < 3; ++c) store_scalar_phys(PU + c, out + c * n3);
+    } catch (...) {
+        for (auto* p : sp)
+            if (p) free_dev(p);
+        throw;
+    }
+    for (auto* p : sp)
+        if (p) free_dev(p);
+    return status;
 }
 
 }  // namespace mlq

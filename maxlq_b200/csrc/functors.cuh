@@ -485,9 +485,10 @@ struct FLSQG {
 struct FLSA {
     static constexpr int NIN = 3, NOUT = 1, NRED = 0;
     double tau;
+    const double* taup = nullptr;  // tau in device memory instead (the device line search)
     template <typename T>
     __device__ void operator()(const T* in, T* out, double*) const {
-        const T t = (T)tau;
+        const T t = (T)(taup ? *taup : tau);
         const T s = in[0] + t * (in[1] + t * in[2]);
         const T g = s <= T(0) ? T(0) : sqrt(s);
         out[0] = g * g;

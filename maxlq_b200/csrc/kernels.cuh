@@ -418,6 +418,12 @@ template <typename V>
 __device__ __forceinline__ void stv(V* p, long i, double2 v) {
     p[i] = V{(decltype(p[i].x))v.x, (decltype(p[i].y))v.y};
 }
+// v as the storage V rounds it (what ldv returns after stv)
+template <typename V>
+__device__ __forceinline__ double2 rndv(double2 v) {
+    const V r{(decltype(V{}.x))v.x, (decltype(V{}.y))v.y};
+    return make_double2((double)r.x, (double)r.y);
+}
 
 // ----------------------------------------------------------------------------
 // z stage, forward (optionally round trip).  grid = (ceil(nx/tx), nb, narr).
@@ -802,9 +808,10 @@ __global__ void spec_direction_kernel(long nt, V* g, double sg, V* d, double bet
     }
 }
 
-// Up to 6 vector inner products in one pass.  kind: 0 L2, 1 H_l weight
+// Up to 8 vector inner products in one pass.  kind: 0 L2, 1 H_l weight
 // (1+(lambda1|K|)^order)^2 (function_ops.f90:3472), 2 divergence energy
-// |K_odd . f|^2 of pair.a (pair.b ignored).
+// |K_odd . f|^2, 3 curl energy |K x f|^2, 4 |K|^4 |f|^2 (kinds 2-4 read
+// pair.a only).
 struct SpecDotPair {
     const void* a;  // state vectors (double2 or float2 storage, the kernel's V)
     const void* b;
@@ -820,19 +827,52 @@ struct SpecDotArgs {
     const void* ax_x = nullptr;
     const void* ax_y = nullptr;
     double ax_a = 0.0;
+    // the distinct vectors of the pass for spec_dot_fixed_kernel, ax_out
+    // last when the pass reads it (ax_last)
+    const void* vec[8];
+    int ax_last = 0;
     const double* hwtab;  // H_l weight (1+(lambda1|K|)^order)^2 by |j|^2 (function_ops.f90:3472), or null
     double* partials;
 };
 
+// One product of a pair at a mode (u = pair.a, w = pair.b there; K = 2 pi
+// (ox, oy, oz) / 2 pi with the Nyquist components zeroed).
+__device__ __forceinline__ double dot_term(int kind, const double2 (&u)[3], const double2 (&w)[3], double ox,
+                                           double oy, double oz, double hw) {
+    if (kind == 3) {
+        // |K x a|^2 (vel2vort, function_ops.f90:2485-2495); in-band modes
+        // have no Nyquist index, so K = 2 pi j on every axis
+        const double w0r = oy * u[2].x - oz * u[1].x, w0i = oy * u[2].y - oz * u[1].y;
+        const double w1r = oz * u[0].x - ox * u[2].x, w1i = oz * u[0].y - ox * u[2].y;
+        const double w2r = ox * u[1].x - oy * u[0].x, w2i = ox * u[1].y - oy * u[0].y;
+        return w0r * w0r + w0i * w0i + w1r * w1r + w1i * w1i + w2r * w2r + w2i * w2i;
+    }
+    if (kind == 4) {  // |K|^4 |a|^2 (||Lap a||^2)
+        const double k2 = ox * ox + oy * oy + oz * oz;
+        double m2 = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) m2 += u[c].x * u[c].x + u[c].y * u[c].y;
+        return k2 * k2 * m2;
+    }
+    if (kind == 2) {  // |K_odd . a|^2
+        const double dr = ox * u[0].x + oy * u[1].x + oz * u[2].x;
+        const double di = ox * u[0].y + oy * u[1].y + oz * u[2].y;
+        return dr * dr + di * di;
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) s += u[c].x * w[c].x + u[c].y * w[c].y;
+    return kind == 1 ? hw * s : s;
+}
+
+// Up to 8 inner products with every pair's vectors loaded per pair (any
+// pattern of operands).  One warp per row, each lane one mode at a time.
 template <typename V>
 __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
     double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     const SpecGeom& g = a.g;
     const double twopi = 2.0 * 3.14159265358979311600;
     const int nrows = g.nb * g.nb;
-    // 32 threads per row: RED_THREADS / 32 rows per block pass; each thread
-    // takes kx = fx and fx + 32 together, so a pair's loads for both are in
-    // flight at once (the second is a weight-0 repeat of the first past nx)
     const int lane = threadIdx.x & 31, wrow = threadIdx.x >> 5, rows_per = blockDim.x >> 5;
     for (int r = blockIdx.x * rows_per + wrow; r < nrows; r += gridDim.x * rows_per) {
         const SpecRow row(g, r);
@@ -840,82 +880,82 @@ __global__ void __launch_bounds__(RED_THREADS) spec_dot_kernel(SpecDotArgs a) {
         const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : twopi * (double)row.jy;
         const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : twopi * (double)row.jz;
         const int jyz = row.jy * row.jy + row.jz * row.jz;
-        for (int fx = lane; fx < g.nx; fx += 64) {
-            const bool two = fx + 32 < g.nx;
-            const int fx1 = two ? fx + 32 : fx;
-            const long i[2] = {base + fx, base + fx1};
-            const double wgt[2] = {kx_weight(g.n, fx), two ? kx_weight(g.n, fx1) : 0.0};
-            const double hw[2] = {a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0, a.hwtab ? a.hwtab[fx1 * fx1 + jyz] : 1.0};
-            const double ox[2] = {(2 * fx == g.n) ? 0.0 : twopi * (double)fx, (2 * fx1 == g.n) ? 0.0 : twopi * (double)fx1};
+        for (int fx = lane; fx < g.nx; fx += 32) {
+            const long i = base + fx;
+            const double wgt = kx_weight(g.n, fx);
+            const double hw = a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0;
+            const double ox = (2 * fx == g.n) ? 0.0 : twopi * (double)fx;
             if (a.ax_out) {
-                for (int e = 0; e < (two ? 2 : 1); ++e)  // not twice when fx + 32 repeats fx
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        const long k = c * g.ncomp + i[e];
-                        const double2 x = ldv((const V*)a.ax_x, k), y = ldv((const V*)a.ax_y, k);
-                        stv((V*)a.ax_out, k, make_double2(x.x + a.ax_a * y.x, x.y + a.ax_a * y.y));
-                    }
+                for (int c = 0; c < 3; ++c) {
+                    const long k = c * g.ncomp + i;
+                    const double2 x = ldv((const V*)a.ax_x, k), y = ldv((const V*)a.ax_y, k);
+                    stv((V*)a.ax_out, k, make_double2(x.x + a.ax_a * y.x, x.y + a.ax_a * y.y));
+                }
             }
             // unrolled to the bound of 8 so that acc stays in registers
 #pragma unroll
             for (int p = 0; p < 8; ++p) {
                 if (p >= a.npairs) break;
                 const SpecDotPair& q = a.pr[p];
-                if (q.kind == 3 || q.kind == 4) {
-                    // 3: |K x a|^2 (vel2vort, function_ops.f90:2485-2495);
-                    // 4: |K|^4 |a|^2 (||Lap a||^2).  In-band modes have no
-                    // Nyquist index, so K = 2 pi j on every axis.
-                    double2 v[2][3];
+                double2 u[3], w[3];
 #pragma unroll
-                    for (int e = 0; e < 2; ++e)
+                for (int c = 0; c < 3; ++c) u[c] = ldv((const V*)q.a, c * g.ncomp + i);
 #pragma unroll
-                        for (int c = 0; c < 3; ++c) v[e][c] = ldv((const V*)q.a, c * g.ncomp + i[e]);
+                for (int c = 0; c < 3; ++c) w[c] = q.kind < 2 ? ldv((const V*)q.b, c * g.ncomp + i) : u[c];
+                acc[p] += wgt * dot_term(q.kind, u, w, ox, oy, oz, hw);
+            }
+        }
+    }
+    block_reduce_store<8>(acc, a.partials, blockIdx.x);
+}
+
+// The same products for a pattern of operands fixed at compile time: the NV
+// distinct vectors are loaded once per mode, pair p reads vec[(PAT >> 6p) & 7]
+// and vec[(PAT >> (6p + 3)) & 7], and the optional update reads
+// vec[(PAT >> 48) & 7] + ax_a vec[(PAT >> 51) & 7] and writes ax_out (which
+// replaces vec[NV - 1] when ax_last).
+template <typename V, int NV, int NP, unsigned long long PAT>
+__global__ void __launch_bounds__(RED_THREADS) spec_dot_fixed_kernel(SpecDotArgs a) {
+    double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const SpecGeom& g = a.g;
+    const double twopi = 2.0 * 3.14159265358979311600;
+    const int nrows = g.nb * g.nb;
+    constexpr int XI = (int)((PAT >> 48) & 7), YI = (int)((PAT >> 51) & 7);
+    // ax_out is read before it is written only when it is an operand of the update
+    const bool load_last = !(a.ax_out && a.ax_last && XI != NV - 1 && YI != NV - 1);
+    const int lane = threadIdx.x & 31, wrow = threadIdx.x >> 5, rows_per = blockDim.x >> 5;
+    for (int r = blockIdx.x * rows_per + wrow; r < nrows; r += gridDim.x * rows_per) {
+        const SpecRow row(g, r);
+        const long base = (long)r * g.nx;
+        const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : twopi * (double)row.jy;
+        const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : twopi * (double)row.jz;
+        const int jyz = row.jy * row.jy + row.jz * row.jz;
+        for (int fx = lane; fx < g.nx; fx += 32) {
+            const long i = base + fx;
+            const double wgt = kx_weight(g.n, fx);
+            const double hw = a.hwtab ? a.hwtab[fx * fx + jyz] : 1.0;
+            const double ox = (2 * fx == g.n) ? 0.0 : twopi * (double)fx;
+            double2 x[NV][3];
 #pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        double s;
-                        if (q.kind == 3) {
-                            const double w0r = oy * v[e][2].x - oz * v[e][1].x, w0i = oy * v[e][2].y - oz * v[e][1].y;
-                            const double w1r = oz * v[e][0].x - ox[e] * v[e][2].x, w1i = oz * v[e][0].y - ox[e] * v[e][2].y;
-                            const double w2r = ox[e] * v[e][1].x - oy * v[e][0].x, w2i = ox[e] * v[e][1].y - oy * v[e][0].y;
-                            s = w0r * w0r + w0i * w0i + w1r * w1r + w1i * w1i + w2r * w2r + w2i * w2i;
-                        } else {
-                            const double k2 = ox[e] * ox[e] + oy * oy + oz * oz;
-                            double m2 = 0.0;
+            for (int v = 0; v < NV; ++v)
 #pragma unroll
-                            for (int c = 0; c < 3; ++c) m2 += v[e][c].x * v[e][c].x + v[e][c].y * v[e][c].y;
-                            s = k2 * k2 * m2;
-                        }
-                        acc[p] += wgt[e] * s;
-                    }
-                } else if (q.kind == 2) {
-                    double2 v[2][3];
+                for (int c = 0; c < 3; ++c)
+                    x[v][c] = (v < NV - 1 || load_last) ? ldv((const V*)a.vec[v], c * g.ncomp + i)
+                                                         : make_double2(0.0, 0.0);
+            if (a.ax_out) {
 #pragma unroll
-                    for (int e = 0; e < 2; ++e)
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) v[e][c] = ldv((const V*)q.a, c * g.ncomp + i[e]);
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        const double dr = ox[e] * v[e][0].x + oy * v[e][1].x + oz * v[e][2].x;
-                        const double di = ox[e] * v[e][0].y + oy * v[e][1].y + oz * v[e][2].y;
-                        acc[p] += wgt[e] * (dr * dr + di * di);
-                    }
-                } else {
-                    double2 u[2][3], v[2][3];
-#pragma unroll
-                    for (int e = 0; e < 2; ++e)
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) {
-                            u[e][c] = ldv((const V*)q.a, c * g.ncomp + i[e]);
-                            v[e][c] = ldv((const V*)q.b, c * g.ncomp + i[e]);
-                        }
-#pragma unroll
-                    for (int e = 0; e < 2; ++e) {
-                        double s = 0.0;
-#pragma unroll
-                        for (int c = 0; c < 3; ++c) s += u[e][c].x * v[e][c].x + u[e][c].y * v[e][c].y;
-                        acc[p] += wgt[e] * (q.kind == 1 ? hw[e] : 1.0) * s;
-                    }
+                for (int c = 0; c < 3; ++c) {
+                    const double2 nv =
+                        rndv<V>(make_double2(x[XI][c].x + a.ax_a * x[YI][c].x, x[XI][c].y + a.ax_a * x[YI][c].y));
+                    stv((V*)a.ax_out, c * g.ncomp + i, nv);
+                    if (a.ax_last) x[NV - 1][c] = nv;
                 }
+            }
+#pragma unroll
+            for (int p = 0; p < NP; ++p) {
+                const int ia = (int)((PAT >> (6 * p)) & 7), ib = (int)((PAT >> (6 * p + 3)) & 7);
+                acc[p] += wgt * dot_term(a.pr[p].kind, x[ia], x[ib], ox, oy, oz, hw);
             }
         }
     }

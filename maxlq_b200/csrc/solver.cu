@@ -115,7 +115,7 @@ class Solver : public SolverBase {
         ++eval_count;
         ++evals_this_iter;
         const Trial t = trial(base, dir, tau);
-        const double J = -1.0 * scaled_R(t);
+        const double J = ls_J(t.R[1], t.R[2], t.lqq, q(), B());
         // The reference's trial rescales the field and transforms it; a NaN
         // there stops the program at the FFT's NaN scan (fftwfunction.f90:78-89).
         // A trial that needs no transform (homogeneity, polynomial path)
@@ -123,134 +123,30 @@ class Solver : public SolverBase {
         if (std::isnan(J)) throw CudaError("NaN in a line-search trial value", MLQ_ERR_NAN);
         return J;
     }
-    double scaled_R(const Trial& t) const {
-        const double nrm = std::pow(t.lqq, 1.0 / q());
-        const double cs = B() / nrm;
-        return std::pow(cs, q()) * t.R[1] + std::pow(cs, q() + 1.0) * t.R[2];
-    }
+    double scaled_R(const Trial& t) const { return -ls_J(t.R[1], t.R[2], t.lqq, q(), B()); }
     int evals_this_iter = 0;
 
+    // the host evaluator of the line-search templates (linesearch.cuh)
+    struct HostEval {
+        Solver* s;
+        const SVec* phi;
+        const SVec* dir;
+        bool operator()(double tau, double* J) {
+            *J = s->lm_eval(phi, dir, tau);
+            return true;
+        }
+    };
     // mnbrak (optimization.f90:613-778)
     int mnbrak(const SVec* phi, const SVec* grad, double tA0, double tB0, double tau_brack[2], int* myflag) {
-        const double GOLD = (1.0 + std::sqrt(5.0)) / 2.0;
-        const double CGOLD = 1.0 / GOLD;
-        const double GLIMIT = 10.0;
-        const int ITMAX = 100;
-        double tA = tA0, tB = std::max(tB0, MACH_EPSILON), tC = 0.0, tP, FP, Pmax, R, Q;
-        double FA = lm_eval(phi, grad, tA);
-        double FB = lm_eval(phi, grad, tB);
-        double FC = 0.0;
-        int brakIter = 0;
-        while (FB > FA && tB > MACH_EPSILON) {
-            tB = CGOLD * tB;
-            FB = lm_eval(phi, grad, tB);
-        }
-        if (tB <= MACH_EPSILON) {
-            *myflag = 1;
-            return 1;
-        }
-        tC = GOLD * tB;
-        FC = lm_eval(phi, grad, tC);
-        while (FB >= FC && brakIter < ITMAX) {
-            brakIter++;
-            tC = GOLD * tC;
-            FC = lm_eval(phi, grad, tC);
-            R = (tB - tA) * (FB - FC);
-            Q = (tB - tC) * (FB - FA);
-            tP = tB - 0.5 * ((tB - tC) * Q - (tB - tA) * R) /
-                          std::copysign(std::max(std::fabs(Q - R), MACH_EPSILON), Q - R);
-            Pmax = tB + GLIMIT * (tC - tB);
-            if ((tB - tP) * (tP - tC) > 0) {
-                FP = lm_eval(phi, grad, tP);
-                if (FP < FC) {
-                    tA = tB; FA = FB; tB = tP; FB = FP;
-                    break;
-                } else if (FP > FB) {
-                    tC = tP; FC = FP;
-                    break;
-                }
-                tP = tC + GOLD * (tC - tB);
-                FP = lm_eval(phi, grad, tP);
-            } else if ((tC - tP) * (tP - Pmax) > 0) {
-                FP = lm_eval(phi, grad, tP);
-                if (FP < FC) {
-                    tB = tC; tC = tP; FB = FC; FC = FP;
-                    tP = tC + GOLD * (tC - tB);
-                    FP = lm_eval(phi, grad, tP);
-                }
-            } else if ((tP - Pmax) * (Pmax - tC) >= 0) {
-                tP = Pmax;
-                FP = lm_eval(phi, grad, tP);
-            } else {
-                tP = tC + GOLD * (tC - tB);
-                FP = lm_eval(phi, grad, tP);
-            }
-            tA = tB; tB = tC; tC = tP;
-            FA = FB; FB = FC; FC = FP;
-        }
-        tau_brack[0] = tA;
-        tau_brack[1] = tC;
-        *myflag = brakIter >= ITMAX ? 2 : 0;
-        return *myflag;
+        HostEval ev{this, phi, grad};
+        return ls_mnbrak(ev, tA0, tB0, tau_brack, myflag);
     }
-
-    // brent (optimization.f90:784-951); the constants are the Fortran
-    // default-real literals TOL = 1E-6, ZEPS = 1E-8, CGOLD = .381966 widened
-    // to double (804-806)
+    // brent (optimization.f90:784-951)
     double brent(const SVec* phi, const SVec* grad, const double tau_brack[2], double* fx_out) {
-        const int ITMAX = 300;
-        const double TOL = (double)1E-6f;
-        const double ZEPS = (double)1E-8f;
-        const double CGOLD = (double).381966f;
-        double D = 0.0, A = std::min(tau_brack[0], tau_brack[1]), Bb = std::max(tau_brack[0], tau_brack[1]);
-        double V = tau_brack[1] * CGOLD, W = V, X = V, E = 0.0, ETEMP, P = 0, Q = 0, R, U, XM, TOL1, TOL2;
-        double FX = lm_eval(phi, grad, D);  // value at tau = 0 written to brent-info (833-840)
-        FX = lm_eval(phi, grad, X);
-        double FV = FX, FW = FX, FU;
-        for (int j = 1; j <= ITMAX; ++j) {
-            XM = 0.5 * (A + Bb);
-            TOL1 = TOL * std::fabs(X) + ZEPS;
-            TOL2 = 2.0 * TOL1;
-            if (std::fabs(X - XM) <= (TOL2 - 0.5 * (Bb - A))) break;
-            int FLAG = 1;
-            if (std::fabs(E) > TOL1) {
-                R = (X - W) * (FX - FV);
-                Q = (X - V) * (FX - FW);
-                P = (X - V) * Q - (X - W) * R;
-                Q = 2.0 * (Q - R);
-                if (Q > 0.0) P = -P;
-                Q = std::fabs(Q);
-                ETEMP = E;
-                E = D;
-                if ((std::fabs(P) >= std::fabs(0.5 * Q * ETEMP)) || (P <= Q * (A - X)) || (P >= Q * (Bb - X)))
-                    FLAG = 1;
-                else
-                    FLAG = 2;
-            }
-            if (FLAG == 1) {
-                E = (X >= XM) ? A - X : Bb - X;
-                D = CGOLD * E;
-            } else {
-                D = P / Q;
-                U = X + D;
-                if ((U - A < TOL2) || (Bb - U < TOL2)) D = std::copysign(TOL1, XM - X);
-            }
-            U = (std::fabs(D) >= TOL1) ? X + D : X + std::copysign(TOL1, D);
-            FU = lm_eval(phi, grad, U);
-            if (FU <= FX) {
-                if (U >= X) A = X; else Bb = X;
-                V = W; FV = FW; W = X; FW = FX; X = U; FX = FU;
-            } else {
-                if (U < X) A = U; else Bb = U;
-                if ((FU <= FW) || (W == X)) {
-                    V = W; FV = FW; W = U; FW = FU;
-                } else if ((FU <= FV) || (V == X) || (V == W)) {
-                    V = U; FV = FU;
-                }
-            }
-        }
-        if (fx_out) *fx_out = FX;
-        return X;
+        HostEval ev{this, phi, grad};
+        double x = 0.0;
+        ls_brent(ev, tau_brack, &x, fx_out);
+        return x;
     }
 
     // ---- CG loop -------------------------------------------------------------
@@ -362,7 +258,28 @@ class Solver : public SolverBase {
         double tb[2] = {0, 0};
         int mflag = 0;
         ls_begin(u, d1);
-        mnbrak(u, d1, 0.0, tau0, tb, &mflag);
+        double fx = 0, tau1 = 0;
+        LsOut lo;
+        if (ls_ready && e.ls_device_search(Bc, 0.0, tau0, &lo) == 0 && lo.status != LS_ERR_CAP) {
+            // mnbrak and Brent ran on the device; one read of the outcome
+            eval_count += lo.evals;
+            evals_this_iter += lo.evals;
+            if (lo.status == MLQ_ERR_NAN) throw CudaError("NaN in a line-search trial value", MLQ_ERR_NAN);
+            mflag = lo.mflag;
+            tb[0] = lo.tb[0];
+            tb[1] = lo.tb[1];
+            if (mflag == 0) {
+                tau1 = lo.tau1;
+                fx = lo.fx;
+                Trial t;
+                for (int k = 0; k < 3; ++k) t.R[k] = lo.R1[k];
+                t.lqq = lo.lqq1;
+                trials[tau1] = t;
+            }
+        } else {
+            mnbrak(u, d1, 0.0, tau0, tb, &mflag);
+            if (mflag == 0) tau1 = brent(u, d1, tb, &fx);  // 297
+        }
         info.J0 = J0;
         info.mnbrak_flag = mflag;
         if (mflag != 0) {
@@ -372,8 +289,6 @@ class Solver : public SolverBase {
             info.seconds = iter_clock_stop();
             return info.status;
         }
-        double fx = 0;
-        double tau1 = brent(u, d1, tb, &fx);  // 297
         info.tau_a = tb[0];
         info.tau_b = tb[1];
         int status = MLQ_OK;

@@ -160,6 +160,13 @@ module maxlq_gpu
     integer(c_int) function mlq_pointwise_R(ctx, u, res) bind(C)
       import; type(c_ptr), value :: ctx; real(c_double), intent(in) :: u(*); real(c_double) :: res(*)
     end function
+    ! type: a NUL-terminated name, e.g. "create-random-poly-b"//c_null_char;
+    ! loaded: c_loc of the field read from the file, or c_null_ptr
+    integer(c_int) function mlq_kappa_perturbation(ctx, mytype, m1, m2, m3, loaded, seed, phi) bind(C)
+      import; type(c_ptr), value :: ctx; character(kind=c_char), intent(in) :: mytype(*)
+      real(c_double), value :: m1, m2, m3; type(c_ptr), value :: loaded
+      integer(c_long_long), value :: seed; real(c_double) :: phi(*)
+    end function
 
     ! ---- optimization.f90 ----
     integer(c_int) function mlq_eval_J(ctx, u, mode, J) bind(C)

@@ -10,6 +10,7 @@
 #include <complex>
 #include <cstdlib>
 #include <cstring>
+#include <string>
 #include <vector>
 #ifdef _OPENMP
 #include <omp.h>
@@ -1095,6 +1096,123 @@ void pointwise_R(orc_ctx* c, const double* u, double* res) {
     }
 }
 
+// ---- kappa_test_pert (function_ops.f90:615-977) ---------------------------
+namespace {
+
+// The random fields of create-random-poly-b and save-random are drawn from
+// Fortran's unseeded random_number there (784-785, 937-938); here from a
+// seeded counter generator (splitmix64 finaliser of seed + (i+1) * golden
+// gamma, top 53 bits), element i in the array order of phi_pert(x,y,z,c).
+double pert_uniform(unsigned long long seed, long i) {
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ULL * (unsigned long long)(i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// faux(:,:,:,ll) *= f(norm_K), 0 where norm_K < MACH_EPSILON, through one
+// fftfwdv / fftbwdv round trip per component (e.g. 771-793)
+template <class F>
+void pert_filter(orc_ctx* c, double* phi, F f) {
+    const int n = c->n;
+    for (int d = 0; d < 3; ++d) {
+        CV a = to_complex(c, phi + d * c->n3);
+        fftfwd(c, a.data());
+#pragma omp parallel for collapse(2)
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) {
+                    const long i = IDX(c, x, y, z);
+                    const double norm_K = std::sqrt(Kx(c, x) * Kx(c, x) + Kx(c, y) * Kx(c, y) + Kx(c, z) * Kx(c, z));
+                    if (norm_K < MACH_EPSILON)
+                        a[i] = 0.0;
+                    else
+                        a[i] *= f(norm_K);
+                }
+        fftbwd(c, a.data());
+        real_part(c, a, phi + d * c->n3);
+    }
+}
+
+// returns 1 when successful (the reference's `successful`), 0 when a load-*
+// type had no field (in == nullptr: phi taken as 0), -1 for an unknown type
+int kappa_pert(orc_ctx* c, const char* type, double m1, double m2, double m3, const double* in,
+               unsigned long long seed, double* phi) {
+    const int n = c->n;
+    const long n3 = c->n3;
+    const std::string t(type);
+    const double PI = c->PI;
+    int ok = 1;
+    auto load = [&] {
+        if (in) {
+            std::memcpy(phi, in, sizeof(double) * 3 * n3);
+        } else {
+            std::memset(phi, 0, sizeof(double) * 3 * n3);
+            ok = 0;
+        }
+    };
+    auto poly = [&](double nk) { return std::pow(10.0, m2) * std::pow(nk / ((double)n / 4.0), m1); };
+    auto random_field = [&] {
+        // random_number, 2 phi - 1, the k = 0 mode removed, divAvg_free, and
+        // phi / (100 <phi, phi>_L2) (784-803, 937-956)
+        for (long i = 0; i < 3 * n3; ++i) phi[i] = 2.0 * pert_uniform(seed, i) - 1.0;
+        pert_filter(c, phi, [](double) { return 1.0; });
+        divavg_free(c, phi);
+        const double normalization_const = 100.0 * field_inner(c, phi, phi, 0);
+        for (long i = 0; i < 3 * n3; ++i) phi[i] = phi[i] / normalization_const;
+    };
+    const double dx = 1.0 / (double)n;
+    if (t == "sine" || t == "divfree-sine") {  // 658-688
+        const bool df = t == "divfree-sine";
+        const double m2e = df ? m1 + m3 : m2;
+        for (int z = 0; z < n; ++z)
+            for (int y = 0; y < n; ++y)
+                for (int x = 0; x < n; ++x) {
+                    const double X = (double)x * dx, Y = (double)y * dx, Z = (double)z * dx;
+                    const long i = IDX(c, x, y, z);
+                    phi[i] = std::sin(2.0 * PI * m1 * X) * std::cos(2.0 * PI * m2e * Y) * std::cos(2.0 * PI * m3 * Z);
+                    phi[n3 + i] =
+                        -std::cos(2.0 * PI * m1 * X) * std::sin(2.0 * PI * m2e * Y) * std::cos(2.0 * PI * m3 * Z);
+                    phi[2 * n3 + i] =
+                        std::cos(2.0 * PI * m1 * X) * std::cos(2.0 * PI * m2e * Y) * std::sin(2.0 * PI * m3 * Z);
+                }
+        if (!df) divavg_free(c, phi);
+    } else if (t == "load-te0080") {  // 652-655
+        load();
+    } else if (t == "load-random-a" || t == "load-random-b") {  // 691-701
+        load();
+        divavg_free(c, phi);
+    } else if (t == "load-random-smooth-a" || t == "load-random-smooth-b") {  // 703-711, 923-930
+        load();
+        for (int d = 0; d < 3; ++d) dealias_scalar(c, phi + d * n3, 20.0);
+        if (t == "load-random-smooth-a") divavg_free(c, phi);
+    } else if (t == "load-k-random-a" || t == "load-k-random-b") {  // 713-765
+        load();
+        pert_filter(c, phi, [&](double) { return m1; });
+        divavg_free(c, phi);
+    } else if (t == "load-random-poly-a" || t == "load-random-poly-b") {  // 768-792, 830-854
+        load();
+        pert_filter(c, phi, poly);
+        divavg_free(c, phi);
+    } else if (t == "load-random-exp-a" || t == "load-random-exp-b") {  // 857-920
+        load();
+        pert_filter(c, phi, [](double nk) { return std::pow(10.0, -nk / 5.0); });
+        divavg_free(c, phi);
+    } else if (t == "create-random-poly-b") {  // 795-827
+        random_field();
+        pert_filter(c, phi, poly);
+        divavg_free(c, phi);
+    } else if (t == "save-random") {  // 932-956 (the field written to n<NNNN>_random.nc)
+        random_field();
+    } else {
+        return -1;
+    }
+    return ok;
+}
+
+}  // namespace
+
 extern "C" {
 
 void orc_default_params(orc_params* p, int n, double q, double B) {
@@ -1165,6 +1283,10 @@ void orc_spectral_data(orc_ctx* c, const double* u, double* out, int normalize) 
 double orc_summed_enstrophy(orc_ctx* c, const double* u) { return summed_enstrophy(c, u); }
 void orc_dEnstrophydt(orc_ctx* c, const double* u, double out[3]) { dEnstrophydt(c, u, out); }
 void orc_pointwise_R(orc_ctx* c, const double* u, double* res) { pointwise_R(c, u, res); }
+int orc_kappa_pert(orc_ctx* c, const char* type, double m1, double m2, double m3, const double* in,
+                   unsigned long long seed, double* out) {
+    return kappa_pert(c, type, m1, m2, m3, in, seed, out);
+}
 int orc_mnbrak(orc_ctx* c, const double* phi, const double* d, double tA0, double tB0, double tau_brack[2],
                int* flag) {
     *flag = 0;

@@ -104,6 +104,10 @@ void orc_spectral_data(orc_ctx* c, const double* u, double* out, int normalize);
 double orc_summed_enstrophy(orc_ctx* c, const double* u);
 void orc_dEnstrophydt(orc_ctx* c, const double* u, double out[3]);
 void orc_pointwise_R(orc_ctx* c, const double* u, double* res);
+/* kappa_test_pert (function_ops.f90:615-977): 1 successful, 0 a load-* type
+   without its field (in = NULL), -1 unknown type */
+int orc_kappa_pert(orc_ctx* c, const char* type, double m1, double m2, double m3, const double* in,
+                   unsigned long long seed, double* out);
 /* optimization.f90:7-514 without the file I/O and kappa tests.  u in/out.
  * Returns the number of iterations; status in *flag (0 converged/limit,
  * 1 mnbrak uphill, 2 mnbrak ITMAX, 4 tau > TAU_MAX, 5 J decreased). */

@@ -75,6 +75,8 @@ def _load():
         "orc_summed_enstrophy": (C.c_double, [vp, _DP]),
         "orc_dEnstrophydt": (None, [vp, _DP, _DP]),
         "orc_pointwise_R": (None, [vp, _DP, _DP]),
+        "orc_kappa_pert": (C.c_int, [vp, C.c_char_p, C.c_double, C.c_double, C.c_double, _DP, C.c_ulonglong,
+                                     _DP]),
         "orc_gradient": (None, [vp, _DP, _DP]),
         "orc_divergence": (None, [vp, _DP, _DP]),
         "orc_laplacian": (None, [vp, _DP]),
@@ -287,6 +289,16 @@ class Oracle:
         out = np.zeros((3, self.n, self.n, self.n))
         self._lib.orc_pointwise_R(self._ctx, _p(self._vec(u)), _p(out))
         return out
+
+    def kappa_test_pert(self, mytype, m1=0.0, m2=0.0, m3=0.0, loaded=None, seed=0):
+        """kappa_test_pert (function_ops.f90:615-977): (phi, successful).
+        loaded: the field a load-* type reads from its file (None: no file)."""
+        out = np.zeros((3, self.n, self.n, self.n))
+        src = None if loaded is None else _p(self._vec(loaded))
+        r = self._lib.orc_kappa_pert(self._ctx, mytype.encode(), m1, m2, m3, src, seed, _p(out))
+        if r < 0:
+            raise ValueError("unknown perturbation type " + mytype)
+        return out, bool(r)
 
     def maxdlqdt(self, u, max_iter=99999, optim_tol=1e-5, start_iter=0, callback=None):
         """Run the CG loop on a copy of u; returns (u, iterations, flag, records)."""

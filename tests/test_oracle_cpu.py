@@ -122,3 +122,22 @@ def test_oracle_cg_loop_increases_R():
     assert all(r["deltaJ"] >= 0 for r in recs)
     assert J[0] <= J[1] <= J[2]
     assert o.lq_norm(u) == pytest.approx(1.0, rel=1e-12)
+
+
+def test_oracle_kappa_perturbations():
+    """kappa_test_pert restated (function_ops.f90:615-977): the divergence-free
+    sine field needs no projection, the projected types have no mean, and
+    the random types depend on the seed only."""
+    n = 16
+    o = Oracle(n, 4.0, 1.0)
+    phi, ok = o.kappa_test_pert("divfree-sine", 2.0, 0.0, 1.0)
+    assert ok
+    div = o.divergence(phi)
+    assert np.abs(div).max() < 1e-11 * np.abs(phi).max() * 2 * np.pi * n
+    a, _ = o.kappa_test_pert("create-random-poly-b", -2.0, -1.0, 0.0, seed=7)
+    b, _ = o.kappa_test_pert("create-random-poly-b", -2.0, -1.0, 0.0, seed=7)
+    c, _ = o.kappa_test_pert("create-random-poly-b", -2.0, -1.0, 0.0, seed=8)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    assert np.abs(a.mean(axis=(1, 2, 3))).max() < 1e-14 * np.abs(a).max()
+    z, ok = o.kappa_test_pert("load-k-random-a", 1.0)
+    assert not ok and not z.any()
