@@ -50,8 +50,13 @@ def test_perturbation_matches_the_oracle(n, mytype, m):
     pg, okg = c.kappa_test_pert(mytype, *m, loaded=loaded, seed=11)
     po, oko = o.kappa_test_pert(mytype, *m, loaded=loaded, seed=11)
     assert okg and oko
-    assert np.abs(po).max() > 0.0
-    assert _rel(pg, po) < 1e-11, (mytype, _rel(pg, po))
+    if np.abs(po).max() == 0.0:
+        # load-random-smooth-a below N = 21: the order-20 dealias keeps only
+        # the mean, which divAvg_free removes
+        assert mytype == "load-random-smooth-a" and n < 21
+        assert np.abs(pg).max() < 1e-13
+    else:
+        assert _rel(pg, po) < 1e-11, (mytype, _rel(pg, po))
 
 
 def test_load_type_without_its_file():
