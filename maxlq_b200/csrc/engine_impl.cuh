@@ -3358,13 +3358,13 @@ int Engine<T>::kappa_pert(const char* type, double m1, double m2, double m3, con
             inv(full, {o});
         }
     };
-    // 100 <phi, phi>_L2 (global_summed_field_inner_product, 3557-3577)
+    // 100 <phi, phi>_L2 (global_summed_field_inner_product, 3557-3577); a
+    // pointwise reduction is already the sum times dV = 1/N^3
     auto norm_const = [&] {
         for (int c = 0; c < 3; ++c) pointwise(FSqRed{}, {PU + c}, {}, 20 + c);
         fetch_results();
-        const double dV = 1.0 / ((double)n * (double)n * (double)n);
         double s = 0.0;
-        for (int c = 0; c < 3; ++c) s = s + h_results[20 + c] * dV;
+        for (int c = 0; c < 3; ++c) s = s + h_results[20 + c];
         return 100.0 * s;
     };
     try {
