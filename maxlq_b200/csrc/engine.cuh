@@ -23,7 +23,8 @@
 namespace mlq {
 
 // launchers of the device line search's kernels (lsdev.cu)
-void ls_launch_coef(LsDevState* s, const double* results, const double* partials, int nblocks, cudaStream_t st);
+void ls_launch_coef(LsDevState* s, const double* results, const double* partials, int nblocks, const LsAnchorSet& an,
+                    cudaStream_t st);
 void ls_launch_ctrl(LsDevState* s, cudaGraphConditionalHandle h_loop, cudaGraphConditionalHandle h_chk,
                     cudaStream_t st);
 void ls_launch_check(LsDevState* s, const double* partials, int nblocks, cudaGraphConditionalHandle h_fft,
@@ -427,7 +428,8 @@ class Engine : public EngineBase {
     // setup forms the tau-coefficient fields once; a trial is then one
     // forward transform of g(tau)^2 plus polynomial evaluations.
     bool ls_ok() const { return !use_e_u && P.q == 4.0; }
-    void ls_setup(const SVec* u, const SVec* d);
+    // tau0: the previous step, whose neighbourhood the trials visit (<= 0: none)
+    void ls_setup(const SVec* u, const SVec* d, double tau0 = 0.0);
     void ls_trial(double tau, double out[3], double* lqq);
     // Where S(tau) = S0 + tau S1 + tau^2 S2 (the dealiased |phi|^2) is >= 0 at
     // every point, the clamp of calc_uk is inactive and P2(g^2) = S(tau): a

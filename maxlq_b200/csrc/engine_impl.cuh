@@ -1392,6 +1392,28 @@ void Engine<T>::release_io_buffers() {
 // ----------------------------------------------------------------------------
 // programs
 // ----------------------------------------------------------------------------
+// D = -i (K_odd . c) / |K|^2 over a band spectrum (0 at k = 0): the gradient
+// of D is grad Lap^-1 div c, as SYM_KK_KSQ summed over the components
+template <typename V, typename T>
+__global__ void spec_div_ksq_kernel(SpecGeom g, const V* __restrict__ c0, const V* __restrict__ c1,
+                                    const V* __restrict__ c2, cpx<T>* __restrict__ out) {
+    const double twopi = 2.0 * 3.14159265358979311600;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncomp; i += (long)gridDim.x * blockDim.x) {
+        const int fx = (int)(i % g.nx);
+        const SpecRow row(g, (int)(i / g.nx));
+        const double kx = twopi * (double)fx, ky = twopi * (double)row.jy, kz = twopi * (double)row.jz;
+        const double ox = (2 * fx == g.n) ? 0.0 : kx;
+        const double oy = (2 * band_fft_index(g.band, row.cy) == g.n) ? 0.0 : ky;
+        const double oz = (2 * band_fft_index(g.band, row.cz) == g.n) ? 0.0 : kz;
+        const double ksq = kx * kx + ky * ky + kz * kz;
+        const double2 a = ldv(c0, i), b = ldv(c1, i), c = ldv(c2, i);
+        const double vx = ox * a.x + oy * b.x + oz * c.x, vy = ox * a.y + oy * b.y + oz * c.y;
+        cpx<T> r = mk(T(0), T(0));
+        if (ksq != 0.0) r = mk((T)(vy / ksq), (T)(-vx / ksq));
+        out[i] = r;
+    }
+}
+
 namespace {
 // physical scratch indices
 enum : int {
@@ -1412,6 +1434,7 @@ enum : int {
 };
 // work spectra (band b2)
 enum : int { WG2 = 0, WA = 1, WP = 2, WT = 3 /*3..5*/, WONE = 6, WCH = 7 /*7..*/ };
+enum : int { WDIV = 52 };  // -i (K . c) / |K|^2 of the gradient program
 }  // namespace
 // line search along phi = u + tau d (q = 4): physical fields and work spectra
 namespace {
@@ -2077,17 +2100,29 @@ void Engine<T>::grad_l2_body(const SVec* u, SVec* v, SVec* c, bool want_lq, bool
             fwd(b, FMul{}, {a2.phys, PT}, {o});
         }
     }
-    // 6. grad aux4 = grad Lap^-1 div c (1155-1158)
+    // 6. grad aux4 = grad Lap^-1 div c (1155-1158): the scalar spectrum
+    // D = -i (K_odd . c) / |K|^2 once, then its three gradients i K_odd,k D
+    // (= K_odd,k (K_odd . c) / |K|^2) from one load of D per column
     {
-        std::vector<InvOut> g;
+        const SpecGeom g2 = geom(b);
+        cudaEvent_t ev = prof_mark();
+        if (state32_)
+            spec_div_ksq_kernel<float2, T><<<grid_for(g2.ncomp, 256), 256, 0, stream>>>(
+                g2, (const float2*)scomp(c, 0), (const float2*)scomp(c, 1), (const float2*)scomp(c, 2), wspec(WDIV));
+        else
+            spec_div_ksq_kernel<double2, T><<<grid_for(g2.ncomp, 256), 256, 0, stream>>>(
+                g2, (const double2*)scomp(c, 0), (const double2*)scomp(c, 1), (const double2*)scomp(c, 2),
+                wspec(WDIV));
+        launched("spec_scale", (double)g2.ncomp * (3.0 * sv_elem() + sizeof(cpx<T>)), ev);
+        std::vector<InvOut> gi;
         for (int k = 0; k < 3; ++k) {
             InvOut o;
-            o.nsrc = 3;
-            for (int j = 0; j < 3; ++j) o.src[j] = ZSrc{scomp(c, j), sf64(), SYM_KK_KSQ, 3 * k + j, 1.0};
+            o.nsrc = 1;
+            o.src[0] = ZSrc{wspec(WDIV), wf64<T>(), SYM_IKX + k, 0, 1.0};
             o.phys_out = PGA + k;
-            g.push_back(o);
+            gi.push_back(o);
         }
-        inv(b, g);
+        inv(b, gi);
     }
     // 7. final sum, one dealias, plus vc nu Lap c (1172-1190)
     {
@@ -2291,66 +2326,58 @@ void Engine<T>::calc_uk(const SVec* u, double k, int dst) {
 
 // Per block: the largest lower end and the smallest upper end, over its
 // points, of the interval around tau = 0 on which s0 + tau s1 + tau^2 s2 >= 0
-// (empty when s0 < 0), as (lo, hi) pairs.
+// (empty when s0 < 0), then the same around each anchor (empty where S is
+// negative at the anchor), as (lo, hi) pairs: 2 (LS_ANCHORS + 1) per block.
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS)
     ls_interval_kernel(const T* __restrict__ s0, const T* __restrict__ s1, const T* __restrict__ s2, long npts,
-                       double* __restrict__ out) {
+                       LsAnchorSet an, double* __restrict__ out) {
+    constexpr int K = LS_ANCHORS + 1;
     const double inf = 1e300;
-    double lo = -inf, hi = inf;
+    double lo[K], hi[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        lo[k] = -inf;
+        hi[k] = inf;
+    }
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long)gridDim.x * blockDim.x) {
         const double a = (double)s2[i], b = (double)s1[i], c = (double)s0[i];
-        if (c < 0.0) {
-            lo = inf;
-            hi = -inf;
-            continue;
-        }
-        if (a == 0.0) {
-            if (b > 0.0) lo = fmax(lo, -c / b);
-            if (b < 0.0) hi = fmin(hi, -c / b);
-            continue;
-        }
-        const double disc = b * b - 4.0 * a * c;
-        if (disc < 0.0) continue;  // a > 0: positive everywhere
-        const double sq = sqrt(disc);
-        const double qq = -0.5 * (b + (b >= 0.0 ? sq : -sq));
-        double r1 = qq / a, r2 = qq != 0.0 ? c / qq : 0.0;
-        if (r1 > r2) {
-            const double t = r1;
-            r1 = r2;
-            r2 = t;
-        }
-        if (a < 0.0) {  // non-negative between the roots
-            lo = fmax(lo, r1);
-            hi = fmin(hi, r2);
-        } else if (r2 <= 0.0) {  // opens up: the side of 0
-            lo = fmax(lo, r2);
-        } else if (r1 >= 0.0) {
-            hi = fmin(hi, r1);
-        } else {
-            lo = fmax(lo, 0.0);
-            hi = fmin(hi, 0.0);
-        }
-    }
-    __shared__ double slo[RED_THREADS / 32], shi[RED_THREADS / 32];
+        const LsRoots r = ls_roots(a, b, c);
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        lo = fmax(lo, __shfl_down_sync(0xffffffffu, lo, o));
-        hi = fmin(hi, __shfl_down_sync(0xffffffffu, hi, o));
+        for (int k = 0; k < K; ++k) {
+            double l, h;
+            if (k == 0)
+                ls_component0(r, a, b, c, l, h);
+            else
+                ls_component(r, a, b, c, an.a[k - 1], l, h);
+            lo[k] = fmax(lo[k], l);
+            hi[k] = fmin(hi[k], h);
+        }
     }
+    __shared__ double slo[K][RED_THREADS / 32], shi[K][RED_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (lane == 0) {
-        slo[warp] = lo;
-        shi[warp] = hi;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = fmax(lo[k], __shfl_down_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmin(hi[k], __shfl_down_sync(0xffffffffu, hi[k], o));
+        }
+        if (lane == 0) {
+            slo[k][warp] = lo[k];
+            shi[k][warp] = hi[k];
+        }
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < K) {
+        const int k = threadIdx.x;
+        double l = slo[k][0], h = shi[k][0];
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-            lo = fmax(lo, slo[w]);
-            hi = fmin(hi, shi[w]);
+            l = fmax(l, slo[k][w]);
+            h = fmin(h, shi[k][w]);
         }
-        out[2 * blockIdx.x] = lo;
-        out[2 * blockIdx.x + 1] = hi;
+        out[2 * K * blockIdx.x + 2 * k] = l;
+        out[2 * K * blockIdx.x + 2 * k + 1] = h;
     }
 }
 
@@ -2376,7 +2403,7 @@ __global__ void __launch_bounds__(RED_THREADS)
 }
 
 template <typename T>
-void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
+void Engine<T>::ls_setup(const SVec* u, const SVec* d, double tau0) {
     const long nc = spec_ncomp();
     ls_free_val_ = -1;
     ls_dev_ = ls_device_ready();
@@ -2502,24 +2529,31 @@ void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
         sdots(*this, p3, 152);
     }
     // the interval of tau around 0 on which S(tau) >= 0 everywhere
+    LsAnchorSet an;
+    ls_anchors(tau0, an.a);
+    constexpr int W = 2 * (LS_ANCHORS + 1);  // interval ends per block
     if (ls_dev_) {
         // on the device, with the coefficients: no host round trip
         const int grid = grid_for(n3, RED_THREADS, 148 * 4);
-        ensure_partials((long)grid * 2);
+        ensure_partials((long)grid * W);
         ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(phys(ls_phys(0)), phys(ls_phys(1)),
-                                                                phys(ls_phys(2)), n3, d_partials);
+                                                                phys(ls_phys(2)), n3, an, d_partials);
         launched();
-        ls_launch_coef(d_ls_, d_results, d_partials, grid, stream);
+        ls_launch_coef(d_ls_, d_results, d_partials, grid, an, stream);
         launched();
         ls_host_poly_ = false;
         return;
     }
-    double lo = -1e300, hi = 1e300;
+    double lo[LS_ANCHORS + 1], hi[LS_ANCHORS + 1];
+    for (int k = 0; k <= LS_ANCHORS; ++k) {
+        lo[k] = -1e300;
+        hi[k] = 1e300;
+    }
     {
         const long npts = slab_ ? (long)zs_ * n * n : n3;
         const int grid = grid_for(npts, RED_THREADS, 148 * 4);
-        ensure_partials((long)grid * 2);
-        std::vector<double> h((size_t)grid * 2);
+        ensure_partials((long)grid * W);
+        std::vector<double> h((size_t)grid * W);
         for (int z0 = 0; z0 < n; z0 += (slab_ ? zs_ : n)) {
             const T* s[3];
             if (slab_) {
@@ -2528,19 +2562,20 @@ void Engine<T>::ls_setup(const SVec* u, const SVec* d) {
             } else {
                 for (int a = 0; a < 3; ++a) s[a] = phys(ls_phys(a));
             }
-            ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(s[0], s[1], s[2], npts, d_partials);
+            ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(s[0], s[1], s[2], npts, an, d_partials);
             launched();
             MLQ_CUDA(cudaMemcpyAsync(h.data(), d_partials, h.size() * sizeof(double), cudaMemcpyDeviceToHost, stream));
             MLQ_CUDA(cudaStreamSynchronize(stream));
-            for (int g = 0; g < grid; ++g) {
-                lo = std::max(lo, h[2 * g]);
-                hi = std::min(hi, h[2 * g + 1]);
-            }
+            for (int g = 0; g < grid; ++g)
+                for (int k = 0; k <= LS_ANCHORS; ++k) {
+                    lo[k] = fmax(lo[k], h[W * g + 2 * k]);
+                    hi[k] = fmin(hi[k], h[W * g + 2 * k + 1]);
+                }
         }
     }
     fetch_results();
     // <S_i, G_a> in slots 140..148 (146.. holds i = 2), <S_i, S_j> in 149..154
-    ls_assemble(h_results + 100, h_results + 140, h_results + 149, lo, hi, ls_c_);
+    ls_assemble(h_results + 100, h_results + 140, h_results + 149, lo[0], hi[0], lo + 1, hi + 1, an.a, ls_c_);
     ls_host_poly_ = true;
 }
 
@@ -2728,7 +2763,7 @@ bool Engine<T>::ls_clamp_free(double tau) {
     if (ls_free_val_ >= 0 && tau == ls_free_tau_) return ls_free_val_ != 0;  // decided by the device search
     if (ls_transform_trials_) return false;
     ls_poly_to_host();
-    bool clamp_off = tau >= ls_c_.tlo && tau <= ls_c_.thi;
+    bool clamp_off = ls_free(ls_c_, tau);
     if (!clamp_off) {
         // outside the interval: one read of S_0..2 decides for this tau
         const long npts = slab_ ? (long)zs_ * n * n : n3;

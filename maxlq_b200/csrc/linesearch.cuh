@@ -24,17 +24,134 @@ constexpr int LS_SUSPEND = -1;
 // |grad phi|^2 ones G_a and with each other, the R2 and R3 integrands as
 // polynomials in tau, and the interval of tau around 0 on which
 // S(tau) >= 0 at every point.
+// Besides that interval, the setup finds the clamp-free interval around
+// each of LS_ANCHORS anchor steps near the previous step (alo[k] > ahi[k]:
+// none), so that most trials away from 0 need no check either.
+constexpr int LS_ANCHORS = 6;
 struct LsPoly {
     double sx[3][3], ss[3][3];
     double r2[5], r3[6];
     double tlo, thi;
+    double alo[LS_ANCHORS], ahi[LS_ANCHORS];
 };
+
+// The anchors for a previous step tau0: tau0 * GOLD^k, k = -3..2 (mnbrak's
+// first trials from tau0 and Brent's refinements near it); none for tau0 <= 0.
+__host__ __device__ inline void ls_anchors(double tau0, double a[LS_ANCHORS]) {
+    const double GOLD = (1.0 + sqrt(5.0)) / 2.0;
+    double t = tau0 > 0.0 ? tau0 / (GOLD * GOLD * GOLD) : 0.0;
+    for (int k = 0; k < LS_ANCHORS; ++k, t *= GOLD) a[k] = t;
+}
+
+// One point's S(tau) = c + b tau + q tau^2 >= 0 set, from its roots (found
+// once per point): kind 0 linear (q = 0), 1 no real root, 2 roots r1 <= r2.
+struct LsRoots {
+    int kind;
+    double r1, r2;
+};
+__host__ __device__ inline LsRoots ls_roots(double q, double b, double c) {
+    LsRoots r{0, 0.0, 0.0};
+    if (q == 0.0) {
+        if (b != 0.0) r.r1 = r.r2 = -c / b;
+        return r;
+    }
+    const double disc = b * b - 4.0 * q * c;
+    if (disc < 0.0) {
+        r.kind = 1;
+        return r;
+    }
+    const double sq = sqrt(disc);
+    const double qq = -0.5 * (b + (b >= 0.0 ? sq : -sq));
+    double r1 = qq / q, r2 = qq != 0.0 ? c / qq : 0.0;
+    if (r1 > r2) {
+        const double t = r1;
+        r1 = r2;
+        r2 = t;
+    }
+    r.kind = 2;
+    r.r1 = r1;
+    r.r2 = r2;
+    return r;
+}
+
+// The point's interval around tau = 0 (empty when S(0) = c < 0).
+__host__ __device__ inline void ls_component0(const LsRoots& r, double q, double b, double c, double& lo,
+                                              double& hi) {
+    const double inf = 1e300;
+    lo = -inf;
+    hi = inf;
+    if (c < 0.0) {
+        lo = inf;
+        hi = -inf;
+        return;
+    }
+    if (r.kind == 0) {
+        if (b > 0.0) lo = r.r1;
+        if (b < 0.0) hi = r.r1;
+    } else if (r.kind == 2) {
+        if (q < 0.0) {  // non-negative between the roots
+            lo = r.r1;
+            hi = r.r2;
+        } else if (r.r2 <= 0.0) {  // opens up: the side of 0
+            lo = r.r2;
+        } else if (r.r1 >= 0.0) {
+            hi = r.r1;
+        } else {
+            lo = 0.0;
+            hi = 0.0;
+        }
+    }
+}
+
+// The point's interval around anchor a (empty when S(a) < 0, or when a
+// falls between the roots of an upward S by rounding).
+__host__ __device__ inline void ls_component(const LsRoots& r, double q, double b, double c, double a, double& lo,
+                                             double& hi) {
+    const double inf = 1e300;
+    lo = -inf;
+    hi = inf;
+    if (c + a * (b + a * q) < 0.0) {
+        lo = inf;
+        hi = -inf;
+        return;
+    }
+    if (r.kind == 0) {
+        if (b > 0.0) lo = r.r1;
+        if (b < 0.0) hi = r.r1;
+    } else if (r.kind == 2) {
+        if (q < 0.0) {
+            lo = r.r1;
+            hi = r.r2;
+        } else if (a <= r.r1) {
+            hi = r.r1;
+        } else if (a >= r.r2) {
+            lo = r.r2;
+        } else {
+            lo = inf;
+            hi = -inf;
+        }
+    }
+}
+
+// the anchors by value (a kernel argument)
+struct LsAnchorSet {
+    double a[LS_ANCHORS];
+};
+
+// A trial with no clamp: inside the interval around 0 or inside the
+// interval around an anchor (clear of its ends).
+__host__ __device__ inline bool ls_free(const LsPoly& c, double tau) {
+    if (tau >= c.tlo && tau <= c.thi) return true;
+    for (int k = 0; k < LS_ANCHORS; ++k)
+        if (tau >= c.alo[k] && tau <= c.ahi[k]) return true;
+    return false;
+}
 
 // The R2/R3 coefficients from the setup's sums r[0..23] (FLSRed slots) and
 // the Parseval products q1[0..8] = <S_i, G_a>, q2[0..5] = <S_i, S_j> (i <= j);
 // lo/hi are the interval ends over all points.
 __host__ __device__ inline void ls_assemble(const double* r, const double* q1, const double* q2, double lo, double hi,
-                                            LsPoly& c) {
+                                            const double* alo, const double* ahi, const double* anchor, LsPoly& c) {
     const double M[3][3] = {{r[0], r[1], r[2]}, {r[1], r[3], r[4]}, {r[2], r[4], r[5]}};
     for (int k = 0; k < 5; ++k) c.r2[k] = 0.0;
     for (int a = 0; a < 3; ++a)
@@ -52,6 +169,11 @@ __host__ __device__ inline void ls_assemble(const double* r, const double* q1, c
     // stay clear of the ends, where the T-precision trial may round either way
     c.tlo = lo <= 0.0 ? lo * (1.0 - 1e-6) : 1.0;
     c.thi = hi >= 0.0 ? hi * (1.0 - 1e-6) : -1.0;
+    for (int k = 0; k < LS_ANCHORS; ++k) {
+        const bool ok = anchor[k] > 0.0 && alo[k] <= anchor[k] && anchor[k] <= ahi[k];
+        c.alo[k] = ok ? alo[k] + 1e-6 * fabs(alo[k]) : 1.0;
+        c.ahi[k] = ok ? ahi[k] - 1e-6 * fabs(ahi[k]) : -1.0;
+    }
 }
 
 // R = (R1 + R2 + R3, R1 + R2, R3) (calc_local_dLqdt_inclParts, function_ops.f90:

@@ -38,7 +38,7 @@ struct DevEval {
                 break;
             }
         if (k < 0) {
-            if (p.transform_trials || !(tau >= s->poly.tlo && tau <= s->poly.thi)) {
+            if (p.transform_trials || !ls_free(s->poly, tau)) {
                 ptau = tau;
                 return false;
             }
@@ -72,14 +72,20 @@ __device__ void ls_stop(LsDevState* s, int status, cudaGraphConditionalHandle h_
 // [140..], [149..]) and the per-block interval ends (partials, 2 per block);
 // clears the table for a new search.
 __global__ void ls_coef_kernel(LsDevState* s, const double* __restrict__ results,
-                               const double* __restrict__ partials, int nblocks) {
+                               const double* __restrict__ partials, int nblocks, LsAnchorSet an) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    double lo = -1e300, hi = 1e300;
-    for (int g = 0; g < nblocks; ++g) {
-        lo = fmax(lo, partials[2 * g]);
-        hi = fmin(hi, partials[2 * g + 1]);
+    constexpr int W = 2 * (LS_ANCHORS + 1);
+    double lo[LS_ANCHORS + 1], hi[LS_ANCHORS + 1];
+    for (int k = 0; k <= LS_ANCHORS; ++k) {
+        lo[k] = -1e300;
+        hi[k] = 1e300;
     }
-    ls_assemble(results + 100, results + 140, results + 149, lo, hi, s->poly);
+    for (int g = 0; g < nblocks; ++g)
+        for (int k = 0; k <= LS_ANCHORS; ++k) {
+            lo[k] = fmax(lo[k], partials[W * g + 2 * k]);
+            hi[k] = fmin(hi[k], partials[W * g + 2 * k + 1]);
+        }
+    ls_assemble(results + 100, results + 140, results + 149, lo[0], hi[0], lo + 1, hi + 1, an.a, s->poly);
     s->ntr = 0;
     s->need = 0;
     s->ptau = 0.0;
@@ -172,8 +178,9 @@ __global__ void ls_fft_kernel(LsDevState* s, const double* __restrict__ r) {
     s->need = 0;
 }
 
-void ls_launch_coef(LsDevState* s, const double* results, const double* partials, int nblocks, cudaStream_t st) {
-    ls_coef_kernel<<<1, 32, 0, st>>>(s, results, partials, nblocks);
+void ls_launch_coef(LsDevState* s, const double* results, const double* partials, int nblocks, const LsAnchorSet& an,
+                    cudaStream_t st) {
+    ls_coef_kernel<<<1, 32, 0, st>>>(s, results, partials, nblocks, an);
 }
 void ls_launch_ctrl(LsDevState* s, cudaGraphConditionalHandle h_loop, cudaGraphConditionalHandle h_chk,
                     cudaStream_t st) {

@@ -91,11 +91,13 @@ class Solver : public SolverBase {
     // Line-search trials go through the polynomial path when q = 4: setup
     // once per (base, dir), then one transform per trial.
     bool ls_ready = false;
-    void ls_begin(const SVec* base, const SVec* dir) {
+    // tau_near: a step the trials will visit the neighbourhood of (the
+    // previous step in the CG loop), for the setup's clamp-free intervals
+    void ls_begin(const SVec* base, const SVec* dir, double tau_near = 0.0) {
         trials.clear();
         ls_ready = false;
         if (e.ls_ok() && dir && e.ls_fits()) {
-            e.ls_setup(base, dir);
+            e.ls_setup(base, dir, tau_near);
             ls_ready = true;
         }
     }
@@ -257,7 +259,7 @@ class Solver : public SolverBase {
         // line search (269-318)
         double tb[2] = {0, 0};
         int mflag = 0;
-        ls_begin(u, d1);
+        ls_begin(u, d1, tau0);
         double fx = 0, tau1 = 0;
         LsOut lo;
         if (ls_ready && e.ls_device_search(Bc, 0.0, tau0, &lo) == 0 && lo.status != LS_ERR_CAP) {
@@ -477,7 +479,7 @@ class Solver : public SolverBase {
     int mnbrak_host(const double* phi, const double* d, double tA0, double tB0, double br[2], int* flag) override {
         load(phi, tmp);
         load(d, c);
-        ls_begin(tmp, c);
+        ls_begin(tmp, c, tB0);
         *flag = 0;
         mnbrak(tmp, c, tA0, tB0, br, flag);
         trials.clear();
@@ -487,7 +489,7 @@ class Solver : public SolverBase {
     double brent_host(const double* phi, const double* d, const double br[2]) override {
         load(phi, tmp);
         load(d, c);
-        ls_begin(tmp, c);
+        ls_begin(tmp, c, std::max(br[0], br[1]) * 0.381966);
         const double x = brent(tmp, c, br, nullptr);
         trials.clear();
         started = false;
