@@ -2342,6 +2342,9 @@ __global__ void __launch_bounds__(RED_THREADS)
     }
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long)gridDim.x * blockDim.x) {
         const double a = (double)s2[i], b = (double)s1[i], c = (double)s0[i];
+        // S > 0 for every tau (upward, no real root) or constant >= 0: no
+        // point constraint, nothing to reduce (most points)
+        if ((a > 0.0 && b * b - 4.0 * a * c < 0.0) || (a == 0.0 && b == 0.0 && c >= 0.0)) continue;
         const LsRoots r = ls_roots(a, b, c);
 #pragma unroll
         for (int k = 0; k < K; ++k) {

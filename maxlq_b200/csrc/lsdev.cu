@@ -73,18 +73,27 @@ __device__ void ls_stop(LsDevState* s, int status, cudaGraphConditionalHandle h_
 // clears the table for a new search.
 __global__ void ls_coef_kernel(LsDevState* s, const double* __restrict__ results,
                                const double* __restrict__ partials, int nblocks, LsAnchorSet an) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    constexpr int W = 2 * (LS_ANCHORS + 1);
-    double lo[LS_ANCHORS + 1], hi[LS_ANCHORS + 1];
-    for (int k = 0; k <= LS_ANCHORS; ++k) {
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    // one warp: each lane takes every 32nd block, then a shuffle tree (max and
+    // min are exact, so any order gives the same ends)
+    constexpr int K = LS_ANCHORS + 1, W = 2 * K;
+    const int lane = threadIdx.x;
+    double lo[K], hi[K];
+    for (int k = 0; k < K; ++k) {
         lo[k] = -1e300;
         hi[k] = 1e300;
     }
-    for (int g = 0; g < nblocks; ++g)
-        for (int k = 0; k <= LS_ANCHORS; ++k) {
+    for (int g = lane; g < nblocks; g += 32)
+        for (int k = 0; k < K; ++k) {
             lo[k] = fmax(lo[k], partials[W * g + 2 * k]);
             hi[k] = fmin(hi[k], partials[W * g + 2 * k + 1]);
         }
+    for (int k = 0; k < K; ++k)
+        for (int o = 16; o > 0; o >>= 1) {
+            lo[k] = fmax(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+            hi[k] = fmin(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+        }
+    if (lane != 0) return;
     ls_assemble(results + 100, results + 140, results + 149, lo[0], hi[0], lo + 1, hi + 1, an.a, s->poly);
     s->ntr = 0;
     s->need = 0;
