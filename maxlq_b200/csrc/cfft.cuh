@@ -858,6 +858,106 @@ __device__ __forceinline__ void zfwd_spectral(const ZFwdOp& op, const SymD<C>& d
     }
 }
 
+// The spectral side of a column-pair item (kx = 2 pr and 2 pr + 1 of row cy):
+// what two zfwd_spectral calls (column 0, then column 1) do, with the row
+// tests, the z wavenumbers and the row offsets computed once for both
+// columns, and both columns stored as one 16-byte vector where the pair is
+// aligned in an FP32 spectrum.  The reductions add column 0's terms before
+// column 1's in the same order, so the sums are those of the two calls.
+template <int N, int E, int TPL>
+__device__ __forceinline__ void zfwd_spectral_pair(const ZFwdOp& op, const SymD<float>& dmain,
+                                                   const SymD<float>& dadd, const float* kt, int t, int cut, int nb,
+                                                   int plane, int nx, int cy, int pr, int fy, cpx<float> (&Ya)[E],
+                                                   cpx<float> (&Yb)[E], ZAcc& acc) {
+    using C = float;
+    const int kx0 = 2 * pr, kx1 = 2 * pr + 1;
+    const bool ok0 = kx0 < nx, ok1 = kx1 < nx;
+    const int kc0 = ok0 ? kx0 : nx - 1, kc1 = ok1 ? kx1 : nx - 1;  // clamped: loads stay in bounds
+    const int col0 = cy * nx + kc0, col1 = cy * nx + kc1;
+    const C oy = kt[N + fy], ky2 = kt[fy] * kt[fy];
+    const C ox0 = kt[N + kc0], ox1 = kt[N + kc1];
+    const C kxy0 = kt[kc0] * kt[kc0] + ky2, kxy1 = kt[kc1] * kt[kc1] + ky2;
+    int roff[E];
+    bool rv[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int fz = t + TPL * m;
+        const int cz = fz <= cut ? fz : (fz >= N - cut ? fz - (N - nb) : -1);
+        rv[m] = cz >= 0;
+        roff[m] = (cz >= 0 ? cz : 0) * plane;
+    }
+    // main symbol (the 1/N^3 folded in) and the optional added term
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        const int fz = t + TPL * m;
+        const C kz = kt[fz], oz = kt[N + fz], kz2 = kz * kz;
+        const C ksq0 = kxy0 + kz2, ksq1 = kxy1 + kz2;
+        const C ri0 = dmain.inv ? rinv_of(ksq0) : C(0), ri1 = dmain.inv ? rinv_of(ksq1) : C(0);
+        Ya[m] = (rv[m] && ok0) ? sym_apply(dmain, ox0, oy, oz, ksq0, ri0, Ya[m]) : mk(C(0), C(0));
+        Yb[m] = (rv[m] && ok1) ? sym_apply(dmain, ox1, oy, oz, ksq1, ri1, Yb[m]) : mk(C(0), C(0));
+    }
+    if (op.add) {
+        cpx<C> A0[E], A1[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            A0[m] = ld_spec_c<C>(op.add, op.add_f64, (long)roff[m] + col0);
+            A1[m] = ld_spec_c<C>(op.add, op.add_f64, (long)roff[m] + col1);
+        }
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const int fz = t + TPL * m;
+            const C kz = kt[fz], oz = kt[N + fz], kz2 = kz * kz;
+            const C ksq0 = kxy0 + kz2, ksq1 = kxy1 + kz2;
+            const C ri0 = dadd.inv ? rinv_of(ksq0) : C(0), ri1 = dadd.inv ? rinv_of(ksq1) : C(0);
+            if (rv[m] && ok0) Ya[m] = Ya[m] + sym_apply(dadd, ox0, oy, oz, ksq0, ri0, A0[m]);
+            if (rv[m] && ok1) Yb[m] = Yb[m] + sym_apply(dadd, ox1, oy, oz, ksq1, ri1, A1[m]);
+        }
+    }
+    const double w0 = kx_weight(N, kx0), w1 = kx_weight(N, kx1);
+    if (op.red_self >= 0) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const double yx = (double)Ya[m].x, yy = (double)Ya[m].y;
+            acc.self += w0 * (yx * yx + yy * yy);
+        }
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const double yx = (double)Yb[m].x, yy = (double)Yb[m].y;
+            acc.self += w1 * (yx * yx + yy * yy);
+        }
+    }
+#pragma unroll 1
+    for (int r = 0; r < 3; ++r) {
+        if (!op.red_with[r]) continue;
+        double s0 = 0.0, s1 = 0.0;
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            const cpx<double> W0 = ld_spec_c<double>(op.red_with[r], op.red_with_f64[r], (long)roff[m] + col0);
+            const cpx<double> W1 = ld_spec_c<double>(op.red_with[r], op.red_with_f64[r], (long)roff[m] + col1);
+            s0 += (double)Ya[m].x * W0.x + (double)Ya[m].y * W0.y;
+            s1 += (double)Yb[m].x * W1.x + (double)Yb[m].y * W1.y;
+        }
+        acc.w[r] += w0 * s0;
+        acc.w[r] += w1 * s1;
+    }
+    if (op.spec_out) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+            if (!rv[m]) continue;
+            const long e0 = (long)roff[m] + col0;
+            float2* p0 = reinterpret_cast<float2*>(op.spec_out) + e0;
+            // one 16-byte store only where the pair's address is 16-byte
+            // aligned (array and component bases are only 8-byte aligned)
+            if (!op.spec_f64 && ok0 && ok1 && (reinterpret_cast<uintptr_t>(p0) & 15) == 0) {
+                *reinterpret_cast<float4*>(p0) = make_float4(Ya[m].x, Ya[m].y, Yb[m].x, Yb[m].y);
+            } else {
+                if (ok0) st_spec_c(op.spec_out, op.spec_f64, e0, Ya[m]);
+                if (ok1) st_spec_c(op.spec_out, op.spec_f64, (long)roff[m] + col1, Yb[m]);
+            }
+        }
+    }
+}
+
 // one reduction record of MAX_RED partials per block from the accumulators
 __device__ __forceinline__ void zfwd_partials(const ZFwdOp& op, const ZAcc& acc, double* part) {
     const bool any_red = op.red_self >= 0 || op.red_with[0] || op.red_with[1] || op.red_with[2];
@@ -1315,20 +1415,7 @@ __global__ void __launch_bounds__(PairShape<N>::THREADS, MINB)
         const int cy = (int)(it / ntile);
         const int pr = (int)(it - (long)cy * ntile) * NP + l;
         const int fy = band_fft_index(a.band, cy);
-        {
-            const int kx = 2 * pr;
-            const bool ok = kx < nx;
-            const int col = cy * nx + (ok ? kx : nx - 1);  // clamped: loads stay in bounds
-            const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
-            zfwd_spectral<N, E, TPL>(op, dmain, dadd, kt, idx, fy, col - cy * nx, kx_weight(N, kx), va, acc);
-        }
-        {
-            const int kx = 2 * pr + 1;
-            const bool ok = kx < nx;
-            const int col = cy * nx + (ok ? kx : nx - 1);
-            const ZCol<N, TPL> idx{t, cut, nb, plane, col, ok};
-            zfwd_spectral<N, E, TPL>(op, dmain, dadd, kt, idx, fy, col - cy * nx, kx_weight(N, kx), vb, acc);
-        }
+        zfwd_spectral_pair<N, E, TPL>(op, dmain, dadd, kt, t, cut, nb, plane, nx, cy, pr, fy, va, vb, acc);
         if (yout) {  // uniform over the block
             SFor<0, CPlan<N, E>::NST>::run(
                 [&](auto sc) { pstage<N, E, decltype(sc)::value, +1>(va, vb, t, l, cur, tw); });
