@@ -18,10 +18,10 @@ def _pinned(a):
     return out, t
 
 
-@pytest.mark.parametrize("prec,planes", [("fp64", 0), ("mixed", 0), ("mixed", 8)])
-def test_pinned_and_pageable_host_buffers_agree(prec, planes, monkeypatch):
+# 512^3 moves each field in several staging chunks (2^25 values each)
+@pytest.mark.parametrize("prec,planes,n", [("fp64", 0, 64), ("mixed", 0, 64), ("mixed", 8, 64), ("mixed", 0, 512)])
+def test_pinned_and_pageable_host_buffers_agree(prec, planes, n, monkeypatch):
     monkeypatch.setenv("MLQ_SLAB_PLANES", str(planes))
-    n = 64
     with mlq.MaxLq(n, 4.0, 1.0, precision=prec, optim_tol=1e-14) as c:
         u0 = c.rescaleLqNorm(c.seed_field(3, 2.0, 4.0))
         pageable = np.ascontiguousarray(u0.copy())
