@@ -478,8 +478,12 @@ class Engine : public EngineBase {
     // spec_f64: storage of spec (-1: this engine's state storage)
     double load_vec(const double* host, SVec* spec, int spec_f64 = -1);
     void store_vec(const SVec* spec, double* host, int spec_f64 = -1);
-    void load_scalar_phys(const double* host, int dst);
-    void store_scalar_phys(int src, double* host);
+    // xs: a copy stream to run on instead of the engine's (not in slab mode);
+    // both return when their copies are done
+    void load_scalar_phys(const double* host, int dst, cudaStream_t xs = nullptr);
+    void store_scalar_phys(int src, double* host, cudaStream_t xs = nullptr);
+    cudaStream_t xstream_ = nullptr;
+    cudaStream_t copy_stream();
 
     // ---- full-band FFT API (fftwfunction.f90) ----
     void fft_c2c(const double* in, double* out, int sign);

@@ -813,6 +813,7 @@ void Engine<T>::launch_xinv(XInvArgs<T>& xa, int narr, const Band& b) {
 template <typename T>
 Engine<T>::~Engine() {
     if (h_stage_) cudaFreeHost(h_stage_);
+    if (xstream_) cudaStreamDestroy(xstream_);
     for (LsGraph& g : lsg_)
         if (g.exec) cudaGraphExecDestroy(g.exec);
     if (h_ls_) cudaFreeHost(h_ls_);
@@ -1431,6 +1432,7 @@ enum : int {
     PCH = 29,  // 29..39 chain fields
     PIO = 40,  // host transfer scratch
     PIO2 = 41,
+    PIO3 = 42,  // second host transfer buffer
 };
 // work spectra (band b2)
 enum : int { WG2 = 0, WA = 1, WP = 2, WT = 3 /*3..5*/, WONE = 6, WCH = 7 /*7..*/ };
@@ -2858,10 +2860,11 @@ static bool host_pinned(const void* p) {
 }
 
 template <typename T>
-void Engine<T>::load_scalar_phys(const double* host, int dst) {
+void Engine<T>::load_scalar_phys(const double* host, int dst, cudaStream_t xs) {
+    const cudaStream_t st = (xs && !slab_) ? xs : stream;  // slab storage is filled on the engine's stream
     if (sizeof(T) == 8 && host_pinned(host)) {
-        MLQ_CUDA(cudaMemcpyAsync(phys(dst), host, n3 * sizeof(T), cudaMemcpyHostToDevice, stream));
-        MLQ_CUDA(cudaStreamSynchronize(stream));
+        MLQ_CUDA(cudaMemcpyAsync(phys(dst), host, n3 * sizeof(T), cudaMemcpyHostToDevice, st));
+        MLQ_CUDA(cudaStreamSynchronize(st));
         if (slab_) slot(dst).kind = PSlot::FULL;
         return;
     }
@@ -2882,26 +2885,27 @@ void Engine<T>::load_scalar_phys(const double* host, int dst) {
             else
                 for (long i = a; i < e; ++i) b[i] = (T)host[off + i];
         });
-        MLQ_CUDA(cudaMemcpyAsync(d + off, b, cnt * sizeof(T), cudaMemcpyHostToDevice, stream));
-        MLQ_CUDA(cudaEventRecord(done[k & 1], stream));
+        MLQ_CUDA(cudaMemcpyAsync(d + off, b, cnt * sizeof(T), cudaMemcpyHostToDevice, st));
+        MLQ_CUDA(cudaEventRecord(done[k & 1], st));
     }
-    MLQ_CUDA(cudaStreamSynchronize(stream));
+    MLQ_CUDA(cudaStreamSynchronize(st));
     ev_give(done[0]);
     ev_give(done[1]);
     if (slab_) slot(dst).kind = PSlot::FULL;
 }
 
 template <typename T>
-void Engine<T>::store_scalar_phys(int src, double* host) {
+void Engine<T>::store_scalar_phys(int src, double* host, cudaStream_t xs) {
+    const cudaStream_t st = (xs && !slab_) ? xs : stream;  // slab expansion runs on the engine's stream
     // chunks of whole slabs in slab mode (each expanded just before its copy)
     const long ch = slab_ ? (long)zs_ * n * n : std::min(n3, XFER_CHUNK);
     if (sizeof(T) == 8 && host_pinned(host)) {
         for (long off = 0; off < n3; off += ch) {
             const long cnt = std::min(ch, n3 - off);
             const T* d = slab_ ? expand(src, (int)(off / ((long)n * n)), 0) : phys(src) + off;
-            MLQ_CUDA(cudaMemcpyAsync(host + off, d, cnt * sizeof(T), cudaMemcpyDeviceToHost, stream));
+            MLQ_CUDA(cudaMemcpyAsync(host + off, d, cnt * sizeof(T), cudaMemcpyDeviceToHost, st));
         }
-        MLQ_CUDA(cudaStreamSynchronize(stream));
+        MLQ_CUDA(cudaStreamSynchronize(st));
         return;
     }
     T* buf[2];
@@ -2911,8 +2915,8 @@ void Engine<T>::store_scalar_phys(int src, double* host) {
     auto issue = [&](long k) {
         const long off = k * ch, cnt = std::min(ch, n3 - off);
         const T* d = slab_ ? expand(src, (int)(off / ((long)n * n)), 0) : phys(src) + off;
-        MLQ_CUDA(cudaMemcpyAsync(buf[k & 1], d, cnt * sizeof(T), cudaMemcpyDeviceToHost, stream));
-        MLQ_CUDA(cudaEventRecord(done[k & 1], stream));
+        MLQ_CUDA(cudaMemcpyAsync(buf[k & 1], d, cnt * sizeof(T), cudaMemcpyDeviceToHost, st));
+        MLQ_CUDA(cudaEventRecord(done[k & 1], st));
     };
     const long nk = (n3 + ch - 1) / ch;
     for (long k = 0; k < std::min(nk, 2L); ++k) issue(k);
@@ -2928,27 +2932,53 @@ void Engine<T>::store_scalar_phys(int src, double* host) {
         });
         if (k + 2 < nk) issue(k + 2);
     }
-    MLQ_CUDA(cudaStreamSynchronize(stream));
+    MLQ_CUDA(cudaStreamSynchronize(st));
     ev_give(done[0]);
     ev_give(done[1]);
 }
 
 // Forward transform of a host vector field into band-b2 state spectra.  The
 // energy the band drops is measured directly, as ||u - F^-1 P2 F u||^2.
+// The second stream of host transfers (copies only), created on first use.
+template <typename T>
+cudaStream_t Engine<T>::copy_stream() {
+    if (!xstream_) MLQ_CUDA(cudaStreamCreateWithFlags(&xstream_, cudaStreamNonBlocking));
+    return xstream_;
+}
+
+// A host vector field in, component by component: each component is copied
+// in on the copy stream while the engine's stream transforms the one before
+// (two physical buffers in turn), then the band check's round trip.
 template <typename T>
 double Engine<T>::load_vec(const double* host, SVec* spec, int spec_f64) {
     const long nc = spec_ncomp();
     if (spec_f64 < 0) spec_f64 = sf64();
+    const int bufs[2] = {PIO, PIO3};
+    cudaStream_t xs = slab_ ? nullptr : copy_stream();
+    cudaEvent_t used[2] = {ev_take(), ev_take()}, loaded = ev_take();
+    // the buffers may still be read by work already on the engine's stream
+    MLQ_CUDA(cudaEventRecord(used[0], stream));
+    MLQ_CUDA(cudaEventRecord(used[1], stream));
     for (int c = 0; c < 3; ++c) {
-        load_scalar_phys(host + c * n3, PIO);
+        const int b = slab_ ? PIO : bufs[c & 1];
+        if (xs) MLQ_CUDA(cudaStreamWaitEvent(xs, used[c & 1], 0));
+        load_scalar_phys(host + c * n3, b, xs);
+        if (xs) {
+            MLQ_CUDA(cudaEventRecord(loaded, xs));
+            MLQ_CUDA(cudaStreamWaitEvent(stream, loaded, 0));
+        }
         FwdOut o;
         o.spec = (char*)spec + (size_t)c * nc * (spec_f64 ? sizeof(double2) : sizeof(float2));
         o.spec_f64 = spec_f64;
         o.phys_out = PIO2;
-        fwd(b2, FCopy{}, {PIO}, {o});
-        pointwise(FDiffSq{}, {PIO, PIO2}, {}, 30 + 2 * c);
+        fwd(b2, FCopy{}, {b}, {o});
+        pointwise(FDiffSq{}, {b, PIO2}, {}, 30 + 2 * c);
+        MLQ_CUDA(cudaEventRecord(used[c & 1], stream));
     }
     fetch_results();
+    ev_give(used[0]);
+    ev_give(used[1]);
+    ev_give(loaded);
     double out = 0, tot = 0;
     for (int c = 0; c < 3; ++c) {
         out += h_results[30 + 2 * c];
@@ -2958,19 +2988,35 @@ double Engine<T>::load_vec(const double* host, SVec* spec, int spec_f64) {
     return tot > 0 ? out / tot : 0.0;
 }
 
+// A vector field out: the inverse transform of component c + 1 runs on the
+// engine's stream while component c is copied out on the copy stream.
 template <typename T>
 void Engine<T>::store_vec(const SVec* spec, double* host, int spec_f64) {
     const long nc = spec_ncomp();
     if (spec_f64 < 0) spec_f64 = sf64();
+    const int bufs[2] = {PIO, PIO3};
+    cudaStream_t xs = slab_ ? nullptr : copy_stream();
+    cudaEvent_t done[3] = {ev_take(), ev_take(), ev_take()};
+    auto out = [&](int c) {
+        if (xs) MLQ_CUDA(cudaStreamWaitEvent(xs, done[c], 0));
+        store_scalar_phys(slab_ ? PIO : bufs[c & 1], host + c * n3, xs);  // returns when the copy is done
+    };
     for (int c = 0; c < 3; ++c) {
+        // the buffer of component c - 2 was copied out by the time out(c - 2) returned
         InvOut o;
         o.nsrc = 1;
         o.src[0] = ZSrc{(const char*)spec + (size_t)c * nc * (spec_f64 ? sizeof(double2) : sizeof(float2)), spec_f64,
                         SYM_ONE, 0, 1.0};
-        o.phys_out = PIO;
+        o.phys_out = slab_ ? PIO : bufs[c & 1];
         inv(b2, {o});
-        store_scalar_phys(PIO, host + c * n3);
+        MLQ_CUDA(cudaEventRecord(done[c], stream));
+        if (slab_)
+            out(c);
+        else if (c >= 1)
+            out(c - 1);
     }
+    if (!slab_) out(2);
+    for (auto e : done) ev_give(e);
 }
 
 // ----------------------------------------------------------------------------
