@@ -2331,7 +2331,7 @@ void Engine<T>::calc_uk(const SVec* u, double k, int dst) {
 // (empty when s0 < 0), then the same around each anchor (empty where S is
 // negative at the anchor), as (lo, hi) pairs: 2 (LS_ANCHORS + 1) per block.
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS)
+__global__ void __launch_bounds__(RED_THREADS, 4)
     ls_interval_kernel(const T* __restrict__ s0, const T* __restrict__ s1, const T* __restrict__ s2, long npts,
                        LsAnchorSet an, double* __restrict__ out) {
     constexpr int K = LS_ANCHORS + 1;
@@ -2342,11 +2342,10 @@ __global__ void __launch_bounds__(RED_THREADS)
         lo[k] = -inf;
         hi[k] = inf;
     }
-    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += (long)gridDim.x * blockDim.x) {
-        const double a = (double)s2[i], b = (double)s1[i], c = (double)s0[i];
+    auto point = [&](double a, double b, double c) {
         // S > 0 for every tau (upward, no real root) or constant >= 0: no
         // point constraint, nothing to reduce (most points)
-        if ((a > 0.0 && b * b - 4.0 * a * c < 0.0) || (a == 0.0 && b == 0.0 && c >= 0.0)) continue;
+        if ((a > 0.0 && b * b - 4.0 * a * c < 0.0) || (a == 0.0 && b == 0.0 && c >= 0.0)) return;
         const LsRoots r = ls_roots(a, b, c);
 #pragma unroll
         for (int k = 0; k < K; ++k) {
@@ -2358,6 +2357,16 @@ __global__ void __launch_bounds__(RED_THREADS)
             lo[k] = fmax(lo[k], l);
             hi[k] = fmin(hi[k], h);
         }
+    };
+    // two points per pass: both points' loads are in flight together
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < npts; i += 2 * stride) {
+        const bool two = i + stride < npts;
+        const long j = two ? i + stride : i;
+        const double a0 = (double)s2[i], b0 = (double)s1[i], c0 = (double)s0[i];
+        const double a1 = (double)s2[j], b1 = (double)s1[j], c1 = (double)s0[j];
+        point(a0, b0, c0);
+        if (two) point(a1, b1, c1);
     }
     __shared__ double slo[K][RED_THREADS / 32], shi[K][RED_THREADS / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -2541,9 +2550,10 @@ void Engine<T>::ls_setup(const SVec* u, const SVec* d, double tau0) {
         // on the device, with the coefficients: no host round trip
         const int grid = grid_for(n3, RED_THREADS, 148 * 4);
         ensure_partials((long)grid * W);
+        cudaEvent_t ev = prof_mark();
         ls_interval_kernel<T><<<grid, RED_THREADS, 0, stream>>>(phys(ls_phys(0)), phys(ls_phys(1)),
                                                                 phys(ls_phys(2)), n3, an, d_partials);
-        launched();
+        launched("ls_interval", 3.0 * n3 * sizeof(T), ev);
         ls_launch_coef(d_ls_, d_results, d_partials, grid, an, stream);
         launched();
         ls_host_poly_ = false;
